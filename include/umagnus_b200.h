@@ -1,0 +1,230 @@
+/*
+ * umagnus_b200.h -- C-ABI of the B200 (sm_100a) effective-field + LLG hot path.
+ *
+ * Drop-in replacement for the hot-path subset of the uMagNUS Go package
+ * `opencl` (device-op layer) plus the engine-level stepper loop.  Every
+ * entry point cites the reference function it replaces (path:line in the
+ * uMagNUS source tree).  All arithmetic is float32 unless stated; device
+ * arrays are structure-of-arrays, one float32 array per vector component,
+ * x fastest (data/slice.go:53-100, data/slice.go:413 Index).
+ *
+ * Conventions kept from the reference:
+ *   - a NULL parameter array means "uniform value = mul" (kernels_src/clh/amul.clh:5-7);
+ *   - region maps are uint8 (NREGION = 256, engine/regions.go:11);
+ *   - per-region LUTs hold 256 floats, symmetric inter-region LUTs hold
+ *     256*257/2 = 32896 floats indexed by symidx (kernels_src/clh/exchange.clh:5);
+ *   - the library never frees caller memory; plans/contexts are opaque
+ *     handles with explicit free.
+ * Every function returns 0 on success or a nonzero UMAG_E* status (the Go
+ * shim maps nonzero to util.Fatal, keeping the reference's abort-on-error
+ * behaviour); umag_last_error() describes the last failure.
+ * All calls are stream-ordered on the library stream (umag_set_stream) and
+ * must come from one host thread, like the reference's single command queue
+ * (opencl/init.go:60,145).
+ */
+#ifndef UMAGNUS_B200_H
+#define UMAGNUS_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define UMAG_OK 0
+#define UMAG_E_CUDA 1        /* CUDA runtime error */
+#define UMAG_E_ARG 2         /* invalid argument */
+#define UMAG_E_UNSUPPORTED 3 /* size/feature outside what this build handles */
+#define UMAG_E_NOMEM 4
+#define UMAG_E_NOT_INIT 5
+#define UMAG_E_SOLVER 6      /* time step underflow / NaN in the solver */
+
+/* ---- device bring-up (opencl/init.go) ------------------------------------ */
+/* opencl/init.go:48 Init(gpu): select the device, create the stream. */
+int umag_init(int device);
+/* opencl/init.go:287 ReleaseAndClean. */
+int umag_release(void);
+const char* umag_last_error(void);
+/* Run subsequent calls on a caller-owned cudaStream_t (NULL = library stream). */
+int umag_set_stream(void* cuda_stream);
+/* Wait for all work queued by the library (ClCmdQueue.Finish, opencl/init.go). */
+int umag_sync(void);
+/* Build/version string. */
+const char* umag_version(void);
+
+/* ---- memory (opencl/slice.go:14-193, opencl/buffer.go:25-106) ------------ */
+int umag_malloc(void** ptr, size_t bytes);       /* opencl/slice.go:14 NewSlice / MemAlloc */
+int umag_free(void* ptr);                        /* data/slice.go Free */
+int umag_memcpy_htod(void* dst, const void* src, size_t bytes); /* opencl/init.go:275 data.Copy hooks */
+int umag_memcpy_dtoh(void* dst, const void* src, size_t bytes);
+int umag_memcpy_dtod(void* dst, const void* src, size_t bytes);
+int umag_memset_f32(float* dst, float value, size_t n); /* opencl/slice.go:156-193 Memset / Zero */
+
+/* ---- local field terms --------------------------------------------------- */
+/* opencl/exchange.go:16 AddExchange (kernel kernels_src/cl/exchange.cl).
+ * Weights 2/c^2 are formed in FP64 and rounded to float32 as the reference
+ * does (opencl/exchange.go:18-20).  pbc = PBC_code bits (1:x, 2:y, 4:z). */
+int umag_add_exchange(float* Bx, float* By, float* Bz, const float* mx, const float* my,
+                      const float* mz, const float* Ms, float Ms_mul, const float* aLUT2d,
+                      const uint8_t* regions, int Nx, int Ny, int Nz, double cx, double cy,
+                      double cz, int pbc);
+/* opencl/dmi.go:15 AddDMI (kernels_src/cl/dmi.cl): exchange + interfacial DMI. */
+int umag_add_dmi(float* Hx, float* Hy, float* Hz, const float* mx, const float* my,
+                 const float* mz, const float* Ms, float Ms_mul, const float* aLUT2d,
+                 const float* dLUT2d, const uint8_t* regions, int Nx, int Ny, int Nz, double cx,
+                 double cy, double cz, int pbc, int openbc);
+/* opencl/anisotropy.go:153 AddUniaxialAnisotropy2 (uniaxialanisotropy2.cl). */
+int umag_add_uniaxial_anisotropy2(float* Bx, float* By, float* Bz, const float* mx,
+                                  const float* my, const float* mz, const float* Ms, float Ms_mul,
+                                  const float* K1, float K1_mul, const float* K2, float K2_mul,
+                                  const float* ux, float ux_mul, const float* uy, float uy_mul,
+                                  const float* uz, float uz_mul, int N);
+/* opencl/region.go:13 RegionAddV (regionaddv.cl): dst += LUT[region]. */
+int umag_region_addv(float* dx, float* dy, float* dz, const float* lutx, const float* luty,
+                     const float* lutz, const uint8_t* regions, int N);
+/* opencl/region.go:108 RegionDecode (regiondecode.cl). */
+int umag_region_decode(float* dst, const float* lut, const uint8_t* regions, int N);
+
+/* ---- torque -------------------------------------------------------------- */
+/* opencl/lltorque.go:16 LLTorque (lltorque2.cl); t may alias h. */
+int umag_lltorque(float* tx, float* ty, float* tz, const float* mx, const float* my,
+                  const float* mz, const float* hx, const float* hy, const float* hz,
+                  const float* alpha, float alpha_mul, int N);
+/* opencl/lltorque.go:97 LLNoPrecess (llnoprecess.cl). */
+int umag_llnoprecess(float* tx, float* ty, float* tz, const float* mx, const float* my,
+                     const float* mz, const float* hx, const float* hy, const float* hz, int N);
+
+/* ---- linear combinations and normalisation ------------------------------- */
+/* opencl/madd.go:111-413 Madd2..Madd7 on ncomp components at once:
+ * dst[c] = sum_j fac[j] * src[j*ncomp + c], 2 <= nsrc <= 7, same rounding
+ * order as madd<n>.cl.  dst may alias a source. */
+int umag_madd(int ncomp, float* const* dst, int nsrc, const float* const* src, const float* fac,
+              int N);
+/* opencl/normalize.go:13 Normalize (normalize2.cl). vol may be NULL. */
+int umag_normalize(float* vx, float* vy, float* vz, const float* vol, int N);
+/* opencl/vecnorm.go:12 VecNorm, opencl/madd.go:60 Div, opencl/dotproduct.go AddDotProduct. */
+int umag_vecnorm(float* dst, const float* ax, const float* ay, const float* az, int N);
+int umag_div(float* dst, const float* a, const float* b, int N);
+int umag_add_dot_product(float* dst, float prefactor, const float* ax, const float* ay,
+                         const float* az, const float* bx, const float* by, const float* bz,
+                         int N);
+
+/* ---- reductions (opencl/reduce.go), results on the host ------------------ */
+/* reduce.go:180 MaxVecNorm: max_i |v_i| (float32 max, FP64 sqrt). */
+int umag_max_vec_norm(const float* x, const float* y, const float* z, int N, double* out);
+/* reduce.go:214 MaxVecDiff: max_i |a_i - b_i|. */
+int umag_max_vec_diff(const float* ax, const float* ay, const float* az, const float* bx,
+                      const float* by, const float* bz, int N, double* out);
+/* reduce.go:105 MaxAbs: max_i |v_i|. */
+int umag_max_abs(const float* v, int N, double* out);
+/* reduce.go:26 Sum / :54 Dot with compensated accumulation (float32 inputs,
+ * Neumaier-compensated float32 per thread, two-sum tree, FP64 final). */
+int umag_sum(const float* v, int N, double* out);
+int umag_dot(const float* a, const float* b, int N, double* out);
+
+/* ---- demag convolution (opencl/conv_demag.go) ---------------------------- */
+typedef struct umag_demag umag_demag;
+/* engine/demag.go:135-143 newellDemagConv: builds the Newell tensor in FP64
+ * on the GPU (mag/newellDemagKernel.go:1108-1324), FFTs it in FP64 and
+ * keeps the real, non-redundant spectrum in float32 (opencl/conv_demag.go:131-202).
+ * pbc[3] must be zero in this build (no periodic images). */
+int umag_demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy,
+                          double cz, int asymptotic_radius, int zero_self_demag,
+                          umag_demag** out);
+/* opencl/conv_demag.go:27 NewDemag with a caller-supplied real-space kernel:
+ * six host arrays (xx, yy, zz, yz, xz, xy) on the padded grid, doubles. */
+int umag_demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6],
+                               umag_demag** out);
+/* opencl/conv_demag.go:43 (*DemagConvolution).Exec: B = demag field of
+ * MU0*Ms*vol*m (B is overwritten).  vol and Ms may be NULL. */
+int umag_demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float* mx,
+                    const float* my, const float* mz, const float* vol, const float* Ms,
+                    float Ms_mul);
+/* Copies the stored float32 kernel spectrum (6 arrays of (Px/2+1)(Py/2+1)(Pz/2+1),
+ * reference layout kernmulrsymm3d.cl) to host arrays; for tests. */
+int umag_demag_get_spectrum(umag_demag* d, float* const host[6]);
+/* Copies the FP64 real-space Newell tensor (6 x Px*Py*Pz) to host; for tests. */
+int umag_demag_get_kernel(umag_demag* d, double* const host[6]);
+int umag_demag_padded_size(umag_demag* d, int P[3]);
+int umag_demag_free(umag_demag* d);
+
+/* ---- engine: a whole simulation on the device ---------------------------- */
+/* Material and mesh description.  Uniform parameters use the *_mul value
+ * with a NULL map; per-cell maps are device pointers owned by the caller
+ * (regiondecode'd values, engine/parameter.go:37-45). */
+typedef struct {
+    int N[3];
+    double cell[3];
+    int pbc[3];
+    const uint8_t* regions;        /* device, N cells; NULL = all region 0 */
+    const float* vol;              /* device geometry mask or NULL */
+    const float* Ms; float Ms_mul; /* saturation magnetisation A/m */
+    const float* alpha; float alpha_mul;
+    const float* Ku1; float Ku1_mul;
+    const float* Ku2; float Ku2_mul;
+    const float* anisU[3]; float anisU_mul[3];
+    const float* aLUT;             /* device, 32896 floats (Aex inter-region LUT) */
+    const float* dLUT;             /* device, 32896 floats (Dind LUT) or NULL */
+    const float* bextLUT[3];       /* device, 256 floats each, or NULL (no Zeeman) */
+    int enable_demag;              /* Newell demag (engine/demag.go EnableNewellDemag) */
+    int openbc;                    /* engine/exchange.go OpenBC */
+    int precess;                   /* engine/torque.go Precess */
+    int asymptotic_radius;         /* engine/demag.go:27, default 32 */
+} umag_sim_params;
+
+/* Solver knobs, engine/run.go:14-43 (defaults by umag_solver_defaults). */
+typedef struct {
+    int solver;      /* 2 Heun, 3 RK23, 4 RK4, 5 RK45DP (engine/run.go:83-95) */
+    double dt, min_dt, max_dt, fix_dt, max_err, rel_err, min_slope, headroom, gamma_ll;
+} umag_solver_params;
+
+/* Snapshot of the solver state (engine/run.go globals). */
+typedef struct {
+    double time, dt, last_err, peak_err, last_torque;
+    long long nsteps, nundone, nevals;
+    int status;      /* 0 ok; nonzero: UMAG_E_SOLVER cause code */
+} umag_solver_state;
+
+typedef struct umag_sim umag_sim;
+void umag_solver_defaults(umag_solver_params* p);
+int umag_sim_new(const umag_sim_params* p, const umag_solver_params* s, umag_sim** out);
+int umag_sim_free(umag_sim* s);
+/* engine/magnetization.go:55 SetArray: copy m (device, 3 arrays) and normalise. */
+int umag_sim_set_m(umag_sim* s, const float* mx, const float* my, const float* mz);
+int umag_sim_get_m(umag_sim* s, float* mx, float* my, float* mz);   /* device destinations */
+/* Device pointers of the current magnetisation (valid until the next step). */
+int umag_sim_m_ptrs(umag_sim* s, float** m3);
+/* engine/torque.go:124 SetTorque / engine/effectivefield.go:14 SetEffectiveField
+ * for the current m: writes torque (and B_eff if non-NULL) to device arrays. */
+int umag_sim_torque(umag_sim* s, float* tx, float* ty, float* tz, float* bx, float* by, float* bz);
+/* engine/run.go:238 step(): n calls of Stepper.Step() without host
+ * synchronisation (device-side step controller). */
+int umag_sim_steps(umag_sim* s, int n);
+/* engine/run.go:190 Run(seconds): steps until the simulated time reaches
+ * t+seconds (alarm honoured by adaptDt, engine/run.go:181-184), checking
+ * the device time every `chunk` steps; max_steps bounds the loop. */
+int umag_sim_run(umag_sim* s, double seconds, int chunk, long long max_steps);
+int umag_sim_get_state(umag_sim* s, umag_solver_state* st);
+int umag_sim_set_time(umag_sim* s, double time, double dt);
+/* Average m over the magnet (engine/average.go:29-40), compensated sum. */
+int umag_sim_average_m(umag_sim* s, double avg[3]);
+/* Capture `steps_per_graph` steps into a CUDA graph and replay it (1 = on,
+ * 0 = plain stream launches).  Default on. */
+int umag_sim_use_graph(umag_sim* s, int enable, int steps_per_graph);
+/* Number of kernel launches one step issues (for launch accounting). */
+int umag_sim_launches_per_step(umag_sim* s, int* n);
+/* Enqueue n effective-field + torque evaluations of the current m into the
+ * FSAL slot (the value it already holds), without host synchronisation; for
+ * timing the field evaluation alone.  No reference counterpart. */
+int umag_sim_torque_evals(umag_sim* s, int n);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

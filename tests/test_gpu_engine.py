@@ -1,0 +1,138 @@
+"""Whole-step parity of the device engine (umag_sim_*) with the oracle.
+
+Levels (the FFT rounding differs, so trajectories are compared at three
+levels):  (1) one torque evaluation on identical m, |d tau| <= 1e-5 max|tau|;
+(2) fixed-dt steps of every solver, max |dm| <= 1e-5 after a few steps;
+(3) adaptive RK45DP runs: average m and accepted-step counts close to the
+oracle's, and the error against the FP64 oracle reported.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import golden_pins as G
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+MU0 = G.MU0
+
+
+@pytest.fixture(scope="module")
+def eng():
+    from umagnus_b200 import engine
+    return engine
+
+
+def thin_film(dtype=np.float32, **kw):
+    """64x64x1 cells of 4x4x3 nm, Ms 8e5, Aex 1.3e-11, alpha 0.1, B=(0,0,10 mT)."""
+    p = dict(N=(64, 64, 1), cell=(4e-9, 4e-9, 3e-9), Ms=8e5, Aex=1.3e-11, alpha=0.1, B_ext=(0, 0, 0.01))
+    p.update(kw)
+    return p
+
+
+def multilayer_small(**kw):
+    """The 3D multilayer material (DMI + anisotropy) on a smaller grid."""
+    p = dict(N=(48, 40, 8), cell=(2e-9, 2e-9, 1e-9), Ms=1.1e6, Aex=1.6e-11, alpha=0.3, Dind=3e-3, Ku1=5e5,
+             anisU=(0, 0, 1), B_ext=(0, 0, 0.05))
+    p.update(kw)
+    return p
+
+
+def make_pair(eng, p, solver=5, fix_dt=0.0, seed=1):
+    g = eng.Simulation(p["N"], p["cell"], p["Ms"], p["Aex"], p["alpha"], Dind=p.get("Dind", 0.0),
+                       Ku1=p.get("Ku1", 0.0), anisU=p.get("anisU", (0, 0, 1)), B_ext=p.get("B_ext"),
+                       solver=solver, FixDt=fix_dt)
+    o = O.Simulation(p["N"], p["cell"], p["Ms"], p["Aex"], p["alpha"], Dind=p.get("Dind", 0.0),
+                     Ku1=p.get("Ku1", 0.0), anisU=p.get("anisU", (0, 0, 1)), B_ext=p.get("B_ext"), solver=solver)
+    o.solver.fix_dt = fix_dt
+    m = G.random_unit(p["N"], seed)
+    g.set_m(m)
+    o.set_m(m)
+    return g, o
+
+
+@pytest.mark.parametrize("p", [thin_film(), multilayer_small()], ids=["film", "multilayer"])
+def test_torque_matches_oracle(eng, p):
+    g, o = make_pair(eng, p)
+    # identical m on both sides (the device normalises in float32 exactly like the oracle)
+    assert np.array_equal(g.get_m().cpu().numpy(), o.m)
+    t, b = g.torque(beff=True)
+    to, bo = o.torque(beff=True)
+    t, b = t.cpu().numpy(), b.cpu().numpy()
+    assert np.abs(b - bo).max() <= 1e-5 * np.abs(bo).max()
+    assert np.abs(t - to).max() <= 1e-5 * np.abs(to).max()
+    g.free()
+
+
+def test_local_terms_bitexact_without_demag(eng):
+    """With demag off every term is per-cell arithmetic: bit-identical to the oracle."""
+    p = multilayer_small()
+    g = eng.Simulation(p["N"], p["cell"], p["Ms"], p["Aex"], p["alpha"], Dind=p["Dind"], Ku1=p["Ku1"],
+                       anisU=p["anisU"], B_ext=p["B_ext"], demag=False)
+    o = O.Simulation(p["N"], p["cell"], p["Ms"], p["Aex"], p["alpha"], Dind=p["Dind"], Ku1=p["Ku1"],
+                     anisU=p["anisU"], B_ext=p["B_ext"], demag=False)
+    m = G.random_unit(p["N"], 4)
+    g.set_m(m)
+    o.set_m(m)
+    t, b = g.torque(beff=True)
+    to, bo = o.torque(beff=True)
+    assert np.array_equal(b.cpu().numpy(), bo)
+    assert np.array_equal(t.cpu().numpy(), to)
+    g.free()
+
+
+@pytest.mark.parametrize("solver", [2, 3, 4, 5])
+def test_fixed_step_trajectory(eng, solver):
+    p = thin_film()
+    g, o = make_pair(eng, p, solver=solver, fix_dt=2e-13)
+    for _ in range(5):
+        o.step()
+    g.steps(5)
+    st = g.state()
+    assert st["nsteps"] == o.solver.nsteps == 5
+    assert st["nevals"] == o.solver.nevals
+    assert abs(st["time"] - o.solver.time) <= 1e-24
+    dm = np.abs(g.get_m().cpu().numpy() - o.m).max()
+    assert dm <= 1e-5
+    g.free()
+
+
+def test_adaptive_rk45dp_short_run(eng):
+    p = thin_film()
+    g, o = make_pair(eng, p)
+    g.run(2e-11)
+    o.run(2e-11)
+    st = g.state()
+    assert st["status"] == 0
+    assert abs(st["time"] - 2e-11) < 1e-22 and abs(o.solver.time - 2e-11) < 1e-22
+    # accepted-step counts may differ by a few when a reject decision flips
+    assert abs(st["nsteps"] - o.solver.nsteps) <= max(2, 0.05 * o.solver.nsteps)
+    avg = np.array(g.average_m())
+    avg_o = o.m.reshape(3, -1).astype(np.float64).mean(axis=1)
+    assert np.abs(avg - avg_o).max() <= 1e-4
+    g.free()
+
+
+def test_graph_and_stream_paths_agree(eng):
+    p = thin_film(N=(32, 32, 1))
+    a, _ = make_pair(eng, p, fix_dt=1e-13)
+    b, _ = make_pair(eng, p, fix_dt=1e-13)
+    a.use_graph(True, 8)
+    b.use_graph(False)
+    a.steps(16)
+    b.steps(16)
+    assert torch.equal(a.get_m(), b.get_m())
+    assert a.state()["nsteps"] == b.state()["nsteps"] == 16
+    a.free()
+    b.free()
+
+
+def test_run_stops_exactly_at_alarm(eng):
+    p = thin_film(N=(32, 32, 1))
+    g, _ = make_pair(eng, p)
+    g.run(1e-12, chunk=7)
+    assert g.state()["time"] == pytest.approx(1e-12, rel=0, abs=1e-24)
+    g.run(5e-13, chunk=3)
+    assert g.state()["time"] == pytest.approx(1.5e-12, rel=0, abs=1e-24)
+    g.free()

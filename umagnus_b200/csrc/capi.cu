@@ -1,0 +1,176 @@
+// capi.cu -- extern "C" entry points declared in include/umagnus_b200.h.
+#include <cstring>
+
+#include "common.cuh"
+#include "demag.cuh"
+#include "engine.cuh"
+#include "ops.cuh"
+
+using namespace umag;
+
+extern "C" {
+
+int umag_init(int device) { return init_device(device); }
+int umag_release(void) { return release_device(); }
+const char* umag_last_error(void) { return last_error(); }
+const char* umag_version(void) { return "umagnus_b200 1.0 (sm_100a)"; }
+
+int umag_set_stream(void* s) {
+    UMAG_TRY(ensure_init());
+    ctx().stream = s ? (cudaStream_t)s : ctx().own_stream;
+    return UMAG_OK;
+}
+
+int umag_sync(void) {
+    UMAG_TRY(ensure_init());
+    UMAG_CUDA(cudaStreamSynchronize(ctx().stream));
+    return UMAG_OK;
+}
+
+int umag_malloc(void** p, size_t bytes) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(p != nullptr, "NULL pointer");
+    if (cudaMalloc(p, bytes ? bytes : 1) != cudaSuccess) return set_error(UMAG_E_NOMEM, "cudaMalloc(%zu)", bytes);
+    return UMAG_OK;
+}
+int umag_free(void* p) {
+    UMAG_TRY(ensure_init());
+    UMAG_CUDA(cudaFree(p));
+    return UMAG_OK;
+}
+int umag_memcpy_htod(void* dst, const void* src, size_t bytes) {
+    UMAG_TRY(ensure_init());
+    UMAG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx().stream));
+    UMAG_CUDA(cudaStreamSynchronize(ctx().stream));
+    return UMAG_OK;
+}
+int umag_memcpy_dtoh(void* dst, const void* src, size_t bytes) {
+    UMAG_TRY(ensure_init());
+    UMAG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx().stream));
+    UMAG_CUDA(cudaStreamSynchronize(ctx().stream));
+    return UMAG_OK;
+}
+int umag_memcpy_dtod(void* dst, const void* src, size_t bytes) {
+    UMAG_TRY(ensure_init());
+    UMAG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx().stream));
+    return UMAG_OK;
+}
+int umag_memset_f32(float* dst, float v, size_t n) { return memset_f32(dst, v, n); }
+
+int umag_add_exchange(float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
+                      const float* Ms, float Ms_mul, const float* aLUT2d, const uint8_t* regions, int Nx, int Ny,
+                      int Nz, double cx, double cy, double cz, int pbc) {
+    return add_exchange(Bx, By, Bz, mx, my, mz, Ms, Ms_mul, aLUT2d, regions, Nx, Ny, Nz, cx, cy, cz, pbc);
+}
+int umag_add_dmi(float* Hx, float* Hy, float* Hz, const float* mx, const float* my, const float* mz, const float* Ms,
+                 float Ms_mul, const float* aLUT2d, const float* dLUT2d, const uint8_t* regions, int Nx, int Ny,
+                 int Nz, double cx, double cy, double cz, int pbc, int openbc) {
+    return add_dmi(Hx, Hy, Hz, mx, my, mz, Ms, Ms_mul, aLUT2d, dLUT2d, regions, Nx, Ny, Nz, cx, cy, cz, pbc, openbc);
+}
+int umag_add_uniaxial_anisotropy2(float* Bx, float* By, float* Bz, const float* mx, const float* my,
+                                  const float* mz, const float* Ms, float Ms_mul, const float* K1, float K1_mul,
+                                  const float* K2, float K2_mul, const float* ux, float ux_mul, const float* uy,
+                                  float uy_mul, const float* uz, float uz_mul, int N) {
+    UniaxParams p{Ms, K1, K2, ux, uy, uz, Ms_mul, K1_mul, K2_mul, ux_mul, uy_mul, uz_mul};
+    return add_uniaxial(Bx, By, Bz, mx, my, mz, p, N);
+}
+int umag_region_addv(float* dx, float* dy, float* dz, const float* lx, const float* ly, const float* lz,
+                     const uint8_t* regions, int N) {
+    return region_addv(dx, dy, dz, lx, ly, lz, regions, N);
+}
+int umag_region_decode(float* dst, const float* lut, const uint8_t* regions, int N) {
+    return region_decode(dst, lut, regions, N);
+}
+int umag_lltorque(float* tx, float* ty, float* tz, const float* mx, const float* my, const float* mz,
+                  const float* hx, const float* hy, const float* hz, const float* alpha, float alpha_mul, int N) {
+    return torque(tx, ty, tz, mx, my, mz, hx, hy, hz, alpha, alpha_mul, N, 1);
+}
+int umag_llnoprecess(float* tx, float* ty, float* tz, const float* mx, const float* my, const float* mz,
+                     const float* hx, const float* hy, const float* hz, int N) {
+    return torque(tx, ty, tz, mx, my, mz, hx, hy, hz, nullptr, 0.f, N, 0);
+}
+int umag_madd(int ncomp, float* const* dst, int nsrc, const float* const* src, const float* fac, int N) {
+    return madd(ncomp, dst, nsrc, src, fac, N);
+}
+int umag_normalize(float* vx, float* vy, float* vz, const float* vol, int N) { return normalize(vx, vy, vz, vol, N); }
+int umag_vecnorm(float* dst, const float* ax, const float* ay, const float* az, int N) {
+    return vecnorm(dst, ax, ay, az, N);
+}
+int umag_div(float* dst, const float* a, const float* b, int N) { return umag::div(dst, a, b, N); }
+int umag_add_dot_product(float* dst, float pre, const float* ax, const float* ay, const float* az, const float* bx,
+                         const float* by, const float* bz, int N) {
+    return add_dot(dst, pre, ax, ay, az, bx, by, bz, N);
+}
+int umag_max_vec_norm(const float* x, const float* y, const float* z, int N, double* out) {
+    return max_vec_norm(x, y, z, N, out);
+}
+int umag_max_vec_diff(const float* ax, const float* ay, const float* az, const float* bx, const float* by,
+                      const float* bz, int N, double* out) {
+    return max_vec_diff(ax, ay, az, bx, by, bz, N, out);
+}
+int umag_max_abs(const float* v, int N, double* out) { return max_abs(v, N, out); }
+int umag_sum(const float* v, int N, double* out) { return sum_dot(v, nullptr, N, out); }
+int umag_dot(const float* a, const float* b, int N, double* out) {
+    UMAG_REQUIRE(b != nullptr, "NULL argument");
+    return sum_dot(a, b, N, out);
+}
+
+int umag_demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy, double cz,
+                          int asymptotic_radius, int zero_self_demag, umag_demag** out) {
+    return demag_new_newell(Nx, Ny, Nz, pbc, cx, cy, cz, asymptotic_radius, zero_self_demag, out);
+}
+int umag_demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6], umag_demag** out) {
+    return demag_new_from_kernel(Nx, Ny, Nz, kern, out);
+}
+int umag_demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
+                    const float* vol, const float* Ms, float Ms_mul) {
+    UMAG_TRY(ensure_init());
+    return demag_exec(d, Bx, By, Bz, mx, my, mz, vol, Ms, Ms_mul);
+}
+int umag_demag_get_spectrum(umag_demag* d, float* const host[6]) { return demag_get_spectrum(d, host); }
+int umag_demag_get_kernel(umag_demag* d, double* const host[6]) { return demag_get_kernel(d, host); }
+int umag_demag_padded_size(umag_demag* d, int P[3]) {
+    UMAG_REQUIRE(d && P, "NULL argument");
+    for (int i = 0; i < 3; i++) P[i] = d->P[i];
+    return UMAG_OK;
+}
+int umag_demag_free(umag_demag* d) {
+    if (d) {
+        cudaStreamSynchronize(ctx().stream);
+        demag_free(d);
+    }
+    return UMAG_OK;
+}
+
+// engine/run.go:14-43 defaults, engine/torque.go:27 GammaLL
+void umag_solver_defaults(umag_solver_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->solver = 5;
+    p->dt = 1e-15;
+    p->max_err = 1e-5;
+    p->rel_err = 1e-4;
+    p->min_slope = 1e8;
+    p->headroom = 0.8;
+    p->gamma_ll = 1.7595e11;
+}
+int umag_sim_new(const umag_sim_params* p, const umag_solver_params* s, umag_sim** out) { return sim_new(p, s, out); }
+int umag_sim_free(umag_sim* s) { return sim_free(s); }
+int umag_sim_set_m(umag_sim* s, const float* mx, const float* my, const float* mz) { return sim_set_m(s, mx, my, mz); }
+int umag_sim_get_m(umag_sim* s, float* mx, float* my, float* mz) { return sim_get_m(s, mx, my, mz); }
+int umag_sim_m_ptrs(umag_sim* s, float** m3) { return sim_m_ptrs(s, m3); }
+int umag_sim_torque(umag_sim* s, float* tx, float* ty, float* tz, float* bx, float* by, float* bz) {
+    return sim_torque(s, tx, ty, tz, bx, by, bz);
+}
+int umag_sim_steps(umag_sim* s, int n) { return sim_steps(s, n); }
+int umag_sim_run(umag_sim* s, double seconds, int chunk, long long max_steps) {
+    return sim_run(s, seconds, chunk, max_steps);
+}
+int umag_sim_get_state(umag_sim* s, umag_solver_state* st) { return sim_get_state(s, st); }
+int umag_sim_set_time(umag_sim* s, double t, double dt) { return sim_set_time(s, t, dt); }
+int umag_sim_average_m(umag_sim* s, double avg[3]) { return sim_average_m(s, avg); }
+int umag_sim_use_graph(umag_sim* s, int enable, int steps) { return sim_use_graph(s, enable, steps); }
+int umag_sim_launches_per_step(umag_sim* s, int* n) { return sim_launches_per_step(s, n); }
+int umag_sim_torque_evals(umag_sim* s, int n) { return sim_torque_evals(s, n); }
+
+}  // extern "C"

@@ -1,0 +1,60 @@
+// demag.cuh -- demag plan shared by the device-op API and the engine.
+#pragma once
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+
+constexpr int kPassThreads = 256;   // passes A and C
+constexpr int kPassBThreads = 512;  // pass B
+constexpr int kChunkW = 32;         // kx columns per z-transform block in passes A/C
+
+struct umag_demag {
+    int N[3], P[3];
+    double cell[3];
+    int arad, zero_self;
+    int M, Hx, HxP, Lx, WB;
+    bool is2d;
+    umag::FftLine<float> fx, fy, fz;  // x: length Px/2 (packed real), y: Py, z: Pz
+    std::vector<float2*> tw_dev;
+    float2* twr = nullptr;            // exp(-2 pi i k / Px), k in [0, Px/4]
+    float2* spec = nullptr;           // 3 * Pz * Ny * Lx
+    float* K[6] = {};                 // xx yy zz yz xz xy (yz, xz NULL in 2D)
+    size_t Kn = 0;
+};
+
+namespace umag {
+
+struct PassArgs {
+    int Nx, Ny, Nz, Px, Py, Pz, M, Hx, HxP, Lx, WB;
+    FftLine<float> fx, fy, fz;
+    const float2* twr;
+    float2* spec;
+    const float* K[6];
+    const float* m[3];
+    // engine use: magnetisation read through a device-side slot
+    // (m_sel ? *m_ind_w : *m_ind) + c*ncell, and a device flag that turns a
+    // skipped step into no-ops.  NULL for the plain device-op API.
+    float* const* m_ind;
+    float* const* m_ind_w;
+    int m_sel;
+    int ncell;
+    const int* active;
+    const float* vol;
+    const float* Ms;
+    float Ms_mul;
+    float* B[3];
+};
+
+int demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy, double cz, int arad,
+                     int zero_self, umag_demag** out);
+int demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6], umag_demag** out);
+int demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
+               const float* vol, const float* Ms, float Ms_mul);
+int demag_get_kernel(umag_demag* d, double* const host[6]);
+int demag_get_spectrum(umag_demag* d, float* const host[6]);
+void demag_free(umag_demag* d);
+void fill_pass_args(const umag_demag* d, PassArgs& a);
+int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st);
+
+}  // namespace umag

@@ -1,0 +1,831 @@
+// engine.cu -- a whole simulation on the device: effective field, torque,
+// RK45DP / RK23 / Heun / RK4 steppers and the step controller.
+//
+// Restates engine/effectivefield.go, engine/torque.go, engine/rk45dp.go,
+// engine/rk23.go, engine/heun.go, engine/rk4.go, engine/stepcontroller.go
+// and engine/run.go:150-188 (adaptDt).  The solver state (time, dt in FP64,
+// counters, accept/reject decision) lives in device memory and is updated
+// by a one-thread controller kernel, so a step never waits for the host and
+// many steps are replayed from one CUDA graph.  Buffers are addressed
+// through a device-side slot table: accepting a step swaps the state and
+// working magnetisation slots and moves k7 into the k1 slot (FSAL,
+// engine/stepcontroller.go:76-78) without copying.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "cellmath.cuh"
+#include "common.cuh"
+#include "demag.cuh"
+#include "engine.cuh"
+#include "ops.cuh"
+
+namespace umag {
+
+// ---------------------------------------------------------------- device state
+struct DevCtl {
+    float* m;        // state magnetisation (3N, SoA)
+    float* mw;       // working / stage magnetisation
+    float* k[7];     // stage torques
+    double t, dt, t0, alarm, stop;
+    float h;         // float32(dt * GammaLL) of the step in progress
+    int active;      // 0: the step in progress is skipped (stop time reached)
+    unsigned int err2, dm2, rel;  // float bit patterns, atomicMax targets
+    int nan_seen;
+    int accepted;
+    double last_err, peak_err, last_torque;
+    long long nsteps, nundone, nevals;
+    int status;
+    double max_err, rel_err, min_dt, max_dt, fix_dt, headroom, min_slope, gamma;
+};
+
+struct LocalArgs {
+    Mesh3 g;
+    int N;
+    DevCtl* ctl;
+    int m_sel;           // 0: ctl->m, 1: ctl->mw
+    int out_slot;        // torque -> ctl->k[out_slot]
+    float* tau_direct;   // if set, torque goes here instead
+    float* beff;         // optional B_eff output
+    const float* bd;     // demag field or NULL
+    const float* aLUT;
+    const float* dLUT;
+    const uint8_t* regions;
+    float wx, wy, wz, cx, cy, cz;
+    int dmi, openbc, anis, zeeman, precess;
+    UniaxParams up;
+    const float* bext[3];
+    const float* alpha;
+    float alpha_mul;
+    const float* Ms;
+    float Ms_mul;
+};
+
+// engine/effectivefield.go:14-24 + engine/torque.go:135-144 for one cell:
+// B = demag; B += exchange(+DMI)/Ms; B += anisotropy; B += B_ext; torque.
+__global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
+    if (!a.ctl->active) return;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    int iz = blockIdx.z;
+    if (ix >= a.g.Nx || iy >= a.g.Ny) return;
+    const int N = a.N;
+    const float* m = a.m_sel ? a.ctl->mw : a.ctl->m;
+    const float *mx = m, *my = m + N, *mz = m + 2 * N;
+    int I = (iz * a.g.Ny + iy) * a.g.Nx + ix;
+    f3 B{0.f, 0.f, 0.f};
+    if (a.bd) B = f3{a.bd[I], a.bd[N + I], a.bd[2 * N + I]};
+    f3 m0 = ld3(mx, my, mz, I);
+    if (!is0(m0)) {
+        int r0 = __ldg(a.regions + I);
+        f3 e = a.dmi ? dmi_sum(mx, my, mz, a.aLUT, a.dLUT, a.regions, a.cx, a.cy, a.cz, a.g, a.openbc != 0, ix, iy,
+                               iz, m0, r0)
+                     : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
+        float inv = inv_msat(a.Ms, a.Ms_mul, I);
+        B.x = fa(B.x, fm(e.x, inv));
+        B.y = fa(B.y, fm(e.y, inv));
+        B.z = fa(B.z, fm(e.z, inv));
+    }
+    if (a.anis) add_uniaxial(B, a.up, m0, I);
+    if (a.zeeman) {
+        int r = __ldg(a.regions + I);
+        B.x = fa(B.x, __ldg(a.bext[0] + r));
+        B.y = fa(B.y, __ldg(a.bext[1] + r));
+        B.z = fa(B.z, __ldg(a.bext[2] + r));
+    }
+    if (a.beff) { a.beff[I] = B.x; a.beff[N + I] = B.y; a.beff[2 * N + I] = B.z; }
+    f3 t = a.precess ? lltorque(m0, B, amul(a.alpha, a.alpha_mul, I)) : llnoprecess(m0, B);
+    float* out = a.tau_direct ? a.tau_direct : a.ctl->k[a.out_slot];
+    out[I] = t.x; out[N + I] = t.y; out[2 * N + I] = t.z;
+}
+
+// ---------------------------------------------------------------- stages
+constexpr int kMaxTerms = 7;
+struct StageArgs {
+    DevCtl* ctl;
+    int N;
+    int nterm;
+    int src_m;             // first term: 0 = ctl->m, 1 = ctl->mw (coefficient 1)
+    int slot[kMaxTerms];   // k slots of terms 1..nterm-1
+    float c[kMaxTerms];    // float32 constants multiplying h (terms 1..)
+    int scale_h;           // 1: fac = c*h ; 0: fac = c
+    int normalize;
+    int only_if_accepted;  // RK4 final solution
+    const float* vol;
+};
+
+// m_w = normalize(src + sum_j (c_j h) k_j) with Madd<n> rounding
+// (opencl/madd.go, madd<n>.cl) then normalize2.cl.
+__global__ void k_stage(StageArgs a) {
+    DevCtl* ctl = a.ctl;
+    if (!ctl->active) return;
+    if (a.only_if_accepted && !ctl->accepted) return;
+    const float h = ctl->h;
+    float fac[kMaxTerms];
+    const float* src[kMaxTerms];
+    fac[0] = 1.0f;
+    src[0] = a.src_m ? ctl->mw : ctl->m;
+#pragma unroll
+    for (int j = 1; j < kMaxTerms; j++) {
+        if (j < a.nterm) {
+            fac[j] = a.scale_h ? fm(a.c[j], h) : a.c[j];
+            src[j] = ctl->k[a.slot[j]];
+        }
+    }
+    float* dst = ctl->mw;
+    const int N = a.N;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        float v[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            int o = c * N + i;
+            float acc;
+            if (a.nterm == 3) {
+                acc = fa(fm(fac[0], src[0][o]), fa(fm(fac[1], src[1][o]), fm(fac[2], src[2][o])));
+            } else {
+                acc = fm(fac[0], src[0][o]);
+                for (int j = 1; j < a.nterm; j++) acc = fa(acc, fm(fac[j], src[j][o]));
+            }
+            v[c] = acc;
+        }
+        if (a.normalize) {
+            float w = a.vol ? a.vol[i] : 1.0f;
+            f3 r = normalize_vol(f3{v[0], v[1], v[2]}, w);
+            v[0] = r.x; v[1] = r.y; v[2] = r.z;
+        }
+        dst[i] = v[0]; dst[N + i] = v[1]; dst[2 * N + i] = v[2];
+    }
+}
+
+// ---------------------------------------------------------------- error norms
+struct ErrArgs {
+    DevCtl* ctl;
+    int N;
+    int nterm;
+    int slot[kMaxTerms];
+    float e[kMaxTerms];
+    int dm_slot;     // slot whose max norm is the torque of the new state (delM / k4 / dy)
+    int heun;        // 1: error = |k[slot0] - k[slot1]| (MaxVecDiff)
+};
+
+// Fused: error combination (Madd rounding), max |Err|^2, max |delM|^2 and
+// max |Err|/|delM| (VecNorm + Div + MaxAbs of stepcontroller.go:51-63);
+// Err itself is never written to memory.
+__global__ void __launch_bounds__(256) k_err_norms(ErrArgs a) {
+    __shared__ float sh[32];
+    DevCtl* ctl = a.ctl;
+    if (!ctl->active) return;
+    const float* k[kMaxTerms];
+#pragma unroll
+    for (int j = 0; j < kMaxTerms; j++)
+        if (j < a.nterm) k[j] = ctl->k[a.slot[j]];
+    const float* dm = ctl->k[a.dm_slot];
+    const int N = a.N;
+    float me = 0.f, md = 0.f, mr = 0.f;
+    int nan = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        f3 E;
+        float* ev = &E.x;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            int o = c * N + i;
+            float acc;
+            if (a.heun) {
+                acc = fs(k[0][o], k[1][o]);
+            } else if (a.nterm == 3) {
+                acc = fa(fm(a.e[0], k[0][o]), fa(fm(a.e[1], k[1][o]), fm(a.e[2], k[2][o])));
+            } else {
+                acc = fm(a.e[0], k[0][o]);
+                for (int j = 1; j < a.nterm; j++) acc = fa(acc, fm(a.e[j], k[j][o]));
+            }
+            ev[c] = acc;
+        }
+        f3 D{dm[i], dm[N + i], dm[2 * N + i]};
+        float e2 = dot3(E, E), d2 = dot3(D, D);
+        float en = __fsqrt_rn(e2), dn = __fsqrt_rn(d2);
+        float r = dn == 0.0f ? 0.0f : fd(en, dn);
+        nan |= (e2 != e2) | (d2 != d2);
+        me = fmaxf(me, e2);
+        md = fmaxf(md, d2);
+        mr = fmaxf(mr, r);
+    }
+    me = block_max<256>(me, sh);
+    md = block_max<256>(md, sh);
+    mr = block_max<256>(mr, sh);
+    nan = __syncthreads_or(nan);
+    if (threadIdx.x == 0) {
+        atomic_max_nonneg(&ctl->err2, me);
+        atomic_max_nonneg(&ctl->dm2, md);
+        atomic_max_nonneg(&ctl->rel, mr);
+        if (nan) atomicOr(&ctl->nan_seen, 1);
+    }
+}
+
+// ---------------------------------------------------------------- controller
+__device__ void adapt_dt(DevCtl* c, double corr) {
+    if (c->fix_dt != 0) { c->dt = c->fix_dt; return; }
+    if (isnan(corr)) corr = 1;
+    if (corr == 0) { c->status = 1; return; }
+    corr *= c->headroom;
+    if (corr > 2) corr = 2;
+    if (corr < 1. / 2.) corr = 1. / 2.;
+    c->dt *= corr;
+    if (c->min_dt != 0 && c->dt < c->min_dt) c->dt = c->min_dt;
+    if (c->max_dt != 0 && c->dt > c->max_dt) c->dt = c->max_dt;
+    if (c->dt == 0) { c->status = 2; return; }
+    if (c->t < c->alarm && c->t + c->dt > c->alarm) c->dt = c->alarm - c->t;
+    if (!(c->dt > 0)) c->status = 3;
+}
+
+// engine/rk45dp.go:16-50 (start of Step): fixed dt, h, t0, clear maxima;
+// skip the step once the run's stop time is reached (engine/run.go:212-231).
+__global__ void k_step_begin(DevCtl* c) {
+    c->active = (c->t < c->stop) && c->status == 0;
+    if (!c->active) return;
+    if (c->fix_dt != 0) c->dt = c->fix_dt;
+    c->h = (float)(c->dt * c->gamma);
+    c->t0 = c->t;
+    c->err2 = 0u; c->dm2 = 0u; c->rel = 0u;
+    c->accepted = 0;
+}
+
+// kind 0: integralController (engine/stepcontroller.go:35-97), FSAL when fsal
+// kind 1: simpleController (:13-32, RK4); kind 2: Heun (engine/heun.go:40-58)
+__global__ void k_controller(DevCtl* c, int kind, int acc, int rej, int fsal_from, int fsal_to, int nevals) {
+    if (!c->active) return;
+    c->nevals += nevals;
+    if (c->nan_seen) c->status = 4;
+    double h = (double)c->h;
+    double err = sqrt((double)__uint_as_float(c->err2)) * h;
+    double maxdm = sqrt((double)__uint_as_float(c->dm2));
+    bool ok = err < c->max_err || c->dt <= c->min_dt || c->fix_dt != 0;
+    if (kind == 0) {
+        if (ok) {
+            int fail = 0;
+            double rlerr = 0.0;
+            if (!(maxdm < c->min_slope)) {
+                rlerr = (double)__uint_as_float(c->rel);
+                fail = 1;
+            }
+            if (fail == 0 || c->rel_err <= 0.0 || rlerr < c->rel_err || c->dt <= c->min_dt || c->fix_dt != 0) {
+                c->last_err = err;
+                if (err > c->peak_err) c->peak_err = err;
+                c->last_torque = maxdm;
+                c->nsteps++;
+                c->t = c->t0 + c->dt;
+                adapt_dt(c, fail == 0 ? pow(c->max_err / err, 1. / acc) : pow(c->rel_err / rlerr, 1. / acc));
+                c->accepted = 1;
+            } else {
+                c->t = c->t0;
+                c->nundone++;
+                adapt_dt(c, pow(c->rel_err / rlerr, 1. / rej));
+            }
+        } else {
+            c->t = c->t0;
+            c->nundone++;
+            adapt_dt(c, pow(c->max_err / err, 1. / rej));
+        }
+    } else if (kind == 1) {  // RK4: Time = t0 + dt was set before stage 4 (rk4.go:51)
+        c->t = c->t0 + c->dt;
+        if (ok) {
+            c->nsteps++;
+            adapt_dt(c, pow(c->max_err / err, 1. / acc));
+            c->last_err = err;
+            if (err > c->peak_err) c->peak_err = err;
+            c->accepted = 1;
+        } else {
+            c->nundone++;
+            adapt_dt(c, pow(c->max_err / err, 1. / rej));
+            c->t = c->t0;
+        }
+    } else {  // Heun: time was advanced before the second evaluation
+        if (ok) {
+            c->t = c->t0 + c->dt;
+            c->nsteps++;
+            adapt_dt(c, pow(c->max_err / err, 1. / 2.));
+            c->last_err = err;
+            if (err > c->peak_err) c->peak_err = err;
+            c->last_torque = maxdm;
+            c->accepted = 1;
+        } else {
+            c->t = c->t0;
+            c->nundone++;
+            adapt_dt(c, pow(c->max_err / err, 1. / 3.));
+        }
+    }
+    if (c->accepted && kind == 0 && fsal_from >= 0) {
+        float* t = c->k[fsal_to];
+        c->k[fsal_to] = c->k[fsal_from];
+        c->k[fsal_from] = t;
+    }
+}
+
+// accepted: the working magnetisation becomes the state (pointer swap);
+// RK4 also records max |k4| here (setMaxTorque, engine/rk4.go:64)
+__global__ void k_step_end(DevCtl* c, int rk4) {
+    if (!c->active) return;
+    if (c->accepted) {
+        float* t = c->m;
+        c->m = c->mw;
+        c->mw = t;
+        if (rk4) c->last_torque = sqrt((double)__uint_as_float(c->dm2));
+    }
+}
+
+// ---------------------------------------------------------------- host side
+struct SimImpl {
+    umag_sim_params p;
+    umag_solver_params sp;
+    int N;
+    Mesh3 g;
+    umag_demag* demag = nullptr;
+    float* bufs = nullptr;        // 2 + 7 slots of 3N
+    float* bd = nullptr;          // demag field 3N
+    uint8_t* zero_regions = nullptr;
+    DevCtl* ctl = nullptr;        // device
+    DevCtl* hctl = nullptr;       // pinned host mirror
+    PassArgs pa{};
+    LocalArgs la{};
+    bool need_k1 = true;
+    bool use_graph = true;
+    int graph_steps = 16;
+    cudaGraphExec_t gexec = nullptr;
+    int launches_per_step = 0;
+};
+
+static cudaStream_t S() { return ctx().stream; }
+
+// one torque evaluation of ctl->(m | mw) into ctl->k[slot] (or a direct buffer)
+static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, float* beff, int* nl) {
+    if (s->p.enable_demag) {
+        PassArgs a = s->pa;
+        a.m_sel = m_sel;
+        UMAG_TRY(demag_launch(s->demag, a, S()));
+        if (nl) *nl += 3;
+    }
+    LocalArgs la = s->la;
+    la.m_sel = m_sel;
+    la.out_slot = slot;
+    la.tau_direct = tau_direct;
+    la.beff = beff;
+    dim3 blk(32, 8, 1), grd((s->g.Nx + 31) / 32, (s->g.Ny + 7) / 8, s->g.Nz);
+    k_local_torque<<<grd, blk, 0, S()>>>(la);
+    UMAG_LAUNCH_CHECK();
+    if (nl) *nl += 1;
+    return UMAG_OK;
+}
+
+static int launch_stage(SimImpl* s, int src_m, std::initializer_list<int> slots, std::initializer_list<double> cs,
+                        bool scale_h, bool normalize, bool only_if_accepted, int* nl) {
+    StageArgs a{};
+    a.ctl = s->ctl;
+    a.N = s->N;
+    a.src_m = src_m;
+    a.nterm = 1 + (int)slots.size();
+    int j = 1;
+    for (int sl : slots) a.slot[j++] = sl;
+    j = 1;
+    for (double c : cs) a.c[j++] = (float)c;  // Go: untyped constant converted to float32
+    a.scale_h = scale_h;
+    a.normalize = normalize;
+    a.only_if_accepted = only_if_accepted;
+    a.vol = s->p.vol;
+    k_stage<<<grid_for(s->N, 256), 256, 0, S()>>>(a);
+    UMAG_LAUNCH_CHECK();
+    *nl += 1;
+    return UMAG_OK;
+}
+
+static int launch_err(SimImpl* s, std::initializer_list<int> slots, std::initializer_list<double> es, int dm_slot,
+                      bool heun, int* nl) {
+    ErrArgs a{};
+    a.ctl = s->ctl;
+    a.N = s->N;
+    a.nterm = (int)slots.size();
+    int j = 0;
+    for (int sl : slots) a.slot[j++] = sl;
+    j = 0;
+    for (double e : es) a.e[j++] = (float)e;
+    a.dm_slot = dm_slot;
+    a.heun = heun;
+    k_err_norms<<<grid_for(s->N, 256, 4), 256, 0, S()>>>(a);
+    UMAG_LAUNCH_CHECK();
+    *nl += 1;
+    return UMAG_OK;
+}
+
+// Slots: k[0] = k1 (FSAL), k[1..6] = k2..k7 buffers.
+static int launch_step(SimImpl* s, int* nl) {
+    DevCtl* c = s->ctl;
+    k_step_begin<<<1, 1, 0, S()>>>(c);
+    UMAG_LAUNCH_CHECK();
+    *nl += 1;
+    switch (s->sp.solver) {
+    case 5: {  // engine/rk45dp.go:52-97
+        UMAG_TRY(launch_stage(s, 0, {0}, {1. / 5.}, true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 1, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {0, 1}, {3. / 40., 9. / 40.}, true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 2, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {0, 1, 2}, {44. / 45., -56. / 15., 32. / 9.}, true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 3, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {0, 1, 2, 3}, {19372. / 6561., -25360. / 2187., 64448. / 6561., -212. / 729.},
+                              true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 4, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {0, 1, 2, 3, 4},
+                              {9017. / 3168., -355. / 33., 46732. / 5247., 49. / 176., -5103. / 18656.}, true, true,
+                              false, nl));
+        UMAG_TRY(launch_torque(s, 1, 5, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {0, 2, 3, 4, 5},
+                              {35. / 384., 500. / 1113., 125. / 192., -2187. / 6784., 11. / 84.}, true, true, false,
+                              nl));
+        UMAG_TRY(launch_torque(s, 1, 6, nullptr, nullptr, nl));
+        // rk45dp.go:95 weight differences, as exact rationals rounded to float32
+        UMAG_TRY(launch_err(s, {0, 2, 3, 4, 5, 6},
+                            {71. / 57600., -71. / 16695., 71. / 1920., -17253. / 339200., 22. / 525., -1. / 40.}, 6,
+                            false, nl));
+        k_controller<<<1, 1, 0, S()>>>(c, 0, 5, 6, 6, 0, 6);
+        break;
+    }
+    case 3: {  // engine/rk23.go:58-83
+        UMAG_TRY(launch_stage(s, 0, {0}, {1. / 2.}, true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 1, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {1}, {3. / 4.}, true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 2, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {0, 1, 2}, {2. / 9., 1. / 3., 4. / 9.}, true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 3, nullptr, nullptr, nl));
+        UMAG_TRY(launch_err(s, {0, 1, 2, 3}, {5. / 72., -1. / 12., -1. / 9., 1. / 8.}, 3, false, nl));
+        k_controller<<<1, 1, 0, S()>>>(c, 0, 3, 4, 3, 0, 3);
+        break;
+    }
+    case 2: {  // engine/heun.go:15-59
+        UMAG_TRY(launch_torque(s, 0, 0, nullptr, nullptr, nl));                      // dy0
+        UMAG_TRY(launch_stage(s, 0, {0}, {1.0}, true, false, false, nl));            // y = y + dt*dy0
+        UMAG_TRY(launch_torque(s, 1, 1, nullptr, nullptr, nl));                      // dy
+        UMAG_TRY(launch_err(s, {0, 1}, {1.0, -1.0}, 1, true, nl));                   // |dy0 - dy|
+        k_controller<<<1, 1, 0, S()>>>(c, 2, 2, 3, -1, -1, 2);
+        UMAG_LAUNCH_CHECK();
+        *nl += 1;
+        // accepted: y = y + 0.5 dt dy - 0.5 dt dy0, normalised (heun.go:45-46)
+        UMAG_TRY(launch_stage(s, 1, {1, 0}, {0.5, -0.5}, true, true, true, nl));
+        k_step_end<<<1, 1, 0, S()>>>(c, 0);
+        UMAG_LAUNCH_CHECK();
+        *nl += 1;
+        return UMAG_OK;
+    }
+    case 4: {  // engine/rk4.go:11-69
+        UMAG_TRY(launch_torque(s, 0, 0, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {0}, {1. / 2.}, true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 1, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {1}, {1. / 2.}, true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 2, nullptr, nullptr, nl));
+        UMAG_TRY(launch_stage(s, 0, {2}, {1.}, true, true, false, nl));
+        UMAG_TRY(launch_torque(s, 1, 3, nullptr, nullptr, nl));
+        UMAG_TRY(launch_err(s, {0, 3}, {1., -1.}, 3, false, nl));
+        k_controller<<<1, 1, 0, S()>>>(c, 1, 4, 5, -1, -1, 4);
+        UMAG_LAUNCH_CHECK();
+        *nl += 1;
+        UMAG_TRY(launch_stage(s, 0, {0, 1, 2, 3}, {1. / 6., 1. / 3., 1. / 3., 1. / 6.}, true, true, true, nl));
+        k_step_end<<<1, 1, 0, S()>>>(c, 1);
+        UMAG_LAUNCH_CHECK();
+        *nl += 1;
+        return UMAG_OK;
+    }
+    default:
+        return set_error(UMAG_E_ARG, "unknown solver %d", s->sp.solver);
+    }
+    UMAG_LAUNCH_CHECK();
+    *nl += 1;
+    k_step_end<<<1, 1, 0, S()>>>(c, 0);
+    UMAG_LAUNCH_CHECK();
+    *nl += 1;
+    return UMAG_OK;
+}
+
+static int sync_ctl_to_host(SimImpl* s) {
+    UMAG_CUDA(cudaMemcpyAsync(s->hctl, s->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    return UMAG_OK;
+}
+static int push_ctl(SimImpl* s) {
+    UMAG_CUDA(cudaMemcpyAsync(s->ctl, s->hctl, sizeof(DevCtl), cudaMemcpyHostToDevice, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    return UMAG_OK;
+}
+
+// FSAL k1 of the current state, before the first step of a run
+// (engine/rk45dp.go:26-29; RunWhile frees the stepper, engine/run.go:207)
+static int ensure_k1(SimImpl* s) {
+    if (!s->need_k1) return UMAG_OK;
+    if (s->sp.solver == 5 || s->sp.solver == 3) {
+        UMAG_TRY(sync_ctl_to_host(s));
+        s->hctl->active = 1;
+        UMAG_TRY(push_ctl(s));
+        UMAG_TRY(launch_torque(s, 0, 0, nullptr, nullptr, nullptr));
+        UMAG_TRY(sync_ctl_to_host(s));
+        s->hctl->nevals += 1;
+        UMAG_TRY(push_ctl(s));
+    }
+    s->need_k1 = false;
+    return UMAG_OK;
+}
+
+static void drop_graph(SimImpl* s) {
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+}
+
+static int build_graph(SimImpl* s) {
+    drop_graph(s);
+    cudaGraph_t graph;
+    UMAG_CUDA(cudaStreamBeginCapture(S(), cudaStreamCaptureModeThreadLocal));
+    int nl = 0;
+    int st = UMAG_OK;
+    for (int i = 0; i < s->graph_steps && st == UMAG_OK; i++) st = launch_step(s, &nl);
+    cudaError_t e = cudaStreamEndCapture(S(), &graph);
+    if (st != UMAG_OK) return st;
+    if (e != cudaSuccess) return set_error(UMAG_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&s->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_error(UMAG_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    return UMAG_OK;
+}
+
+// n steps with the stop time already in ctl
+static int run_steps(SimImpl* s, long long n) {
+    UMAG_TRY(ensure_k1(s));
+    if (s->use_graph && n >= s->graph_steps) {
+        if (!s->gexec) UMAG_TRY(build_graph(s));
+        while (n >= s->graph_steps) {
+            UMAG_CUDA(cudaGraphLaunch(s->gexec, S()));
+            n -= s->graph_steps;
+        }
+    }
+    for (long long i = 0; i < n; i++) {
+        int nl = 0;
+        UMAG_TRY(launch_step(s, &nl));
+    }
+    return UMAG_OK;
+}
+
+int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** out) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(p && sp && out, "NULL argument");
+    UMAG_REQUIRE(p->N[0] > 0 && p->N[1] > 0 && p->N[2] > 0, "bad mesh size");
+    UMAG_REQUIRE(p->aLUT != nullptr, "aLUT (exchange LUT) is required");
+    UMAG_REQUIRE(sp->solver == 2 || sp->solver == 3 || sp->solver == 4 || sp->solver == 5,
+                 "solver must be 2 (Heun), 3 (RK23), 4 (RK4) or 5 (RK45DP)");
+    if (p->pbc[0] || p->pbc[1] || p->pbc[2])
+        return set_error(UMAG_E_UNSUPPORTED, "periodic boundary conditions are not supported by this build");
+    SimImpl* s = new SimImpl();
+    s->p = *p;
+    s->sp = *sp;
+    s->N = p->N[0] * p->N[1] * p->N[2];
+    s->g = Mesh3{p->N[0], p->N[1], p->N[2], 0};
+    int st = UMAG_OK;
+    size_t b3 = sizeof(float) * 3 * (size_t)s->N;
+    auto fail = [&](int code) { sim_free(reinterpret_cast<umag_sim*>(s)); return code; };
+    if (cudaMalloc(&s->bufs, b3 * 9) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "state buffers"));
+    cudaMemset(s->bufs, 0, b3 * 9);
+    if (!p->regions) {
+        if (cudaMalloc(&s->zero_regions, s->N) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "regions"));
+        cudaMemset(s->zero_regions, 0, s->N);
+        s->p.regions = s->zero_regions;
+    }
+    if (p->enable_demag) {
+        int pbc[3] = {0, 0, 0};
+        st = demag_new_newell(p->N[0], p->N[1], p->N[2], pbc, p->cell[0], p->cell[1], p->cell[2],
+                              p->asymptotic_radius > 0 ? p->asymptotic_radius : 32, 0, &s->demag);
+        if (st != UMAG_OK) return fail(st);
+        if (cudaMalloc(&s->bd, b3) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "demag field"));
+    }
+    if (cudaMalloc(&s->ctl, sizeof(DevCtl)) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "ctl"));
+    if (cudaMallocHost(&s->hctl, sizeof(DevCtl)) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "ctl host"));
+    DevCtl& c = *s->hctl;
+    memset(&c, 0, sizeof(c));
+    c.m = s->bufs;
+    c.mw = s->bufs + 3 * (size_t)s->N;
+    for (int i = 0; i < 7; i++) c.k[i] = s->bufs + (2 + i) * 3 * (size_t)s->N;
+    c.dt = sp->dt;
+    c.alarm = 0.0;
+    c.stop = INFINITY;
+    c.max_err = sp->max_err; c.rel_err = sp->rel_err; c.min_dt = sp->min_dt; c.max_dt = sp->max_dt;
+    c.fix_dt = sp->fix_dt; c.headroom = sp->headroom; c.min_slope = sp->min_slope; c.gamma = sp->gamma_ll;
+    c.active = 1;
+    st = push_ctl(s);
+    if (st != UMAG_OK) return fail(st);
+    // pass / local arguments
+    if (s->demag) {
+        fill_pass_args(s->demag, s->pa);
+        s->pa.m_ind = &s->ctl->m;
+        s->pa.m_ind_w = &s->ctl->mw;
+        s->pa.active = &s->ctl->active;
+        s->pa.vol = p->vol;
+        s->pa.Ms = p->Ms;
+        s->pa.Ms_mul = p->Ms_mul;
+        s->pa.ncell = s->N;
+        for (int i = 0; i < 3; i++) s->pa.B[i] = s->bd + (size_t)i * s->N;
+    }
+    LocalArgs& la = s->la;
+    la.g = s->g;
+    la.N = s->N;
+    la.ctl = s->ctl;
+    la.bd = s->bd;
+    la.aLUT = p->aLUT;
+    la.dLUT = p->dLUT;
+    la.regions = s->p.regions;
+    la.wx = (float)(2 / (p->cell[0] * p->cell[0]));
+    la.wy = (float)(2 / (p->cell[1] * p->cell[1]));
+    la.wz = (float)(2 / (p->cell[2] * p->cell[2]));
+    la.cx = (float)p->cell[0]; la.cy = (float)p->cell[1]; la.cz = (float)p->cell[2];
+    la.dmi = p->dLUT != nullptr;
+    la.openbc = p->openbc;
+    la.anis = (p->Ku1 != nullptr || p->Ku1_mul != 0.f || p->Ku2 != nullptr || p->Ku2_mul != 0.f);
+    la.up = UniaxParams{p->Ms, p->Ku1, p->Ku2, p->anisU[0], p->anisU[1], p->anisU[2],
+                        p->Ms_mul, p->Ku1_mul, p->Ku2_mul, p->anisU_mul[0], p->anisU_mul[1], p->anisU_mul[2]};
+    la.zeeman = p->bextLUT[0] != nullptr;
+    for (int i = 0; i < 3; i++) la.bext[i] = p->bextLUT[i];
+    la.alpha = p->alpha;
+    la.alpha_mul = p->alpha_mul;
+    la.precess = p->precess;
+    la.Ms = p->Ms;
+    la.Ms_mul = p->Ms_mul;
+    if (la.zeeman && (!p->bextLUT[1] || !p->bextLUT[2])) return fail(set_error(UMAG_E_ARG, "bextLUT needs 3 arrays"));
+    int nl = 0;
+    // count launches of one step (not enqueued: measured on a dry capture below)
+    s->launches_per_step = 0;
+    {
+        cudaGraph_t graph;
+        if (cudaStreamBeginCapture(S(), cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            st = launch_step(s, &nl);
+            cudaStreamEndCapture(S(), &graph);
+            cudaGraphDestroy(graph);
+            if (st != UMAG_OK) return fail(st);
+            s->launches_per_step = nl;
+        }
+    }
+    *out = reinterpret_cast<umag_sim*>(s);
+    return UMAG_OK;
+}
+
+int sim_free(umag_sim* h) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    if (!s) return UMAG_OK;
+    cudaStreamSynchronize(S());
+    drop_graph(s);
+    if (s->demag) demag_free(s->demag);
+    cudaFree(s->bufs);
+    cudaFree(s->bd);
+    cudaFree(s->zero_regions);
+    cudaFree(s->ctl);
+    if (s->hctl) cudaFreeHost(s->hctl);
+    delete s;
+    return UMAG_OK;
+}
+
+int sim_set_m(umag_sim* h, const float* mx, const float* my, const float* mz) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && mx && my && mz, "NULL argument");
+    UMAG_TRY(sync_ctl_to_host(s));
+    float* m = s->hctl->m;
+    size_t b = sizeof(float) * s->N;
+    UMAG_CUDA(cudaMemcpyAsync(m, mx, b, cudaMemcpyDeviceToDevice, S()));
+    UMAG_CUDA(cudaMemcpyAsync(m + s->N, my, b, cudaMemcpyDeviceToDevice, S()));
+    UMAG_CUDA(cudaMemcpyAsync(m + 2 * s->N, mz, b, cudaMemcpyDeviceToDevice, S()));
+    // engine/magnetization.go:34 normalize() (normalize2.cl)
+    UMAG_TRY(normalize(m, m + s->N, m + 2 * s->N, s->p.vol, s->N));
+    s->need_k1 = true;
+    return UMAG_OK;
+}
+
+int sim_m_ptrs(umag_sim* h, float** m3) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && m3, "NULL argument");
+    UMAG_TRY(sync_ctl_to_host(s));
+    for (int c = 0; c < 3; c++) m3[c] = s->hctl->m + (size_t)c * s->N;
+    return UMAG_OK;
+}
+
+int sim_get_m(umag_sim* h, float* mx, float* my, float* mz) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && mx && my && mz, "NULL argument");
+    float* m3[3];
+    UMAG_TRY(sim_m_ptrs(h, m3));
+    size_t b = sizeof(float) * s->N;
+    float* dst[3] = {mx, my, mz};
+    for (int c = 0; c < 3; c++) UMAG_CUDA(cudaMemcpyAsync(dst[c], m3[c], b, cudaMemcpyDefault, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    return UMAG_OK;
+}
+
+int sim_torque(umag_sim* h, float* tx, float* ty, float* tz, float* bx, float* by, float* bz) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && tx && ty && tz, "NULL argument");
+    UMAG_REQUIRE(ty == tx + s->N && tz == tx + 2 * s->N, "torque arrays must be one contiguous 3N buffer");
+    if (bx) UMAG_REQUIRE(by == bx + s->N && bz == bx + 2 * s->N, "B_eff arrays must be one contiguous 3N buffer");
+    UMAG_TRY(sync_ctl_to_host(s));
+    s->hctl->active = 1;
+    UMAG_TRY(push_ctl(s));
+    UMAG_TRY(launch_torque(s, 0, 0, tx, bx, nullptr));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    return UMAG_OK;
+}
+
+int sim_steps(umag_sim* h, int n) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && n >= 0, "bad argument");
+    UMAG_TRY(sync_ctl_to_host(s));
+    s->hctl->stop = INFINITY;
+    UMAG_TRY(push_ctl(s));
+    return run_steps(s, n);
+}
+
+int sim_run(umag_sim* h, double seconds, int chunk, long long max_steps) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && seconds >= 0, "bad argument");
+    if (chunk <= 0) chunk = 64;
+    UMAG_TRY(sync_ctl_to_host(s));
+    double stop = s->hctl->t + seconds;
+    s->hctl->stop = stop;
+    s->hctl->alarm = stop;  // engine/run.go:190-195: adaptDt must not cross it
+    UMAG_TRY(push_ctl(s));
+    s->need_k1 = true;      // RunWhile frees the stepper (engine/run.go:207)
+    long long done = 0;
+    while (done < max_steps) {
+        long long n = chunk;
+        if (max_steps - done < n) n = max_steps - done;
+        UMAG_TRY(run_steps(s, n));
+        done += n;
+        UMAG_TRY(sync_ctl_to_host(s));
+        if (s->hctl->status != 0) return set_error(UMAG_E_SOLVER, "solver failure code %d at t=%g", s->hctl->status,
+                                                   s->hctl->t);
+        if (!(s->hctl->t < stop)) break;
+    }
+    return UMAG_OK;
+}
+
+int sim_get_state(umag_sim* h, umag_solver_state* st) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && st, "NULL argument");
+    UMAG_TRY(sync_ctl_to_host(s));
+    const DevCtl& c = *s->hctl;
+    st->time = c.t; st->dt = c.dt; st->last_err = c.last_err; st->peak_err = c.peak_err;
+    st->last_torque = c.last_torque; st->nsteps = c.nsteps; st->nundone = c.nundone; st->nevals = c.nevals;
+    st->status = c.status;
+    return UMAG_OK;
+}
+
+int sim_set_time(umag_sim* h, double t, double dt) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s, "NULL argument");
+    UMAG_TRY(sync_ctl_to_host(s));
+    s->hctl->t = t;
+    if (dt > 0) s->hctl->dt = dt;
+    return push_ctl(s);
+}
+
+int sim_average_m(umag_sim* h, double avg[3]) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && avg, "NULL argument");
+    float* m3[3];
+    UMAG_TRY(sim_m_ptrs(h, m3));
+    // engine/average.go:29-40: sum (or vol-weighted sum) over the magnet / cell count
+    double ncell = (double)s->N;
+    if (s->p.vol) UMAG_TRY(sum_dot(s->p.vol, nullptr, s->N, &ncell));
+    for (int c = 0; c < 3; c++) {
+        double v;
+        UMAG_TRY(sum_dot(m3[c], s->p.vol, s->N, &v));
+        avg[c] = v / ncell;
+    }
+    return UMAG_OK;
+}
+
+int sim_use_graph(umag_sim* h, int enable, int steps) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s, "NULL argument");
+    s->use_graph = enable != 0;
+    if (steps > 0 && steps != s->graph_steps) {
+        s->graph_steps = steps;
+        drop_graph(s);
+    }
+    return UMAG_OK;
+}
+
+int sim_torque_evals(umag_sim* h, int n) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && n >= 0, "bad argument");
+    UMAG_TRY(ensure_k1(s));
+    UMAG_TRY(sync_ctl_to_host(s));
+    s->hctl->active = 1;
+    UMAG_TRY(push_ctl(s));
+    for (int i = 0; i < n; i++) UMAG_TRY(launch_torque(s, 0, 0, nullptr, nullptr, nullptr));
+    return UMAG_OK;
+}
+
+int sim_launches_per_step(umag_sim* h, int* n) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && n, "NULL argument");
+    *n = s->launches_per_step;
+    return UMAG_OK;
+}
+
+}  // namespace umag

@@ -1,0 +1,20 @@
+// engine.cuh -- simulation context entry points (C++ side of the C-ABI).
+#pragma once
+#include "../../include/umagnus_b200.h"
+
+namespace umag {
+int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** out);
+int sim_free(umag_sim* s);
+int sim_set_m(umag_sim* s, const float* mx, const float* my, const float* mz);
+int sim_get_m(umag_sim* s, float* mx, float* my, float* mz);
+int sim_m_ptrs(umag_sim* s, float** m3);
+int sim_torque(umag_sim* s, float* tx, float* ty, float* tz, float* bx, float* by, float* bz);
+int sim_steps(umag_sim* s, int n);
+int sim_run(umag_sim* s, double seconds, int chunk, long long max_steps);
+int sim_get_state(umag_sim* s, umag_solver_state* st);
+int sim_set_time(umag_sim* s, double t, double dt);
+int sim_average_m(umag_sim* s, double avg[3]);
+int sim_use_graph(umag_sim* s, int enable, int steps);
+int sim_launches_per_step(umag_sim* s, int* n);
+int sim_torque_evals(umag_sim* s, int n);
+}  // namespace umag

@@ -1,0 +1,225 @@
+"""Engine-level API: one simulation whose effective field, torque and time
+stepping run on the device (libumagnus_b200.so, umag_sim_*).
+
+Mirrors the reference's engine globals and functions used on the hot path:
+SetEffectiveField / SetTorque (engine/effectivefield.go, engine/torque.go),
+the Stepper interface and SetSolver (engine/run.go:69-125), Run / Steps
+(engine/run.go:190-200), m.average() (engine/average.go) and the solver
+knobs MaxErr, RelErr, MinDt, MaxDt, FixDt, Headroom (engine/run.go:14-43).
+Parameters follow engine/parameter.go: a scalar is a uniform value, a
+tensor a per-cell map; exchange and DMI are per-region values expanded into
+the symmetric inter-region LUT exactly as engine/exchange.go:153-201 does.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import SimParams, SolverParams, SolverState, UmagError, check
+
+NREGION = 256  # engine/regions.go:11
+GAMMA_LL = 1.7595e11  # engine/torque.go:27
+HEUN, BOGAKISHAMPINE, RUNGEKUTTA, DORMANDPRINCE = 2, 3, 4, 5  # engine/run.go:83-95
+
+
+def symmidx(i, j):
+    """engine/exchange.go:181-187"""
+    return i * (i + 1) // 2 + j if j <= i else j * (j + 1) // 2 + i
+
+
+def exch_average(exi, exj):
+    """engine/exchange.go:193-201 (float32 arithmetic)."""
+    exi, exj = np.float32(exi), np.float32(exj)
+    if exi * exj >= 0:
+        with np.errstate(divide="ignore"):
+            return np.float32(2) / (np.float32(1) / exi + np.float32(1) / exj)
+    a, b = float(exi), float(exj)
+    sign = np.copysign(1.0, a + b)
+    return np.float32(sign * np.sqrt(np.sqrt(-a * b) * abs(a + b) / 2))
+
+
+def exchange_lut(values, scale=None, inter=None):
+    """engine/exchange.go:153-167: lut[symidx(i,j)] = scale*avg(ex_i, ex_j) + inter."""
+    ex = np.zeros(NREGION, np.float32)
+    v = np.asarray(values, np.float32).ravel()
+    ex[: v.size] = v
+    if v.size == 1:
+        ex[:] = v[0]
+    lut = np.zeros(NREGION * (NREGION + 1) // 2, np.float32)
+    a = ex[:, None]
+    b = ex[None, :]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        same = (a * b) >= 0
+        harm = np.float32(2) / (np.float32(1) / a + np.float32(1) / b)
+    I, J = np.tril_indices(NREGION)
+    vals = np.where(same[I, J], harm[I, J], 0).astype(np.float32)
+    for k in np.nonzero(~same[I, J])[0]:
+        vals[k] = exch_average(ex[I[k]], ex[J[k]])
+    idx = I * (I + 1) // 2 + J
+    sc = np.ones(lut.size, np.float32) if scale is None else np.asarray(scale, np.float32)
+    it = np.zeros(lut.size, np.float32) if inter is None else np.asarray(inter, np.float32)
+    lut[idx] = sc[idx] * vals + it[idx]
+    return lut
+
+
+def _dev(x, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype).cuda()
+
+
+class Simulation:
+    """A micromagnetic simulation on one GPU.
+
+    N: (Nx, Ny, Nz); cell: cell size in m; Msat, alpha, Ku1, Ku2: scalar or
+    per-cell (Nz, Ny, Nx) array; Aex, Dind: scalar or 256 per-region values;
+    anisU: 3-vector or (3, Nz, Ny, Nx); B_ext: 3-vector (T) or (256, 3)
+    per-region; regions: uint8 (Nz, Ny, Nx) map; geom: cell volume fraction.
+    """
+
+    def __init__(self, N, cell, Msat, Aex, alpha, Dind=0.0, Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
+                 regions=None, geom=None, demag=True, open_bc=False, precess=True, solver=DORMANDPRINCE,
+                 dt=1e-15, MaxErr=1e-5, RelErr=1e-4, MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8,
+                 device=0, asymptotic_radius=32):
+        self.L = _lib.init(device)
+        self.N = tuple(int(n) for n in N)
+        self.ncell = self.N[0] * self.N[1] * self.N[2]
+        self.shape = (self.N[2], self.N[1], self.N[0])
+        self._keep = []
+        p = SimParams()
+        p.N[:] = self.N
+        p.cell[:] = [float(c) for c in cell]
+        p.pbc[:] = (0, 0, 0)
+
+        def keep(t):
+            self._keep.append(t)
+            return t.data_ptr()
+
+        if regions is not None:
+            p.regions = keep(_dev(np.asarray(regions, np.uint8).reshape(self.shape), torch.uint8))
+        if geom is not None:
+            p.vol = keep(_dev(np.asarray(geom, np.float32).reshape(self.shape)))
+
+        def param(v):
+            if np.isscalar(v):
+                return None, float(np.float32(v))
+            return keep(_dev(np.asarray(v, np.float32).reshape(self.shape))), 1.0
+
+        p.Ms, p.Ms_mul = param(Msat)
+        p.alpha, p.alpha_mul = param(alpha)
+        p.Ku1, p.Ku1_mul = param(Ku1)
+        p.Ku2, p.Ku2_mul = param(Ku2)
+        u = np.asarray(anisU, np.float64)
+        for c in range(3):
+            if u.ndim == 1:
+                p.anisU[c], p.anisU_mul[c] = None, float(np.float32(u[c]))
+            else:
+                p.anisU[c], p.anisU_mul[c] = param(u[c])
+        self.aLUT = _dev(exchange_lut(Aex))
+        p.aLUT = keep(self.aLUT)
+        if np.any(np.asarray(Dind) != 0):
+            self.dLUT = _dev(exchange_lut(Dind))
+            p.dLUT = keep(self.dLUT)
+        if B_ext is not None:
+            b = np.asarray(B_ext, np.float32)
+            lut = np.tile(b, (NREGION, 1)) if b.ndim == 1 else b
+            self.bext = _dev(np.ascontiguousarray(lut.T))
+            keep(self.bext)
+            for c in range(3):
+                p.bextLUT[c] = self.bext[c].data_ptr()
+        p.enable_demag = int(bool(demag))
+        p.openbc = int(bool(open_bc))
+        p.precess = int(bool(precess))
+        p.asymptotic_radius = int(asymptotic_radius)
+        sp = SolverParams()
+        self.L.umag_solver_defaults(ctypes.byref(sp))
+        sp.solver = int(solver)
+        sp.dt, sp.max_err, sp.rel_err, sp.min_dt, sp.max_dt = dt, MaxErr, RelErr, MinDt, MaxDt
+        sp.fix_dt, sp.headroom, sp.gamma_ll = FixDt, Headroom, GAMMA_LL
+        self.params, self.solver = p, sp
+        h = ctypes.c_void_p()
+        torch.cuda.synchronize()
+        check(self.L.umag_sim_new(ctypes.byref(p), ctypes.byref(sp), ctypes.byref(h)))
+        self._h = h.value
+
+    # ---------------------------------------------------------------- state
+    def set_m(self, m):
+        """m = array (3, Nz, Ny, Nx); normalised on the device (engine/magnetization.go:55)."""
+        t = _dev(np.asarray(m, np.float32).reshape((3,) + self.shape)) if not torch.is_tensor(m) else m.contiguous()
+        torch.cuda.synchronize()
+        check(self.L.umag_sim_set_m(self._h, t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr()))
+        check(self.L.umag_sync())
+
+    def m_ptrs(self):
+        ptrs = (ctypes.c_void_p * 3)()
+        check(self.L.umag_sim_m_ptrs(self._h, ptrs))
+        return [ptrs[i] for i in range(3)]
+
+    def get_m(self, out=None):
+        """Copy of the current m as a (3, Nz, Ny, Nx) CUDA tensor."""
+        if out is None:
+            out = torch.empty((3,) + self.shape, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        check(self.L.umag_sim_get_m(self._h, out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr()))
+        return out
+
+    def torque(self, beff=False):
+        """engine/torque.go:124 SetTorque of the current m (and B_eff if asked)."""
+        t = torch.empty((3,) + self.shape, dtype=torch.float32, device="cuda")
+        b = torch.empty_like(t) if beff else None
+        torch.cuda.synchronize()
+        bp = (b[0].data_ptr(), b[1].data_ptr(), b[2].data_ptr()) if beff else (None, None, None)
+        check(self.L.umag_sim_torque(self._h, t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), *bp))
+        return (t, b) if beff else t
+
+    # ---------------------------------------------------------------- stepping
+    def steps(self, n):
+        """engine/run.go:197 Steps(n) without host synchronisation."""
+        check(self.L.umag_sim_steps(self._h, int(n)))
+
+    def run(self, seconds, chunk=64, max_steps=10 ** 12):
+        """engine/run.go:190 Run(seconds)."""
+        check(self.L.umag_sim_run(self._h, float(seconds), int(chunk), int(max_steps)))
+
+    def sync(self):
+        check(self.L.umag_sync())
+
+    def state(self):
+        st = SolverState()
+        check(self.L.umag_sim_get_state(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in SolverState._fields_}
+
+    def set_time(self, t, dt=0.0):
+        check(self.L.umag_sim_set_time(self._h, float(t), float(dt)))
+
+    def average_m(self):
+        """engine/average.go:29 (compensated sums)."""
+        out = (ctypes.c_double * 3)()
+        check(self.L.umag_sim_average_m(self._h, out))
+        return [out[0], out[1], out[2]]
+
+    def use_graph(self, enable=True, steps_per_graph=16):
+        check(self.L.umag_sim_use_graph(self._h, int(bool(enable)), int(steps_per_graph)))
+
+    def torque_evals(self, n):
+        """Enqueue n field + torque evaluations of the current m (timing aid)."""
+        check(self.L.umag_sim_torque_evals(self._h, int(n)))
+
+    def set_stream(self, stream):
+        """Queue all library work on a torch.cuda.Stream (None = library stream)."""
+        check(self.L.umag_set_stream(None if stream is None else stream.cuda_stream))
+
+    def launches_per_step(self):
+        n = ctypes.c_int()
+        check(self.L.umag_sim_launches_per_step(self._h, ctypes.byref(n)))
+        return n.value
+
+    def free(self):
+        if getattr(self, "_h", None):
+            self.L.umag_sim_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libumagnus_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["ops.cu", "demag.cu", "engine.cu", "capi.cu"]
+SOURCES = ["ops.cu", "demag.cu", "demag_fast.cu", "engine.cu", "capi.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -26,7 +26,7 @@ def build(verbose=False, force=False, ptxas_info=False):
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(os.path.dirname(HERE), "include", "umagnus_b200.h"))
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
@@ -37,7 +37,12 @@ def build(verbose=False, force=False, ptxas_info=False):
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    # translation units compile in parallel
+    procs = [subprocess.Popen(c) for c in cmds]
+    codes = [p.wait() for p in procs]
+    if any(codes):
+        raise subprocess.CalledProcessError(max(codes), "nvcc")
     if force or _needs(OUT, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"]
         if verbose:

@@ -157,6 +157,82 @@ __device__ __forceinline__ f3 dmi_sum(const float* __restrict__ mx, const float*
     return h;
 }
 
+// Per region-pair DMI coefficients, precomputed on the device with the same
+// operations dmi_sum performs per neighbour (so results are bit-identical):
+// s[d] = 2A/c_d^2, dc[d] = D/c_d, q[d] = c_d * (0.5 D / A).
+struct DmiPairLut {
+    const float *sx, *sy, *sz, *dcx, *dcy, *qx, *qy;
+};
+
+__device__ __forceinline__ f3 dmi_sum_lut(const float* __restrict__ mx, const float* __restrict__ my,
+                                          const float* __restrict__ mz, const DmiPairLut& L,
+                                          const uint8_t* __restrict__ regions, Mesh3 g, bool openbc, int ix,
+                                          int iy, int iz, f3 m0, int r0) {
+    f3 h{0.f, 0.f, 0.f};
+#pragma unroll
+    for (int d = 0; d < 2; d++) {
+#pragma unroll
+        for (int side = -1; side <= 1; side += 2) {
+            f3 mn{0.f, 0.f, 0.f};
+            int i_;
+            bool inside;
+            if (d == 0) {
+                int xx = side < 0 ? lclamp(ix - 1, g.Nx, g.pbc & 1) : hclamp(ix + 1, g.Nx, g.pbc & 1);
+                i_ = (iz * g.Ny + iy) * g.Nx + xx;
+                inside = (side < 0 ? ix - 1 >= 0 : ix + 1 < g.Nx) || (g.pbc & 1);
+            } else {
+                int yy = side < 0 ? lclamp(iy - 1, g.Ny, g.pbc & 2) : hclamp(iy + 1, g.Ny, g.pbc & 2);
+                i_ = (iz * g.Ny + yy) * g.Nx + ix;
+                inside = (side < 0 ? iy - 1 >= 0 : iy + 1 < g.Ny) || (g.pbc & 2);
+            }
+            if (inside) mn = ld3(mx, my, mz, i_);
+            bool missing = is0(mn);
+            int rn = missing ? r0 : __ldg(regions + i_);
+            int si = symidx(r0, rn);
+            if (!missing || !openbc) {
+                if (missing) {
+                    float q = __ldg((d == 0 ? L.qx : L.qy) + si);
+                    if (side < 0) q = -q;
+                    if (d == 0) {
+                        mn.x = fs(m0.x, fm(q, m0.z));
+                        mn.y = m0.y;
+                        mn.z = fa(m0.z, fm(q, m0.x));
+                    } else {
+                        mn.x = m0.x;
+                        mn.y = fs(m0.y, fm(q, m0.z));
+                        mn.z = fa(m0.z, fm(q, m0.y));
+                    }
+                }
+                float s = __ldg((d == 0 ? L.sx : L.sy) + si);
+                h.x = fa(h.x, fm(s, fs(mn.x, m0.x)));
+                h.y = fa(h.y, fm(s, fs(mn.y, m0.y)));
+                h.z = fa(h.z, fm(s, fs(mn.z, m0.z)));
+                float Dc = __ldg((d == 0 ? L.dcx : L.dcy) + si);
+                float tz = side < 0 ? -mn.z : mn.z;
+                float tp = d == 0 ? mn.x : mn.y;
+                tp = side < 0 ? -tp : tp;
+                if (d == 0) h.x = fa(h.x, fm(Dc, tz));
+                else h.y = fa(h.y, fm(Dc, tz));
+                h.z = fs(h.z, fm(Dc, tp));
+            }
+        }
+    }
+    if (g.Nz != 1) {
+#pragma unroll
+        for (int side = -1; side <= 1; side += 2) {
+            int zz = side < 0 ? lclamp(iz - 1, g.Nz, g.pbc & 4) : hclamp(iz + 1, g.Nz, g.pbc & 4);
+            int i_ = (zz * g.Ny + iy) * g.Nx + ix;
+            f3 mn = ld3(mx, my, mz, i_);
+            if (is0(mn)) mn = m0;
+            float s = __ldg(L.sz + symidx(r0, __ldg(regions + i_)));
+            h.x = fa(h.x, fm(s, fs(mn.x, m0.x)));
+            h.y = fa(h.y, fm(s, fs(mn.y, m0.y)));
+            h.z = fa(h.z, fm(s, fs(mn.z, m0.z)));
+        }
+    }
+    return h;
+}
+
 struct UniaxParams {
     const float *Ms, *K1, *K2, *ux, *uy, *uz;
     float Ms_mul, K1_mul, K2_mul, ux_mul, uy_mul, uz_mul;

@@ -135,7 +135,7 @@ __global__ void k_fft_axis(typename Cplx<T>::t* data, FftLine<T> f, int Px, int 
         // s[t*L + j]
         for (int e = threadIdx.x; e < gcount * L; e += blockDim.x) s[e] = data[base + e];
         __syncthreads();
-        int cap = blockDim.x * fft_line_cap(f) / L;
+        int cap = fft_lines_per_batch(f, gcount);
         for (int t0 = 0; t0 < gcount; t0 += cap) {
             int nt = gcount - t0 < cap ? gcount - t0 : cap;
             smem_fft<T>(s + t0 * L, nt, L, 1, f, dir, false);
@@ -158,7 +158,7 @@ __global__ void k_fft_axis(typename Cplx<T>::t* data, FftLine<T> f, int Px, int 
         s[e] = v;
     }
     __syncthreads();
-    int cap = blockDim.x * fft_line_cap(f) / L;
+    int cap = fft_lines_per_batch(f, G);
     for (int t0 = 0; t0 < G; t0 += cap) {
         int nt = G - t0 < cap ? G - t0 : cap;
         smem_fft<T>(s + t0, nt, 1, G, f, dir, true);
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kPassThreads) k_pass_a(PassArgs a) {
     __syncthreads();
     // 2. complex FFT of length M on every row
     {
-        int cap = blockDim.x * fft_line_cap(a.fx) / (M > 0 ? M : 1);
+        int cap = fft_lines_per_batch(a.fx, a.Nz);
         for (int t0 = 0; t0 < a.Nz; t0 += cap) {
             int nt = a.Nz - t0 < cap ? a.Nz - t0 : cap;
             smem_fft<float>(X1 + t0 * a.HxP, nt, a.HxP, 1, a.fx, -1, false);
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(kPassThreads) k_pass_c(PassArgs a) {
     __syncthreads();
     // 3. inverse complex FFT of every row
     {
-        int cap = blockDim.x * fft_line_cap(a.fx) / (M > 0 ? M : 1);
+        int cap = fft_lines_per_batch(a.fx, a.Nz);
         for (int t0 = 0; t0 < a.Nz; t0 += cap) {
             int nt = a.Nz - t0 < cap ? a.Nz - t0 : cap;
             smem_fft<float>(X1 + t0 * a.HxP, nt, a.HxP, 1, a.fx, +1, false);
@@ -429,6 +429,10 @@ static int plan_common(umag_demag* d) {
     UMAG_TRY(make_line<float>(d->M, d->fx, &tw)); d->tw_dev.push_back(tw);
     UMAG_TRY(make_line<float>(d->P[1], d->fy, &tw)); d->tw_dev.push_back(tw);
     UMAG_TRY(make_line<float>(d->P[2], d->fz, &tw)); d->tw_dev.push_back(tw);
+    if (!fft_line_fits(d->fx, kPassThreads))
+        return set_error(UMAG_E_UNSUPPORTED, "Nx = %d too large for the x pass", d->N[0]);
+    if (d->P[2] > 1 && (long)kChunkW * d->P[2] > (long)kPassThreads * fft_line_cap(d->fz))
+        return set_error(UMAG_E_UNSUPPORTED, "Nz = %d too large for the z transform", d->N[2]);
     auto twr = twiddles<float2>(d->P[0], d->M / 2 + 1);
     UMAG_CUDA(cudaMalloc(&d->twr, sizeof(float2) * twr.size()));
     UMAG_CUDA(cudaMemcpy(d->twr, twr.data(), sizeof(float2) * twr.size(), cudaMemcpyHostToDevice));
@@ -442,9 +446,15 @@ static int plan_common(umag_demag* d) {
         if (d->is2d && (c == 3 || c == 4)) continue;  // yz, xz vanish in 2D (newellDemagKernel.go:1314-1317)
         UMAG_CUDA(cudaMalloc(&d->K[c], sizeof(float) * kn));
     }
-    UMAG_CUDA(cudaFuncSetAttribute(k_pass_a, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_ac_smem(d)));
-    UMAG_CUDA(cudaFuncSetAttribute(k_pass_c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_ac_smem(d)));
-    UMAG_CUDA(cudaFuncSetAttribute(k_pass_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_b_smem(d)));
+    // the opt-in limit is per kernel and process-wide: set it to the maximum
+    // so plans of different sizes can coexist
+    const int maxsm = 227 * 1024;
+    UMAG_CUDA(cudaFuncSetAttribute(k_pass_a, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+    UMAG_CUDA(cudaFuncSetAttribute(k_pass_c, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+    UMAG_CUDA(cudaFuncSetAttribute(k_pass_b, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+    UMAG_CUDA(cudaFuncSetAttribute(k_fft_axis<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+    UMAG_TRY(demag_fast_setup());
+    d->use_fast = getenv("UMAG_GENERIC_FFT") == nullptr && demag_fast_select(d->M, d->P[1], d->P[2], d->fast);
     return UMAG_OK;
 }
 
@@ -457,7 +467,11 @@ static int kernel_to_spectrum(umag_demag* d, double* const Kr[6], cudaStream_t s
     FftLine<double> fl[3];
     double2* tws[3] = {nullptr, nullptr, nullptr};
     int st_ok = UMAG_OK;
-    for (int ax = 0; ax < 3 && st_ok == UMAG_OK; ax++) st_ok = make_line<double>(d->P[ax], fl[ax], &tws[ax]);
+    for (int ax = 0; ax < 3 && st_ok == UMAG_OK; ax++) {
+        st_ok = make_line<double>(d->P[ax], fl[ax], &tws[ax]);
+        if (st_ok == UMAG_OK && !fft_line_fits(fl[ax], 256))
+            st_ok = set_error(UMAG_E_UNSUPPORTED, "kernel FFT line %d too long", d->P[ax]);
+    }
     unsigned long long* dmax = nullptr;
     if (st_ok == UMAG_OK) st_ok = cudaMalloc(&dmax, sizeof(unsigned long long)) == cudaSuccess ? UMAG_OK : UMAG_E_CUDA;
     const int threads = 256;
@@ -471,7 +485,6 @@ static int kernel_to_spectrum(umag_demag* d, double* const Kr[6], cudaStream_t s
             while (ax == 0 && (G * 2) * L * 16 <= 64 * 1024 && G < 8) G *= 2;
             size_t sm = sizeof(double2) * (size_t)G * L;
             if (sm > 200 * 1024) { st_ok = set_error(UMAG_E_UNSUPPORTED, "kernel FFT line %d too long", L); break; }
-            cudaFuncSetAttribute(k_fft_axis<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             long blocks;
             if (ax == 0) blocks = ((long)Py * Pz + G - 1) / G;
             else blocks = (long)((Px + G - 1) / G) * (ax == 1 ? Pz : Py);
@@ -624,6 +637,16 @@ void fill_pass_args(const umag_demag* d, PassArgs& a) {
 }
 
 int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st) {
+    if (d->use_fast) {
+        const FastPasses& f = d->fast;
+        f.a<<<dim3(d->N[1], 3), 256, f.smem_ac, st>>>(a);
+        UMAG_LAUNCH_CHECK();
+        f.b<<<dim3((d->Hx + f.wb - 1) / f.wb, d->P[2]), 512, f.smem_b, st>>>(a);
+        UMAG_LAUNCH_CHECK();
+        f.c<<<dim3(d->N[1], 3), 256, f.smem_ac, st>>>(a);
+        UMAG_LAUNCH_CHECK();
+        return UMAG_OK;
+    }
     size_t sac = pass_ac_smem(d), sb = pass_b_smem(d);
     k_pass_a<<<dim3(d->N[1], 3), kPassThreads, sac, st>>>(a);
     UMAG_LAUNCH_CHECK();

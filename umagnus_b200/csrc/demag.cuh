@@ -9,7 +9,21 @@ constexpr int kPassThreads = 256;   // passes A and C
 constexpr int kPassBThreads = 512;  // pass B
 constexpr int kChunkW = 32;         // kx columns per z-transform block in passes A/C
 
+namespace umag {
+struct PassArgs;
+// compile-time-planned pass kernels for one mesh size (demag_fast.cu)
+struct FastPasses {
+    void (*a)(PassArgs) = nullptr;
+    void (*b)(PassArgs) = nullptr;
+    void (*c)(PassArgs) = nullptr;
+    size_t smem_ac = 0, smem_b = 0;
+    int wb = 0;
+};
+}  // namespace umag
+
 struct umag_demag {
+    umag::FastPasses fast;
+    bool use_fast = false;
     int N[3], P[3];
     double cell[3];
     int arad, zero_self;
@@ -56,5 +70,7 @@ int demag_get_spectrum(umag_demag* d, float* const host[6]);
 void demag_free(umag_demag* d);
 void fill_pass_args(const umag_demag* d, PassArgs& a);
 int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st);
+bool demag_fast_select(int M, int Py, int Pz, FastPasses& f);
+int demag_fast_setup();
 
 }  // namespace umag

@@ -1,0 +1,318 @@
+// demag_fast.cu -- the demag passes with compile-time FFT plans.
+//
+// Same three passes and data layout as demag.cu (see its header comment),
+// instantiated for the mesh sizes the benchmarks and common simulations use:
+// every FFT index computation is a constant, register arrays are unrolled,
+// twiddles are staged in shared memory.  demag_fast_select() returns the
+// instantiation for a plan, or nothing (the generic kernels then run).
+#include "demag.cuh"
+#include "fft_static.cuh"
+
+namespace umag {
+
+static constexpr double kMu0f = 4 * 3.1415926535897932384626433 * 1e-7;  // clh/constants.clh:5
+
+constexpr int nz_of_pz(int PZ) { return PZ == 1 ? 1 : (PZ % 2 == 0 ? PZ / 2 : (PZ + 1) / 2); }
+constexpr int kNT = 256;       // passes A, C
+constexpr int kNTB = 512;      // pass B
+constexpr int kElemCap = 24;   // complex elements per thread per FFT batch
+
+template <int M, int PZ> struct AcShape {
+    static constexpr int NZ = nz_of_pz(PZ);
+    static constexpr int XP = M + 1;                                  // row pitch (holds X[0..M])
+    static constexpr int ZB = sp_divisor_le(NZ, (kElemCap * kNT) / M);  // rows per x-FFT batch
+    static constexpr int CW = PZ == 1 ? 1 : sp_divisor_le(M, (kElemCap * kNT) / PZ < 64 ? (kElemCap * kNT) / PZ : 64);
+    static constexpr size_t smem = sizeof(float2) * ((size_t)M + PZ + (M / 2 + 1) + (size_t)NZ * XP +
+                                                     (PZ > 1 ? (size_t)PZ * CW : 0));
+};
+
+// copypadmul2.cl:13-20: MU0*Ms (FP64 product rounded to float32) * vol * m
+__device__ __forceinline__ float scaled_m(const PassArgs& a, const float* __restrict__ m, int i) {
+    float fac = a.Ms == nullptr ? a.Ms_mul : __fmul_rn(a.Ms_mul, __ldg(a.Ms + i));
+    float bsat = (float)(kMu0f * (double)fac);
+    float w = a.vol == nullptr ? 1.0f : __fmul_rn(1.0f, __ldg(a.vol + i));
+    return __fmul_rn(__fmul_rn(bsat, w), __ldg(m + i));
+}
+
+template <int M, int PZ>
+__global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) {
+    using S = AcShape<M, PZ>;
+    constexpr int NZ = S::NZ, XP = S::XP, CW = S::CW, H = M / 2;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* twx = sm;
+    float2* twz = twx + M;
+    float2* twr = twz + PZ;
+    float2* X1 = twr + (H + 1);
+    float2* Z2 = X1 + NZ * XP;
+    if (a.active && !*a.active) return;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < M; i += kNT) twx[i] = a.fx.tw[i];
+    if (PZ > 1)
+        for (int i = tid; i < PZ; i += kNT) twz[i] = a.fz.tw[i];
+    for (int i = tid; i <= H; i += kNT) twr[i] = a.twr[i];
+    const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
+    const float* __restrict__ m = a.m_ind ? (a.m_sel ? *a.m_ind_w : *a.m_ind) + (long)c * a.ncell : a.m[c];
+    // 1. scaled m, pairs of reals packed into complex (x = 2n, 2n+1), Nx = M
+    for (int e = tid; e < NZ * M; e += kNT) {
+        const int z = e / M, n = e % M;
+        float2 v = make_float2(0.f, 0.f);  // x >= Nx is zero padding
+        if (n < H) {
+            const int i = (z * Ny + y) * M + 2 * n;
+            v = make_float2(scaled_m(a, m, i), scaled_m(a, m, i + 1));
+        }
+        X1[z * XP + n] = v;
+    }
+    __syncthreads();
+    // 2. length-M complex FFT of every row
+#pragma unroll 1
+    for (int rb = 0; rb < NZ; rb += S::ZB) sfft<float2, M, S::ZB, kNT, XP, 1, false, -1>(X1 + rb * XP, twx);
+    // 3. R2C unpack: X[k] = E + W^k O, X[M-k] = conj(E - W^k O)
+    for (int e = tid; e < NZ * (H + 1); e += kNT) {
+        const int z = e / (H + 1), k = e % (H + 1);
+        float2* row = X1 + z * XP;
+        const int k2 = M - k;
+        float2 A = row[k], B = row[k == 0 ? 0 : k2];
+        float2 E = make_float2(0.5f * (A.x + B.x), 0.5f * (A.y - B.y));
+        float2 D = make_float2(0.5f * (A.x - B.x), 0.5f * (A.y + B.y));
+        float2 O = make_float2(D.y, -D.x);
+        float2 W = twr[k];
+        float2 WO = make_float2(W.x * O.x - W.y * O.y, W.x * O.y + W.y * O.x);
+        row[k] = make_float2(E.x + WO.x, E.y + WO.y);
+        row[k2] = make_float2(E.x - WO.x, WO.y - E.y);
+    }
+    __syncthreads();
+    float2* out = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
+    const long kzs = (long)Ny * a.Lx;
+    if constexpr (PZ == 1) {
+        for (int k = tid; k <= M; k += kNT) out[k] = X1[k];
+    } else {
+        // 4. forward z FFT per block of CW columns, then the Nyquist column kx = M
+#pragma unroll 1
+        for (int kx0 = 0; kx0 < M; kx0 += CW) {
+            for (int e = tid; e < PZ * CW; e += kNT) {
+                const int z = e / CW, w = e % CW;
+                Z2[e] = z < NZ ? X1[z * XP + kx0 + w] : make_float2(0.f, 0.f);
+            }
+            __syncthreads();
+            sfft<float2, PZ, CW, kNT, 1, CW, true, -1>(Z2, twz);
+            for (int e = tid; e < PZ * CW; e += kNT) {
+                const int kz = e / CW, w = e % CW;
+                out[kz * kzs + kx0 + w] = Z2[e];
+            }
+            __syncthreads();
+        }
+        for (int z = tid; z < PZ; z += kNT) Z2[z] = z < NZ ? X1[z * XP + M] : make_float2(0.f, 0.f);
+        __syncthreads();
+        sfft<float2, PZ, 1, kNT, 1, 1, true, -1>(Z2, twz);
+        for (int kz = tid; kz < PZ; kz += kNT) out[kz * kzs + M] = Z2[kz];
+    }
+}
+
+template <int M, int PZ>
+__global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) {
+    using S = AcShape<M, PZ>;
+    constexpr int NZ = S::NZ, XP = S::XP, CW = S::CW, H = M / 2;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* twx = sm;
+    float2* twz = twx + M;
+    float2* twr = twz + PZ;
+    float2* X1 = twr + (H + 1);
+    float2* Z2 = X1 + NZ * XP;
+    if (a.active && !*a.active) return;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < M; i += kNT) twx[i] = a.fx.tw[i];
+    if (PZ > 1)
+        for (int i = tid; i < PZ; i += kNT) twz[i] = a.fz.tw[i];
+    for (int i = tid; i <= H; i += kNT) twr[i] = a.twr[i];
+    const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
+    const float2* in = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
+    const long kzs = (long)Ny * a.Lx;
+    // 1. inverse z FFT per block of columns, keep z < NZ
+    if constexpr (PZ == 1) {
+        for (int k = tid; k <= M; k += kNT) X1[k] = in[k];
+    } else {
+#pragma unroll 1
+        for (int kx0 = 0; kx0 < M; kx0 += CW) {
+            for (int e = tid; e < PZ * CW; e += kNT) {
+                const int kz = e / CW, w = e % CW;
+                Z2[e] = in[kz * kzs + kx0 + w];
+            }
+            __syncthreads();
+            sfft<float2, PZ, CW, kNT, 1, CW, true, +1>(Z2, twz);
+            for (int e = tid; e < NZ * CW; e += kNT) {
+                const int z = e / CW, w = e % CW;
+                X1[z * XP + kx0 + w] = Z2[e];
+            }
+            __syncthreads();
+        }
+        for (int kz = tid; kz < PZ; kz += kNT) Z2[kz] = in[kz * kzs + M];
+        __syncthreads();
+        sfft<float2, PZ, 1, kNT, 1, 1, true, +1>(Z2, twz);
+        for (int z = tid; z < NZ; z += kNT) X1[z * XP + M] = Z2[z];
+    }
+    __syncthreads();
+    // 2. C2R pack: Z[k] = (X[k] + conj X[M-k]) + i conj(W^k) (X[k] - conj X[M-k])
+    for (int e = tid; e < NZ * (H + 1); e += kNT) {
+        const int z = e / (H + 1), k = e % (H + 1);
+        float2* row = X1 + z * XP;
+        const int k2 = M - k;
+        float2 Xk = row[k], Xm = row[k2];
+        if (k == 0) { Xk.y = 0.f; Xm.y = 0.f; }
+        float2 W = twr[k];
+        float2 S1 = make_float2(Xk.x + Xm.x, Xk.y - Xm.y);
+        float2 D1 = make_float2(Xk.x - Xm.x, Xk.y + Xm.y);
+        float2 T1 = make_float2(W.x * D1.x + W.y * D1.y, W.x * D1.y - W.y * D1.x);  // conj(W) * D1
+        float2 Zk = make_float2(S1.x - T1.y, S1.y + T1.x);
+        if (k == 0) {
+            row[0] = Zk;
+        } else {
+            float2 S2 = make_float2(Xm.x + Xk.x, Xm.y - Xk.y);
+            float2 D2 = make_float2(Xm.x - Xk.x, Xm.y + Xk.y);
+            float2 T2 = make_float2(-(W.x * D2.x - W.y * D2.y), -(W.x * D2.y + W.y * D2.x));  // -W * D2
+            row[k] = Zk;
+            row[k2] = make_float2(S2.x - T2.y, S2.y + T2.x);
+        }
+    }
+    __syncthreads();
+    // 3. inverse length-M FFT of every row
+#pragma unroll 1
+    for (int rb = 0; rb < NZ; rb += S::ZB) sfft<float2, M, S::ZB, kNT, XP, 1, false, +1>(X1 + rb * XP, twx);
+    // 4. unpack even/odd samples, crop and overwrite B (copyunpad.cl)
+    float* __restrict__ B = a.B[c];
+    for (int e = tid; e < NZ * H; e += kNT) {
+        const int z = e / H, n = e % H;
+        float2 v = X1[z * XP + n];
+        *reinterpret_cast<float2*>(B + (z * Ny + y) * M + 2 * n) = v;
+    }
+}
+
+template <int PY> struct BShape {
+    static constexpr int WB0 = (kElemCap * kNTB) / (3 * PY);
+    static constexpr int WB = WB0 >= 32 ? 32 : WB0 >= 16 ? 16 : WB0 >= 8 ? 8 : WB0 >= 4 ? 4 : WB0 >= 2 ? 2 : 1;
+    static constexpr size_t smem = sizeof(float2) * ((size_t)PY + (size_t)PY * 3 * WB);
+};
+
+template <int PY>
+__global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) {
+    constexpr int WB = BShape<PY>::WB, W3 = 3 * WB, NY = PY / 2, HY = PY / 2 + 1;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* twy = sm;
+    float2* S = twy + PY;  // [PY][3*WB]
+    if (a.active && !*a.active) return;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < PY; i += kNTB) twy[i] = a.fy.tw[i];
+    const int kx0 = blockIdx.x * WB, kz = blockIdx.y;
+    const int hx = a.Hx, Pz = a.Pz;
+    const long cs = (long)Pz * NY * a.Lx;
+    const float2* in = a.spec + (long)kz * NY * a.Lx + kx0;
+    for (int e = tid; e < PY * W3; e += kNTB) {
+        const int yy = e / W3, r = e % W3, c = r / WB, w = r % WB;
+        float2 v = make_float2(0.f, 0.f);
+        if (yy < NY && kx0 + w < hx) v = in[c * cs + (long)yy * a.Lx + w];
+        S[e] = v;
+    }
+    __syncthreads();
+    sfft<float2, PY, W3, kNTB, 1, W3, true, -1>(S, twy);
+    // kernel multiply with the mirror symmetry of kernmulrsymm3d.cl:62-82
+    int kzm = kz;
+    float sz = 1.f;
+    if (kz > Pz / 2) { kzm = Pz - kz; sz = -1.f; }
+    const bool k3d = a.K[3] != nullptr;
+    for (int e = tid; e < PY * WB; e += kNTB) {
+        const int ky = e / WB, w = e % WB;
+        const int kx = kx0 + w;
+        if (kx >= hx) continue;
+        int kym = ky;
+        float sy = 1.f;
+        if (ky > NY) { kym = PY - ky; sy = -1.f; }
+        const long I = ((long)kzm * HY + kym) * hx + kx;
+        const float Kxx = __ldg(a.K[0] + I), Kyy = __ldg(a.K[1] + I), Kzz = __ldg(a.K[2] + I);
+        const float Kxy = __ldg(a.K[5] + I) * sy;
+        float Kyz = 0.f, Kxz = 0.f;
+        if (k3d) {
+            Kyz = __ldg(a.K[3] + I) * (sy * sz);
+            Kxz = __ldg(a.K[4] + I) * sz;
+        }
+        float2* row = S + ky * W3;
+        const float2 mx = row[w], my = row[WB + w], mz = row[2 * WB + w];
+        row[w] = make_float2(mx.x * Kxx + my.x * Kxy + mz.x * Kxz, mx.y * Kxx + my.y * Kxy + mz.y * Kxz);
+        row[WB + w] = make_float2(mx.x * Kxy + my.x * Kyy + mz.x * Kyz, mx.y * Kxy + my.y * Kyy + mz.y * Kyz);
+        row[2 * WB + w] = make_float2(mx.x * Kxz + my.x * Kyz + mz.x * Kzz, mx.y * Kxz + my.y * Kyz + mz.y * Kzz);
+    }
+    __syncthreads();
+    sfft<float2, PY, W3, kNTB, 1, W3, true, +1>(S, twy);
+    float2* outp = a.spec + (long)kz * NY * a.Lx + kx0;
+    for (int e = tid; e < NY * W3; e += kNTB) {
+        const int yy = e / W3, r = e % W3, c = r / WB, w = r % WB;
+        if (kx0 + w < hx) outp[c * cs + (long)yy * a.Lx + w] = S[e];
+    }
+}
+
+// ------------------------------------------------------------------ dispatch
+template <int M, int PZ> static void fill_ac(FastPasses& f) {
+    f.a = k_fast_a<M, PZ>;
+    f.c = k_fast_c<M, PZ>;
+    f.smem_ac = AcShape<M, PZ>::smem;
+}
+template <int PY> static void fill_b(FastPasses& f) {
+    f.b = k_fast_b<PY>;
+    f.smem_b = BShape<PY>::smem;
+    f.wb = BShape<PY>::WB;
+}
+
+bool demag_fast_select(int M, int Py, int Pz, FastPasses& f) {
+    f = FastPasses{};
+    bool ac = true;
+#define AC(m, pz) else if (M == m && Pz == pz) fill_ac<m, pz>(f);
+    if (false) {}
+    AC(16, 1) AC(24, 1) AC(32, 1) AC(48, 1) AC(64, 1) AC(96, 1) AC(128, 1) AC(192, 1) AC(256, 1) AC(384, 1)
+    AC(512, 1) AC(1024, 1)
+    AC(64, 12) AC(64, 16) AC(64, 32) AC(64, 64)
+    AC(128, 12) AC(128, 16) AC(128, 32) AC(128, 64)
+    AC(256, 12) AC(256, 16) AC(256, 32) AC(256, 64)
+    AC(512, 12) AC(512, 16) AC(512, 32) AC(512, 64)
+    else ac = false;
+#undef AC
+    bool b = true;
+#define BB(py) else if (Py == py) fill_b<py>(f);
+    if (false) {}
+    BB(32) BB(48) BB(64) BB(96) BB(128) BB(192) BB(256) BB(384) BB(512) BB(1024) BB(2048)
+    else b = false;
+#undef BB
+    if (!(ac && b)) f = FastPasses{};
+    return ac && b;
+}
+
+int demag_fast_setup() {
+    static bool done = false;
+    if (done) return UMAG_OK;
+    const int maxsm = 227 * 1024;
+    FastPasses f;
+    const int Ms[] = {16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 1024};
+    for (int m : Ms) {
+        if (demag_fast_select(m, 2 * m > 2048 ? 2048 : 2 * m, 1, f)) {
+            UMAG_CUDA(cudaFuncSetAttribute(f.a, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+            UMAG_CUDA(cudaFuncSetAttribute(f.c, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+        }
+    }
+    const int m3[] = {64, 128, 256, 512}, pz3[] = {12, 16, 32, 64};
+    for (int m : m3)
+        for (int pz : pz3)
+            if (demag_fast_select(m, 2 * m, pz, f)) {
+                UMAG_CUDA(cudaFuncSetAttribute(f.a, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+                UMAG_CUDA(cudaFuncSetAttribute(f.c, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+            }
+    // pass B instantiations
+    {
+        FastPasses g{};
+#define SETB(py)                                                                                     \
+    fill_b<py>(g);                                                                                   \
+    UMAG_CUDA(cudaFuncSetAttribute(g.b, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+        SETB(32) SETB(48) SETB(64) SETB(96) SETB(128) SETB(192) SETB(256) SETB(384) SETB(512) SETB(1024) SETB(2048)
+#undef SETB
+    }
+    done = true;
+    return UMAG_OK;
+}
+
+}  // namespace umag

@@ -39,6 +39,17 @@ struct DevCtl {
     double max_err, rel_err, min_dt, max_dt, fix_dt, headroom, min_slope, gamma;
 };
 
+// Uniform parameters evaluated once on the device with the operations the
+// per-cell path uses (bit-identical), so the per-cell kernel does no
+// divisions or square roots for them.
+struct LocalConsts {
+    float inv_ms;  // inv_msat of a uniform Ms (amul.clh:19-26)
+    float gilb;    // -1/(1+alpha^2) of a uniform alpha (lltorque2.cl:18)
+    float u[3];    // normalised uniform easy axis (uniaxialanisotropy2.cl:19)
+    float f1k;     // 2*(K1/Ms) for uniform K1 and Ms
+    float f2k;     // 4*(K2/Ms) for uniform K2 and Ms
+};
+
 struct LocalArgs {
     Mesh3 g;
     int N;
@@ -53,6 +64,9 @@ struct LocalArgs {
     const uint8_t* regions;
     float wx, wy, wz, cx, cy, cz;
     int dmi, openbc, anis, zeeman, precess;
+    int ms_uniform, alpha_uniform, anis_uniform;
+    DmiPairLut dl;
+    LocalConsts kc;
     UniaxParams up;
     const float* bext[3];
     const float* alpha;
@@ -60,6 +74,43 @@ struct LocalArgs {
     const float* Ms;
     float Ms_mul;
 };
+
+__global__ void k_local_consts(LocalArgs a, LocalConsts* out) {
+    LocalConsts c{};
+    c.inv_ms = a.Ms_mul == 0.0f ? 0.0f : fd(1.0f, a.Ms_mul);
+    c.gilb = fd(-1.0f, fa(1.0f, fm(a.alpha_mul, a.alpha_mul)));
+    f3 u{a.up.ux_mul, a.up.uy_mul, a.up.uz_mul};
+    float len = __fsqrt_rn(dot3(u, u));
+    float il = (len != 0.0f) ? fd(1.0f, len) : 0.0f;
+    c.u[0] = fm(il, u.x); c.u[1] = fm(il, u.y); c.u[2] = fm(il, u.z);
+    c.f1k = fm(2.0f, fm(a.up.K1_mul, c.inv_ms));
+    c.f2k = fm(4.0f, fm(a.up.K2_mul, c.inv_ms));
+    *out = c;
+}
+
+// DMI coefficients per region pair (see DmiPairLut)
+__global__ void k_dmi_pairs(const float* __restrict__ aLUT, const float* __restrict__ dLUT, float cx, float cy,
+                            float cz, float* sx, float* sy, float* sz, float* dcx, float* dcy, float* qx, float* qy,
+                            int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float A = aLUT[i], D = dLUT[i];
+        sx[i] = fd(fm(2.0f, A), fm(cx, cx));
+        sy[i] = fd(fm(2.0f, A), fm(cy, cy));
+        sz[i] = fd(fm(2.0f, A), fm(cz, cz));
+        dcx[i] = fd(D, cx);
+        dcy[i] = fd(D, cy);
+        float t = fd(fm(0.5f, D), A);
+        qx[i] = fm(cx, t);
+        qy[i] = fm(cy, t);
+    }
+}
+
+__device__ __forceinline__ f3 lltorque_g(f3 m, f3 H, float alpha, float gilb) {
+    f3 mxH = cross3(m, H);
+    f3 mmxH = cross3(m, mxH);
+    return f3{fm(gilb, fa(mxH.x, fm(alpha, mmxH.x))), fm(gilb, fa(mxH.y, fm(alpha, mmxH.y))),
+              fm(gilb, fa(mxH.z, fm(alpha, mmxH.z)))};
+}
 
 // engine/effectivefield.go:14-24 + engine/torque.go:135-144 for one cell:
 // B = demag; B += exchange(+DMI)/Ms; B += anisotropy; B += B_ext; torque.
@@ -74,19 +125,30 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
     const float *mx = m, *my = m + N, *mz = m + 2 * N;
     int I = (iz * a.g.Ny + iy) * a.g.Nx + ix;
     f3 B{0.f, 0.f, 0.f};
-    if (a.bd) B = f3{a.bd[I], a.bd[N + I], a.bd[2 * N + I]};
+    if (a.bd) B = f3{__ldg(a.bd + I), __ldg(a.bd + N + I), __ldg(a.bd + 2 * N + I)};
     f3 m0 = ld3(mx, my, mz, I);
     if (!is0(m0)) {
         int r0 = __ldg(a.regions + I);
-        f3 e = a.dmi ? dmi_sum(mx, my, mz, a.aLUT, a.dLUT, a.regions, a.cx, a.cy, a.cz, a.g, a.openbc != 0, ix, iy,
-                               iz, m0, r0)
+        f3 e = a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
                      : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
-        float inv = inv_msat(a.Ms, a.Ms_mul, I);
+        float inv = a.ms_uniform ? a.kc.inv_ms : inv_msat(a.Ms, a.Ms_mul, I);
         B.x = fa(B.x, fm(e.x, inv));
         B.y = fa(B.y, fm(e.y, inv));
         B.z = fa(B.z, fm(e.z, inv));
     }
-    if (a.anis) add_uniaxial(B, a.up, m0, I);
+    if (a.anis) {
+        if (a.anis_uniform) {  // uniaxialanisotropy2.cl:27-34 with the uniform factors hoisted
+            f3 u{a.kc.u[0], a.kc.u[1], a.kc.u[2]};
+            float mu = dot3(m0, u);
+            float f1 = fm(a.kc.f1k, mu);
+            float f2 = fm(a.kc.f2k, fm(fm(mu, mu), mu));
+            B.x = fa(B.x, fa(fm(f1, u.x), fm(f2, u.x)));
+            B.y = fa(B.y, fa(fm(f1, u.y), fm(f2, u.y)));
+            B.z = fa(B.z, fa(fm(f1, u.z), fm(f2, u.z)));
+        } else {
+            add_uniaxial(B, a.up, m0, I);
+        }
+    }
     if (a.zeeman) {
         int r = __ldg(a.regions + I);
         B.x = fa(B.x, __ldg(a.bext[0] + r));
@@ -94,7 +156,10 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
         B.z = fa(B.z, __ldg(a.bext[2] + r));
     }
     if (a.beff) { a.beff[I] = B.x; a.beff[N + I] = B.y; a.beff[2 * N + I] = B.z; }
-    f3 t = a.precess ? lltorque(m0, B, amul(a.alpha, a.alpha_mul, I)) : llnoprecess(m0, B);
+    f3 t;
+    if (!a.precess) t = llnoprecess(m0, B);
+    else if (a.alpha_uniform) t = lltorque_g(m0, B, a.alpha_mul, a.kc.gilb);
+    else t = lltorque(m0, B, amul(a.alpha, a.alpha_mul, I));
     float* out = a.tau_direct ? a.tau_direct : a.ctl->k[a.out_slot];
     out[I] = t.x; out[N + I] = t.y; out[2 * N + I] = t.z;
 }
@@ -115,22 +180,21 @@ struct StageArgs {
 };
 
 // m_w = normalize(src + sum_j (c_j h) k_j) with Madd<n> rounding
-// (opencl/madd.go, madd<n>.cl) then normalize2.cl.
-__global__ void k_stage(StageArgs a) {
+// (opencl/madd.go, madd<n>.cl) then normalize2.cl.  NT = number of terms.
+template <int NT>
+__global__ void __launch_bounds__(256) k_stage(StageArgs a) {
     DevCtl* ctl = a.ctl;
     if (!ctl->active) return;
     if (a.only_if_accepted && !ctl->accepted) return;
     const float h = ctl->h;
-    float fac[kMaxTerms];
-    const float* src[kMaxTerms];
+    float fac[NT];
+    const float* src[NT];
     fac[0] = 1.0f;
     src[0] = a.src_m ? ctl->mw : ctl->m;
 #pragma unroll
-    for (int j = 1; j < kMaxTerms; j++) {
-        if (j < a.nterm) {
-            fac[j] = a.scale_h ? fm(a.c[j], h) : a.c[j];
-            src[j] = ctl->k[a.slot[j]];
-        }
+    for (int j = 1; j < NT; j++) {
+        fac[j] = a.scale_h ? fm(a.c[j], h) : a.c[j];
+        src[j] = ctl->k[a.slot[j]];
     }
     float* dst = ctl->mw;
     const int N = a.N;
@@ -138,13 +202,14 @@ __global__ void k_stage(StageArgs a) {
         float v[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            int o = c * N + i;
+            const int o = c * N + i;
             float acc;
-            if (a.nterm == 3) {
+            if constexpr (NT == 3) {
                 acc = fa(fm(fac[0], src[0][o]), fa(fm(fac[1], src[1][o]), fm(fac[2], src[2][o])));
             } else {
                 acc = fm(fac[0], src[0][o]);
-                for (int j = 1; j < a.nterm; j++) acc = fa(acc, fm(fac[j], src[j][o]));
+#pragma unroll
+                for (int j = 1; j < NT; j++) acc = fa(acc, fm(fac[j], src[j][o]));
             }
             v[c] = acc;
         }
@@ -171,14 +236,18 @@ struct ErrArgs {
 // Fused: error combination (Madd rounding), max |Err|^2, max |delM|^2 and
 // max |Err|/|delM| (VecNorm + Div + MaxAbs of stepcontroller.go:51-63);
 // Err itself is never written to memory.
+template <int NT, bool HEUN>
 __global__ void __launch_bounds__(256) k_err_norms(ErrArgs a) {
     __shared__ float sh[32];
     DevCtl* ctl = a.ctl;
     if (!ctl->active) return;
-    const float* k[kMaxTerms];
+    const float* k[NT];
+    float e[NT];
 #pragma unroll
-    for (int j = 0; j < kMaxTerms; j++)
-        if (j < a.nterm) k[j] = ctl->k[a.slot[j]];
+    for (int j = 0; j < NT; j++) {
+        k[j] = ctl->k[a.slot[j]];
+        e[j] = a.e[j];
+    }
     const float* dm = ctl->k[a.dm_slot];
     const int N = a.N;
     float me = 0.f, md = 0.f, mr = 0.f;
@@ -190,13 +259,14 @@ __global__ void __launch_bounds__(256) k_err_norms(ErrArgs a) {
         for (int c = 0; c < 3; c++) {
             int o = c * N + i;
             float acc;
-            if (a.heun) {
+            if constexpr (HEUN) {
                 acc = fs(k[0][o], k[1][o]);
-            } else if (a.nterm == 3) {
-                acc = fa(fm(a.e[0], k[0][o]), fa(fm(a.e[1], k[1][o]), fm(a.e[2], k[2][o])));
+            } else if constexpr (NT == 3) {
+                acc = fa(fm(e[0], k[0][o]), fa(fm(e[1], k[1][o]), fm(e[2], k[2][o])));
             } else {
-                acc = fm(a.e[0], k[0][o]);
-                for (int j = 1; j < a.nterm; j++) acc = fa(acc, fm(a.e[j], k[j][o]));
+                acc = fm(e[0], k[0][o]);
+#pragma unroll
+                for (int j = 1; j < NT; j++) acc = fa(acc, fm(e[j], k[j][o]));
             }
             ev[c] = acc;
         }
@@ -342,6 +412,8 @@ struct SimImpl {
     float* bufs = nullptr;        // 2 + 7 slots of 3N
     float* bd = nullptr;          // demag field 3N
     uint8_t* zero_regions = nullptr;
+    float* dmi_pairs = nullptr;   // 7 x 32896 region-pair DMI coefficients
+    LocalConsts* kc_dev = nullptr;
     DevCtl* ctl = nullptr;        // device
     DevCtl* hctl = nullptr;       // pinned host mirror
     PassArgs pa{};
@@ -390,7 +462,15 @@ static int launch_stage(SimImpl* s, int src_m, std::initializer_list<int> slots,
     a.normalize = normalize;
     a.only_if_accepted = only_if_accepted;
     a.vol = s->p.vol;
-    k_stage<<<grid_for(s->N, 256), 256, 0, S()>>>(a);
+    const int g = grid_for(s->N, 256);
+    switch (a.nterm) {
+    case 2: k_stage<2><<<g, 256, 0, S()>>>(a); break;
+    case 3: k_stage<3><<<g, 256, 0, S()>>>(a); break;
+    case 4: k_stage<4><<<g, 256, 0, S()>>>(a); break;
+    case 5: k_stage<5><<<g, 256, 0, S()>>>(a); break;
+    case 6: k_stage<6><<<g, 256, 0, S()>>>(a); break;
+    default: return set_error(UMAG_E_ARG, "stage with %d terms", a.nterm);
+    }
     UMAG_LAUNCH_CHECK();
     *nl += 1;
     return UMAG_OK;
@@ -408,7 +488,12 @@ static int launch_err(SimImpl* s, std::initializer_list<int> slots, std::initial
     for (double e : es) a.e[j++] = (float)e;
     a.dm_slot = dm_slot;
     a.heun = heun;
-    k_err_norms<<<grid_for(s->N, 256, 4), 256, 0, S()>>>(a);
+    const int g = grid_for(s->N, 256, 4);
+    if (heun) k_err_norms<2, true><<<g, 256, 0, S()>>>(a);
+    else if (a.nterm == 2) k_err_norms<2, false><<<g, 256, 0, S()>>>(a);
+    else if (a.nterm == 4) k_err_norms<4, false><<<g, 256, 0, S()>>>(a);
+    else if (a.nterm == 6) k_err_norms<6, false><<<g, 256, 0, S()>>>(a);
+    else return set_error(UMAG_E_ARG, "error combination with %d terms", a.nterm);
     UMAG_LAUNCH_CHECK();
     *nl += 1;
     return UMAG_OK;
@@ -649,6 +734,27 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
     la.precess = p->precess;
     la.Ms = p->Ms;
     la.Ms_mul = p->Ms_mul;
+    la.ms_uniform = p->Ms == nullptr;
+    la.alpha_uniform = p->alpha == nullptr;
+    la.anis_uniform = p->Ms == nullptr && p->Ku1 == nullptr && p->Ku2 == nullptr && p->anisU[0] == nullptr &&
+                      p->anisU[1] == nullptr && p->anisU[2] == nullptr;
+    {  // uniform factors, evaluated on the device (bit-identical to the per-cell path)
+        if (cudaMalloc(&s->kc_dev, sizeof(LocalConsts)) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "consts"));
+        k_local_consts<<<1, 1, 0, S()>>>(la, s->kc_dev);
+        if (cudaMemcpyAsync(&la.kc, s->kc_dev, sizeof(LocalConsts), cudaMemcpyDeviceToHost, S()) != cudaSuccess ||
+            cudaStreamSynchronize(S()) != cudaSuccess)
+            return fail(set_error(UMAG_E_CUDA, "uniform constants"));
+    }
+    if (la.dmi) {
+        const int np = 256 * 257 / 2;
+        if (cudaMalloc(&s->dmi_pairs, sizeof(float) * 7 * np) != cudaSuccess)
+            return fail(set_error(UMAG_E_NOMEM, "DMI pair table"));
+        float* t = s->dmi_pairs;
+        la.dl = DmiPairLut{t, t + np, t + 2 * np, t + 3 * np, t + 4 * np, t + 5 * np, t + 6 * np};
+        k_dmi_pairs<<<grid_for(np, 256), 256, 0, S()>>>(p->aLUT, p->dLUT, la.cx, la.cy, la.cz, t, t + np, t + 2 * np,
+                                                        t + 3 * np, t + 4 * np, t + 5 * np, t + 6 * np, np);
+        if (cudaStreamSynchronize(S()) != cudaSuccess) return fail(set_error(UMAG_E_CUDA, "DMI pair table"));
+    }
     if (la.zeeman && (!p->bextLUT[1] || !p->bextLUT[2])) return fail(set_error(UMAG_E_ARG, "bextLUT needs 3 arrays"));
     int nl = 0;
     // count launches of one step (not enqueued: measured on a dry capture below)
@@ -676,6 +782,8 @@ int sim_free(umag_sim* h) {
     cudaFree(s->bufs);
     cudaFree(s->bd);
     cudaFree(s->zero_regions);
+    cudaFree(s->dmi_pairs);
+    cudaFree(s->kc_dev);
     cudaFree(s->ctl);
     if (s->hctl) cudaFreeHost(s->hctl);
     delete s;

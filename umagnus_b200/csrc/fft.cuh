@@ -144,6 +144,18 @@ template <typename T> __host__ __device__ inline int fft_line_cap(const FftLine<
     return f.nst ? c : (1 << 30);
 }
 
+// Lines of f one batch may hold (>= 1; the host checks that one line fits).
+template <typename T> __device__ __forceinline__ int fft_lines_per_batch(const FftLine<T>& f, int ntr) {
+    if (f.nst == 0) return ntr > 0 ? ntr : 1;
+    long c = (long)blockDim.x * fft_line_cap(f) / f.L;
+    if (c < 1) c = 1;
+    return c < ntr ? (int)c : (ntr > 0 ? ntr : 1);
+}
+// Host check: one line of length L fits a CTA of `threads` threads.
+template <typename T> inline bool fft_line_fits(const FftLine<T>& f, int threads) {
+    return f.nst == 0 || (long)threads * fft_line_cap(f) >= f.L;
+}
+
 // One Stockham stage of radix R over ntr lines in shared memory.
 // Element j of line t is s[t*ts + j*es].  tfast selects the butterfly
 // order (lines fastest, or elements fastest) so that consecutive threads

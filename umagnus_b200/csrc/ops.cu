@@ -465,23 +465,24 @@ static int reduce_max(int kind, const float* x, const float* y, const float* z, 
 }
 
 int max_vec_norm(const float* x, const float* y, const float* z, int N, double* out) {
-    UMAG_REQUIRE(x && y && z, "NULL argument");
+    UMAG_REQUIRE((x && y && z) || N <= 0, "NULL argument");
     return reduce_max(0, x, y, z, nullptr, nullptr, nullptr, N, out, true);
 }
 int max_vec_diff(const float* ax, const float* ay, const float* az, const float* bx, const float* by,
                  const float* bz, int N, double* out) {
-    UMAG_REQUIRE(ax && ay && az && bx && by && bz, "NULL argument");
+    UMAG_REQUIRE((ax && ay && az && bx && by && bz) || N <= 0, "NULL argument");
     return reduce_max(1, ax, ay, az, bx, by, bz, N, out, true);
 }
 int max_abs(const float* v, int N, double* out) {
-    UMAG_REQUIRE(v, "NULL argument");
+    UMAG_REQUIRE(v || N <= 0, "NULL argument");
     return reduce_max(2, v, nullptr, nullptr, nullptr, nullptr, nullptr, N, out, false);
 }
 
 int sum_dot(const float* a, const float* b, int N, double* out) {
     UMAG_TRY(ensure_init());
-    UMAG_REQUIRE(a && out, "NULL argument");
+    UMAG_REQUIRE(out != nullptr, "NULL output");
     if (N <= 0) { *out = 0.0; return UMAG_OK; }
+    UMAG_REQUIRE(a != nullptr, "NULL argument");
     cudaStream_t s = ctx().stream;
     double* part = (double*)ctx().red_dev + 8;
     int g = grid_for(N, 256, 4);

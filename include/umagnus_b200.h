@@ -150,6 +150,23 @@ int umag_demag_get_spectrum(umag_demag* d, float* const host[6]);
 int umag_demag_get_kernel(umag_demag* d, double* const host[6]);
 int umag_demag_padded_size(umag_demag* d, int P[3]);
 int umag_demag_free(umag_demag* d);
+/* Demag field for callers that cannot allocate device memory when they need
+ * it (an external pool that owns the device, a runtime that forbids
+ * allocation after start-up).  No counterpart in the reference.  It needs
+ * neither umag_init nor a plan: K holds the six float32 kernel-spectrum
+ * arrays (the layout umag_demag_get_spectrum returns, yz/xz may be NULL for
+ * Nz == 1) on the device, and all working memory lives in one 16 MiB
+ * __device__ array that every GPU loading this library keeps until the
+ * process exits.  Meshes whose spectrum and twiddles exceed 16 MiB, or
+ * without a compile-time FFT plan, return UMAG_E_UNSUPPORTED.  The first
+ * call on a device looks up the array's device address (make that call
+ * before any stream capture).  Work is queued on `stream` (a cudaStream_t,
+ * NULL = legacy default stream); every call shares the array, so calls that
+ * overlap on the GPU (other streams, other host threads) race.  Calls no
+ * cudaMalloc, cudaFree or other allocating routine. */
+int umag_demag_exec_noalloc(int Nx, int Ny, int Nz, const float* const K[6], float* Bx, float* By, float* Bz,
+                            const float* mx, const float* my, const float* mz, const float* vol, const float* Ms,
+                            float Ms_mul, void* stream);
 
 /* ---- engine: a whole simulation on the device ---------------------------- */
 /* Material and mesh description.  Uniform parameters use the *_mul value

@@ -233,6 +233,104 @@ __device__ __forceinline__ f3 dmi_sum_lut(const float* __restrict__ mx, const fl
     return h;
 }
 
+// Region-free variants (every cell in region 0): the pair coefficients are the
+// (0,0) entries, passed as scalars, so no region or table loads are needed.
+// Same operations, hence the same rounding, as exchange_sum / dmi_sum_lut.
+struct PairCoef {
+    float wax, way, waz;            // exchange: w_d * A(0,0)
+    float sx, sy, sz, dcx, dcy, qx, qy;  // DMI: see DmiPairLut
+};
+
+__device__ __forceinline__ f3 exchange_sum_u(const float* __restrict__ mx, const float* __restrict__ my,
+                                             const float* __restrict__ mz, const PairCoef& P, Mesh3 g, int ix,
+                                             int iy, int iz, f3 m0) {
+    f3 b{0.f, 0.f, 0.f};
+    int nb[6];
+    nb[0] = (iz * g.Ny + iy) * g.Nx + lclamp(ix - 1, g.Nx, g.pbc & 1);
+    nb[1] = (iz * g.Ny + iy) * g.Nx + hclamp(ix + 1, g.Nx, g.pbc & 1);
+    nb[2] = (iz * g.Ny + lclamp(iy - 1, g.Ny, g.pbc & 2)) * g.Nx + ix;
+    nb[3] = (iz * g.Ny + hclamp(iy + 1, g.Ny, g.pbc & 2)) * g.Nx + ix;
+    nb[4] = (lclamp(iz - 1, g.Nz, g.pbc & 4) * g.Ny + iy) * g.Nx + ix;
+    nb[5] = (hclamp(iz + 1, g.Nz, g.pbc & 4) * g.Ny + iy) * g.Nx + ix;
+    const int nn = (g.Nz != 1) ? 6 : 4;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        if (k >= nn) break;
+        const float s = k < 2 ? P.wax : (k < 4 ? P.way : P.waz);
+        f3 mn = ld3(mx, my, mz, nb[k]);
+        if (is0(mn)) mn = m0;
+        b.x = fa(b.x, fm(s, fs(mn.x, m0.x)));
+        b.y = fa(b.y, fm(s, fs(mn.y, m0.y)));
+        b.z = fa(b.z, fm(s, fs(mn.z, m0.z)));
+    }
+    return b;
+}
+
+__device__ __forceinline__ f3 dmi_sum_u(const float* __restrict__ mx, const float* __restrict__ my,
+                                        const float* __restrict__ mz, const PairCoef& P, Mesh3 g, bool openbc,
+                                        int ix, int iy, int iz, f3 m0) {
+    f3 h{0.f, 0.f, 0.f};
+#pragma unroll
+    for (int d = 0; d < 2; d++) {
+#pragma unroll
+        for (int side = -1; side <= 1; side += 2) {
+            f3 mn{0.f, 0.f, 0.f};
+            int i_;
+            bool inside;
+            if (d == 0) {
+                int xx = side < 0 ? lclamp(ix - 1, g.Nx, g.pbc & 1) : hclamp(ix + 1, g.Nx, g.pbc & 1);
+                i_ = (iz * g.Ny + iy) * g.Nx + xx;
+                inside = (side < 0 ? ix - 1 >= 0 : ix + 1 < g.Nx) || (g.pbc & 1);
+            } else {
+                int yy = side < 0 ? lclamp(iy - 1, g.Ny, g.pbc & 2) : hclamp(iy + 1, g.Ny, g.pbc & 2);
+                i_ = (iz * g.Ny + yy) * g.Nx + ix;
+                inside = (side < 0 ? iy - 1 >= 0 : iy + 1 < g.Ny) || (g.pbc & 2);
+            }
+            if (inside) mn = ld3(mx, my, mz, i_);
+            const bool missing = is0(mn);
+            if (!missing || !openbc) {
+                if (missing) {
+                    float q = d == 0 ? P.qx : P.qy;
+                    if (side < 0) q = -q;
+                    if (d == 0) {
+                        mn.x = fs(m0.x, fm(q, m0.z));
+                        mn.y = m0.y;
+                        mn.z = fa(m0.z, fm(q, m0.x));
+                    } else {
+                        mn.x = m0.x;
+                        mn.y = fs(m0.y, fm(q, m0.z));
+                        mn.z = fa(m0.z, fm(q, m0.y));
+                    }
+                }
+                const float s = d == 0 ? P.sx : P.sy;
+                h.x = fa(h.x, fm(s, fs(mn.x, m0.x)));
+                h.y = fa(h.y, fm(s, fs(mn.y, m0.y)));
+                h.z = fa(h.z, fm(s, fs(mn.z, m0.z)));
+                const float Dc = d == 0 ? P.dcx : P.dcy;
+                float tz = side < 0 ? -mn.z : mn.z;
+                float tp = d == 0 ? mn.x : mn.y;
+                tp = side < 0 ? -tp : tp;
+                if (d == 0) h.x = fa(h.x, fm(Dc, tz));
+                else h.y = fa(h.y, fm(Dc, tz));
+                h.z = fs(h.z, fm(Dc, tp));
+            }
+        }
+    }
+    if (g.Nz != 1) {
+#pragma unroll
+        for (int side = -1; side <= 1; side += 2) {
+            int zz = side < 0 ? lclamp(iz - 1, g.Nz, g.pbc & 4) : hclamp(iz + 1, g.Nz, g.pbc & 4);
+            int i_ = (zz * g.Ny + iy) * g.Nx + ix;
+            f3 mn = ld3(mx, my, mz, i_);
+            if (is0(mn)) mn = m0;
+            h.x = fa(h.x, fm(P.sz, fs(mn.x, m0.x)));
+            h.y = fa(h.y, fm(P.sz, fs(mn.y, m0.y)));
+            h.z = fa(h.z, fm(P.sz, fs(mn.z, m0.z)));
+        }
+    }
+    return h;
+}
+
 struct UniaxParams {
     const float *Ms, *K1, *K2, *ux, *uy, *uz;
     float Ms_mul, K1_mul, K2_mul, ux_mul, uy_mul, uz_mul;

@@ -174,14 +174,16 @@ __global__ void k_real_to_cplx(const double* src, double2* dst, long n) {
         dst[i] = make_double2(src[i], 0.0);
 }
 
-// Real parts of the non-redundant block, scaled; max |imag| into *maximg.
-__global__ void k_extract_spectrum(const double2* a, float* out, int Px, int Py, int Pz, double scale,
+// Real parts of the non-redundant block, scaled, rows of pitch Kp (the pad
+// columns are zero); max |imag| into *maximg.
+__global__ void k_extract_spectrum(const double2* a, float* out, int Px, int Py, int Pz, int Kp, double scale,
                                    unsigned long long* maximg) {
     int hx = Px / 2 + 1, hy = Py / 2 + 1, hz = Pz / 2 + 1;
-    long n = (long)hx * hy * hz;
+    long n = (long)Kp * hy * hz;
     double mi = 0.0;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        int x = (int)(i % hx), y = (int)((i / hx) % hy), z = (int)(i / ((long)hx * hy));
+        int x = (int)(i % Kp), y = (int)((i / Kp) % hy), z = (int)(i / ((long)Kp * hy));
+        if (x >= hx) { out[i] = 0.f; continue; }
         double2 v = a[((long)z * Py + y) * Px + x];
         out[i] = (float)(v.x * scale);
         mi = fmax(mi, fabs(v.y));
@@ -298,7 +300,7 @@ __global__ void __launch_bounds__(kPassBThreads) k_pass_b(PassArgs a) {
         int kym = ky;
         float sy = 1.f;
         if (ky > a.Py / 2) { kym = a.Py - ky; sy = -1.f; }
-        long I = ((long)kzm * hy + kym) * hx + kx;
+        long I = ((long)kzm * hy + kym) * a.Kp + kx;
         float Kxx = __ldg(a.K[0] + I), Kyy = __ldg(a.K[1] + I), Kzz = __ldg(a.K[2] + I);
         float Kxy = __ldg(a.K[5] + I) * sy;
         float Kyz = 0.f, Kxz = 0.f;
@@ -433,13 +435,14 @@ static int plan_common(umag_demag* d) {
         return set_error(UMAG_E_UNSUPPORTED, "Nx = %d too large for the x pass", d->N[0]);
     if (d->P[2] > 1 && (long)kChunkW * d->P[2] > (long)kPassThreads * fft_line_cap(d->fz))
         return set_error(UMAG_E_UNSUPPORTED, "Nz = %d too large for the z transform", d->N[2]);
-    auto twr = twiddles<float2>(d->P[0], d->M / 2 + 1);
+    auto twr = twiddles<float2>(d->P[0], d->M > 1 ? d->M : 2);  // exp(-2 pi i k / Px), k < Px/2
     UMAG_CUDA(cudaMalloc(&d->twr, sizeof(float2) * twr.size()));
     UMAG_CUDA(cudaMemcpy(d->twr, twr.data(), sizeof(float2) * twr.size(), cudaMemcpyHostToDevice));
     size_t spec_elems = (size_t)3 * d->P[2] * d->N[1] * d->Lx;
     UMAG_CUDA(cudaMalloc(&d->spec, sizeof(float2) * spec_elems));
     UMAG_CUDA(cudaMemset(d->spec, 0, sizeof(float2) * spec_elems));
-    size_t kn = (size_t)(d->P[0] / 2 + 1) * (d->P[1] / 2 + 1) * (d->P[2] / 2 + 1);
+    d->Kp = (d->Hx + 3) / 4 * 4;
+    size_t kn = (size_t)d->Kp * (d->P[1] / 2 + 1) * (d->P[2] / 2 + 1);
     d->Kn = kn;
     for (int c = 0; c < 6; c++) {
         d->K[c] = nullptr;
@@ -492,8 +495,8 @@ static int kernel_to_spectrum(umag_demag* d, double* const Kr[6], cudaStream_t s
         }
         cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), st);
         long kn = (long)d->Kn;
-        k_extract_spectrum<<<grid_for(kn, threads), threads, 0, st>>>(buf, d->K[c], Px, Py, Pz, 1.0 / (double)n,
-                                                                       dmax);
+        k_extract_spectrum<<<grid_for(kn, threads), threads, 0, st>>>(buf, d->K[c], Px, Py, Pz, d->Kp,
+                                                                       1.0 / (double)n, dmax);
         unsigned long long hm = 0;
         cudaMemcpyAsync(&hm, dmax, sizeof(hm), cudaMemcpyDeviceToHost, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) { st_ok = set_error(UMAG_E_CUDA, "kernel FFT failed"); break; }
@@ -620,8 +623,12 @@ int demag_get_spectrum(umag_demag* d, float* const host[6]) {
     UMAG_CUDA(cudaStreamSynchronize(ctx().stream));
     for (int c = 0; c < 6; c++) {
         if (!host[c]) continue;
-        if (d->K[c]) UMAG_CUDA(cudaMemcpy(host[c], d->K[c], sizeof(float) * d->Kn, cudaMemcpyDeviceToHost));
-        else memset(host[c], 0, sizeof(float) * d->Kn);
+        // reference layout: rows of Px/2+1 floats (the device rows are padded to Kp)
+        const size_t rows = d->Kn / d->Kp;
+        if (d->K[c])
+            UMAG_CUDA(cudaMemcpy2D(host[c], sizeof(float) * d->Hx, d->K[c], sizeof(float) * d->Kp,
+                                   sizeof(float) * d->Hx, rows, cudaMemcpyDeviceToHost));
+        else memset(host[c], 0, sizeof(float) * d->Hx * rows);
     }
     return UMAG_OK;
 }
@@ -634,16 +641,17 @@ void fill_pass_args(const umag_demag* d, PassArgs& a) {
     a.twr = d->twr;
     a.spec = d->spec;
     for (int c = 0; c < 6; c++) a.K[c] = d->K[c];
+    a.Kp = d->Kp;
 }
 
 int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st) {
     if (d->use_fast) {
         const FastPasses& f = d->fast;
-        f.a<<<dim3(d->N[1], 3), 256, f.smem_ac, st>>>(a);
+        f.a<<<dim3(d->N[1], 3), f.nt_ac, f.smem_ac, st>>>(a);
         UMAG_LAUNCH_CHECK();
-        f.b<<<dim3((d->Hx + f.wb - 1) / f.wb, d->P[2]), 512, f.smem_b, st>>>(a);
+        f.b<<<dim3((d->Hx + f.wb - 1) / f.wb, d->P[2]), f.nt_b, f.smem_b, st>>>(a);
         UMAG_LAUNCH_CHECK();
-        f.c<<<dim3(d->N[1], 3), 256, f.smem_ac, st>>>(a);
+        f.c<<<dim3(d->N[1], 3), f.nt_ac, f.smem_ac, st>>>(a);
         UMAG_LAUNCH_CHECK();
         return UMAG_OK;
     }

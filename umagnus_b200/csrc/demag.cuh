@@ -18,6 +18,8 @@ struct FastPasses {
     void (*c)(PassArgs) = nullptr;
     size_t smem_ac = 0, smem_b = 0;
     int wb = 0;
+    int nt_b = 512;   // threads per pass-B CTA
+    int nt_ac = 256;  // threads per pass-A/C CTA
 };
 }  // namespace umag
 
@@ -31,10 +33,11 @@ struct umag_demag {
     bool is2d;
     umag::FftLine<float> fx, fy, fz;  // x: length Px/2 (packed real), y: Py, z: Pz
     std::vector<float2*> tw_dev;
-    float2* twr = nullptr;            // exp(-2 pi i k / Px), k in [0, Px/4]
+    float2* twr = nullptr;            // exp(-2 pi i k / Px), k in [0, Px/2)
     float2* spec = nullptr;           // 3 * Pz * Ny * Lx
     float* K[6] = {};                 // xx yy zz yz xz xy (yz, xz NULL in 2D)
-    size_t Kn = 0;
+    size_t Kn = 0;  // floats per kernel array (Kp * (Py/2+1) * (Pz/2+1))
+    int Kp = 0;     // row pitch: Px/2+1 rounded up to 4 floats (16-byte rows)
 };
 
 namespace umag {
@@ -45,6 +48,7 @@ struct PassArgs {
     const float2* twr;
     float2* spec;
     const float* K[6];
+    int Kp;  // row pitch (floats) of the kernel arrays: Hx padded to 4 in plans, Hx for caller-owned spectra
     const float* m[3];
     // engine use: magnetisation read through a device-side slot
     // (m_sel ? *m_ind_w : *m_ind) + c*ncell, and a device flag that turns a

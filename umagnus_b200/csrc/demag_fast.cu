@@ -6,6 +6,7 @@
 // twiddles are staged in shared memory.  demag_fast_select() returns the
 // instantiation for a plan, or nothing (the generic kernels then run).
 #include "demag.cuh"
+#include "fft_reg.cuh"
 #include "fft_static.cuh"
 
 namespace umag {
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) {
         int kym = ky;
         float sy = 1.f;
         if (ky > NY) { kym = PY - ky; sy = -1.f; }
-        const long I = ((long)kzm * HY + kym) * hx + kx;
+        const long I = ((long)kzm * HY + kym) * a.Kp + kx;
         const float Kxx = __ldg(a.K[0] + I), Kyy = __ldg(a.K[1] + I), Kzz = __ldg(a.K[2] + I);
         const float Kxy = __ldg(a.K[5] + I) * sy;
         float Kyz = 0.f, Kxz = 0.f;
@@ -248,16 +249,305 @@ __global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) {
     }
 }
 
+// Pass B with the register-blocked FFT (power-of-two Py): thread (t, w) holds
+// rows t + T*m (m < 8) of column kx0 + w for all three components.  Rows
+// y >= Ny are zero padding (m >= 4): the loads are skipped and the first
+// butterflies fold; only rows y < Ny are computed by the inverse and stored.
+template <int PY, int WB>
+__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
+    constexpr int T = PY / 8, NT = T * WB, NY = PY / 2, HY = PY / 2 + 1;
+    constexpr int LP = rg_line<PY>();
+    extern __shared__ __align__(16) float2 sm[];
+    float2* tw = sm;                  // PY twiddles
+    float2* ex = tw + PY;             // [3][WB][LP] exchange lines
+    float* Ks = reinterpret_cast<float*>(ex + 3 * WB * LP);  // [6][HY][WB] kernel block
+    if (a.active && !*a.active) return;
+    const int tid = threadIdx.x;
+    const int w = tid % WB, t = tid / WB;
+    for (int i = tid; i < PY; i += NT) tw[i] = a.fy.tw[i];
+    const int kx0 = blockIdx.x * WB, kz = blockIdx.y;
+    const int kx = kx0 + w, hx = a.Hx, Pz = a.Pz;
+    // the kernel block this CTA multiplies with: asynchronous copies that
+    // complete while the forward transform runs
+    int kzm = kz;
+    float sz = 1.f;
+    if (kz > Pz / 2) { kzm = Pz - kz; sz = -1.f; }
+    const bool k3d = a.K[3] != nullptr;
+    {
+        const int ncomp = k3d ? 6 : 4;
+        const long kbase = (long)kzm * HY * a.Kp + kx0;
+        bool wide = false;
+        if constexpr (WB % 4 == 0) {
+            // 16-byte rows (plan layout: pitch padded to 4 floats, pad columns zero)
+            wide = a.Kp % 4 == 0 && kx0 + WB <= a.Kp;
+            if (wide) {
+                constexpr int CH = WB / 4;
+                for (int e = tid; e < ncomp * HY * CH; e += NT) {
+                    const int cc = e / (HY * CH), r = e % (HY * CH), ky = r / CH, ch = r % CH;
+                    const int comp = k3d ? cc : (cc == 3 ? 5 : cc);  // 2D stores xx yy zz xy
+                    const float* src = a.K[comp] + kbase + (long)ky * a.Kp + 4 * ch;
+                    const unsigned d = (unsigned)__cvta_generic_to_shared(Ks + comp * HY * WB + ky * WB + 4 * ch);
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+                }
+            }
+        }
+        if (!wide) {
+            for (int e = tid; e < ncomp * HY * WB; e += NT) {
+                const int cc = e / (HY * WB), r = e % (HY * WB), ky = r / WB, ww = r % WB;
+                const int comp = k3d ? cc : (cc == 3 ? 5 : cc);
+                float* dst = Ks + comp * HY * WB + ky * WB + ww;
+                if (kx0 + ww < hx) {
+                    const float* src = a.K[comp] + kbase + (long)ky * a.Kp + ww;
+                    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+                } else {
+                    *dst = 0.f;
+                }
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    }
+    const bool col = kx < hx;
+    const long cs = (long)Pz * NY * a.Lx;
+    const float2* in = a.spec + (long)kz * NY * a.Lx + kx;
+    float2 v[3][8];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const int y = t + T * m;
+            v[c][m] = (m < 4 && col) ? in[c * cs + (long)y * a.Lx] : make_float2(0.f, 0.f);
+        }
+    __syncthreads();  // twiddles
+    float2* exl = ex + w * LP;
+    const int exs = WB * LP;
+    rg_fft_fwd<PY, 3>(v, t, exl, exs, tw);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+    // kernel multiply (kernmulrsymm3d.cl:41-90), mirrored into the stored block
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        const int ky = t + T * m;
+        int kym = ky;
+        float sy = 1.f;
+        if (ky > NY) { kym = PY - ky; sy = -1.f; }
+        const float* kr = Ks + kym * WB + w;
+        const float Kxx = kr[0], Kyy = kr[HY * WB], Kzz = kr[2 * HY * WB];
+        const float Kxy = kr[5 * HY * WB] * sy;
+        float Kyz = 0.f, Kxz = 0.f;
+        if (k3d) {
+            Kyz = kr[3 * HY * WB] * (sy * sz);
+            Kxz = kr[4 * HY * WB] * sz;
+        }
+        const float2 mx = v[0][m], my = v[1][m], mz = v[2][m];
+        // conjugated products: the inverse is conj(FFT(conj(.)))
+        v[0][m] = make_float2(mx.x * Kxx + my.x * Kxy + mz.x * Kxz, -(mx.y * Kxx + my.y * Kxy + mz.y * Kxz));
+        v[1][m] = make_float2(mx.x * Kxy + my.x * Kyy + mz.x * Kyz, -(mx.y * Kxy + my.y * Kyy + mz.y * Kyz));
+        v[2][m] = make_float2(mx.x * Kxz + my.x * Kyz + mz.x * Kzz, -(mx.y * Kxz + my.y * Kyz + mz.y * Kzz));
+    }
+    rg_fft_fwd<PY, 3>(v, t, exl, exs, tw);
+    if (col) {
+        float2* out = a.spec + (long)kz * NY * a.Lx + kx;
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                const int y = t + T * m;
+                out[c * cs + (long)y * a.Lx] = make_float2(v[c][m].x, -v[c][m].y);
+            }
+    }
+}
+
+// ---- passes A and C with the register-blocked FFT (3D, power-of-two sizes)
+// x transform: TX = M/8 threads per row (one row per warp or less), rows z
+// of one (y, component) slab; z transform: TZ = PZ/8 threads per column.
+template <int M, int PZ> struct RegAC {
+    static constexpr int NZ = nz_of_pz(PZ), TX = M / 8, TZ = PZ / 8, NT = NZ * TX, CPR = NT / TZ;
+    static constexpr int XP = ((M + 1 + 11) / 16) * 16 + 4;  // Xs row pitch, = 4 (mod 16) against bank conflicts
+    static constexpr int LX = rg_line<M, 4>(), LZ = rg_line<PZ, 3>();
+    static constexpr int EXN = NZ * LX > CPR * LZ ? NZ * LX : CPR * LZ;
+    static constexpr size_t smem = sizeof(float2) * ((size_t)2 * M + PZ + (size_t)NZ * XP + EXN);
+    static constexpr bool ok = rg_ok(M) && rg_ok(PZ) && TX <= 32 && PZ % 2 == 0 && NT % TZ == 0 && NT <= 1024;
+};
+
+template <int M, int PZ>
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) {
+    using S = RegAC<M, PZ>;
+    constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
+    constexpr int HX = M + 1;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* twx = sm;          // M
+    float2* twz = twx + M;     // PZ
+    float2* twr = twz + PZ;    // M: exp(-2 pi i k / Px)
+    float2* Xs = twr + M;      // [NZ][XP]
+    float2* ex = Xs + NZ * XP; // exchange lines
+    if (a.active && !*a.active) return;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < M; i += NT) { twx[i] = a.fx.tw[i]; twr[i] = a.twr[i]; }
+    for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
+    const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
+    const float* __restrict__ mp = a.m_ind ? (a.m_sel ? *a.m_ind_w : *a.m_ind) + (long)c * a.ncell : a.m[c];
+    // x phase: row z, lane t holds packed z[n] = x[2n] + i x[2n+1], n = t + TX*j
+    const int z = tid / TX, t = tid % TX;
+    float2 v[1][8];
+    const int rowi = (z * Ny + y) * M;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        if (j < 4) {  // n < M/2 carries data, the rest is zero padding
+            const int i = rowi + 2 * (t + TX * j);
+            v[0][j] = make_float2(scaled_m(a, mp, i), scaled_m(a, mp, i + 1));
+        } else {
+            v[0][j] = make_float2(0.f, 0.f);
+        }
+    }
+    __syncthreads();
+    rg_fft_fwd<M, 1, true, 4>(v, t, ex + z * S::LX, 0, twx);
+    // R2C unpack: partner element Z[M-k] lives in lane (TX - t) % TX, element 7-j
+    // (or (8-j) & 7 for t = 0); exchanged with warp shuffles.
+    const int lane = threadIdx.x & 31;
+    const int plane = (lane & ~(TX - 1)) | ((TX - t) & (TX - 1));
+    float2 Bv[8];
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+        float2 r;
+        r.x = __shfl_sync(0xffffffffu, v[0][s].x, plane);
+        r.y = __shfl_sync(0xffffffffu, v[0][s].y, plane);
+        if (t != 0) Bv[7 - s] = r;
+        else Bv[(8 - s) & 7] = r;
+    }
+    float2* xrow = Xs + z * XP;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const int k = t + TX * j;
+        const float2 A = v[0][j], B = Bv[j];
+        float2 E = make_float2(0.5f * (A.x + B.x), 0.5f * (A.y - B.y));
+        float2 D = make_float2(0.5f * (A.x - B.x), 0.5f * (A.y + B.y));
+        float2 O = make_float2(D.y, -D.x);
+        float2 W = twr[k];
+        float2 WO = make_float2(W.x * O.x - W.y * O.y, W.x * O.y + W.y * O.x);
+        xrow[k] = make_float2(E.x + WO.x, E.y + WO.y);
+        if (k == 0) xrow[M] = make_float2(A.x - A.y, 0.f);  // Nyquist: Re Z0 - Im Z0
+    }
+    __syncthreads();
+    // z phase: column kx, TZ lanes, rows z = tz + TZ*j (zero padding for j >= 4)
+    float2* out = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
+    const long kzs = (long)Ny * a.Lx;
+    const int tz = tid % TZ, cl = tid / TZ;
+    float2* exz = ex + cl * S::LZ;
+#pragma unroll 1
+    for (int kx0 = 0; kx0 < HX; kx0 += CPR) {
+        const int kx = kx0 + cl;
+        const bool act = kx < HX;
+        float2 u[1][8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) u[0][j] = (j < 4 && act) ? Xs[(tz + TZ * j) * XP + kx] : make_float2(0.f, 0.f);
+        rg_fft_fwd<PZ, 1, true>(u, tz, exz, 0, twz);
+        if (act) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) out[(tz + TZ * j) * kzs + kx] = u[0][j];
+        }
+    }
+}
+
+template <int M, int PZ>
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) {
+    using S = RegAC<M, PZ>;
+    constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
+    constexpr int HX = M + 1;
+    extern __shared__ __align__(16) float2 sm[];
+    float2* twx = sm;
+    float2* twz = twx + M;
+    float2* twr = twz + PZ;
+    float2* Xs = twr + M;
+    float2* ex = Xs + NZ * XP;
+    if (a.active && !*a.active) return;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < M; i += NT) { twx[i] = a.fx.tw[i]; twr[i] = a.twr[i]; }
+    for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
+    __syncthreads();
+    const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
+    const float2* in = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
+    const long kzs = (long)Ny * a.Lx;
+    // z phase: inverse transform (conjugate trick) of every column, keep z < NZ
+    const int tz = tid % TZ, cl = tid / TZ;
+    float2* exz = ex + cl * S::LZ;
+#pragma unroll 1
+    for (int kx0 = 0; kx0 < HX; kx0 += CPR) {
+        const int kx = kx0 + cl;
+        const bool act = kx < HX;
+        float2 u[1][8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            float2 q = act ? in[(tz + TZ * j) * kzs + kx] : make_float2(0.f, 0.f);
+            u[0][j] = make_float2(q.x, -q.y);
+        }
+        rg_fft_fwd<PZ, 1, true>(u, tz, exz, 0, twz);
+        if (act) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) Xs[(tz + TZ * j) * XP + kx] = make_float2(u[0][j].x, -u[0][j].y);
+        }
+    }
+    __syncthreads();
+    // x phase: C2R pack Z[k] = (X[k] + conj X[M-k]) + i conj(W^k)(X[k] - conj X[M-k]),
+    // inverse transform by the conjugate trick, even/odd samples to B
+    const int z = tid / TX, t = tid % TX;
+    const float2* xrow = Xs + z * XP;
+    float2 v[1][8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const int k = t + TX * j;
+        float2 Xk = xrow[k], Xm = xrow[M - k];
+        if (k == 0) { Xk.y = 0.f; Xm.y = 0.f; }
+        const float2 W = twr[k];
+        const float2 S1 = make_float2(Xk.x + Xm.x, Xk.y - Xm.y);
+        const float2 D1 = make_float2(Xk.x - Xm.x, Xk.y + Xm.y);
+        const float2 T1 = make_float2(W.x * D1.x + W.y * D1.y, W.x * D1.y - W.y * D1.x);
+        v[0][j] = make_float2(S1.x - T1.y, -(S1.y + T1.x));  // conj(Z[k])
+    }
+    rg_fft_fwd<M, 1, true, 4>(v, t, ex + z * S::LX, 0, twx);
+    float* __restrict__ B = a.B[c];
+    const int rowo = (z * Ny + y) * M;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int n = t + TX * j;
+        *reinterpret_cast<float2*>(B + rowo + 2 * n) = make_float2(v[0][j].x, -v[0][j].y);
+    }
+}
+
+template <int PY> struct RegB {
+    static constexpr int T = PY / 8;
+    static constexpr int WB = T >= 256 ? 1 : 256 / T > 16 ? 16 : 256 / T;
+    static constexpr int NT = T * WB;
+    static constexpr size_t smem = sizeof(float2) * ((size_t)PY + (size_t)3 * WB * rg_line<PY>()) +
+                                   sizeof(float) * (size_t)6 * (PY / 2 + 1) * WB;
+};
+
 // ------------------------------------------------------------------ dispatch
 template <int M, int PZ> static void fill_ac(FastPasses& f) {
-    f.a = k_fast_a<M, PZ>;
-    f.c = k_fast_c<M, PZ>;
-    f.smem_ac = AcShape<M, PZ>::smem;
+    if constexpr (RegAC<M, PZ>::ok && PZ >= 8) {
+        f.a = k_reg_a<M, PZ>;
+        f.c = k_reg_c<M, PZ>;
+        f.smem_ac = RegAC<M, PZ>::smem;
+        f.nt_ac = RegAC<M, PZ>::NT;
+    } else {
+        f.a = k_fast_a<M, PZ>;
+        f.c = k_fast_c<M, PZ>;
+        f.smem_ac = AcShape<M, PZ>::smem;
+        f.nt_ac = kNT;
+    }
 }
 template <int PY> static void fill_b(FastPasses& f) {
-    f.b = k_fast_b<PY>;
-    f.smem_b = BShape<PY>::smem;
-    f.wb = BShape<PY>::WB;
+    if constexpr (rg_ok(PY) && PY >= 32) {
+        f.b = k_reg_b<PY, RegB<PY>::WB>;
+        f.smem_b = RegB<PY>::smem;
+        f.wb = RegB<PY>::WB;
+        f.nt_b = RegB<PY>::NT;
+    } else {
+        f.b = k_fast_b<PY>;
+        f.smem_b = BShape<PY>::smem;
+        f.wb = BShape<PY>::WB;
+        f.nt_b = kNTB;
+    }
 }
 
 bool demag_fast_select(int M, int Py, int Pz, FastPasses& f) {
@@ -286,28 +576,32 @@ bool demag_fast_select(int M, int Py, int Pz, FastPasses& f) {
 int demag_fast_setup() {
     static bool done = false;
     if (done) return UMAG_OK;
-    const int maxsm = 227 * 1024;
+    // opt in to the full 227 KB and ask for the largest shared-memory carveout,
+    // so several CTAs of these shared-memory-heavy kernels fit on one SM
+    auto attrs = [](void (*k)(PassArgs)) -> int {
+        UMAG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        UMAG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       cudaSharedmemCarveoutMaxShared));
+        return UMAG_OK;
+    };
     FastPasses f;
     const int Ms[] = {16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 1024};
-    for (int m : Ms) {
+    for (int m : Ms)
         if (demag_fast_select(m, 2 * m > 2048 ? 2048 : 2 * m, 1, f)) {
-            UMAG_CUDA(cudaFuncSetAttribute(f.a, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
-            UMAG_CUDA(cudaFuncSetAttribute(f.c, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+            UMAG_TRY(attrs(f.a));
+            UMAG_TRY(attrs(f.c));
         }
-    }
     const int m3[] = {64, 128, 256, 512}, pz3[] = {12, 16, 32, 64};
     for (int m : m3)
         for (int pz : pz3)
             if (demag_fast_select(m, 2 * m, pz, f)) {
-                UMAG_CUDA(cudaFuncSetAttribute(f.a, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
-                UMAG_CUDA(cudaFuncSetAttribute(f.c, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+                UMAG_TRY(attrs(f.a));
+                UMAG_TRY(attrs(f.c));
             }
     // pass B instantiations
     {
         FastPasses g{};
-#define SETB(py)                                                                                     \
-    fill_b<py>(g);                                                                                   \
-    UMAG_CUDA(cudaFuncSetAttribute(g.b, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+#define SETB(py) fill_b<py>(g); UMAG_TRY(attrs(g.b));
         SETB(32) SETB(48) SETB(64) SETB(96) SETB(128) SETB(192) SETB(256) SETB(384) SETB(512) SETB(1024) SETB(2048)
 #undef SETB
     }

@@ -48,6 +48,7 @@ struct LocalConsts {
     float u[3];    // normalised uniform easy axis (uniaxialanisotropy2.cl:19)
     float f1k;     // 2*(K1/Ms) for uniform K1 and Ms
     float f2k;     // 4*(K2/Ms) for uniform K2 and Ms
+    PairCoef pc;   // region (0,0) exchange / DMI coefficients
 };
 
 struct LocalArgs {
@@ -85,6 +86,19 @@ __global__ void k_local_consts(LocalArgs a, LocalConsts* out) {
     c.u[0] = fm(il, u.x); c.u[1] = fm(il, u.y); c.u[2] = fm(il, u.z);
     c.f1k = fm(2.0f, fm(a.up.K1_mul, c.inv_ms));
     c.f2k = fm(4.0f, fm(a.up.K2_mul, c.inv_ms));
+    const float A = a.aLUT[0];
+    c.pc.wax = fm(a.wx, A);
+    c.pc.way = fm(a.wy, A);
+    c.pc.waz = fm(a.wz, A);
+    const float D = a.dLUT ? a.dLUT[0] : 0.0f;
+    c.pc.sx = fd(fm(2.0f, A), fm(a.cx, a.cx));
+    c.pc.sy = fd(fm(2.0f, A), fm(a.cy, a.cy));
+    c.pc.sz = fd(fm(2.0f, A), fm(a.cz, a.cz));
+    c.pc.dcx = fd(D, a.cx);
+    c.pc.dcy = fd(D, a.cy);
+    const float t = fd(fm(0.5f, D), A);
+    c.pc.qx = fm(a.cx, t);
+    c.pc.qy = fm(a.cy, t);
     *out = c;
 }
 
@@ -114,6 +128,9 @@ __device__ __forceinline__ f3 lltorque_g(f3 m, f3 H, float alpha, float gilb) {
 
 // engine/effectivefield.go:14-24 + engine/torque.go:135-144 for one cell:
 // B = demag; B += exchange(+DMI)/Ms; B += anisotropy; B += B_ext; torque.
+// UREG: every cell is in region 0 (no region map), so the region-pair
+// coefficients are scalars and no region is loaded.
+template <bool UREG>
 __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
     if (!a.ctl->active) return;
     int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -128,9 +145,15 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
     if (a.bd) B = f3{__ldg(a.bd + I), __ldg(a.bd + N + I), __ldg(a.bd + 2 * N + I)};
     f3 m0 = ld3(mx, my, mz, I);
     if (!is0(m0)) {
-        int r0 = __ldg(a.regions + I);
-        f3 e = a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
-                     : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
+        f3 e;
+        if constexpr (UREG) {
+            e = a.dmi ? dmi_sum_u(mx, my, mz, a.kc.pc, a.g, a.openbc != 0, ix, iy, iz, m0)
+                      : exchange_sum_u(mx, my, mz, a.kc.pc, a.g, ix, iy, iz, m0);
+        } else {
+            int r0 = __ldg(a.regions + I);
+            e = a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
+                      : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
+        }
         float inv = a.ms_uniform ? a.kc.inv_ms : inv_msat(a.Ms, a.Ms_mul, I);
         B.x = fa(B.x, fm(e.x, inv));
         B.y = fa(B.y, fm(e.y, inv));
@@ -150,7 +173,7 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
         }
     }
     if (a.zeeman) {
-        int r = __ldg(a.regions + I);
+        const int r = UREG ? 0 : __ldg(a.regions + I);
         B.x = fa(B.x, __ldg(a.bext[0] + r));
         B.y = fa(B.y, __ldg(a.bext[1] + r));
         B.z = fa(B.z, __ldg(a.bext[2] + r));
@@ -441,7 +464,8 @@ static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, flo
     la.tau_direct = tau_direct;
     la.beff = beff;
     dim3 blk(32, 8, 1), grd((s->g.Nx + 31) / 32, (s->g.Ny + 7) / 8, s->g.Nz);
-    k_local_torque<<<grd, blk, 0, S()>>>(la);
+    if (s->zero_regions) k_local_torque<true><<<grd, blk, 0, S()>>>(la);
+    else k_local_torque<false><<<grd, blk, 0, S()>>>(la);
     UMAG_LAUNCH_CHECK();
     if (nl) *nl += 1;
     return UMAG_OK;

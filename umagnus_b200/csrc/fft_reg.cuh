@@ -1,0 +1,129 @@
+// fft_reg.cuh -- register-blocked Stockham FFT for power-of-two lengths.
+//
+// A line of length L is held by T = L/8 threads, thread t owning the eight
+// elements {t + T*m : m = 0..7} in registers.  Every Stockham stage reads
+// exactly that element set (for any radix R dividing 8, butterfly
+// j = t + T*i uses elements j + r*L/R = t + T*(i + r*8/R)), so a stage is:
+// butterflies in registers, then -- except after the last stage -- write the
+// outputs to their Stockham positions in a padded shared-memory line and read
+// the thread's set back.  The last stage's outputs land on the thread's own
+// set (natural order X[t + T*m]), so a pointwise operation between a forward
+// and an inverse transform needs no exchange, and the inverse is the forward
+// transform of the conjugate.  Loads of zero padding and stores of discarded
+// outputs disappear at compile time when the caller passes literal zeros /
+// ignores elements.  Radices 8, then 4 or 2 for the remaining power of two.
+#pragma once
+#include "fft.cuh"
+
+namespace umag {
+
+constexpr int rg_log2(int L) { return L <= 1 ? 0 : 1 + rg_log2(L / 2); }
+constexpr int rg_nst(int L) { return (rg_log2(L) + 2) / 3; }
+// radix of stage s: 8 except a final 4 or 2 when log2(L) is not a multiple of 3
+constexpr int rg_radix(int L, int s) {
+    return (s < rg_log2(L) / 3) ? 8 : (rg_log2(L) % 3 == 1 ? 2 : 4);
+}
+constexpr bool rg_ok(int L) { return L >= 8 && (L & (L - 1)) == 0; }
+// padded shared-memory index: one slot of padding after every 2^PS elements
+// (PS = 3 when threads of several lines share a warp, 4 for one line per
+// warp: the choices with the fewest 8-byte bank conflicts for these access
+// patterns)
+template <int PS> __host__ __device__ constexpr int rg_pad(int i) { return i + (i >> PS); }
+// exchange-line stride: padded length rounded up to 4 (mod 16) 8-byte slots,
+// so lines accessed by neighbouring threads start in different banks
+template <int L, int PS = 3> __host__ __device__ constexpr int rg_line() {
+    return ((rg_pad<PS>(L - 1) + 1 + 11) / 16) * 16 + 4;
+}
+
+template <int DIR> __device__ __forceinline__ float2 rg_tw(const float2* __restrict__ tw, int e) {
+    float2 w = tw[e];
+    if (DIR > 0) w.y = -w.y;
+    return w;
+}
+
+// Barrier between exchange phases: the whole CTA, or only the warp when all
+// threads sharing the exchange lines belong to one warp.
+template <bool WARP> __device__ __forceinline__ void rg_sync() {
+    if constexpr (WARP) __syncwarp();
+    else __syncthreads();
+}
+
+// One stage for NC lines held by this thread (v[c][m] = element t + T*m of
+// line c).  ex + c*exs is the padded exchange line of component c.
+template <int L, int NC, int DIR, int ST, int NS, bool WARP = false, int PS = 3>
+__device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, int exs,
+                                         const float2* __restrict__ tw) {
+    if constexpr (ST < rg_nst(L)) {
+        constexpr int R = rg_radix(L, ST);
+        constexpr int NB = 8 / R;          // butterflies per thread
+        constexpr int T = L / 8;
+        constexpr int TWS = L / (NS * R);
+        constexpr bool last = (ST + 1 == rg_nst(L));
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            const int j = t + T * i;
+            const int k = j % NS;
+            // twiddles are shared by the NC lines: read them once
+            float2 w[R];
+            if constexpr (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) w[r] = rg_tw<DIR>(tw, r * k * TWS);
+            }
+#pragma unroll
+            for (int c = 0; c < NC; c++) {
+                float2 u[R];
+#pragma unroll
+                for (int r = 0; r < R; r++) u[r] = v[c][i + r * NB];
+                if constexpr (NS > 1) {
+#pragma unroll
+                    for (int r = 1; r < R; r++) u[r] = cmul(u[r], w[r]);
+                }
+                if constexpr (R == 2) dft2(u);
+                else if constexpr (R == 4) dft4(u, DIR);
+                else dft8<float>(u, DIR);
+                if constexpr (last) {
+#pragma unroll
+                    for (int q = 0; q < R; q++) v[c][i + q * NB] = u[q];
+                } else {
+                    const int o = (j / NS) * NS * R + k;
+                    if constexpr (NS % (1 << PS) == 0) {  // pad(o + q*NS) = pad(o) + q*pad(NS)
+                        float2* base = ex + c * exs + rg_pad<PS>(o);
+#pragma unroll
+                        for (int q = 0; q < R; q++) base[q * (NS + (NS >> PS))] = u[q];
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < R; q++) ex[c * exs + rg_pad<PS>(o + q * NS)] = u[q];
+                    }
+                }
+            }
+        }
+        if constexpr (!last) {
+            rg_sync<WARP>();
+            if constexpr (T % (1 << PS) == 0) {  // pad(t + T*m) = pad(t) + m*pad(T)
+                const float2* base = ex + rg_pad<PS>(t);
+#pragma unroll
+                for (int c = 0; c < NC; c++)
+#pragma unroll
+                    for (int m = 0; m < 8; m++) v[c][m] = base[c * exs + m * (T + (T >> PS))];
+            } else {
+#pragma unroll
+                for (int c = 0; c < NC; c++)
+#pragma unroll
+                    for (int m = 0; m < 8; m++) v[c][m] = ex[c * exs + rg_pad<PS>(t + T * m)];
+            }
+            rg_sync<WARP>();
+            rg_stage<L, NC, DIR, ST + 1, NS * R, WARP, PS>(v, t, ex, exs, tw);
+        }
+    }
+}
+
+// Unnormalised forward FFT (DIR = -1) of NC lines.  All threads that share
+// the exchange lines must call it: the whole CTA, or (WARP = true) one warp.
+template <int L, int NC, bool WARP = false, int PS = 3>
+__device__ __forceinline__ void rg_fft_fwd(float2 (&v)[NC][8], int t, float2* ex, int exs,
+                                           const float2* __restrict__ tw) {
+    static_assert(rg_ok(L), "register FFT needs a power-of-two length >= 8");
+    rg_stage<L, NC, -1, 0, 1, WARP, PS>(v, t, ex, exs, tw);
+}
+
+}  // namespace umag

@@ -46,7 +46,7 @@ static int noalloc_scratch(void** out) {
 
 // twiddles exp(-2 pi i j / L) of the four tables, evaluated in FP64 on the device
 __global__ void k_noalloc_twiddles(float2* tw, int M, int Py, int Pz, int Px) {
-    const int n = M + Py + Pz + (M / 2 + 1);
+    const int n = M + Py + Pz + M;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         int j = e, L = M;
         if (j >= M) {
@@ -88,9 +88,9 @@ extern "C" __attribute__((visibility("default"))) int umag_demag_exec_noalloc(
         return set_error(UMAG_E_UNSUPPORTED, "mesh %dx%dx%d has no compile-time FFT plan (no-alloc path)", Nx, Ny, Nz);
     d.use_fast = true;
     d.WB = d.fast.wb;
-    // scratch layout: spectrum | tw(M) | tw(Py) | tw(Pz) | exp(-2 pi i k/Px), k <= M/2
+    // scratch layout: spectrum | tw(M) | tw(Py) | tw(Pz) | exp(-2 pi i k/Px), k < M
     const size_t spec = (size_t)3 * d.P[2] * Ny * d.Lx;
-    const size_t ntw = (size_t)d.M + d.P[1] + d.P[2] + (d.M / 2 + 1);
+    const size_t ntw = (size_t)d.M + d.P[1] + d.P[2] + d.M;
     const size_t need = sizeof(float2) * (spec + ntw);
     if (need > kNoallocScratchBytes)
         return set_error(UMAG_E_UNSUPPORTED, "mesh %dx%dx%d needs %zu bytes of scratch, the no-alloc limit is %zu",
@@ -115,6 +115,7 @@ extern "C" __attribute__((visibility("default"))) int umag_demag_exec_noalloc(
     a.twr = tw + d.M + d.P[1] + d.P[2];
     a.spec = sp;
     for (int c = 0; c < 6; c++) a.K[c] = K[c];
+    a.Kp = d.Hx;  // caller's spectrum: reference layout, rows of Px/2+1 floats
     if (d.is2d) a.K[3] = a.K[4] = nullptr;
     a.m[0] = mx; a.m[1] = my; a.m[2] = mz;
     a.B[0] = Bx; a.B[1] = By; a.B[2] = Bz;

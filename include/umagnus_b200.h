@@ -143,6 +143,14 @@ int umag_demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[
 int umag_demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float* mx,
                     const float* my, const float* mz, const float* vol, const float* Ms,
                     float Ms_mul);
+/* One of the three passes of umag_demag_exec, for timing them one by one:
+ * 0 = x/z forward transforms of MU0*Ms*vol*m into the plan's spectrum,
+ * 1 = y transform, kernel multiply and inverse y transform in place,
+ * 2 = inverse z/x transforms of the spectrum into B.  Running 0, 1, 2 in
+ * order equals umag_demag_exec.  No counterpart in the reference. */
+int umag_demag_exec_pass(umag_demag* d, int pass, float* Bx, float* By, float* Bz,
+                         const float* mx, const float* my, const float* mz, const float* vol,
+                         const float* Ms, float Ms_mul);
 /* Copies the stored float32 kernel spectrum (6 arrays of (Px/2+1)(Py/2+1)(Pz/2+1),
  * reference layout kernmulrsymm3d.cl) to host arrays; for tests. */
 int umag_demag_get_spectrum(umag_demag* d, float* const host[6]);

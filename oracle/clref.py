@@ -25,6 +25,11 @@ def lib():
     return _lib
 
 
+def set_threads(n):
+    """Spread every later kernel call over n host threads (1 = in order)."""
+    lib().clref_set_threads(ctypes.c_int(int(n)))
+
+
 def _sfx(dt):
     return "f32" if np.dtype(dt) == np.float32 else "f64"
 

@@ -15,6 +15,8 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <thread>
+#include <vector>
 
 #define __kernel
 #define __global
@@ -71,21 +73,41 @@ static inline size_t get_local_size(int d) { return clshim_cur.lsize[d]; }
 static inline size_t get_group_id(int d) { return clshim_cur.grp[d]; }
 static inline size_t get_num_groups(int d) { return clshim_cur.gsize[d] / clshim_cur.lsize[d]; }
 
+// Host threads an NDRange is spread over (clref_set_threads); 1 = in order.
+extern int clshim_nthreads;
+
 // Runs body once per work-item of an NDRange with global size g and local
-// size l (g a multiple of l in every dimension), in order.
+// size l (g a multiple of l in every dimension).  With clshim_nthreads > 1
+// the linear work-item range is cut into one contiguous chunk per thread:
+// valid for the wrapped kernels, which have no barriers and write only the
+// elements of their own work-item.
 template <class F>
 static void clshim_ndrange(const size_t g[3], const size_t l[3], F body) {
-    for (size_t z = 0; z < g[2]; z++)
-        for (size_t y = 0; y < g[1]; y++)
-            for (size_t x = 0; x < g[0]; x++) {
-                size_t p[3] = {x, y, z};
-                for (int d = 0; d < 3; d++) {
-                    clshim_cur.gid[d] = p[d];
-                    clshim_cur.gsize[d] = g[d];
-                    clshim_cur.lsize[d] = l[d];
-                    clshim_cur.lid[d] = p[d] % l[d];
-                    clshim_cur.grp[d] = p[d] / l[d];
-                }
-                body();
+    const size_t total = g[0] * g[1] * g[2];
+    auto run = [&](size_t b, size_t e) {
+        for (size_t i = b; i < e; i++) {
+            const size_t p[3] = {i % g[0], (i / g[0]) % g[1], i / (g[0] * g[1])};
+            for (int d = 0; d < 3; d++) {
+                clshim_cur.gid[d] = p[d];
+                clshim_cur.gsize[d] = g[d];
+                clshim_cur.lsize[d] = l[d];
+                clshim_cur.lid[d] = p[d] % l[d];
+                clshim_cur.grp[d] = p[d] / l[d];
             }
+            body();
+        }
+    };
+    const int nt = clshim_nthreads;
+    if (nt <= 1 || total < 8192) {
+        run(0, total);
+        return;
+    }
+    const size_t chunk = (total + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) {
+        const size_t b = t * chunk, e = b + chunk < total ? b + chunk : total;
+        if (b < e) th.emplace_back(run, b, e);
+    }
+    run(0, chunk < total ? chunk : total);
+    for (auto& t : th) t.join();
 }

@@ -70,6 +70,7 @@ _SIGS = {
                               ctypes.POINTER(c_void_p)],
     "umag_demag_new_from_kernel": [c_int, c_int, c_int, P, ctypes.POINTER(c_void_p)],
     "umag_demag_exec": [P, P, P, P, P, P, P, P, P, c_float],
+    "umag_demag_exec_pass": [P, c_int, P, P, P, P, P, P, P, P, c_float],
     "umag_demag_get_spectrum": [P, P], "umag_demag_get_kernel": [P, P],
     "umag_demag_padded_size": [P, ctypes.POINTER(c_int)], "umag_demag_free": [P],
     "umag_demag_exec_noalloc": [c_int, c_int, c_int, P, P, P, P, P, P, P, P, P, c_float, P],

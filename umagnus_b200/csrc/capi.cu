@@ -127,6 +127,12 @@ int umag_demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float*
     UMAG_TRY(ensure_init());
     return demag_exec(d, Bx, By, Bz, mx, my, mz, vol, Ms, Ms_mul);
 }
+int umag_demag_exec_pass(umag_demag* d, int pass, float* Bx, float* By, float* Bz, const float* mx, const float* my,
+                         const float* mz, const float* vol, const float* Ms, float Ms_mul) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(pass >= 0 && pass <= 2, "pass must be 0, 1 or 2");
+    return demag_exec(d, Bx, By, Bz, mx, my, mz, vol, Ms, Ms_mul, pass);
+}
 int umag_demag_get_spectrum(umag_demag* d, float* const host[6]) { return demag_get_spectrum(d, host); }
 int umag_demag_get_kernel(umag_demag* d, double* const host[6]) { return demag_get_kernel(d, host); }
 int umag_demag_padded_size(umag_demag* d, int P[3]) {

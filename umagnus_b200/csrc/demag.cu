@@ -175,14 +175,24 @@ __global__ void k_real_to_cplx(const double* src, double2* dst, long n) {
 }
 
 // Real parts of the non-redundant block, scaled, rows of pitch Kp (the pad
-// columns are zero); max |imag| into *maximg.
-__global__ void k_extract_spectrum(const double2* a, float* out, int Px, int Py, int Pz, int Kp, double scale,
-                                   unsigned long long* maximg) {
+// columns are zero) or, when blocked, 4-column blocks [z][x/4][y][x%4];
+// max |imag| into *maximg.
+__global__ void k_extract_spectrum(const double2* a, float* out, int Px, int Py, int Pz, int Kp, int blocked,
+                                   double scale, unsigned long long* maximg) {
     int hx = Px / 2 + 1, hy = Py / 2 + 1, hz = Pz / 2 + 1;
     long n = (long)Kp * hy * hz;
     double mi = 0.0;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        int x = (int)(i % Kp), y = (int)((i / Kp) % hy), z = (int)(i / ((long)Kp * hy));
+        int x, y, z;
+        if (blocked) {
+            const long q = i >> 2;
+            y = (int)(q % hy);
+            const long zb = q / hy;
+            x = (int)(zb % (Kp >> 2)) * 4 + (int)(i & 3);
+            z = (int)(zb / (Kp >> 2));
+        } else {
+            x = (int)(i % Kp); y = (int)((i / Kp) % hy); z = (int)(i / ((long)Kp * hy));
+        }
         if (x >= hx) { out[i] = 0.f; continue; }
         double2 v = a[((long)z * Py + y) * Px + x];
         out[i] = (float)(v.x * scale);
@@ -458,6 +468,7 @@ static int plan_common(umag_demag* d) {
     UMAG_CUDA(cudaFuncSetAttribute(k_fft_axis<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
     UMAG_TRY(demag_fast_setup());
     d->use_fast = getenv("UMAG_GENERIC_FFT") == nullptr && demag_fast_select(d->M, d->P[1], d->P[2], d->fast);
+    if (d->use_fast) UMAG_TRY(demag_fast_grid(d->fast, d->M, d->P[2]));
     return UMAG_OK;
 }
 
@@ -496,6 +507,7 @@ static int kernel_to_spectrum(umag_demag* d, double* const Kr[6], cudaStream_t s
         cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), st);
         long kn = (long)d->Kn;
         k_extract_spectrum<<<grid_for(kn, threads), threads, 0, st>>>(buf, d->K[c], Px, Py, Pz, d->Kp,
+                                                                       d->use_fast && d->fast.blocked ? 1 : 0,
                                                                        1.0 / (double)n, dmax);
         unsigned long long hm = 0;
         cudaMemcpyAsync(&hm, dmax, sizeof(hm), cudaMemcpyDeviceToHost, st);
@@ -621,14 +633,26 @@ int demag_get_kernel(umag_demag* d, double* const host[6]) {
 int demag_get_spectrum(umag_demag* d, float* const host[6]) {
     UMAG_REQUIRE(d != nullptr, "NULL plan");
     UMAG_CUDA(cudaStreamSynchronize(ctx().stream));
+    const size_t hy = d->P[1] / 2 + 1, rows = d->Kn / d->Kp;  // rows = hy * hz
+    const bool blocked = d->use_fast && d->fast.blocked;
+    std::vector<float> tmp(blocked ? d->Kn : 0);
     for (int c = 0; c < 6; c++) {
         if (!host[c]) continue;
-        // reference layout: rows of Px/2+1 floats (the device rows are padded to Kp)
-        const size_t rows = d->Kn / d->Kp;
-        if (d->K[c])
+        if (!d->K[c]) {
+            memset(host[c], 0, sizeof(float) * d->Hx * rows);
+        } else if (!blocked) {
+            // reference layout: rows of Px/2+1 floats (the device rows are padded to Kp)
             UMAG_CUDA(cudaMemcpy2D(host[c], sizeof(float) * d->Hx, d->K[c], sizeof(float) * d->Kp,
                                    sizeof(float) * d->Hx, rows, cudaMemcpyDeviceToHost));
-        else memset(host[c], 0, sizeof(float) * d->Hx * rows);
+        } else {
+            UMAG_CUDA(cudaMemcpy(tmp.data(), d->K[c], sizeof(float) * d->Kn, cudaMemcpyDeviceToHost));
+            const size_t nb = d->Kp / 4;
+            for (size_t r = 0; r < rows; r++) {  // r = z * hy + y
+                const size_t z = r / hy, y = r % hy;
+                for (int x = 0; x < d->Hx; x++)
+                    host[c][r * d->Hx + x] = tmp[((z * nb + x / 4) * hy + y) * 4 + x % 4];
+            }
+        }
     }
     return UMAG_OK;
 }
@@ -642,6 +666,8 @@ void fill_pass_args(const umag_demag* d, PassArgs& a) {
     a.spec = d->spec;
     for (int c = 0; c < 6; c++) a.K[c] = d->K[c];
     a.Kp = d->Kp;
+    a.blocked = d->use_fast && d->fast.blocked ? 1 : 0;
+    a.Kblocked = a.blocked;
 }
 
 int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st) {
@@ -649,7 +675,7 @@ int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st) {
         const FastPasses& f = d->fast;
         f.a<<<dim3(d->N[1], 3), f.nt_ac, f.smem_ac, st>>>(a);
         UMAG_LAUNCH_CHECK();
-        f.b<<<dim3((d->Hx + f.wb - 1) / f.wb, d->P[2]), f.nt_b, f.smem_b, st>>>(a);
+        f.b<<<dim3(f.gbx, f.gby), f.nt_b, f.smem_b, st>>>(a);
         UMAG_LAUNCH_CHECK();
         f.c<<<dim3(d->N[1], 3), f.nt_ac, f.smem_ac, st>>>(a);
         UMAG_LAUNCH_CHECK();
@@ -665,15 +691,34 @@ int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st) {
     return UMAG_OK;
 }
 
+// one pass of demag_launch (0: A, 1: B, 2: C)
+static int demag_launch_pass(const umag_demag* d, const PassArgs& a, cudaStream_t st, int pass) {
+    if (d->use_fast) {
+        const FastPasses& f = d->fast;
+        if (pass == 0) f.a<<<dim3(d->N[1], 3), f.nt_ac, f.smem_ac, st>>>(a);
+        else if (pass == 1) f.b<<<dim3(f.gbx, f.gby), f.nt_b, f.smem_b, st>>>(a);
+        else f.c<<<dim3(d->N[1], 3), f.nt_ac, f.smem_ac, st>>>(a);
+    } else {
+        size_t sac = pass_ac_smem(d), sb = pass_b_smem(d);
+        if (pass == 0) k_pass_a<<<dim3(d->N[1], 3), kPassThreads, sac, st>>>(a);
+        else if (pass == 1) k_pass_b<<<dim3((d->Hx + d->WB - 1) / d->WB, d->P[2]), kPassBThreads, sb, st>>>(a);
+        else k_pass_c<<<dim3(d->N[1], 3), kPassThreads, sac, st>>>(a);
+    }
+    UMAG_LAUNCH_CHECK();
+    return UMAG_OK;
+}
+
 int demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
-               const float* vol, const float* Ms, float Ms_mul) {
+               const float* vol, const float* Ms, float Ms_mul, int pass) {
     UMAG_REQUIRE(d != nullptr, "NULL plan");
     UMAG_REQUIRE(Bx && By && Bz && mx && my && mz, "NULL field or magnetisation pointer");
+    UMAG_REQUIRE(pass >= -1 && pass <= 2, "pass must be -1 (all), 0, 1 or 2");
     PassArgs a{};
     fill_pass_args(d, a);
     a.m[0] = mx; a.m[1] = my; a.m[2] = mz;
     a.B[0] = Bx; a.B[1] = By; a.B[2] = Bz;
     a.vol = vol; a.Ms = Ms; a.Ms_mul = Ms_mul;
+    if (pass >= 0) return demag_launch_pass(d, a, ctx().stream, pass);
     return demag_launch(d, a, ctx().stream);
 }
 

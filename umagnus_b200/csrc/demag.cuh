@@ -20,6 +20,11 @@ struct FastPasses {
     int wb = 0;
     int nt_b = 512;   // threads per pass-B CTA
     int nt_ac = 256;  // threads per pass-A/C CTA
+    bool ac_reg = false, b_reg = false;  // register-FFT kernels (k_reg_a/c, k_reg_b)
+    // spectrum stored in blocks of 4 columns, [c][kz][kx/4][y][kx%4], so that
+    // pass B's column reads and writes are contiguous (set when ac_reg && b_reg)
+    bool blocked = false;
+    unsigned gbx = 0, gby = 0;  // pass-B grid (demag_fast_grid)
 };
 }  // namespace umag
 
@@ -49,6 +54,10 @@ struct PassArgs {
     float2* spec;
     const float* K[6];
     int Kp;  // row pitch (floats) of the kernel arrays: Hx padded to 4 in plans, Hx for caller-owned spectra
+    // layouts: blocked = spectrum in 4-column blocks [c][kz][kx/4][y][kx%4]
+    // (else rows [c][kz][y][kx]); Kblocked = kernel arrays in 4-column blocks
+    // [kz][kx/4][ky][kx%4] (else rows [kz][ky][kx] of pitch Kp)
+    int blocked, Kblocked;
     const float* m[3];
     // engine use: magnetisation read through a device-side slot
     // (m_sel ? *m_ind_w : *m_ind) + c*ncell, and a device flag that turns a
@@ -68,13 +77,15 @@ int demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double
                      int zero_self, umag_demag** out);
 int demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6], umag_demag** out);
 int demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
-               const float* vol, const float* Ms, float Ms_mul);
+               const float* vol, const float* Ms, float Ms_mul, int pass = -1);
 int demag_get_kernel(umag_demag* d, double* const host[6]);
 int demag_get_spectrum(umag_demag* d, float* const host[6]);
 void demag_free(umag_demag* d);
 void fill_pass_args(const umag_demag* d, PassArgs& a);
 int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st);
 bool demag_fast_select(int M, int Py, int Pz, FastPasses& f);
+// pass-B launch grid for a selected plan (after demag_fast_setup; current device)
+int demag_fast_grid(FastPasses& f, int M, int Pz);
 int demag_fast_setup();
 
 }  // namespace umag

@@ -249,10 +249,40 @@ __global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) {
     }
 }
 
+// cp.async (global -> shared, asynchronous) helpers
+__device__ __forceinline__ void cpa16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src));
+}
+__device__ __forceinline__ void cpa8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src));
+}
+__device__ __forceinline__ void cpa4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src));
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// Offset of spectrum column kx within one (component, kz, y = 0) plane, and
+// the stride between rows y: blocked layout [kx/4][y][kx%4] or rows [y][kx].
+__device__ __forceinline__ long spec_col(const PassArgs& a, int kx) {
+    return a.blocked ? (long)(kx >> 2) * (a.Ny * 4) + (kx & 3) : (long)kx;
+}
+__device__ __forceinline__ long spec_rowstride(const PassArgs& a) { return a.blocked ? 4 : a.Lx; }
+// Index of kernel element (kz, ky, kx), kz/ky in the stored non-redundant block
+__device__ __forceinline__ long kern_idx(const PassArgs& a, int kz, int ky, int kx, int hy) {
+    return a.Kblocked ? (((long)kz * (a.Kp >> 2) + (kx >> 2)) * hy + ky) * 4 + (kx & 3)
+                      : ((long)kz * hy + ky) * a.Kp + kx;
+}
+
 // Pass B with the register-blocked FFT (power-of-two Py): thread (t, w) holds
 // rows t + T*m (m < 8) of column kx0 + w for all three components.  Rows
 // y >= Ny are zero padding (m >= 4): the loads are skipped and the first
 // butterflies fold; only rows y < Ny are computed by the inverse and stored.
+// With the blocked layouts a warp's loads and stores of one component are one
+// contiguous run (WB = 4: 8 rows x 4 columns = 256 bytes).
 template <int PY, int WB>
 __global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
     constexpr int T = PY / 8, NT = T * WB, NY = PY / 2, HY = PY / 2 + 1;
@@ -275,19 +305,17 @@ __global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
     const bool k3d = a.K[3] != nullptr;
     {
         const int ncomp = k3d ? 6 : 4;
-        const long kbase = (long)kzm * HY * a.Kp + kx0;
         bool wide = false;
         if constexpr (WB % 4 == 0) {
-            // 16-byte rows (plan layout: pitch padded to 4 floats, pad columns zero)
+            // 16-byte pieces of 4 columns: plan layouts (pitch padded to 4
+            // floats, pad columns zero); blocked pieces are consecutive in ky
             wide = a.Kp % 4 == 0 && kx0 + WB <= a.Kp;
             if (wide) {
                 constexpr int CH = WB / 4;
                 for (int e = tid; e < ncomp * HY * CH; e += NT) {
                     const int cc = e / (HY * CH), r = e % (HY * CH), ky = r / CH, ch = r % CH;
                     const int comp = k3d ? cc : (cc == 3 ? 5 : cc);  // 2D stores xx yy zz xy
-                    const float* src = a.K[comp] + kbase + (long)ky * a.Kp + 4 * ch;
-                    const unsigned d = (unsigned)__cvta_generic_to_shared(Ks + comp * HY * WB + ky * WB + 4 * ch);
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+                    cpa16(Ks + comp * HY * WB + ky * WB + 4 * ch, a.K[comp] + kern_idx(a, kzm, ky, kx0 + 4 * ch, HY));
                 }
             }
         }
@@ -296,33 +324,28 @@ __global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
                 const int cc = e / (HY * WB), r = e % (HY * WB), ky = r / WB, ww = r % WB;
                 const int comp = k3d ? cc : (cc == 3 ? 5 : cc);
                 float* dst = Ks + comp * HY * WB + ky * WB + ww;
-                if (kx0 + ww < hx) {
-                    const float* src = a.K[comp] + kbase + (long)ky * a.Kp + ww;
-                    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
-                } else {
-                    *dst = 0.f;
-                }
+                if (kx0 + ww < hx) cpa4(dst, a.K[comp] + kern_idx(a, kzm, ky, kx0 + ww, HY));
+                else *dst = 0.f;
             }
         }
-        asm volatile("cp.async.commit_group;\n" ::);
+        cpa_commit();
     }
     const bool col = kx < hx;
-    const long cs = (long)Pz * NY * a.Lx;
-    const float2* in = a.spec + (long)kz * NY * a.Lx + kx;
+    const long cs = (long)Pz * NY * a.Lx, rs = spec_rowstride(a);
+    const float2* in = a.spec + (long)kz * NY * a.Lx + spec_col(a, kx);
     float2 v[3][8];
 #pragma unroll
     for (int c = 0; c < 3; c++)
 #pragma unroll
         for (int m = 0; m < 8; m++) {
             const int y = t + T * m;
-            v[c][m] = (m < 4 && col) ? in[c * cs + (long)y * a.Lx] : make_float2(0.f, 0.f);
+            v[c][m] = (m < 4 && col) ? in[c * cs + y * rs] : make_float2(0.f, 0.f);
         }
     __syncthreads();  // twiddles
     float2* exl = ex + w * LP;
     const int exs = WB * LP;
     rg_fft_fwd<PY, 3>(v, t, exl, exs, tw);
-    asm volatile("cp.async.wait_group 0;\n" ::);
+    cpa_wait_all();
     __syncthreads();
     // kernel multiply (kernmulrsymm3d.cl:41-90), mirrored into the stored block
 #pragma unroll
@@ -347,13 +370,13 @@ __global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
     }
     rg_fft_fwd<PY, 3>(v, t, exl, exs, tw);
     if (col) {
-        float2* out = a.spec + (long)kz * NY * a.Lx + kx;
+        float2* out = a.spec + (long)kz * NY * a.Lx + spec_col(a, kx);
 #pragma unroll
         for (int c = 0; c < 3; c++)
 #pragma unroll
             for (int m = 0; m < 4; m++) {
                 const int y = t + T * m;
-                out[c * cs + (long)y * a.Lx] = make_float2(v[c][m].x, -v[c][m].y);
+                out[c * cs + y * rs] = make_float2(v[c][m].x, -v[c][m].y);
             }
     }
 }
@@ -374,7 +397,6 @@ template <int M, int PZ>
 __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) {
     using S = RegAC<M, PZ>;
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
-    constexpr int HX = M + 1;
     extern __shared__ __align__(16) float2 sm[];
     float2* twx = sm;          // M
     float2* twz = twx + M;     // PZ
@@ -429,23 +451,55 @@ __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) {
         if (k == 0) xrow[M] = make_float2(A.x - A.y, 0.f);  // Nyquist: Re Z0 - Im Z0
     }
     __syncthreads();
-    // z phase: column kx, TZ lanes, rows z = tz + TZ*j (zero padding for j >= 4)
-    float2* out = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
+    // z phase: column kx, TZ lanes, rows z = tz + TZ*j (zero padding for j >= 4).
+    // The DC and Nyquist columns are real in z, so they share one complex
+    // transform (x0 + i xM), split afterwards by Hermitian symmetry:
+    // X0[k] = (P[k] + conj P[-k]) / 2, XM[k] = (P[k] - conj P[-k]) / 2i.
+    // The M - 1 other columns then fill exactly M / CPR = 2 rounds.
+    static_assert(M == 2 * CPR, "z rounds: M columns over CPR column groups");
+    float2* out = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
     const long kzs = (long)Ny * a.Lx;
     const int tz = tid % TZ, cl = tid / TZ;
     float2* exz = ex + cl * S::LZ;
-#pragma unroll 1
-    for (int kx0 = 0; kx0 < HX; kx0 += CPR) {
-        const int kx = kx0 + cl;
-        const bool act = kx < HX;
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int kx = r * CPR + cl;
+        const bool pk = kx == 0;
         float2 u[1][8];
 #pragma unroll
-        for (int j = 0; j < 8; j++) u[0][j] = (j < 4 && act) ? Xs[(tz + TZ * j) * XP + kx] : make_float2(0.f, 0.f);
-        rg_fft_fwd<PZ, 1, true>(u, tz, exz, 0, twz);
-        if (act) {
-#pragma unroll
-            for (int j = 0; j < 8; j++) out[(tz + TZ * j) * kzs + kx] = u[0][j];
+        for (int j = 0; j < 8; j++) {
+            float2 q = make_float2(0.f, 0.f);
+            if (j < 4) {
+                q = Xs[(tz + TZ * j) * XP + kx];
+                if (pk) q.y = Xs[(tz + TZ * j) * XP + M].x;
+            }
+            u[0][j] = q;
         }
+        rg_fft_fwd<PZ, 1, true>(u, tz, exz, 0, twz);
+        if (r == 0 && tid < 32) {  // the warp holding column group 0
+            const int pl = (lane & ~(TZ - 1)) | ((TZ - tz) & (TZ - 1));
+            float2 pr[8];
+#pragma unroll
+            for (int s = 0; s < 8; s++) {
+                float2 q;
+                q.x = __shfl_sync(0xffffffffu, u[0][s].x, pl);
+                q.y = __shfl_sync(0xffffffffu, u[0][s].y, pl);
+                if (tz != 0) pr[7 - s] = q;
+                else pr[(8 - s) & 7] = q;
+            }
+            if (pk) {
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const float2 P = u[0][j], Q = pr[j];
+                    out[(tz + TZ * j) * kzs] = make_float2(0.5f * (P.x + Q.x), 0.5f * (P.y - Q.y));
+                    out[(tz + TZ * j) * kzs + spec_col(a, M)] = make_float2(0.5f * (P.y + Q.y), -0.5f * (P.x - Q.x));
+                }
+                continue;
+            }
+        }
+        const long ko = spec_col(a, kx);
+#pragma unroll
+        for (int j = 0; j < 8; j++) out[(tz + TZ * j) * kzs + ko] = u[0][j];
     }
 }
 
@@ -453,7 +507,6 @@ template <int M, int PZ>
 __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) {
     using S = RegAC<M, PZ>;
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
-    constexpr int HX = M + 1;
     extern __shared__ __align__(16) float2 sm[];
     float2* twx = sm;
     float2* twz = twx + M;
@@ -466,25 +519,43 @@ __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) {
     for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
     __syncthreads();
     const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
-    const float2* in = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
+    const float2* in = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
     const long kzs = (long)Ny * a.Lx;
-    // z phase: inverse transform (conjugate trick) of every column, keep z < NZ
+    // z phase: inverse transform (conjugate trick) of every column, keep z < NZ.
+    // The DC and Nyquist columns invert to real sequences, so they share one
+    // transform of G0 + i GM (real part -> column 0, imaginary -> column M);
+    // the other columns fill exactly two rounds, whose loads are all issued
+    // before the first transform.
+    static_assert(M == 2 * CPR, "z rounds: M columns over CPR column groups");
     const int tz = tid % TZ, cl = tid / TZ;
     float2* exz = ex + cl * S::LZ;
-#pragma unroll 1
-    for (int kx0 = 0; kx0 < HX; kx0 += CPR) {
-        const int kx = kx0 + cl;
-        const bool act = kx < HX;
-        float2 u[1][8];
+    float2 u[2][1][8];
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const long ko = spec_col(a, r * CPR + cl), kM = spec_col(a, M);
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-            float2 q = act ? in[(tz + TZ * j) * kzs + kx] : make_float2(0.f, 0.f);
-            u[0][j] = make_float2(q.x, -q.y);
+            float2 q = in[(tz + TZ * j) * kzs + ko];
+            if (r == 0 && cl == 0) {
+                const float2 g = in[(tz + TZ * j) * kzs + kM];
+                q = make_float2(q.x - g.y, q.y + g.x);
+            }
+            u[r][0][j] = make_float2(q.x, -q.y);
         }
-        rg_fft_fwd<PZ, 1, true>(u, tz, exz, 0, twz);
-        if (act) {
+    }
 #pragma unroll
-            for (int j = 0; j < 4; j++) Xs[(tz + TZ * j) * XP + kx] = make_float2(u[0][j].x, -u[0][j].y);
+    for (int r = 0; r < 2; r++) {
+        const int kx = r * CPR + cl;
+        rg_fft_fwd<PZ, 1, true>(u[r], tz, exz, 0, twz);
+        if (r == 0 && cl == 0) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                Xs[(tz + TZ * j) * XP] = make_float2(u[r][0][j].x, 0.f);
+                Xs[(tz + TZ * j) * XP + M] = make_float2(-u[r][0][j].y, 0.f);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) Xs[(tz + TZ * j) * XP + kx] = make_float2(u[r][0][j].x, -u[r][0][j].y);
         }
     }
     __syncthreads();
@@ -529,6 +600,7 @@ template <int M, int PZ> static void fill_ac(FastPasses& f) {
         f.c = k_reg_c<M, PZ>;
         f.smem_ac = RegAC<M, PZ>::smem;
         f.nt_ac = RegAC<M, PZ>::NT;
+        f.ac_reg = true;
     } else {
         f.a = k_fast_a<M, PZ>;
         f.c = k_fast_c<M, PZ>;
@@ -542,6 +614,7 @@ template <int PY> static void fill_b(FastPasses& f) {
         f.smem_b = RegB<PY>::smem;
         f.wb = RegB<PY>::WB;
         f.nt_b = RegB<PY>::NT;
+        f.b_reg = true;
     } else {
         f.b = k_fast_b<PY>;
         f.smem_b = BShape<PY>::smem;
@@ -570,7 +643,15 @@ bool demag_fast_select(int M, int Py, int Pz, FastPasses& f) {
     else b = false;
 #undef BB
     if (!(ac && b)) f = FastPasses{};
+    // 4-column-block spectrum layout when all three passes are register kernels
+    f.blocked = ac && b && f.ac_reg && f.b_reg;
     return ac && b;
+}
+
+int demag_fast_grid(FastPasses& f, int M, int Pz) {
+    f.gbx = (unsigned)((M + 1 + f.wb - 1) / f.wb);
+    f.gby = (unsigned)Pz;
+    return UMAG_OK;
 }
 
 int demag_fast_setup() {

@@ -84,8 +84,10 @@ extern "C" __attribute__((visibility("default"))) int umag_demag_exec_noalloc(
     d.Lx = (d.Hx + 3) / 4 * 4;
     d.is2d = Nz == 1;
     if (Nz > 1) UMAG_REQUIRE(K[3] && K[4], "NULL yz/xz kernel spectrum for a 3D mesh");
+    UMAG_TRY(demag_fast_setup());
     if (!demag_fast_select(d.M, d.P[1], d.P[2], d.fast))
         return set_error(UMAG_E_UNSUPPORTED, "mesh %dx%dx%d has no compile-time FFT plan (no-alloc path)", Nx, Ny, Nz);
+    UMAG_TRY(demag_fast_grid(d.fast, d.M, d.P[2]));
     d.use_fast = true;
     d.WB = d.fast.wb;
     // scratch layout: spectrum | tw(M) | tw(Py) | tw(Pz) | exp(-2 pi i k/Px), k < M
@@ -97,7 +99,6 @@ extern "C" __attribute__((visibility("default"))) int umag_demag_exec_noalloc(
                          Nx, Ny, Nz, need, kNoallocScratchBytes);
     void* base = nullptr;
     UMAG_TRY(noalloc_scratch(&base));
-    UMAG_TRY(demag_fast_setup());
     float2* sp = reinterpret_cast<float2*>(base);
     float2* tw = sp + spec;
     cudaStream_t st = (cudaStream_t)stream;
@@ -116,6 +117,8 @@ extern "C" __attribute__((visibility("default"))) int umag_demag_exec_noalloc(
     a.spec = sp;
     for (int c = 0; c < 6; c++) a.K[c] = K[c];
     a.Kp = d.Hx;  // caller's spectrum: reference layout, rows of Px/2+1 floats
+    a.Kblocked = 0;
+    a.blocked = d.fast.blocked ? 1 : 0;
     if (d.is2d) a.K[3] = a.K[4] = nullptr;
     a.m[0] = mx; a.m[1] = my; a.m[2] = mz;
     a.B[0] = Bx; a.B[1] = By; a.B[2] = Bz;

@@ -341,6 +341,14 @@ class DemagConvolution:
         check(L.umag_demag_exec(self._h, *_comps(B), *_comps(m), _p(vol), ms.ptr(), ms.mul))
         Sync()
 
+    def ExecPass(self, p, B, m, vol, Msat):
+        """One pass (0: x/z forward, 1: y + kernel multiply, 2: inverse z/x) of
+        Exec, queued without a synchronize (for timing the passes one by one)."""
+        L = _L()
+        _in()
+        ms = _ms(Msat)
+        check(L.umag_demag_exec_pass(self._h, int(p), *_comps(B), *_comps(m), _p(vol), ms.ptr(), ms.mul))
+
     def padded_size(self):
         import ctypes
         P = (ctypes.c_int * 3)()

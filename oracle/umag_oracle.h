@@ -11,8 +11,9 @@
  * variants exist for the per-cell kernels: *_f32 follows the reference's
  * float32 evaluation order (compile with -ffp-contract=off, like the OpenCL
  * program that is built without -cl-mad-enable, opencl/init.go:175) and
- * *_f64 is the uMagNUS64 (FP64) oracle.  The FFT is always FP64 (the
- * reference's VkFFT rounding is not reproducible).
+ * *_f64 is the uMagNUS64 (FP64) oracle.  The FFT is always FP64: the
+ * reference's float32 FFT library rounding is not reproducible, so demag
+ * results are compared within a stated tolerance, not bit for bit.
  */
 #ifndef UMAG_ORACLE_H
 #define UMAG_ORACLE_H

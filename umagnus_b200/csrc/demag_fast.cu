@@ -6,6 +6,7 @@
 // twiddles are staged in shared memory.  demag_fast_select() returns the
 // instantiation for a plan, or nothing (the generic kernels then run).
 #include "demag.cuh"
+#include "fft_pair.cuh"
 #include "fft_reg.cuh"
 #include "fft_static.cuh"
 
@@ -451,55 +452,96 @@ __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) {
         if (k == 0) xrow[M] = make_float2(A.x - A.y, 0.f);  // Nyquist: Re Z0 - Im Z0
     }
     __syncthreads();
-    // z phase: column kx, TZ lanes, rows z = tz + TZ*j (zero padding for j >= 4).
-    // The DC and Nyquist columns are real in z, so they share one complex
-    // transform (x0 + i xM), split afterwards by Hermitian symmetry:
-    // X0[k] = (P[k] + conj P[-k]) / 2, XM[k] = (P[k] - conj P[-k]) / 2i.
-    // The M - 1 other columns then fill exactly M / CPR = 2 rounds.
-    static_assert(M == 2 * CPR, "z rounds: M columns over CPR column groups");
     float2* out = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
     const long kzs = (long)Ny * a.Lx;
-    const int tz = tid % TZ, cl = tid / TZ;
-    float2* exz = ex + cl * S::LZ;
+    if constexpr (PZ == 16 || PZ == 32) {
+        // z phase on lane pairs, decimation in frequency: with x[n] = 0 for
+        // n >= PZ/2, X[2r + t] = DFT_{PZ/2}( x[n] W_PZ^{n t} )[r], so lane t
+        // of a pair produces the kz of parity t from the same PZ/2 inputs --
+        // no exchange and no twiddle table.  The DC and Nyquist columns are
+        // real in z and share one transform P of (x0 + i xM), split by
+        // Hermitian symmetry (X0 = (P[k] + conj P[-k]) / 2, XM = (P[k] -
+        // conj P[-k]) / 2i); P[-k] has the parity of k, so it is in the lane.
+        constexpr int E2 = PZ / 2, CP2 = NT / 2;
+        static_assert(E2 == NZ && M % CP2 == 0, "pair z phase");
+        const int t2 = tid & 1, cl2 = tid >> 1;
+        const long kM = spec_col(a, M);
 #pragma unroll
-    for (int r = 0; r < 2; r++) {
-        const int kx = r * CPR + cl;
-        const bool pk = kx == 0;
-        float2 u[1][8];
+        for (int r0 = 0; r0 < M / CP2; r0++) {
+            const int kx = r0 * CP2 + cl2;
+            const bool pk = kx == 0;
+            float2 u[E2];
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            float2 q = make_float2(0.f, 0.f);
-            if (j < 4) {
-                q = Xs[(tz + TZ * j) * XP + kx];
-                if (pk) q.y = Xs[(tz + TZ * j) * XP + M].x;
+            for (int n = 0; n < E2; n++) {
+                float2 q = Xs[n * XP + kx];
+                if (pk) q.y = Xs[n * XP + M].x;
+                u[n] = q;
             }
-            u[0][j] = q;
-        }
-        rg_fft_fwd<PZ, 1, true>(u, tz, exz, 0, twz);
-        if (r == 0 && tid < 32) {  // the warp holding column group 0
-            const int pl = (lane & ~(TZ - 1)) | ((TZ - tz) & (TZ - 1));
-            float2 pr[8];
-#pragma unroll
-            for (int s = 0; s < 8; s++) {
-                float2 q;
-                q.x = __shfl_sync(0xffffffffu, u[0][s].x, pl);
-                q.y = __shfl_sync(0xffffffffu, u[0][s].y, pl);
-                if (tz != 0) pr[7 - s] = q;
-                else pr[(8 - s) & 7] = q;
-            }
+            if (t2) tw_ramp<PZ, 1, 0, E2>(u);
+            reg_dft<E2>(u);  // u[r] = X[2r + t2]
             if (pk) {
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const float2 P = u[0][j], Q = pr[j];
-                    out[(tz + TZ * j) * kzs] = make_float2(0.5f * (P.x + Q.x), 0.5f * (P.y - Q.y));
-                    out[(tz + TZ * j) * kzs + spec_col(a, M)] = make_float2(0.5f * (P.y + Q.y), -0.5f * (P.x - Q.x));
+                for (int r = 0; r < E2; r++) {
+                    const float2 P = u[r], Q = t2 ? u[E2 - 1 - r] : u[(E2 - r) & (E2 - 1)];
+                    const long o = (long)(2 * r + t2) * kzs;
+                    out[o] = make_float2(0.5f * (P.x + Q.x), 0.5f * (P.y - Q.y));
+                    out[o + kM] = make_float2(0.5f * (P.y + Q.y), -0.5f * (P.x - Q.x));
                 }
-                continue;
+            } else {
+                const long ko = spec_col(a, kx);
+#pragma unroll
+                for (int r = 0; r < E2; r++) out[(long)(2 * r + t2) * kzs + ko] = u[r];
             }
         }
-        const long ko = spec_col(a, kx);
-#pragma unroll
-        for (int j = 0; j < 8; j++) out[(tz + TZ * j) * kzs + ko] = u[0][j];
+    } else {
+        // z phase: column kx, TZ lanes, rows z = tz + TZ*j (zero padding for j >= 4).
+        // The DC and Nyquist columns are real in z, so they share one complex
+        // transform (x0 + i xM), split afterwards by Hermitian symmetry:
+        // X0[k] = (P[k] + conj P[-k]) / 2, XM[k] = (P[k] - conj P[-k]) / 2i.
+        // The M - 1 other columns then fill exactly M / CPR = 2 rounds.
+        static_assert(M == 2 * CPR, "z rounds: M columns over CPR column groups");
+        const int tz = tid % TZ, cl = tid / TZ;
+        float2* exz = ex + cl * S::LZ;
+    #pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int kx = r * CPR + cl;
+            const bool pk = kx == 0;
+            float2 u[1][8];
+    #pragma unroll
+            for (int j = 0; j < 8; j++) {
+                float2 q = make_float2(0.f, 0.f);
+                if (j < 4) {
+                    q = Xs[(tz + TZ * j) * XP + kx];
+                    if (pk) q.y = Xs[(tz + TZ * j) * XP + M].x;
+                }
+                u[0][j] = q;
+            }
+            rg_fft_fwd<PZ, 1, true>(u, tz, exz, 0, twz);
+            if (r == 0 && tid < 32) {  // the warp holding column group 0
+                const int pl = (lane & ~(TZ - 1)) | ((TZ - tz) & (TZ - 1));
+                float2 pr[8];
+    #pragma unroll
+                for (int s = 0; s < 8; s++) {
+                    float2 q;
+                    q.x = __shfl_sync(0xffffffffu, u[0][s].x, pl);
+                    q.y = __shfl_sync(0xffffffffu, u[0][s].y, pl);
+                    if (tz != 0) pr[7 - s] = q;
+                    else pr[(8 - s) & 7] = q;
+                }
+                if (pk) {
+    #pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        const float2 P = u[0][j], Q = pr[j];
+                        out[(tz + TZ * j) * kzs] = make_float2(0.5f * (P.x + Q.x), 0.5f * (P.y - Q.y));
+                        out[(tz + TZ * j) * kzs + spec_col(a, M)] = make_float2(0.5f * (P.y + Q.y), -0.5f * (P.x - Q.x));
+                    }
+                    continue;
+                }
+            }
+            const long ko = spec_col(a, kx);
+    #pragma unroll
+            for (int j = 0; j < 8; j++) out[(tz + TZ * j) * kzs + ko] = u[0][j];
+        }
     }
 }
 
@@ -521,41 +563,89 @@ __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) {
     const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
     const float2* in = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
     const long kzs = (long)Ny * a.Lx;
-    // z phase: inverse transform (conjugate trick) of every column, keep z < NZ.
-    // The DC and Nyquist columns invert to real sequences, so they share one
-    // transform of G0 + i GM (real part -> column 0, imaginary -> column M);
-    // the other columns fill exactly two rounds, whose loads are all issued
-    // before the first transform.
-    static_assert(M == 2 * CPR, "z rounds: M columns over CPR column groups");
-    const int tz = tid % TZ, cl = tid / TZ;
-    float2* exz = ex + cl * S::LZ;
-    float2 u[2][1][8];
+    if constexpr (PZ == 16 || PZ == 32) {
+        // z phase on lane pairs, inverse by the conjugate trick, decimation in
+        // time: lane t transforms the samples kz = 2j + t (u = conj G), lane 1
+        // scales by W_PZ^k, and the kept outputs z < PZ/2 are
+        // X[z] = A[z] + W^z B[z]; lane 0 forms z < PZ/4 and lane 1 the rest,
+        // exchanging one value per output by shuffle.  The DC and Nyquist
+        // columns invert to real sequences and share one transform of
+        // G0 + i GM (real part -> column 0, imaginary -> column M).
+        constexpr int E2 = PZ / 2, H2 = E2 / 2, CP2 = NT / 2;
+        static_assert(E2 == NZ && M % CP2 == 0, "pair z phase");
+        const int t2 = tid & 1, cl2 = tid >> 1;
+        const long kM = spec_col(a, M);
 #pragma unroll
-    for (int r = 0; r < 2; r++) {
-        const long ko = spec_col(a, r * CPR + cl), kM = spec_col(a, M);
+        for (int r0 = 0; r0 < M / CP2; r0++) {
+            const int kx = r0 * CP2 + cl2;
+            const bool pk = kx == 0;
+            const long ko = spec_col(a, kx);
+            float2 u[E2];
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            float2 q = in[(tz + TZ * j) * kzs + ko];
-            if (r == 0 && cl == 0) {
-                const float2 g = in[(tz + TZ * j) * kzs + kM];
-                q = make_float2(q.x - g.y, q.y + g.x);
+            for (int j = 0; j < E2; j++) {
+                float2 q = in[(long)(2 * j + t2) * kzs + ko];
+                if (pk) {
+                    const float2 g = in[(long)(2 * j + t2) * kzs + kM];
+                    q = make_float2(q.x - g.y, q.y + g.x);
+                }
+                u[j] = make_float2(q.x, -q.y);
             }
-            u[r][0][j] = make_float2(q.x, -q.y);
+            reg_dft<E2>(u);
+            if (t2) tw_ramp<PZ, 1, 0, E2>(u);
+#pragma unroll
+            for (int i = 0; i < H2; i++) {
+                const float2 snd = t2 ? u[i] : u[H2 + i];
+                float2 rcv;
+                rcv.x = __shfl_xor_sync(0xffffffffu, snd.x, 1);
+                rcv.y = __shfl_xor_sync(0xffffffffu, snd.y, 1);
+                const float2 own = t2 ? u[H2 + i] : u[i];
+                const float2 X = make_float2(own.x + rcv.x, own.y + rcv.y);
+                const int z = i + H2 * t2;
+                if (pk) {
+                    Xs[z * XP] = make_float2(X.x, 0.f);
+                    Xs[z * XP + M] = make_float2(-X.y, 0.f);
+                } else {
+                    Xs[z * XP + kx] = make_float2(X.x, -X.y);
+                }
+            }
         }
-    }
-#pragma unroll
-    for (int r = 0; r < 2; r++) {
-        const int kx = r * CPR + cl;
-        rg_fft_fwd<PZ, 1, true>(u[r], tz, exz, 0, twz);
-        if (r == 0 && cl == 0) {
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                Xs[(tz + TZ * j) * XP] = make_float2(u[r][0][j].x, 0.f);
-                Xs[(tz + TZ * j) * XP + M] = make_float2(-u[r][0][j].y, 0.f);
+    } else {
+        // z phase: inverse transform (conjugate trick) of every column, keep z < NZ.
+        // The DC and Nyquist columns invert to real sequences, so they share one
+        // transform of G0 + i GM (real part -> column 0, imaginary -> column M);
+        // the other columns fill exactly two rounds, whose loads are all issued
+        // before the first transform.
+        static_assert(M == 2 * CPR, "z rounds: M columns over CPR column groups");
+        const int tz = tid % TZ, cl = tid / TZ;
+        float2* exz = ex + cl * S::LZ;
+        float2 u[2][1][8];
+    #pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const long ko = spec_col(a, r * CPR + cl), kM = spec_col(a, M);
+    #pragma unroll
+            for (int j = 0; j < 8; j++) {
+                float2 q = in[(tz + TZ * j) * kzs + ko];
+                if (r == 0 && cl == 0) {
+                    const float2 g = in[(tz + TZ * j) * kzs + kM];
+                    q = make_float2(q.x - g.y, q.y + g.x);
+                }
+                u[r][0][j] = make_float2(q.x, -q.y);
             }
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; j++) Xs[(tz + TZ * j) * XP + kx] = make_float2(u[r][0][j].x, -u[r][0][j].y);
+        }
+    #pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int kx = r * CPR + cl;
+            rg_fft_fwd<PZ, 1, true>(u[r], tz, exz, 0, twz);
+            if (r == 0 && cl == 0) {
+    #pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    Xs[(tz + TZ * j) * XP] = make_float2(u[r][0][j].x, 0.f);
+                    Xs[(tz + TZ * j) * XP + M] = make_float2(-u[r][0][j].y, 0.f);
+                }
+            } else {
+    #pragma unroll
+                for (int j = 0; j < 4; j++) Xs[(tz + TZ * j) * XP + kx] = make_float2(u[r][0][j].x, -u[r][0][j].y);
+            }
         }
     }
     __syncthreads();

@@ -444,7 +444,8 @@ struct SimImpl {
     bool need_k1 = true;
     bool use_graph = true;
     int graph_steps = 16;
-    cudaGraphExec_t gexec = nullptr;
+    cudaGraphExec_t gexec = nullptr;   // graph_steps steps
+    cudaGraphExec_t gexec1 = nullptr;  // one step
     int launches_per_step = 0;
 };
 
@@ -640,34 +641,41 @@ static int ensure_k1(SimImpl* s) {
 
 static void drop_graph(SimImpl* s) {
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    if (s->gexec1) cudaGraphExecDestroy(s->gexec1);
     s->gexec = nullptr;
+    s->gexec1 = nullptr;
 }
 
-static int build_graph(SimImpl* s) {
-    drop_graph(s);
+// capture `steps` steps into *out
+static int capture_steps(SimImpl* s, int steps, cudaGraphExec_t* out) {
     cudaGraph_t graph;
     UMAG_CUDA(cudaStreamBeginCapture(S(), cudaStreamCaptureModeThreadLocal));
     int nl = 0;
     int st = UMAG_OK;
-    for (int i = 0; i < s->graph_steps && st == UMAG_OK; i++) st = launch_step(s, &nl);
+    for (int i = 0; i < steps && st == UMAG_OK; i++) st = launch_step(s, &nl);
     cudaError_t e = cudaStreamEndCapture(S(), &graph);
     if (st != UMAG_OK) return st;
     if (e != cudaSuccess) return set_error(UMAG_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&s->gexec, graph, 0);
+    e = cudaGraphInstantiate(out, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return set_error(UMAG_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
     return UMAG_OK;
 }
 
-// n steps with the stop time already in ctl
+// n steps with the stop time already in ctl: graphs of graph_steps steps,
+// the remainder from a one-step graph
 static int run_steps(SimImpl* s, long long n) {
     UMAG_TRY(ensure_k1(s));
-    if (s->use_graph && n >= s->graph_steps) {
-        if (!s->gexec) UMAG_TRY(build_graph(s));
-        while (n >= s->graph_steps) {
-            UMAG_CUDA(cudaGraphLaunch(s->gexec, S()));
-            n -= s->graph_steps;
+    if (s->use_graph) {
+        if (n >= s->graph_steps) {
+            if (!s->gexec) UMAG_TRY(capture_steps(s, s->graph_steps, &s->gexec));
+            for (; n >= s->graph_steps; n -= s->graph_steps) UMAG_CUDA(cudaGraphLaunch(s->gexec, S()));
         }
+        if (n > 0) {
+            if (!s->gexec1) UMAG_TRY(capture_steps(s, 1, &s->gexec1));
+            for (; n > 0; n--) UMAG_CUDA(cudaGraphLaunch(s->gexec1, S()));
+        }
+        return UMAG_OK;
     }
     for (long long i = 0; i < n; i++) {
         int nl = 0;

@@ -19,17 +19,17 @@ template <typename T> struct Cplx;
 template <> struct Cplx<float> { using t = float2; };
 template <> struct Cplx<double> { using t = double2; };
 
-template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
     C r;
     r.x = a.x * b.x - a.y * b.y;
     r.y = a.x * b.y + a.y * b.x;
     return r;
 }
-template <typename C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
-template <typename C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
-template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+template <typename C> __host__ __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename C> __host__ __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
 // multiply by -i (dir < 0, forward) or +i (dir > 0, inverse)
-template <typename C> __device__ __forceinline__ C mul_mi(C a, int dir) {
+template <typename C> __host__ __device__ __forceinline__ C mul_mi(C a, int dir) {
     C r;
     if (dir < 0) { r.x = a.y; r.y = -a.x; }
     else { r.x = -a.y; r.y = a.x; }
@@ -76,12 +76,12 @@ inline int fft_min_radix(const int* R, int n) {
     return n ? r : 1;
 }
 
-template <typename C> __device__ __forceinline__ void dft2(C* v) {
+template <typename C> __host__ __device__ __forceinline__ void dft2(C* v) {
     C a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
 }
-template <typename C> __device__ __forceinline__ void dft4(C* v, int dir) {
+template <typename C> __host__ __device__ __forceinline__ void dft4(C* v, int dir) {
     C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
     C t2 = cadd(v[1], v[3]), t3 = mul_mi(csub(v[1], v[3]), dir);
     v[0] = cadd(t0, t2);
@@ -89,7 +89,7 @@ template <typename C> __device__ __forceinline__ void dft4(C* v, int dir) {
     v[1] = cadd(t1, t3);
     v[3] = csub(t1, t3);
 }
-template <typename T, typename C> __device__ __forceinline__ void dft8(C* v, int dir) {
+template <typename T, typename C> __host__ __device__ __forceinline__ void dft8(C* v, int dir) {
     C e[4] = {v[0], v[2], v[4], v[6]};
     C o[4] = {v[1], v[3], v[5], v[7]};
     dft4(e, dir);

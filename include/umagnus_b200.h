@@ -245,6 +245,20 @@ int umag_sim_launches_per_step(umag_sim* s, int* n);
  * FSAL slot (the value it already holds), without host synchronisation; for
  * timing the field evaluation alone.  No reference counterpart. */
 int umag_sim_torque_evals(umag_sim* s, int n);
+/* engine/energy.go:27-35 GetTotalEnergy and its terms for the current m, in
+ * joules: E[0] total, E[1] demag (engine/demag.go:146 GetDemagEnergy),
+ * E[2] exchange including DMI (engine/exchange.go:79), E[3] uniaxial
+ * anisotropy (engine/anisotropy.go:210), E[4] Zeeman (engine/zeeman.go:15).
+ * Each term is -k V sum(M_full . B_term) with float32 dot products per cell
+ * and FP64 accumulation. */
+int umag_sim_energies(umag_sim* s, double E[5]);
+/* engine/relax.go:23-112 Relax(): RK23 without precession; steps while the
+ * total energy decreases (checked every 3 steps), then while the mean
+ * squared torque decreases, lowering MaxErr by sqrt(2) down to 1e-9 --
+ * or, with torque_threshold > 0 (RelaxTorqueThreshold), while the maximum
+ * torque exceeds it.  The time is left unchanged; solver, MaxErr, FixDt and
+ * precession are restored afterwards. */
+int umag_sim_relax(umag_sim* s, double torque_threshold);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

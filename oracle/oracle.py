@@ -319,6 +319,10 @@ class Simulation:
         self.N = tuple(N)
         self.ncell = N[0] * N[1] * N[2]
         self._keep = []
+        # the material as given, for the energy restatement (energies())
+        self.cfg = dict(cell=tuple(cell), Ms=Ms, Aex=Aex, Dind=Dind, Ku1=Ku1, Ku2=Ku2, anisU=anisU, B_ext=B_ext,
+                        vol=vol, Aex_regions=Aex_regions, Dind_regions=Dind_regions, Bext_regions=Bext_regions,
+                        demag=demag, openbc=openbc)
         s = OrcSystem()
         s.N[:] = N
         s.pbc[:] = pbc
@@ -418,3 +422,117 @@ class Simulation:
             if on_step is not None:
                 on_step(self, ok)
         return n
+
+
+# ---------------------------------------------------------------- energies / relax
+def energies(sim, m=None):
+    """engine/energy.go:27-35 GetTotalEnergy and its terms, in FP64, for an
+    oracle Simulation: E_demag = -1/2 V sum M_full.B_demag (engine/demag.go:146),
+    E_exch = -1/2 V sum M_full.B_exch incl. DMI (engine/exchange.go:79),
+    E_anis = V sum(-1/2 M_full.B_K1 - 1/4 M_full.B_K2) (engine/anisotropy.go:164-216),
+    E_Zeeman = -V sum M_full.B_ext (engine/zeeman.go:15); M_full = Ms m (vol)
+    (engine/demag.go:101-121).  Total in the terms' registration order."""
+    c = sim.cfg
+    f8 = np.float64
+    m = np.asarray(sim.m if m is None else m, f8).reshape((3,) + tuple(reversed(sim.N)))
+    cell = c["cell"]
+    V = cell[0] * cell[1] * cell[2]
+    shape = m.shape[1:]
+    regions = sim.regions.reshape(shape)
+    vol = None if c["vol"] is None else np.asarray(c["vol"], f8).reshape(shape)
+    Ms = c["Ms"]
+    Ms_arr = np.full(shape, float(Ms)) if np.isscalar(Ms) else np.asarray(Ms, f8).reshape(shape)
+    Mf = m * Ms_arr
+    if vol is not None:
+        Mf = Mf * vol
+    E = {}
+    Bd = demag_field(sim.Kf, sim.P, m, Ms, vol=vol, dtype=f8) if c["demag"] else np.zeros_like(m)
+    E["demag"] = -0.5 * V * float(np.sum(Mf * Bd))
+    aex = np.full(256, c["Aex"], f8) if c["Aex_regions"] is None else np.asarray(c["Aex_regions"], f8)
+    alut = exch_lut(aex, dtype=f8)
+    Be = np.zeros_like(m)
+    din = np.full(256, c["Dind"], f8) if c["Dind_regions"] is None else np.asarray(c["Dind_regions"], f8)
+    if np.any(din != 0):
+        add_dmi(Be, m, alut, exch_lut(din, dtype=f8), regions, cell, Ms, 0, int(c["openbc"]))
+    else:
+        add_exchange(Be, m, alut, regions, cell, Ms)
+    E["exchange"] = -0.5 * V * float(np.sum(Mf * Be))
+    Ea = 0.0
+    if not (np.all(np.asarray(c["Ku1"]) == 0) and np.all(np.asarray(c["Ku2"]) == 0)):
+        B1 = np.zeros_like(m)
+        add_uniaxial(B1, m, Ms, c["Ku1"], 0.0, c["anisU"])
+        B2 = np.zeros_like(m)
+        add_uniaxial(B2, m, Ms, 0.0, c["Ku2"], c["anisU"])
+        Ea = V * float(np.sum(-0.5 * np.sum(Mf * B1, axis=0) - 0.25 * np.sum(Mf * B2, axis=0)))
+    E["anisotropy"] = Ea
+    Ez = 0.0
+    if c["Bext_regions"] is not None or c["B_ext"] is not None:
+        lut = c["Bext_regions"]
+        if lut is None:
+            lut = np.tile(np.asarray(c["B_ext"], f8), (256, 1))
+        lut = np.ascontiguousarray(np.asarray(lut, f8).T)
+        Bz = np.zeros_like(m)
+        region_addv(Bz, lut, regions)
+        Ez = -1.0 * V * float(np.sum(Mf * Bz))
+    E["zeeman"] = Ez
+    E["total"] = ((E["anisotropy"] + E["demag"]) + E["exchange"]) + E["zeeman"]
+    return E
+
+
+def relax(sim, torque_threshold=-1.0, max_relax_steps=10 ** 6):
+    """engine/relax.go:23-112 Relax() on an oracle Simulation: RK23 without
+    precession; 3-step chunks while the total energy decreases, then the
+    torque phase (max |k1| against the threshold, or the mean squared torque
+    while MaxErr is lowered by sqrt(2) down to 1e-9).  Time is restored after
+    every chunk (relax.go:134-141); solver settings are restored at the end."""
+    s = sim.solver
+    prev = (s.solver, s.max_err, s.fix_dt, sim.sys.precess)
+    s.solver, s.fix_dt, sim.sys.precess = 3, 0.0, 0
+    s.have_k1 = 0
+    budget = [max_relax_steps]
+
+    def steps(n):
+        t0 = s.time
+        target = s.nsteps + n
+        s.have_k1 = 0  # runWhile frees the stepper
+        while s.nsteps < target:
+            sim.step()
+            budget[0] -= 1
+            if budget[0] < 0:
+                raise RuntimeError("relax: step budget exhausted")
+        s.time = t0
+
+    def etot():
+        return energies(sim)["total"]
+
+    def k1():
+        return sim.k1.reshape(3, -1)
+
+    try:
+        n = 3
+        steps(n)
+        E0 = etot()
+        steps(n)
+        E1 = etot()
+        while E1 < E0:
+            steps(n)
+            E0, E1 = E1, etot()
+        if torque_threshold > 0:
+            while True:
+                while max_vec_norm(k1()) > torque_threshold:
+                    steps(n)
+                s.max_err /= np.sqrt(2)
+                if s.max_err < 1e-9:
+                    break
+        else:
+            T1 = np.float32(rdot(k1(), k1()))
+            while s.max_err > 1e-9:
+                s.max_err /= np.sqrt(2)
+                steps(n)
+                T0, T1 = T1, np.float32(rdot(k1(), k1()))
+                while T1 < T0:
+                    steps(n)
+                    T0, T1 = T1, np.float32(rdot(k1(), k1()))
+    finally:
+        s.solver, s.max_err, s.fix_dt, sim.sys.precess = prev
+        s.have_k1 = 0

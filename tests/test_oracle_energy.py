@@ -1,0 +1,59 @@
+"""The oracle's energy restatement (engine/energy.go terms) against closed
+forms, and its Relax() restatement on a small film (CPU only)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import golden_pins as G
+
+MU0 = 4e-7 * np.pi
+
+
+def _uniform(N, v):
+    m = np.empty((3, N[2], N[1], N[0]), np.float32)
+    for c in range(3):
+        m[c] = v[c]
+    return m
+
+
+def test_energy_closed_forms():
+    """Uniform state of a box: exchange 0; Zeeman -V N Ms m.B; uniaxial
+    -V N (K1 cos^2 + K2 cos^4 / ... ) in the reference's convention
+    (B_K1.M = 2 K1 cos^2, B_K2.M = 4 K2 cos^4); demag 1/2 mu0 Ms^2 V_tot m.N.m
+    with the Aharoni prism factors."""
+    N, cell = (12, 10, 6), (3e-9, 2.5e-9, 2e-9)
+    Ms, K1, K2 = 8e5, 4e4, 1.5e4
+    u = (0.0, 0.6, 0.8)
+    b = (0.02, -0.01, 0.03)
+    m = np.array([0.36, 0.48, 0.8])
+    sim = O.Simulation(N, cell, Ms, 1.3e-11, 0.1, dtype=np.float64, Ku1=K1, Ku2=K2, anisU=u, B_ext=b)
+    E = O.energies(sim, _uniform(N, m))
+    n = N[0] * N[1] * N[2]
+    V = cell[0] * cell[1] * cell[2]
+    cos = float(np.dot(m, u))
+    assert abs(E["exchange"]) < 1e-12 * abs(E["zeeman"])
+    assert E["zeeman"] == pytest.approx(-V * n * Ms * float(np.dot(m, b)), rel=1e-12)
+    want_anis = V * n * (-0.5 * 2 * K1 * cos ** 2 - 0.25 * 4 * K2 * cos ** 4)
+    assert E["anisotropy"] == pytest.approx(want_anis, rel=1e-12)
+    Nf = G.prism_factors(N, cell)
+    want_demag = 0.5 * MU0 * Ms ** 2 * V * n * sum(Nf[i] * m[i] ** 2 for i in range(3))
+    assert E["demag"] == pytest.approx(want_demag, rel=1e-9)
+    assert E["total"] == pytest.approx(E["anisotropy"] + E["demag"] + E["exchange"] + E["zeeman"], rel=1e-15)
+
+
+def test_relax_lowers_energy_and_torque():
+    """Relax() from a tilted uniform state of a small film: total energy goes
+    down, the torque ends far below its start, time is unchanged."""
+    N, cell = (16, 8, 1), (4e-9, 4e-9, 3e-9)
+    sim = O.Simulation(N, cell, 8e5, 1.3e-11, 0.02, Ku1=1e4, anisU=(1, 0, 0))
+    sim.set_m(_uniform(N, (1.0, 1.0, 0.2)))
+    E0 = O.energies(sim)["total"]
+    tau0 = O.max_vec_norm(sim.torque().reshape(3, -1))
+    t0 = sim.solver.time
+    O.relax(sim)
+    E1 = O.energies(sim)["total"]
+    tau1 = O.max_vec_norm(sim.torque().reshape(3, -1))
+    assert E1 < E0
+    assert tau1 < 1e-3 * tau0
+    assert sim.solver.time == t0
+    assert sim.solver.solver == 5 and sim.sys.precess == 1

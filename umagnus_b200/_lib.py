@@ -82,6 +82,7 @@ _SIGS = {
     "umag_sim_set_time": [P, c_double, c_double], "umag_sim_average_m": [P, ctypes.POINTER(c_double)],
     "umag_sim_use_graph": [P, c_int, c_int], "umag_sim_launches_per_step": [P, ctypes.POINTER(c_int)],
     "umag_sim_torque_evals": [P, c_int],
+    "umag_sim_energies": [P, ctypes.POINTER(c_double)], "umag_sim_relax": [P, c_double],
 }
 _RESTYPE = {"umag_last_error": ctypes.c_char_p, "umag_version": ctypes.c_char_p, "umag_solver_defaults": None}
 

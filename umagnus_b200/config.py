@@ -1,0 +1,56 @@
+"""Initial magnetisation and geometry on the mesh, evaluated at cell centres
+as the reference does (engine/util.go:132 Index2Coord, engine/magnetization.go:89
+SetInShape): the mesh is centred on the origin.
+
+Configurations follow engine/config.go, shapes engine/shape.go.  They are
+host-side helpers producing arrays for Simulation.set_m / Simulation(geom=...).
+"""
+import numpy as np
+
+
+def coords(N, cell):
+    """(x, y, z) of every cell centre, each an array of shape (Nz, Ny, Nx)."""
+    Nx, Ny, Nz = N
+    cx, cy, cz = cell
+    x = cx * (np.arange(Nx) - 0.5 * (Nx - 1))
+    y = cy * (np.arange(Ny) - 0.5 * (Ny - 1))
+    z = cz * (np.arange(Nz) - 0.5 * (Nz - 1))
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    return X, Y, Z
+
+
+def uniform(N, mx, my, mz):
+    """engine/config.go:55 Uniform."""
+    shape = (3, N[2], N[1], N[0])
+    m = np.empty(shape, np.float32)
+    m[0], m[1], m[2] = mx, my, mz
+    return m
+
+
+def vortex(N, cell, circ, pol):
+    """engine/config.go:63-73 Vortex: in-plane curl with circulation circ and a
+    core of polarisation pol smoothed over 2*cellsize_x^2."""
+    X, Y, _ = coords(N, cell)
+    diam2 = 2.0 * cell[0] ** 2
+    r2 = X * X + Y * Y
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.sqrt(r2)
+        mx = -Y * circ / r
+        my = X * circ / r
+    mz = 1.5 * pol * np.exp(-r2 / diam2)
+    bad = np.isnan(mx) | np.isnan(my) | np.isnan(mz)  # engine/config.go:128-134 noNaN
+    mx = np.where(bad, 0.0, mx)
+    my = np.where(bad, 0.0, my)
+    mz = np.where(bad, float(pol), mz)
+    return np.stack([mx, my, mz]).astype(np.float32)
+
+
+def ellipsoid(N, cell, dx, dy, dz=np.inf):
+    """engine/shape.go:39-47 Ellipsoid / Ellipse: 1 inside, 0 outside (cell centre test)."""
+    X, Y, Z = coords(N, cell)
+    zt = 0.0 if np.isinf(dz) else (Z / dz) ** 2
+    return ((X / dx) ** 2 + (Y / dy) ** 2 + zt <= 0.25).astype(np.float32)
+
+
+def ellipse(N, cell, dx, dy):
+    return ellipsoid(N, cell, dx, dy)

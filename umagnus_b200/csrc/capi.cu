@@ -178,5 +178,7 @@ int umag_sim_average_m(umag_sim* s, double avg[3]) { return sim_average_m(s, avg
 int umag_sim_use_graph(umag_sim* s, int enable, int steps) { return sim_use_graph(s, enable, steps); }
 int umag_sim_launches_per_step(umag_sim* s, int* n) { return sim_launches_per_step(s, n); }
 int umag_sim_torque_evals(umag_sim* s, int n) { return sim_torque_evals(s, n); }
+int umag_sim_energies(umag_sim* s, double E[5]) { return sim_energies(s, E); }
+int umag_sim_relax(umag_sim* s, double torque_threshold) { return sim_relax(s, torque_threshold); }
 
 }  // extern "C"

@@ -425,6 +425,66 @@ __global__ void k_step_end(DevCtl* c, int rk4) {
     }
 }
 
+// ---------------------------------------------------------------- energies
+// Per-term sums of dot(M_full, B_term) over the cells (engine/energy.go:51-69
+// makeEdensAdder / dot, engine/anisotropy.go:164-216): M_full = Ms * m (* vol),
+// the dot products in float32 as opencl.AddDotProduct/Dot form them, the sums
+// accumulated in FP64 (compensated relative to the reference's float32
+// reduction).  sums: [0] demag, [1] exchange (+DMI), [2] anisotropy from K1
+// alone, [3] anisotropy from K2 alone, [4] Zeeman.
+__global__ void __launch_bounds__(256) k_energy_terms(LocalArgs a, const float* __restrict__ vol, double* sums) {
+    __shared__ double sh[5][8];
+    const int N = a.N;
+    const float* m = a.ctl->m;
+    const float *mx = m, *my = m + N, *mz = m + 2 * N;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x) {
+        const int ix = I % a.g.Nx, iy = (I / a.g.Nx) % a.g.Ny, iz = I / (a.g.Nx * a.g.Ny);
+        const f3 m0 = ld3(mx, my, mz, I);
+        const float ms = amul(a.Ms, a.Ms_mul, I);
+        f3 Mf{fm(m0.x, ms), fm(m0.y, ms), fm(m0.z, ms)};
+        if (vol) {
+            const float w = __ldg(vol + I);
+            Mf = f3{fm(Mf.x, w), fm(Mf.y, w), fm(Mf.z, w)};
+        }
+        if (a.bd) acc[0] += (double)dot3(Mf, f3{__ldg(a.bd + I), __ldg(a.bd + N + I), __ldg(a.bd + 2 * N + I)});
+        if (!is0(m0)) {
+            const int r0 = __ldg(a.regions + I);
+            const f3 e = a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
+                               : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
+            const float inv = inv_msat(a.Ms, a.Ms_mul, I);
+            acc[1] += (double)dot3(Mf, f3{fm(e.x, inv), fm(e.y, inv), fm(e.z, inv)});
+        }
+        if (a.anis) {
+            UniaxParams p1 = a.up, p2 = a.up;
+            p1.K2 = nullptr; p1.K2_mul = 0.f;
+            p2.K1 = nullptr; p2.K1_mul = 0.f;
+            f3 B1{0.f, 0.f, 0.f}, B2{0.f, 0.f, 0.f};
+            add_uniaxial(B1, p1, m0, I);
+            add_uniaxial(B2, p2, m0, I);
+            acc[2] += (double)dot3(Mf, B1);
+            acc[3] += (double)dot3(Mf, B2);
+        }
+        if (a.zeeman) {
+            const int r = __ldg(a.regions + I);
+            acc[4] += (double)dot3(Mf, f3{__ldg(a.bext[0] + r), __ldg(a.bext[1] + r), __ldg(a.bext[2] + r)});
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int t = 0; t < 5; t++) {
+        double v = acc[t];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[t][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double v = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sh[threadIdx.x][w];
+        atomicAdd(sums + threadIdx.x, v);
+    }
+}
+
 // ---------------------------------------------------------------- host side
 struct SimImpl {
     umag_sim_params p;
@@ -447,6 +507,7 @@ struct SimImpl {
     cudaGraphExec_t gexec = nullptr;   // graph_steps steps
     cudaGraphExec_t gexec1 = nullptr;  // one step
     int launches_per_step = 0;
+    double* esum = nullptr;            // energy term sums (5 doubles)
 };
 
 static cudaStream_t S() { return ctx().stream; }
@@ -816,6 +877,7 @@ int sim_free(umag_sim* h) {
     cudaFree(s->zero_regions);
     cudaFree(s->dmi_pairs);
     cudaFree(s->kc_dev);
+    cudaFree(s->esum);
     cudaFree(s->ctl);
     if (s->hctl) cudaFreeHost(s->hctl);
     delete s;
@@ -959,6 +1021,156 @@ int sim_torque_evals(umag_sim* h, int n) {
     UMAG_TRY(push_ctl(s));
     for (int i = 0; i < n; i++) UMAG_TRY(launch_torque(s, 0, 0, nullptr, nullptr, nullptr));
     return UMAG_OK;
+}
+
+// engine/energy.go:27-35 GetTotalEnergy and its terms for the current m:
+// E[0] total, E[1] demag (engine/demag.go:146), E[2] exchange incl. DMI
+// (engine/exchange.go:79), E[3] anisotropy (engine/anisotropy.go:210),
+// E[4] Zeeman (engine/zeeman.go:15).  Joules.
+int sim_energies(umag_sim* h, double E[5]) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && E, "NULL argument");
+    if (!s->esum) UMAG_CUDA(cudaMalloc(&s->esum, 5 * sizeof(double)));
+    UMAG_TRY(sync_ctl_to_host(s));
+    s->hctl->active = 1;
+    UMAG_TRY(push_ctl(s));
+    if (s->p.enable_demag) {
+        PassArgs a = s->pa;
+        a.m_sel = 0;
+        UMAG_TRY(demag_launch(s->demag, a, S()));
+    }
+    UMAG_CUDA(cudaMemsetAsync(s->esum, 0, 5 * sizeof(double), S()));
+    k_energy_terms<<<grid_for(s->N, 256, 4), 256, 0, S()>>>(s->la, s->p.vol, s->esum);
+    UMAG_LAUNCH_CHECK();
+    double t[5];
+    UMAG_CUDA(cudaMemcpyAsync(t, s->esum, sizeof(t), cudaMemcpyDeviceToHost, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    const double V = s->p.cell[0] * s->p.cell[1] * s->p.cell[2];  // engine/energy.go:45-48 cellVolume
+    const double Ed = -0.5 * V * t[0], Ee = -0.5 * V * t[1];
+    const double Ea = V * (-0.5 * t[2] - 0.25 * t[3]), Ez = -1.0 * V * t[4];
+    E[1] = Ed; E[2] = Ee; E[3] = Ea; E[4] = Ez;
+    // registration order of the terms (files anisotropy, demag, exchange, zeeman)
+    E[0] = ((Ea + Ed) + Ee) + Ez;
+    return UMAG_OK;
+}
+
+// switch the stepper / precession (engine/run.go:92-125 SetSolver); the
+// stepper restarts (its FSAL torque is recomputed) and the step graphs are rebuilt
+static void set_stepper(SimImpl* s, int solver, int precess) {
+    if (s->sp.solver != solver || s->la.precess != precess) {
+        s->sp.solver = solver;
+        s->la.precess = precess;
+        drop_graph(s);
+    }
+    s->need_k1 = true;
+}
+
+// engine/relax.go:134-141 relaxSteps: n accepted steps, then time is restored
+static int relax_steps(SimImpl* s, int n) {
+    UMAG_TRY(sync_ctl_to_host(s));
+    const double t0 = s->hctl->t;
+    const long long target = s->hctl->nsteps + n;
+    s->hctl->stop = INFINITY;
+    UMAG_TRY(push_ctl(s));
+    s->need_k1 = true;  // runWhile frees the stepper (engine/run.go:207)
+    for (int guard = 0; guard < 1000; guard++) {
+        UMAG_TRY(sync_ctl_to_host(s));
+        if (s->hctl->status != 0)
+            return set_error(UMAG_E_SOLVER, "solver failure code %d during relax", s->hctl->status);
+        if (s->hctl->nsteps >= target) break;
+        UMAG_TRY(run_steps(s, target - s->hctl->nsteps));
+    }
+    UMAG_TRY(sync_ctl_to_host(s));
+    s->hctl->t = t0;
+    return push_ctl(s);
+}
+
+static int k1_max_norm(SimImpl* s, double* out) {
+    UMAG_TRY(sync_ctl_to_host(s));
+    const float* k = s->hctl->k[0];
+    return max_vec_norm(k, k + s->N, k + 2 * (size_t)s->N, s->N, out);
+}
+static int k1_dot(SimImpl* s, float* out) {  // opencl.Dot(k1, k1), returned as float32
+    UMAG_TRY(sync_ctl_to_host(s));
+    double tot = 0;
+    for (int c = 0; c < 3; c++) {
+        const float* k = s->hctl->k[0] + (size_t)c * s->N;
+        double v;
+        UMAG_TRY(sum_dot(k, k, s->N, &v));
+        tot += v;
+    }
+    *out = (float)tot;
+    return UMAG_OK;
+}
+
+// engine/relax.go:23-112 Relax(): RK23 without precession, energy descent in
+// chunks of 3 steps, then torque descent with MaxErr lowered by sqrt(2)
+// down to 1e-9 (threshold <= 0), or steps while max |torque| > threshold.
+int sim_relax(umag_sim* h, double threshold) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s, "NULL argument");
+    UMAG_TRY(sync_ctl_to_host(s));
+    const int prev_solver = s->sp.solver, prev_precess = s->la.precess;
+    const double prev_err = s->hctl->max_err, prev_fix = s->hctl->fix_dt;
+    set_stepper(s, 3, 0);
+    s->hctl->fix_dt = 0;
+    UMAG_TRY(push_ctl(s));
+    auto body = [&]() -> int {
+        const int n = 3;  // evaluate the energy every 3 steps (relax.go:54)
+        double E[5];
+        UMAG_TRY(relax_steps(s, n));
+        UMAG_TRY(sim_energies(h, E));
+        double E0 = E[0];
+        UMAG_TRY(relax_steps(s, n));
+        UMAG_TRY(sim_energies(h, E));
+        double E1 = E[0];
+        for (int guard = 0; E1 < E0 && guard < 1000000; guard++) {
+            UMAG_TRY(relax_steps(s, n));
+            UMAG_TRY(sim_energies(h, E));
+            E0 = E1;
+            E1 = E[0];
+        }
+        if (threshold > 0) {
+            for (;;) {
+                double mt;
+                UMAG_TRY(k1_max_norm(s, &mt));
+                for (int guard = 0; mt > threshold && guard < 1000000; guard++) {
+                    UMAG_TRY(relax_steps(s, n));
+                    UMAG_TRY(k1_max_norm(s, &mt));
+                }
+                UMAG_TRY(sync_ctl_to_host(s));
+                s->hctl->max_err /= std::sqrt(2.0);
+                UMAG_TRY(push_ctl(s));
+                if (s->hctl->max_err < 1e-9) break;
+            }
+        } else {
+            float T0 = 0, T1;
+            UMAG_TRY(k1_dot(s, &T1));
+            for (;;) {
+                UMAG_TRY(sync_ctl_to_host(s));
+                if (!(s->hctl->max_err > 1e-9)) break;
+                s->hctl->max_err /= std::sqrt(2.0);
+                UMAG_TRY(push_ctl(s));
+                UMAG_TRY(relax_steps(s, n));
+                T0 = T1;
+                UMAG_TRY(k1_dot(s, &T1));
+                for (int guard = 0; T1 < T0 && guard < 1000000; guard++) {
+                    UMAG_TRY(relax_steps(s, n));
+                    T0 = T1;
+                    UMAG_TRY(k1_dot(s, &T1));
+                }
+            }
+        }
+        return UMAG_OK;
+    };
+    const int st = body();
+    // restore the caller's settings (relax.go:36-45)
+    sync_ctl_to_host(s);
+    s->hctl->max_err = prev_err;
+    s->hctl->fix_dt = prev_fix;
+    push_ctl(s);
+    set_stepper(s, prev_solver, prev_precess);
+    return st;
 }
 
 int sim_launches_per_step(umag_sim* h, int* n) {

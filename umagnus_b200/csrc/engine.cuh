@@ -17,4 +17,6 @@ int sim_average_m(umag_sim* s, double avg[3]);
 int sim_use_graph(umag_sim* s, int enable, int steps);
 int sim_launches_per_step(umag_sim* s, int* n);
 int sim_torque_evals(umag_sim* s, int n);
+int sim_energies(umag_sim* s, double E[5]);
+int sim_relax(umag_sim* s, double threshold);
 }  // namespace umag

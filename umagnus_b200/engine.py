@@ -197,6 +197,31 @@ class Simulation:
         check(self.L.umag_sim_average_m(self._h, out))
         return [out[0], out[1], out[2]]
 
+    def set_B_ext(self, B_ext):
+        """Change the applied field (engine/zeeman.go B_ext = ...): a 3-vector (T)
+        or (256, 3) per-region values.  The simulation must have been created
+        with a B_ext (possibly zero); the device table is overwritten in place,
+        so captured step graphs see the new value."""
+        if getattr(self, "bext", None) is None:
+            raise UmagError("set_B_ext needs a Simulation created with B_ext")
+        b = np.asarray(B_ext, np.float32)
+        lut = np.tile(b, (NREGION, 1)) if b.ndim == 1 else b
+        torch.cuda.synchronize()
+        self.sync()
+        self.bext.copy_(torch.from_numpy(np.ascontiguousarray(lut.T)))
+        torch.cuda.synchronize()
+
+    def energies(self):
+        """engine/energy.go:27 GetTotalEnergy and its terms (J) for the current m:
+        dict with total, demag, exchange (incl. DMI), anisotropy, zeeman."""
+        out = (ctypes.c_double * 5)()
+        check(self.L.umag_sim_energies(self._h, out))
+        return dict(zip(("total", "demag", "exchange", "anisotropy", "zeeman"), list(out)))
+
+    def relax(self, torque_threshold=-1.0):
+        """engine/relax.go:23 Relax() (RelaxTorqueThreshold = torque_threshold)."""
+        check(self.L.umag_sim_relax(self._h, float(torque_threshold)))
+
     def use_graph(self, enable=True, steps_per_graph=16):
         check(self.L.umag_sim_use_graph(self._h, int(bool(enable)), int(steps_per_graph)))
 

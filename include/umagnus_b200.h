@@ -260,6 +260,34 @@ int umag_sim_energies(umag_sim* s, double E[5]);
  * precession are restored afterwards. */
 int umag_sim_relax(umag_sim* s, double torque_threshold);
 
+/* ---- field files (oommf/*.go, dump/*.go) ----------------------------------
+ * Host arrays of float32, structure of arrays [c][z][y][x] (x fastest), the
+ * layout of data.Slice.Tensors(); numbers in headers and text data are
+ * written as the reference's Go fmt %v writes them. */
+typedef struct {
+    int N[3];          /* xnodes, ynodes, znodes */
+    int ncomp;         /* valuedim */
+    double cell[3];    /* x/y/z stepsize (m) */
+    double time;       /* total simulation time (s) */
+    char title[64];
+    char unit[32];
+} umag_field_info;
+/* oommf/oommf.go:16-46 Read / ReadFile and dump/read.go:17 Read: OVF 1.0
+ * (text, binary 4, binary 8, big-endian), OVF 2.0 (text, binary 4,
+ * binary 8) or the "#dump002" format (CRC-64 checked), detected from the
+ * file's first bytes.  _info reads the header only. */
+int umag_field_read_info(const char* path, umag_field_info* info);
+int umag_field_read(const char* path, float* dst, size_t capacity, umag_field_info* info);
+/* oommf/ovf2.go:13 WriteOVF2 (version 2) and oommf/ovf1.go:14 WriteOVF1
+ * (version 1, 3 components only); format "text" or "binary 4". */
+int umag_ovf_write(const char* path, const float* src, const umag_field_info* info, const char* format,
+                   int version);
+/* dump/write.go:17 Write: the legacy "#dump002" format with its CRC-64. */
+int umag_dump_write(const char* path, const float* src, const umag_field_info* info);
+/* A number as Go's fmt %v prints it (bits 64: float64, 32: float32), as
+ * the table writer (engine/table.go:112-133) needs. */
+int umag_format_float(double v, int bits, char* buf, int cap);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -83,6 +83,9 @@ _SIGS = {
     "umag_sim_use_graph": [P, c_int, c_int], "umag_sim_launches_per_step": [P, ctypes.POINTER(c_int)],
     "umag_sim_torque_evals": [P, c_int],
     "umag_sim_energies": [P, ctypes.POINTER(c_double)], "umag_sim_relax": [P, c_double],
+    "umag_field_read_info": [ctypes.c_char_p, P], "umag_field_read": [ctypes.c_char_p, P, c_size_t, P],
+    "umag_ovf_write": [ctypes.c_char_p, P, P, ctypes.c_char_p, c_int], "umag_dump_write": [ctypes.c_char_p, P, P],
+    "umag_format_float": [c_double, c_int, ctypes.c_char_p, c_int],
 }
 _RESTYPE = {"umag_last_error": ctypes.c_char_p, "umag_version": ctypes.c_char_p, "umag_solver_defaults": None}
 

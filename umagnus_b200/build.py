@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libumagnus_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["ops.cu", "demag.cu", "demag_fast.cu", "engine.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["ops.cu", "demag.cu", "demag_fast.cu", "engine.cu", "capi.cu", "noalloc.cu", "ovf.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",

@@ -134,6 +134,13 @@ typedef struct umag_demag umag_demag;
 int umag_demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy,
                           double cz, int asymptotic_radius, int zero_self_demag,
                           umag_demag** out);
+/* engine/demag.go:124-133 demagConv with EnableDemag (the reference's
+ * default): mag/demagkernel.go:113-336 CalcDemagKernel, the brute-force
+ * kernel (face charges integrated over the cells, point counts set by
+ * `accuracy`, DemagAccuracy = 6 by default), built in FP64 on the GPU and
+ * rounded to float32 like the reference's kernel slices. */
+int umag_demag_new_brute(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy, double cz,
+                         double accuracy, umag_demag** out);
 /* opencl/conv_demag.go:27 NewDemag with a caller-supplied real-space kernel:
  * six host arrays (xx, yy, zz, yz, xz, xy) on the padded grid, doubles. */
 int umag_demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6],
@@ -198,6 +205,8 @@ typedef struct {
     int openbc;                    /* engine/exchange.go OpenBC */
     int precess;                   /* engine/torque.go Precess */
     int asymptotic_radius;         /* engine/demag.go:27, default 32 */
+    int demag_kernel;              /* 0 Newell (EnableNewellDemag), 1 brute force (EnableDemag) */
+    double demag_accuracy;         /* brute force: DemagAccuracy (engine/demag.go:25); <= 0 -> 6 */
 } umag_sim_params;
 
 /* Solver knobs, engine/run.go:14-43 (defaults by umag_solver_defaults). */

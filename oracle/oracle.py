@@ -66,6 +66,7 @@ class OrcSolver(ctypes.Structure):
 def _declare(L):
     L.orc_pad_size.argtypes = [ip, ip, ip]
     L.orc_newell_kernel.argtypes = [ip, ip, f64p, ctypes.c_int, ctypes.c_int, f64p * 6]
+    L.orc_brute_kernel.argtypes = [ip, ip, f64p, ctypes.c_double, ctypes.POINTER(ctypes.c_float) * 6]
     L.orc_newell_f.restype = ctypes.c_double
     L.orc_newell_g.restype = ctypes.c_double
     L.orc_self_demag_nx.restype = ctypes.c_double
@@ -122,6 +123,18 @@ def newell_kernel(size, cellsize, pbc=(0, 0, 0), asymptotic_radius=32, zero_self
     ptrs = (f64p * 6)(*[K[c].ctypes.data_as(f64p) for c in range(6)])
     lib().orc_newell_kernel((ctypes.c_int * 3)(*size), (ctypes.c_int * 3)(*pbc),
                             (ctypes.c_double * 3)(*cellsize), asymptotic_radius, zero_self_demag, ptrs)
+    return K
+
+
+def brute_kernel(size, cellsize, pbc=(0, 0, 0), accuracy=6.0):
+    """mag/demagkernel.go:113 CalcDemagKernel (engine/demag.go:25 DemagAccuracy = 6):
+    float32 real-space kernel (xx, yy, zz, yz, xz, xy), shape (6, Pz, Py, Px)."""
+    P = pad_size(size, pbc)
+    K = np.zeros((6, P[2], P[1], P[0]), dtype=np.float32)
+    f32p = ctypes.POINTER(ctypes.c_float)
+    ptrs = (f32p * 6)(*[K[c].ctypes.data_as(f32p) for c in range(6)])
+    lib().orc_brute_kernel((ctypes.c_int * 3)(*size), (ctypes.c_int * 3)(*pbc), (ctypes.c_double * 3)(*cellsize),
+                           float(accuracy), ptrs)
     return K
 
 

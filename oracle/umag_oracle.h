@@ -35,6 +35,12 @@ void orc_pad_size(const int size[3], const int pbc[3], int padded[3]);
 int orc_newell_kernel(const int size[3], const int pbc[3], const double cellsize[3],
                       int asymptotic_radius, int zero_self_demag, double* K[6]);
 
+/* mag/demagkernel.go:113-336 CalcDemagKernel: brute-force kernel (FP64
+ * integration, float32 result as the reference stores it), six arrays
+ * (xx yy zz yz xz xy) of the padded grid. */
+int orc_brute_kernel(const int size[3], const int pbc[3], const double cellsize[3], double accuracy,
+                     float* const K[6]);
+
 /* Individual Newell pieces, exported for the golden tests. */
 double orc_newell_f(double x, double y, double z);
 double orc_newell_g(double x, double y, double z);

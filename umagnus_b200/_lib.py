@@ -29,6 +29,7 @@ class SimParams(ctypes.Structure):
         ("anisU", P * 3), ("anisU_mul", c_float * 3),
         ("aLUT", P), ("dLUT", P), ("bextLUT", P * 3),
         ("enable_demag", c_int), ("openbc", c_int), ("precess", c_int), ("asymptotic_radius", c_int),
+        ("demag_kernel", c_int), ("demag_accuracy", c_double),
     ]
 
 
@@ -70,6 +71,7 @@ _SIGS = {
                               ctypes.POINTER(c_void_p)],
     "umag_demag_new_from_kernel": [c_int, c_int, c_int, P, ctypes.POINTER(c_void_p)],
     "umag_demag_exec": [P, P, P, P, P, P, P, P, P, c_float],
+    "umag_demag_new_brute": [c_int, c_int, c_int, P, c_double, c_double, c_double, c_double, P],
     "umag_demag_exec_pass": [P, c_int, P, P, P, P, P, P, P, P, c_float],
     "umag_demag_get_spectrum": [P, P], "umag_demag_get_kernel": [P, P],
     "umag_demag_padded_size": [P, ctypes.POINTER(c_int)], "umag_demag_free": [P],

@@ -8,7 +8,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libumagnus_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["ops.cu", "demag.cu", "demag_fast.cu", "engine.cu", "capi.cu", "noalloc.cu", "ovf.cu"]
+SOURCES = ["ops.cu", "demag.cu", "demag_fast.cu", "engine.cu", "capi.cu", "noalloc.cu", "ovf.cu", "brute.cu"]
+# per-file flags: the brute-force kernel keeps the reference's FP64 operation
+# order (no fused multiply-adds)
+FILE_FLAGS = {"brute.cu": ["-fmad=false"]}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -32,7 +35,7 @@ def build(verbose=False, force=False, ptxas_info=False):
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _needs(o, [s] + headers):
-            cmd = [NVCC] + ARCH + FLAGS + ["-c", s, "-o", o]
+            cmd = [NVCC] + ARCH + FLAGS + FILE_FLAGS.get(src, []) + ["-c", s, "-o", o]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             if verbose:

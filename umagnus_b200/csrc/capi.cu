@@ -119,6 +119,10 @@ int umag_demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, d
                           int asymptotic_radius, int zero_self_demag, umag_demag** out) {
     return demag_new_newell(Nx, Ny, Nz, pbc, cx, cy, cz, asymptotic_radius, zero_self_demag, out);
 }
+int umag_demag_new_brute(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy, double cz, double accuracy,
+                         umag_demag** out) {
+    return demag_new_brute(Nx, Ny, Nz, pbc, cx, cy, cz, accuracy, out);
+}
 int umag_demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6], umag_demag** out) {
     return demag_new_from_kernel(Nx, Ny, Nz, kern, out);
 }

@@ -594,11 +594,41 @@ int demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double
     return UMAG_OK;
 }
 
+// mag/demagkernel.go:113 CalcDemagKernel (engine/demag.go:124-133 demagConv):
+// the brute-force kernel built on the GPU, FFT'd in FP64 like the Newell one
+int demag_new_brute(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy, double cz, double accuracy,
+                    umag_demag** out) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(out != nullptr, "out is NULL");
+    if (pbc && (pbc[0] || pbc[1] || pbc[2]))
+        return set_error(UMAG_E_UNSUPPORTED, "periodic boundary conditions are not supported by this build");
+    UMAG_REQUIRE(cx > 0 && cy > 0 && cz > 0, "cell size must be positive");
+    UMAG_REQUIRE(accuracy > 0, "demag accuracy must be positive");
+    umag_demag* d = new umag_demag();
+    d->N[0] = Nx; d->N[1] = Ny; d->N[2] = Nz;
+    d->cell[0] = cx; d->cell[1] = cy; d->cell[2] = cz;
+    d->kind = 1;
+    d->accuracy = accuracy;
+    int s = plan_common(d);
+    if (s != UMAG_OK) { demag_free(d); return s; }
+    cudaStream_t st = ctx().stream;
+    long n = (long)d->P[0] * d->P[1] * d->P[2];
+    double* Kr[6] = {};
+    for (int c = 0; c < 6 && s == UMAG_OK; c++)
+        if (cudaMalloc(&Kr[c], sizeof(double) * n) != cudaSuccess) s = set_error(UMAG_E_NOMEM, "kernel buffers");
+    if (s == UMAG_OK) s = build_brute(d, accuracy, Kr, st);
+    if (s == UMAG_OK) s = kernel_to_spectrum(d, Kr, st);
+    for (int c = 0; c < 6; c++) cudaFree(Kr[c]);
+    if (s != UMAG_OK) { demag_free(d); return s; }
+    *out = d;
+    return UMAG_OK;
+}
 int demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6], umag_demag** out) {
     UMAG_TRY(ensure_init());
     UMAG_REQUIRE(out != nullptr && kern != nullptr, "NULL argument");
     umag_demag* d = new umag_demag();
     d->N[0] = Nx; d->N[1] = Ny; d->N[2] = Nz;
+    d->kind = 2;
     int s = plan_common(d);
     if (s != UMAG_OK) { demag_free(d); return s; }
     long n = (long)d->P[0] * d->P[1] * d->P[2];
@@ -622,7 +652,11 @@ int demag_get_kernel(umag_demag* d, double* const host[6]) {
     int s = UMAG_OK;
     for (int c = 0; c < 6 && s == UMAG_OK; c++)
         if (cudaMalloc(&Kr[c], sizeof(double) * n) != cudaSuccess) s = set_error(UMAG_E_NOMEM, "kernel buffers");
-    if (s == UMAG_OK) s = build_newell(d, d->cell, d->arad, d->zero_self, Kr, ctx().stream);
+    if (s == UMAG_OK) {
+        if (d->kind == 0) s = build_newell(d, d->cell, d->arad, d->zero_self, Kr, ctx().stream);
+        else if (d->kind == 1) s = build_brute(d, d->accuracy, Kr, ctx().stream);
+        else s = set_error(UMAG_E_UNSUPPORTED, "the plan was built from a caller-supplied kernel, which it does not keep");
+    }
     for (int c = 0; c < 6 && s == UMAG_OK; c++)
         if (host[c] && cudaMemcpy(host[c], Kr[c], sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
             s = set_error(UMAG_E_CUDA, "copy kernel");

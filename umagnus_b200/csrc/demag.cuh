@@ -34,6 +34,8 @@ struct umag_demag {
     int N[3], P[3];
     double cell[3];
     int arad, zero_self;
+    int kind = 0;           // real-space kernel: 0 Newell, 1 brute force, 2 caller-supplied
+    double accuracy = 6.0;  // brute force: DemagAccuracy (engine/demag.go:25)
     int M, Hx, HxP, Lx, WB;
     bool is2d;
     umag::FftLine<float> fx, fy, fz;  // x: length Px/2 (packed real), y: Py, z: Pz
@@ -76,6 +78,10 @@ struct PassArgs {
 int demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy, double cz, int arad,
                      int zero_self, umag_demag** out);
 int demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6], umag_demag** out);
+int demag_new_brute(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy, double cz, double accuracy,
+                    umag_demag** out);
+// brute-force real-space kernel (brute.cu) into six device arrays of the padded grid
+int build_brute(const umag_demag* d, double accuracy, double* Kr[6], cudaStream_t st);
 int demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
                const float* vol, const float* Ms, float Ms_mul, int pass = -1);
 int demag_get_kernel(umag_demag* d, double* const host[6]);

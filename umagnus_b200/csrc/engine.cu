@@ -771,8 +771,12 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
     }
     if (p->enable_demag) {
         int pbc[3] = {0, 0, 0};
-        st = demag_new_newell(p->N[0], p->N[1], p->N[2], pbc, p->cell[0], p->cell[1], p->cell[2],
-                              p->asymptotic_radius > 0 ? p->asymptotic_radius : 32, 0, &s->demag);
+        if (p->demag_kernel == 1)
+            st = demag_new_brute(p->N[0], p->N[1], p->N[2], pbc, p->cell[0], p->cell[1], p->cell[2],
+                                 p->demag_accuracy > 0 ? p->demag_accuracy : 6.0, &s->demag);
+        else
+            st = demag_new_newell(p->N[0], p->N[1], p->N[2], pbc, p->cell[0], p->cell[1], p->cell[2],
+                                  p->asymptotic_radius > 0 ? p->asymptotic_radius : 32, 0, &s->demag);
         if (st != UMAG_OK) return fail(st);
         if (cudaMalloc(&s->bd, b3) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "demag field"));
     }

@@ -73,13 +73,15 @@ class Simulation:
     N: (Nx, Ny, Nz); cell: cell size in m; Msat, alpha, Ku1, Ku2: scalar or
     per-cell (Nz, Ny, Nx) array; Aex, Dind: scalar or 256 per-region values;
     anisU: 3-vector or (3, Nz, Ny, Nx); B_ext: 3-vector (T) or (256, 3)
-    per-region; regions: uint8 (Nz, Ny, Nx) map; geom: cell volume fraction.
+    per-region; regions: uint8 (Nz, Ny, Nx) map; geom: cell volume fraction;
+    demag_kernel: "newell" (EnableNewellDemag) or "brute" (EnableDemag, the
+    reference default, with DemagAccuracy = demag_accuracy).
     """
 
     def __init__(self, N, cell, Msat, Aex, alpha, Dind=0.0, Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
                  regions=None, geom=None, demag=True, open_bc=False, precess=True, solver=DORMANDPRINCE,
                  dt=1e-15, MaxErr=1e-5, RelErr=1e-4, MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8,
-                 device=0, asymptotic_radius=32):
+                 device=0, asymptotic_radius=32, demag_kernel="newell", demag_accuracy=6.0):
         self.L = _lib.init(device)
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
@@ -130,6 +132,11 @@ class Simulation:
         p.openbc = int(bool(open_bc))
         p.precess = int(bool(precess))
         p.asymptotic_radius = int(asymptotic_radius)
+        # engine/demag.go:21-27: EnableDemag (brute force, the reference default) or EnableNewellDemag
+        if demag_kernel not in ("newell", "brute"):
+            raise ValueError("demag_kernel must be 'newell' or 'brute'")
+        p.demag_kernel = 1 if demag_kernel == "brute" else 0
+        p.demag_accuracy = float(demag_accuracy)
         sp = SolverParams()
         self.L.umag_solver_defaults(ctypes.byref(sp))
         sp.solver = int(solver)

@@ -17,7 +17,7 @@ from ._lib import UmagError, check
 __all__ = ["Init", "ReleaseAndClean", "NewSlice", "Zero", "Memset", "Mesh", "MSlice", "AddExchange", "AddDMI",
            "AddUniaxialAnisotropy2", "RegionAddV", "RegionDecode", "LLTorque", "LLNoPrecess", "Madd", "Madd2",
            "Madd3", "Madd4", "Madd5", "Madd6", "Madd7", "Normalize", "VecNorm", "Div", "AddDotProduct", "MaxVecNorm",
-           "MaxVecDiff", "MaxAbs", "Sum", "Dot", "DemagConvolution", "NewNewellDemag", "NewDemag", "UmagError",
+           "MaxVecDiff", "MaxAbs", "Sum", "Dot", "DemagConvolution", "NewNewellDemag", "NewBruteDemag", "NewDemag", "UmagError",
            "Sync"]
 
 
@@ -394,6 +394,18 @@ def NewNewellDemag(inputSize, PBC, cellsize, asymptotic_radius=32, zero_self_dem
     pbc = (ctypes.c_int * 3)(*PBC)
     check(L.umag_demag_new_newell(inputSize[0], inputSize[1], inputSize[2], pbc, cellsize[0], cellsize[1],
                                   cellsize[2], asymptotic_radius, zero_self_demag, ctypes.byref(h)))
+    return DemagConvolution(h.value, inputSize)
+
+
+def NewBruteDemag(inputSize, PBC, cellsize, accuracy=6.0):
+    """engine/demag.go:124-133 demagConv with EnableDemag: mag/demagkernel.go:113
+    CalcDemagKernel (brute force, built on the GPU) + plan."""
+    import ctypes
+    L = _L()
+    h = ctypes.c_void_p()
+    pbc = (ctypes.c_int * 3)(*PBC)
+    check(L.umag_demag_new_brute(inputSize[0], inputSize[1], inputSize[2], pbc, cellsize[0], cellsize[1],
+                                 cellsize[2], float(accuracy), ctypes.byref(h)))
     return DemagConvolution(h.value, inputSize)
 
 

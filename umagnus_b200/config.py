@@ -54,3 +54,16 @@ def ellipsoid(N, cell, dx, dy, dz=np.inf):
 
 def ellipse(N, cell, dx, dy):
     return ellipsoid(N, cell, dx, dy)
+
+
+def two_domain(N, cell, m1, mwall, m2):
+    """engine/config.go TwoDomain: m1 for x < 0, m2 for x >= 0, a Gaussian
+    wall of width 2*cellsize_x blending in mwall."""
+    X, _, _ = coords(N, cell)
+    ww = 2 * cell[0]
+    gauss = np.exp(-((X / ww) ** 2))
+    out = []
+    for c in range(3):
+        side = np.where(X < 0, m1[c], m2[c])
+        out.append((1 - gauss) * side + gauss * mwall[c])
+    return np.stack(out).astype(np.float32)

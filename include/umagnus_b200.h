@@ -269,6 +269,35 @@ int umag_sim_energies(umag_sim* s, double E[5]);
  * precession are restored afterwards. */
 int umag_sim_relax(umag_sim* s, double torque_threshold);
 
+/* ---- ensembles: many independent simulations at once --------------------
+ * No counterpart in the reference, which runs one simulation per process.
+ * Each instance has its own mesh (instances with the same mesh and cell
+ * size are batched into one set of launches), its own uniform material and
+ * applied field, its own time, dt and step controller (the solver knobs of
+ * `sp` are shared); Newell demag when enable_demag.  Regions, per-cell maps,
+ * geometry masks and PBC are not supported here. */
+typedef struct {
+    int N[3];
+    double cell[3];
+    float Ms, Aex, alpha, Dind, Ku1, Ku2;
+    float anisU[3];
+    float B_ext[3];   /* T */
+} umag_ens_instance;
+typedef struct umag_ens umag_ens;
+int umag_ens_new(int n, const umag_ens_instance* instances, const umag_solver_params* sp, int enable_demag,
+                 umag_ens** out);
+int umag_ens_free(umag_ens* e);
+/* host arrays of 3*N floats (SoA); set_m normalises (engine/magnetization.go:34) */
+int umag_ens_set_m(umag_ens* e, int i, const float* host_m);
+int umag_ens_get_m(umag_ens* e, int i, float* host_m);
+int umag_ens_get_state(umag_ens* e, int i, umag_solver_state* st);
+/* engine/run.go:190 Run(seconds) for every instance from its own current
+ * time; steps are replayed from one CUDA graph (16 steps of every class per
+ * replay, finished instances idle), checked on the host every `chunk`
+ * replays, at most max_replays replays. */
+int umag_ens_run(umag_ens* e, double seconds, int chunk, long long max_replays);
+int umag_ens_count(umag_ens* e, int* n_instances, int* n_classes);
+
 /* ---- field files (oommf/*.go, dump/*.go) ----------------------------------
  * Host arrays of float32, structure of arrays [c][z][y][x] (x fastest), the
  * layout of data.Slice.Tensors(); numbers in headers and text data are

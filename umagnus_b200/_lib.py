@@ -45,6 +45,11 @@ class SolverState(ctypes.Structure):
                 ("status", c_int)]
 
 
+class EnsInstance(ctypes.Structure):
+    _fields_ = [("N", c_int * 3), ("cell", c_double * 3), ("Ms", c_float), ("Aex", c_float), ("alpha", c_float),
+                ("Dind", c_float), ("Ku1", c_float), ("Ku2", c_float), ("anisU", c_float * 3), ("B_ext", c_float * 3)]
+
+
 # name -> argtypes (restype int unless listed in _RESTYPE)
 _SIGS = {
     "umag_init": [c_int], "umag_release": [], "umag_last_error": [], "umag_set_stream": [P], "umag_sync": [],
@@ -88,6 +93,9 @@ _SIGS = {
     "umag_field_read_info": [ctypes.c_char_p, P], "umag_field_read": [ctypes.c_char_p, P, c_size_t, P],
     "umag_ovf_write": [ctypes.c_char_p, P, P, ctypes.c_char_p, c_int], "umag_dump_write": [ctypes.c_char_p, P, P],
     "umag_format_float": [c_double, c_int, ctypes.c_char_p, c_int],
+    "umag_ens_new": [c_int, P, P, c_int, ctypes.POINTER(c_void_p)], "umag_ens_free": [P],
+    "umag_ens_set_m": [P, c_int, P], "umag_ens_get_m": [P, c_int, P], "umag_ens_get_state": [P, c_int, P],
+    "umag_ens_run": [P, c_double, c_int, c_ll], "umag_ens_count": [P, ctypes.POINTER(c_int), ctypes.POINTER(c_int)],
 }
 _RESTYPE = {"umag_last_error": ctypes.c_char_p, "umag_version": ctypes.c_char_p, "umag_solver_defaults": None}
 

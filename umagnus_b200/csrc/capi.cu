@@ -184,5 +184,16 @@ int umag_sim_launches_per_step(umag_sim* s, int* n) { return sim_launches_per_st
 int umag_sim_torque_evals(umag_sim* s, int n) { return sim_torque_evals(s, n); }
 int umag_sim_energies(umag_sim* s, double E[5]) { return sim_energies(s, E); }
 int umag_sim_relax(umag_sim* s, double torque_threshold) { return sim_relax(s, torque_threshold); }
+int umag_ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int enable_demag, umag_ens** out) {
+    return ens_new(n, in, sp, enable_demag, out);
+}
+int umag_ens_free(umag_ens* e) { return ens_free(e); }
+int umag_ens_set_m(umag_ens* e, int i, const float* host_m) { return ens_set_m(e, i, host_m); }
+int umag_ens_get_m(umag_ens* e, int i, float* host_m) { return ens_get_m(e, i, host_m); }
+int umag_ens_get_state(umag_ens* e, int i, umag_solver_state* st) { return ens_get_state(e, i, st); }
+int umag_ens_run(umag_ens* e, double seconds, int chunk, long long max_replays) {
+    return ens_run(e, seconds, chunk, max_replays);
+}
+int umag_ens_count(umag_ens* e, int* n_instances, int* n_classes) { return ens_count(e, n_instances, n_classes); }
 
 }  // extern "C"

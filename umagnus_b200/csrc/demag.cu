@@ -725,6 +725,21 @@ int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st) {
     return UMAG_OK;
 }
 
+// the three passes for nb same-size instances at once (batched kernels; the
+// per-instance pointers are shifted by the strides in PassArgs)
+int demag_launch_batch(const umag_demag* d, const PassArgs& a, int nb, cudaStream_t st) {
+    UMAG_REQUIRE(d->use_fast && d->fast.ab && d->fast.bb && d->fast.cb, "batched demag needs a compile-time FFT plan");
+    UMAG_REQUIRE(nb >= 1 && 3L * nb <= 65535 && (long)d->fast.gby * nb <= 65535, "too many instances in one batch");
+    const FastPasses& f = d->fast;
+    f.ab<<<dim3(d->N[1], 3 * nb), f.nt_ac, f.smem_ac, st>>>(a);
+    UMAG_LAUNCH_CHECK();
+    f.bb<<<dim3(f.gbx, f.gby * nb), f.nt_b, f.smem_b, st>>>(a);
+    UMAG_LAUNCH_CHECK();
+    f.cb<<<dim3(d->N[1], 3 * nb), f.nt_ac, f.smem_ac, st>>>(a);
+    UMAG_LAUNCH_CHECK();
+    return UMAG_OK;
+}
+
 // one pass of demag_launch (0: A, 1: B, 2: C)
 static int demag_launch_pass(const umag_demag* d, const PassArgs& a, cudaStream_t st, int pass) {
     if (d->use_fast) {

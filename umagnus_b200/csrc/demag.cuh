@@ -16,6 +16,10 @@ struct FastPasses {
     void (*a)(PassArgs) = nullptr;
     void (*b)(PassArgs) = nullptr;
     void (*c)(PassArgs) = nullptr;
+    // batched variants (grid.y extended by the instance count; demag_batch_fix)
+    void (*ab)(PassArgs) = nullptr;
+    void (*bb)(PassArgs) = nullptr;
+    void (*cb)(PassArgs) = nullptr;
     size_t smem_ac = 0, smem_b = 0;
     int wb = 0;
     int nt_b = 512;   // threads per pass-B CTA
@@ -60,6 +64,11 @@ struct PassArgs {
     // (else rows [c][kz][y][kx]); Kblocked = kernel arrays in 4-column blocks
     // [kz][kx/4][ky][kx%4] (else rows [kz][ky][kx] of pitch Kp)
     int blocked, Kblocked;
+    // batched launches: per-instance strides of the spectrum scratch (float2),
+    // of the field output (floats) and of the controller structs holding
+    // m_ind / m_ind_w / active (bytes); per-instance Ms (NULL: Ms_mul for all)
+    long spec_stride, b_stride, ctl_stride;
+    const float* ms_mul_b;
     const float* m[3];
     // engine use: magnetisation read through a device-side slot
     // (m_sel ? *m_ind_w : *m_ind) + c*ncell, and a device flag that turns a
@@ -89,6 +98,7 @@ int demag_get_spectrum(umag_demag* d, float* const host[6]);
 void demag_free(umag_demag* d);
 void fill_pass_args(const umag_demag* d, PassArgs& a);
 int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st);
+int demag_launch_batch(const umag_demag* d, const PassArgs& a, int nb, cudaStream_t st);
 bool demag_fast_select(int M, int Py, int Pz, FastPasses& f);
 // pass-B launch grid for a selected plan (after demag_fast_setup; current device)
 int demag_fast_grid(FastPasses& f, int M, int Pz);

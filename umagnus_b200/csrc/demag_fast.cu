@@ -36,8 +36,21 @@ __device__ __forceinline__ float scaled_m(const PassArgs& a, const float* __rest
     return __fmul_rn(__fmul_rn(bsat, w), __ldg(m + i));
 }
 
+// Batched launches (an ensemble of same-size instances): shift the pointers
+// of PassArgs to instance b -- spectrum scratch, field output, the
+// instance's controller fields (m slots, active flag) and its Ms.
+__device__ __forceinline__ void demag_batch_fix(PassArgs& A, int b) {
+    A.spec += (long)b * A.spec_stride;
+    for (int c = 0; c < 3; c++) A.B[c] += (long)b * A.b_stride;
+    const long o = (long)b * A.ctl_stride;
+    if (A.m_ind) A.m_ind = reinterpret_cast<float* const*>(reinterpret_cast<const char*>(A.m_ind) + o);
+    if (A.m_ind_w) A.m_ind_w = reinterpret_cast<float* const*>(reinterpret_cast<const char*>(A.m_ind_w) + o);
+    if (A.active) A.active = reinterpret_cast<const int*>(reinterpret_cast<const char*>(A.active) + o);
+    if (A.ms_mul_b) A.Ms_mul = A.ms_mul_b[b];
+}
+
 template <int M, int PZ>
-__global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) {
+__device__ __forceinline__ void k_fast_a_body(const PassArgs& a, const int bx, const int by) {
     using S = AcShape<M, PZ>;
     constexpr int NZ = S::NZ, XP = S::XP, CW = S::CW, H = M / 2;
     extern __shared__ __align__(16) float2 sm[];
@@ -52,7 +65,7 @@ __global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) {
     if (PZ > 1)
         for (int i = tid; i < PZ; i += kNT) twz[i] = a.fz.tw[i];
     for (int i = tid; i <= H; i += kNT) twr[i] = a.twr[i];
-    const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
+    const int y = bx, c = by, Ny = a.Ny;
     const float* __restrict__ m = a.m_ind ? (a.m_sel ? *a.m_ind_w : *a.m_ind) + (long)c * a.ncell : a.m[c];
     // 1. scaled m, pairs of reals packed into complex (x = 2n, 2n+1), Nx = M
     for (int e = tid; e < NZ * M; e += kNT) {
@@ -109,9 +122,19 @@ __global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) {
         for (int kz = tid; kz < PZ; kz += kNT) out[kz * kzs + M] = Z2[kz];
     }
 }
+template <int M, int PZ>
+__global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) { k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y); }
+// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+template <int M, int PZ>
+__global__ void __launch_bounds__(kNT) k_fast_a_bat(PassArgs a) {
+    const int per = 3, b = blockIdx.y / per;
+    PassArgs A = a;
+    demag_batch_fix(A, b);
+    k_fast_a_body<M, PZ>(A, blockIdx.x, blockIdx.y - b * per);
+}
 
 template <int M, int PZ>
-__global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) {
+__device__ __forceinline__ void k_fast_c_body(const PassArgs& a, const int bx, const int by) {
     using S = AcShape<M, PZ>;
     constexpr int NZ = S::NZ, XP = S::XP, CW = S::CW, H = M / 2;
     extern __shared__ __align__(16) float2 sm[];
@@ -126,7 +149,7 @@ __global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) {
     if (PZ > 1)
         for (int i = tid; i < PZ; i += kNT) twz[i] = a.fz.tw[i];
     for (int i = tid; i <= H; i += kNT) twr[i] = a.twr[i];
-    const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
+    const int y = bx, c = by, Ny = a.Ny;
     const float2* in = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
     const long kzs = (long)Ny * a.Lx;
     // 1. inverse z FFT per block of columns, keep z < NZ
@@ -187,6 +210,16 @@ __global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) {
         *reinterpret_cast<float2*>(B + (z * Ny + y) * M + 2 * n) = v;
     }
 }
+template <int M, int PZ>
+__global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) { k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y); }
+// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+template <int M, int PZ>
+__global__ void __launch_bounds__(kNT) k_fast_c_bat(PassArgs a) {
+    const int per = 3, b = blockIdx.y / per;
+    PassArgs A = a;
+    demag_batch_fix(A, b);
+    k_fast_c_body<M, PZ>(A, blockIdx.x, blockIdx.y - b * per);
+}
 
 template <int PY> struct BShape {
     static constexpr int WB0 = (kElemCap * kNTB) / (3 * PY);
@@ -195,7 +228,7 @@ template <int PY> struct BShape {
 };
 
 template <int PY>
-__global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) {
+__device__ __forceinline__ void k_fast_b_body(const PassArgs& a, const int bx, const int by) {
     constexpr int WB = BShape<PY>::WB, W3 = 3 * WB, NY = PY / 2, HY = PY / 2 + 1;
     extern __shared__ __align__(16) float2 sm[];
     float2* twy = sm;
@@ -203,7 +236,7 @@ __global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) {
     if (a.active && !*a.active) return;
     const int tid = threadIdx.x;
     for (int i = tid; i < PY; i += kNTB) twy[i] = a.fy.tw[i];
-    const int kx0 = blockIdx.x * WB, kz = blockIdx.y;
+    const int kx0 = bx * WB, kz = by;
     const int hx = a.Hx, Pz = a.Pz;
     const long cs = (long)Pz * NY * a.Lx;
     const float2* in = a.spec + (long)kz * NY * a.Lx + kx0;
@@ -249,6 +282,16 @@ __global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) {
         if (kx0 + w < hx) outp[c * cs + (long)yy * a.Lx + w] = S[e];
     }
 }
+template <int PY>
+__global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) { k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y); }
+// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+template <int PY>
+__global__ void __launch_bounds__(kNTB) k_fast_b_bat(PassArgs a) {
+    const int per = a.Pz, b = blockIdx.y / per;
+    PassArgs A = a;
+    demag_batch_fix(A, b);
+    k_fast_b_body<PY>(A, blockIdx.x, blockIdx.y - b * per);
+}
 
 // cp.async (global -> shared, asynchronous) helpers
 __device__ __forceinline__ void cpa16(void* dst, const void* src) {
@@ -285,7 +328,7 @@ __device__ __forceinline__ long kern_idx(const PassArgs& a, int kz, int ky, int 
 // With the blocked layouts a warp's loads and stores of one component are one
 // contiguous run (WB = 4: 8 rows x 4 columns = 256 bytes).
 template <int PY, int WB>
-__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
+__device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, const int by) {
     constexpr int T = PY / 8, NT = T * WB, NY = PY / 2, HY = PY / 2 + 1;
     constexpr int LP = rg_line<PY>();
     extern __shared__ __align__(16) float2 sm[];
@@ -296,7 +339,7 @@ __global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
     const int tid = threadIdx.x;
     const int w = tid % WB, t = tid / WB;
     for (int i = tid; i < PY; i += NT) tw[i] = a.fy.tw[i];
-    const int kx0 = blockIdx.x * WB, kz = blockIdx.y;
+    const int kx0 = bx * WB, kz = by;
     const int kx = kx0 + w, hx = a.Hx, Pz = a.Pz;
     // the kernel block this CTA multiplies with: asynchronous copies that
     // complete while the forward transform runs
@@ -381,6 +424,16 @@ __global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
             }
     }
 }
+template <int PY, int WB>
+__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) { k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y); }
+// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+template <int PY, int WB>
+__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b_bat(PassArgs a) {
+    const int per = a.Pz, b = blockIdx.y / per;
+    PassArgs A = a;
+    demag_batch_fix(A, b);
+    k_reg_b_body<PY, WB>(A, blockIdx.x, blockIdx.y - b * per);
+}
 
 // ---- passes A and C with the register-blocked FFT (3D, power-of-two sizes)
 // x transform: TX = M/8 threads per row (one row per warp or less), rows z
@@ -395,7 +448,7 @@ template <int M, int PZ> struct RegAC {
 };
 
 template <int M, int PZ>
-__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) {
+__device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, const int by) {
     using S = RegAC<M, PZ>;
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
     extern __shared__ __align__(16) float2 sm[];
@@ -408,7 +461,7 @@ __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) {
     const int tid = threadIdx.x;
     for (int i = tid; i < M; i += NT) { twx[i] = a.fx.tw[i]; twr[i] = a.twr[i]; }
     for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
-    const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
+    const int y = bx, c = by, Ny = a.Ny;
     const float* __restrict__ mp = a.m_ind ? (a.m_sel ? *a.m_ind_w : *a.m_ind) + (long)c * a.ncell : a.m[c];
     // x phase: row z, lane t holds packed z[n] = x[2n] + i x[2n+1], n = t + TX*j
     const int z = tid / TX, t = tid % TX;
@@ -544,9 +597,19 @@ __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) {
         }
     }
 }
+template <int M, int PZ>
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) { k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y); }
+// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+template <int M, int PZ>
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a_bat(PassArgs a) {
+    const int per = 3, b = blockIdx.y / per;
+    PassArgs A = a;
+    demag_batch_fix(A, b);
+    k_reg_a_body<M, PZ>(A, blockIdx.x, blockIdx.y - b * per);
+}
 
 template <int M, int PZ>
-__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) {
+__device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, const int by) {
     using S = RegAC<M, PZ>;
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
     extern __shared__ __align__(16) float2 sm[];
@@ -560,7 +623,7 @@ __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) {
     for (int i = tid; i < M; i += NT) { twx[i] = a.fx.tw[i]; twr[i] = a.twr[i]; }
     for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
     __syncthreads();
-    const int y = blockIdx.x, c = blockIdx.y, Ny = a.Ny;
+    const int y = bx, c = by, Ny = a.Ny;
     const float2* in = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
     const long kzs = (long)Ny * a.Lx;
     if constexpr (PZ == 16 || PZ == 32) {
@@ -674,6 +737,16 @@ __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) {
         *reinterpret_cast<float2*>(B + rowo + 2 * n) = make_float2(v[0][j].x, -v[0][j].y);
     }
 }
+template <int M, int PZ>
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) { k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y); }
+// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+template <int M, int PZ>
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c_bat(PassArgs a) {
+    const int per = 3, b = blockIdx.y / per;
+    PassArgs A = a;
+    demag_batch_fix(A, b);
+    k_reg_c_body<M, PZ>(A, blockIdx.x, blockIdx.y - b * per);
+}
 
 template <int PY> struct RegB {
     static constexpr int T = PY / 8;
@@ -688,12 +761,16 @@ template <int M, int PZ> static void fill_ac(FastPasses& f) {
     if constexpr (RegAC<M, PZ>::ok && PZ >= 8) {
         f.a = k_reg_a<M, PZ>;
         f.c = k_reg_c<M, PZ>;
+        f.ab = k_reg_a_bat<M, PZ>;
+        f.cb = k_reg_c_bat<M, PZ>;
         f.smem_ac = RegAC<M, PZ>::smem;
         f.nt_ac = RegAC<M, PZ>::NT;
         f.ac_reg = true;
     } else {
         f.a = k_fast_a<M, PZ>;
         f.c = k_fast_c<M, PZ>;
+        f.ab = k_fast_a_bat<M, PZ>;
+        f.cb = k_fast_c_bat<M, PZ>;
         f.smem_ac = AcShape<M, PZ>::smem;
         f.nt_ac = kNT;
     }
@@ -701,12 +778,14 @@ template <int M, int PZ> static void fill_ac(FastPasses& f) {
 template <int PY> static void fill_b(FastPasses& f) {
     if constexpr (rg_ok(PY) && PY >= 32) {
         f.b = k_reg_b<PY, RegB<PY>::WB>;
+        f.bb = k_reg_b_bat<PY, RegB<PY>::WB>;
         f.smem_b = RegB<PY>::smem;
         f.wb = RegB<PY>::WB;
         f.nt_b = RegB<PY>::NT;
         f.b_reg = true;
     } else {
         f.b = k_fast_b<PY>;
+        f.bb = k_fast_b_bat<PY>;
         f.smem_b = BShape<PY>::smem;
         f.wb = BShape<PY>::WB;
         f.nt_b = kNTB;
@@ -761,6 +840,8 @@ int demag_fast_setup() {
         if (demag_fast_select(m, 2 * m > 2048 ? 2048 : 2 * m, 1, f)) {
             UMAG_TRY(attrs(f.a));
             UMAG_TRY(attrs(f.c));
+            UMAG_TRY(attrs(f.ab));
+            UMAG_TRY(attrs(f.cb));
         }
     const int m3[] = {64, 128, 256, 512}, pz3[] = {12, 16, 32, 64};
     for (int m : m3)
@@ -768,11 +849,13 @@ int demag_fast_setup() {
             if (demag_fast_select(m, 2 * m, pz, f)) {
                 UMAG_TRY(attrs(f.a));
                 UMAG_TRY(attrs(f.c));
+                UMAG_TRY(attrs(f.ab));
+                UMAG_TRY(attrs(f.cb));
             }
     // pass B instantiations
     {
         FastPasses g{};
-#define SETB(py) fill_b<py>(g); UMAG_TRY(attrs(g.b));
+#define SETB(py) fill_b<py>(g); UMAG_TRY(attrs(g.b)); UMAG_TRY(attrs(g.bb));
         SETB(32) SETB(48) SETB(64) SETB(96) SETB(128) SETB(192) SETB(256) SETB(384) SETB(512) SETB(1024) SETB(2048)
 #undef SETB
     }

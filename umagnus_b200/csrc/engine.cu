@@ -11,6 +11,7 @@
 // working magnetisation slots and moves k7 into the k1 slot (FSAL,
 // engine/stepcontroller.go:76-78) without copying.
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
@@ -27,6 +28,7 @@ struct DevCtl {
     float* m;        // state magnetisation (3N, SoA)
     float* mw;       // working / stage magnetisation
     float* k[7];     // stage torques
+    float* bd;       // demag field of this instance (batched ensembles)
     double t, dt, t0, alarm, stop;
     float h;         // float32(dt * GammaLL) of the step in progress
     int active;      // 0: the step in progress is skipped (stop time reached)
@@ -49,6 +51,16 @@ struct LocalConsts {
     float f1k;     // 2*(K1/Ms) for uniform K1 and Ms
     float f2k;     // 4*(K2/Ms) for uniform K2 and Ms
     PairCoef pc;   // region (0,0) exchange / DMI coefficients
+};
+
+// Per-instance uniform parameters of a batched ensemble (one record per
+// instance, device memory): the LocalConsts of that instance's material,
+// alpha, the applied field and Ms.
+struct InstParams {
+    LocalConsts kc;
+    float alpha_mul, Ms_mul;
+    float bext[3];
+    int dmi;  // this instance uses the exchange+DMI stencil (engine/exchange.go:49-66: Dind != 0)
 };
 
 struct LocalArgs {
@@ -74,6 +86,7 @@ struct LocalArgs {
     float alpha_mul;
     const float* Ms;
     float Ms_mul;
+    const InstParams* ip;  // batched: per-instance parameters (uniform maps only)
 };
 
 __global__ void k_local_consts(LocalArgs a, LocalConsts* out) {
@@ -130,41 +143,60 @@ __device__ __forceinline__ f3 lltorque_g(f3 m, f3 H, float alpha, float gilb) {
 // B = demag; B += exchange(+DMI)/Ms; B += anisotropy; B += B_ext; torque.
 // UREG: every cell is in region 0 (no region map), so the region-pair
 // coefficients are scalars and no region is loaded.
-template <bool UREG>
+template <bool UREG, bool BAT>
 __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
-    if (!a.ctl->active) return;
+    // BAT: blockIdx.z = iz + Nz * instance; the instance's controller,
+    // demag field and uniform parameters replace the shared ones
+    static_assert(!BAT || UREG, "batched ensembles have no region maps");
+    int iz = blockIdx.z;
+    DevCtl* ctl = a.ctl;
+    const float* bd = a.bd;
+    const LocalConsts* kcp = &a.kc;
+    float alpha_mul = a.alpha_mul;
+    const InstParams* ip = nullptr;
+    if constexpr (BAT) {
+        const int b = iz / a.g.Nz;
+        iz -= b * a.g.Nz;
+        ctl += b;
+        bd = ctl->bd;
+        ip = a.ip + b;
+        kcp = &ip->kc;
+        alpha_mul = ip->alpha_mul;
+    }
+    const LocalConsts& kc = *kcp;
+    const bool dmi = BAT ? ip->dmi != 0 : a.dmi != 0;
+    if (!ctl->active) return;
     int ix = blockIdx.x * blockDim.x + threadIdx.x;
     int iy = blockIdx.y * blockDim.y + threadIdx.y;
-    int iz = blockIdx.z;
     if (ix >= a.g.Nx || iy >= a.g.Ny) return;
     const int N = a.N;
-    const float* m = a.m_sel ? a.ctl->mw : a.ctl->m;
+    const float* m = a.m_sel ? ctl->mw : ctl->m;
     const float *mx = m, *my = m + N, *mz = m + 2 * N;
     int I = (iz * a.g.Ny + iy) * a.g.Nx + ix;
     f3 B{0.f, 0.f, 0.f};
-    if (a.bd) B = f3{__ldg(a.bd + I), __ldg(a.bd + N + I), __ldg(a.bd + 2 * N + I)};
+    if (bd) B = f3{__ldg(bd + I), __ldg(bd + N + I), __ldg(bd + 2 * N + I)};
     f3 m0 = ld3(mx, my, mz, I);
     if (!is0(m0)) {
         f3 e;
         if constexpr (UREG) {
-            e = a.dmi ? dmi_sum_u(mx, my, mz, a.kc.pc, a.g, a.openbc != 0, ix, iy, iz, m0)
-                      : exchange_sum_u(mx, my, mz, a.kc.pc, a.g, ix, iy, iz, m0);
+            e = dmi ? dmi_sum_u(mx, my, mz, kc.pc, a.g, a.openbc != 0, ix, iy, iz, m0)
+                    : exchange_sum_u(mx, my, mz, kc.pc, a.g, ix, iy, iz, m0);
         } else {
             int r0 = __ldg(a.regions + I);
             e = a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
                       : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
         }
-        float inv = a.ms_uniform ? a.kc.inv_ms : inv_msat(a.Ms, a.Ms_mul, I);
+        float inv = (BAT || a.ms_uniform) ? kc.inv_ms : inv_msat(a.Ms, a.Ms_mul, I);
         B.x = fa(B.x, fm(e.x, inv));
         B.y = fa(B.y, fm(e.y, inv));
         B.z = fa(B.z, fm(e.z, inv));
     }
     if (a.anis) {
-        if (a.anis_uniform) {  // uniaxialanisotropy2.cl:27-34 with the uniform factors hoisted
-            f3 u{a.kc.u[0], a.kc.u[1], a.kc.u[2]};
+        if (BAT || a.anis_uniform) {  // uniaxialanisotropy2.cl:27-34 with the uniform factors hoisted
+            f3 u{kc.u[0], kc.u[1], kc.u[2]};
             float mu = dot3(m0, u);
-            float f1 = fm(a.kc.f1k, mu);
-            float f2 = fm(a.kc.f2k, fm(fm(mu, mu), mu));
+            float f1 = fm(kc.f1k, mu);
+            float f2 = fm(kc.f2k, fm(fm(mu, mu), mu));
             B.x = fa(B.x, fa(fm(f1, u.x), fm(f2, u.x)));
             B.y = fa(B.y, fa(fm(f1, u.y), fm(f2, u.y)));
             B.z = fa(B.z, fa(fm(f1, u.z), fm(f2, u.z)));
@@ -173,17 +205,23 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
         }
     }
     if (a.zeeman) {
-        const int r = UREG ? 0 : __ldg(a.regions + I);
-        B.x = fa(B.x, __ldg(a.bext[0] + r));
-        B.y = fa(B.y, __ldg(a.bext[1] + r));
-        B.z = fa(B.z, __ldg(a.bext[2] + r));
+        if constexpr (BAT) {
+            B.x = fa(B.x, ip->bext[0]);
+            B.y = fa(B.y, ip->bext[1]);
+            B.z = fa(B.z, ip->bext[2]);
+        } else {
+            const int r = UREG ? 0 : __ldg(a.regions + I);
+            B.x = fa(B.x, __ldg(a.bext[0] + r));
+            B.y = fa(B.y, __ldg(a.bext[1] + r));
+            B.z = fa(B.z, __ldg(a.bext[2] + r));
+        }
     }
     if (a.beff) { a.beff[I] = B.x; a.beff[N + I] = B.y; a.beff[2 * N + I] = B.z; }
     f3 t;
     if (!a.precess) t = llnoprecess(m0, B);
-    else if (a.alpha_uniform) t = lltorque_g(m0, B, a.alpha_mul, a.kc.gilb);
+    else if (BAT || a.alpha_uniform) t = lltorque_g(m0, B, alpha_mul, kc.gilb);
     else t = lltorque(m0, B, amul(a.alpha, a.alpha_mul, I));
-    float* out = a.tau_direct ? a.tau_direct : a.ctl->k[a.out_slot];
+    float* out = a.tau_direct ? a.tau_direct : ctl->k[a.out_slot];
     out[I] = t.x; out[N + I] = t.y; out[2 * N + I] = t.z;
 }
 
@@ -204,9 +242,9 @@ struct StageArgs {
 
 // m_w = normalize(src + sum_j (c_j h) k_j) with Madd<n> rounding
 // (opencl/madd.go, madd<n>.cl) then normalize2.cl.  NT = number of terms.
-template <int NT>
+template <int NT, bool BAT>
 __global__ void __launch_bounds__(256) k_stage(StageArgs a) {
-    DevCtl* ctl = a.ctl;
+    DevCtl* ctl = a.ctl + (BAT ? blockIdx.y : 0);  // BAT: one grid row per instance
     if (!ctl->active) return;
     if (a.only_if_accepted && !ctl->accepted) return;
     const float h = ctl->h;
@@ -259,10 +297,10 @@ struct ErrArgs {
 // Fused: error combination (Madd rounding), max |Err|^2, max |delM|^2 and
 // max |Err|/|delM| (VecNorm + Div + MaxAbs of stepcontroller.go:51-63);
 // Err itself is never written to memory.
-template <int NT, bool HEUN>
+template <int NT, bool HEUN, bool BAT>
 __global__ void __launch_bounds__(256) k_err_norms(ErrArgs a) {
     __shared__ float sh[32];
-    DevCtl* ctl = a.ctl;
+    DevCtl* ctl = a.ctl + (BAT ? blockIdx.y : 0);  // BAT: one grid row per instance
     if (!ctl->active) return;
     const float* k[NT];
     float e[NT];
@@ -332,7 +370,10 @@ __device__ void adapt_dt(DevCtl* c, double corr) {
 
 // engine/rk45dp.go:16-50 (start of Step): fixed dt, h, t0, clear maxima;
 // skip the step once the run's stop time is reached (engine/run.go:212-231).
-__global__ void k_step_begin(DevCtl* c) {
+__global__ void k_step_begin(DevCtl* c0, int nb) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per instance
+    if (b >= nb) return;
+    DevCtl* c = c0 + b;
     c->active = (c->t < c->stop) && c->status == 0;
     if (!c->active) return;
     if (c->fix_dt != 0) c->dt = c->fix_dt;
@@ -344,7 +385,11 @@ __global__ void k_step_begin(DevCtl* c) {
 
 // kind 0: integralController (engine/stepcontroller.go:35-97), FSAL when fsal
 // kind 1: simpleController (:13-32, RK4); kind 2: Heun (engine/heun.go:40-58)
-__global__ void k_controller(DevCtl* c, int kind, int acc, int rej, int fsal_from, int fsal_to, int nevals) {
+__global__ void k_controller(DevCtl* c0, int nb, int kind, int acc, int rej, int fsal_from, int fsal_to,
+                             int nevals) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per instance
+    if (b >= nb) return;
+    DevCtl* c = c0 + b;
     if (!c->active) return;
     c->nevals += nevals;
     if (c->nan_seen) c->status = 4;
@@ -415,7 +460,10 @@ __global__ void k_controller(DevCtl* c, int kind, int acc, int rej, int fsal_fro
 
 // accepted: the working magnetisation becomes the state (pointer swap);
 // RK4 also records max |k4| here (setMaxTorque, engine/rk4.go:64)
-__global__ void k_step_end(DevCtl* c, int rk4) {
+__global__ void k_step_end(DevCtl* c0, int nb, int rk4) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per instance
+    if (b >= nb) return;
+    DevCtl* c = c0 + b;
     if (!c->active) return;
     if (c->accepted) {
         float* t = c->m;
@@ -508,16 +556,25 @@ struct SimImpl {
     cudaGraphExec_t gexec1 = nullptr;  // one step
     int launches_per_step = 0;
     double* esum = nullptr;            // energy term sums (5 doubles)
+    // batched ensemble class: nb same-size instances with uniform parameters
+    int nb = 1;
+    bool batched = false;
+    InstParams* ip_dev = nullptr;
 };
 
-static cudaStream_t S() { return ctx().stream; }
+// stream the step/field launches go to: the library stream, or the stream of
+// the ensemble class being captured
+static thread_local cudaStream_t g_launch_stream = nullptr;
+static cudaStream_t S() { return g_launch_stream ? g_launch_stream : ctx().stream; }
+static unsigned ctl_grid(const SimImpl* s) { return (unsigned)((s->nb + 127) / 128); }
 
 // one torque evaluation of ctl->(m | mw) into ctl->k[slot] (or a direct buffer)
 static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, float* beff, int* nl) {
     if (s->p.enable_demag) {
         PassArgs a = s->pa;
         a.m_sel = m_sel;
-        UMAG_TRY(demag_launch(s->demag, a, S()));
+        if (s->batched) UMAG_TRY(demag_launch_batch(s->demag, a, s->nb, S()));
+        else UMAG_TRY(demag_launch(s->demag, a, S()));
         if (nl) *nl += 3;
     }
     LocalArgs la = s->la;
@@ -525,9 +582,10 @@ static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, flo
     la.out_slot = slot;
     la.tau_direct = tau_direct;
     la.beff = beff;
-    dim3 blk(32, 8, 1), grd((s->g.Nx + 31) / 32, (s->g.Ny + 7) / 8, s->g.Nz);
-    if (s->zero_regions) k_local_torque<true><<<grd, blk, 0, S()>>>(la);
-    else k_local_torque<false><<<grd, blk, 0, S()>>>(la);
+    dim3 blk(32, 8, 1), grd((s->g.Nx + 31) / 32, (s->g.Ny + 7) / 8, s->g.Nz * s->nb);
+    if (s->batched) k_local_torque<true, true><<<grd, blk, 0, S()>>>(la);
+    else if (s->zero_regions) k_local_torque<true, false><<<grd, blk, 0, S()>>>(la);
+    else k_local_torque<false, false><<<grd, blk, 0, S()>>>(la);
     UMAG_LAUNCH_CHECK();
     if (nl) *nl += 1;
     return UMAG_OK;
@@ -548,15 +606,17 @@ static int launch_stage(SimImpl* s, int src_m, std::initializer_list<int> slots,
     a.normalize = normalize;
     a.only_if_accepted = only_if_accepted;
     a.vol = s->p.vol;
-    const int g = grid_for(s->N, 256);
+    const dim3 g(s->batched ? (unsigned)((s->N + 255) / 256) : (unsigned)grid_for(s->N, 256), s->nb);
+#define STAGE(n)                                                    \
+    case n:                                                         \
+        if (s->batched) k_stage<n, true><<<g, 256, 0, S()>>>(a);    \
+        else k_stage<n, false><<<g, 256, 0, S()>>>(a);              \
+        break;
     switch (a.nterm) {
-    case 2: k_stage<2><<<g, 256, 0, S()>>>(a); break;
-    case 3: k_stage<3><<<g, 256, 0, S()>>>(a); break;
-    case 4: k_stage<4><<<g, 256, 0, S()>>>(a); break;
-    case 5: k_stage<5><<<g, 256, 0, S()>>>(a); break;
-    case 6: k_stage<6><<<g, 256, 0, S()>>>(a); break;
+        STAGE(2) STAGE(3) STAGE(4) STAGE(5) STAGE(6)
     default: return set_error(UMAG_E_ARG, "stage with %d terms", a.nterm);
     }
+#undef STAGE
     UMAG_LAUNCH_CHECK();
     *nl += 1;
     return UMAG_OK;
@@ -574,12 +634,18 @@ static int launch_err(SimImpl* s, std::initializer_list<int> slots, std::initial
     for (double e : es) a.e[j++] = (float)e;
     a.dm_slot = dm_slot;
     a.heun = heun;
-    const int g = grid_for(s->N, 256, 4);
-    if (heun) k_err_norms<2, true><<<g, 256, 0, S()>>>(a);
-    else if (a.nterm == 2) k_err_norms<2, false><<<g, 256, 0, S()>>>(a);
-    else if (a.nterm == 4) k_err_norms<4, false><<<g, 256, 0, S()>>>(a);
-    else if (a.nterm == 6) k_err_norms<6, false><<<g, 256, 0, S()>>>(a);
+    const dim3 g(s->batched ? (unsigned)((s->N + 255) / 256) : (unsigned)grid_for(s->N, 256, 4), s->nb);
+#define ERRN(n, hn)                                                       \
+    do {                                                                  \
+        if (s->batched) k_err_norms<n, hn, true><<<g, 256, 0, S()>>>(a);  \
+        else k_err_norms<n, hn, false><<<g, 256, 0, S()>>>(a);            \
+    } while (0)
+    if (heun) ERRN(2, true);
+    else if (a.nterm == 2) ERRN(2, false);
+    else if (a.nterm == 4) ERRN(4, false);
+    else if (a.nterm == 6) ERRN(6, false);
     else return set_error(UMAG_E_ARG, "error combination with %d terms", a.nterm);
+#undef ERRN
     UMAG_LAUNCH_CHECK();
     *nl += 1;
     return UMAG_OK;
@@ -588,7 +654,7 @@ static int launch_err(SimImpl* s, std::initializer_list<int> slots, std::initial
 // Slots: k[0] = k1 (FSAL), k[1..6] = k2..k7 buffers.
 static int launch_step(SimImpl* s, int* nl) {
     DevCtl* c = s->ctl;
-    k_step_begin<<<1, 1, 0, S()>>>(c);
+    k_step_begin<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb);
     UMAG_LAUNCH_CHECK();
     *nl += 1;
     switch (s->sp.solver) {
@@ -614,7 +680,7 @@ static int launch_step(SimImpl* s, int* nl) {
         UMAG_TRY(launch_err(s, {0, 2, 3, 4, 5, 6},
                             {71. / 57600., -71. / 16695., 71. / 1920., -17253. / 339200., 22. / 525., -1. / 40.}, 6,
                             false, nl));
-        k_controller<<<1, 1, 0, S()>>>(c, 0, 5, 6, 6, 0, 6);
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0, 5, 6, 6, 0, 6);
         break;
     }
     case 3: {  // engine/rk23.go:58-83
@@ -625,7 +691,7 @@ static int launch_step(SimImpl* s, int* nl) {
         UMAG_TRY(launch_stage(s, 0, {0, 1, 2}, {2. / 9., 1. / 3., 4. / 9.}, true, true, false, nl));
         UMAG_TRY(launch_torque(s, 1, 3, nullptr, nullptr, nl));
         UMAG_TRY(launch_err(s, {0, 1, 2, 3}, {5. / 72., -1. / 12., -1. / 9., 1. / 8.}, 3, false, nl));
-        k_controller<<<1, 1, 0, S()>>>(c, 0, 3, 4, 3, 0, 3);
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0, 3, 4, 3, 0, 3);
         break;
     }
     case 2: {  // engine/heun.go:15-59
@@ -633,12 +699,12 @@ static int launch_step(SimImpl* s, int* nl) {
         UMAG_TRY(launch_stage(s, 0, {0}, {1.0}, true, false, false, nl));            // y = y + dt*dy0
         UMAG_TRY(launch_torque(s, 1, 1, nullptr, nullptr, nl));                      // dy
         UMAG_TRY(launch_err(s, {0, 1}, {1.0, -1.0}, 1, true, nl));                   // |dy0 - dy|
-        k_controller<<<1, 1, 0, S()>>>(c, 2, 2, 3, -1, -1, 2);
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 2, 2, 3, -1, -1, 2);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         // accepted: y = y + 0.5 dt dy - 0.5 dt dy0, normalised (heun.go:45-46)
         UMAG_TRY(launch_stage(s, 1, {1, 0}, {0.5, -0.5}, true, true, true, nl));
-        k_step_end<<<1, 1, 0, S()>>>(c, 0);
+        k_step_end<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         return UMAG_OK;
@@ -652,11 +718,11 @@ static int launch_step(SimImpl* s, int* nl) {
         UMAG_TRY(launch_stage(s, 0, {2}, {1.}, true, true, false, nl));
         UMAG_TRY(launch_torque(s, 1, 3, nullptr, nullptr, nl));
         UMAG_TRY(launch_err(s, {0, 3}, {1., -1.}, 3, false, nl));
-        k_controller<<<1, 1, 0, S()>>>(c, 1, 4, 5, -1, -1, 4);
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 1, 4, 5, -1, -1, 4);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         UMAG_TRY(launch_stage(s, 0, {0, 1, 2, 3}, {1. / 6., 1. / 3., 1. / 3., 1. / 6.}, true, true, true, nl));
-        k_step_end<<<1, 1, 0, S()>>>(c, 1);
+        k_step_end<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 1);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         return UMAG_OK;
@@ -666,19 +732,19 @@ static int launch_step(SimImpl* s, int* nl) {
     }
     UMAG_LAUNCH_CHECK();
     *nl += 1;
-    k_step_end<<<1, 1, 0, S()>>>(c, 0);
+    k_step_end<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0);
     UMAG_LAUNCH_CHECK();
     *nl += 1;
     return UMAG_OK;
 }
 
 static int sync_ctl_to_host(SimImpl* s) {
-    UMAG_CUDA(cudaMemcpyAsync(s->hctl, s->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, S()));
+    UMAG_CUDA(cudaMemcpyAsync(s->hctl, s->ctl, sizeof(DevCtl) * s->nb, cudaMemcpyDeviceToHost, S()));
     UMAG_CUDA(cudaStreamSynchronize(S()));
     return UMAG_OK;
 }
 static int push_ctl(SimImpl* s) {
-    UMAG_CUDA(cudaMemcpyAsync(s->ctl, s->hctl, sizeof(DevCtl), cudaMemcpyHostToDevice, S()));
+    UMAG_CUDA(cudaMemcpyAsync(s->ctl, s->hctl, sizeof(DevCtl) * s->nb, cudaMemcpyHostToDevice, S()));
     UMAG_CUDA(cudaStreamSynchronize(S()));
     return UMAG_OK;
 }
@@ -689,11 +755,11 @@ static int ensure_k1(SimImpl* s) {
     if (!s->need_k1) return UMAG_OK;
     if (s->sp.solver == 5 || s->sp.solver == 3) {
         UMAG_TRY(sync_ctl_to_host(s));
-        s->hctl->active = 1;
+        for (int b = 0; b < s->nb; b++) s->hctl[b].active = 1;
         UMAG_TRY(push_ctl(s));
         UMAG_TRY(launch_torque(s, 0, 0, nullptr, nullptr, nullptr));
         UMAG_TRY(sync_ctl_to_host(s));
-        s->hctl->nevals += 1;
+        for (int b = 0; b < s->nb; b++) s->hctl[b].nevals += 1;
         UMAG_TRY(push_ctl(s));
     }
     s->need_k1 = false;
@@ -1175,6 +1241,346 @@ int sim_relax(umag_sim* h, double threshold) {
     push_ctl(s);
     set_stepper(s, prev_solver, prev_precess);
     return st;
+}
+
+// ================================================================ ensembles
+// Many independent simulations advanced together (no reference counterpart:
+// uMagNUS runs one simulation per process).  Instances with the same mesh
+// form a class, run as one batched SimImpl: every field / stage / error
+// kernel handles all instances of the class in one launch (grid extended by
+// the instance index) and one controller thread per instance keeps its own
+// time, dt and accept/reject decisions.  One CUDA graph steps every class,
+// the classes on parallel branches.
+struct EnsClass {
+    SimImpl* s = nullptr;
+    std::vector<int> members;  // ensemble index of each instance
+    float2* spec = nullptr;    // nb spectrum scratch copies
+    float* params = nullptr;   // device: Ms[nb], A00[nb], D00[nb]
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+};
+struct EnsImpl {
+    std::vector<EnsClass> cls;
+    std::vector<std::pair<int, int>> where;  // instance -> (class, index in class)
+    umag_solver_params sp;
+    int graph_steps = 16;
+    cudaGraphExec_t gexec = nullptr;
+    cudaEvent_t fork = nullptr;
+};
+
+static void ens_class_free(EnsClass& c) {
+    if (c.s) {
+        SimImpl* s = c.s;
+        drop_graph(s);
+        if (s->demag) demag_free(s->demag);
+        cudaFree(s->bufs);
+        cudaFree(s->bd);
+        cudaFree(s->zero_regions);
+        cudaFree(s->kc_dev);
+        cudaFree(s->ip_dev);
+        cudaFree(s->ctl);
+        if (s->hctl) cudaFreeHost(s->hctl);
+        delete s;
+        c.s = nullptr;
+    }
+    cudaFree(c.spec);
+    cudaFree(c.params);
+    if (c.st) cudaStreamDestroy(c.st);
+    if (c.done) cudaEventDestroy(c.done);
+    c.spec = nullptr;
+    c.params = nullptr;
+    c.st = nullptr;
+    c.done = nullptr;
+}
+
+int ens_free(umag_ens* h) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    if (!e) return UMAG_OK;
+    cudaDeviceSynchronize();
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->fork) cudaEventDestroy(e->fork);
+    for (auto& c : e->cls) ens_class_free(c);
+    delete e;
+    return UMAG_OK;
+}
+
+// one class: nb instances of mesh N, cell, with the listed parameters
+static int ens_class_new(EnsClass& C, const umag_ens_instance* in, const std::vector<int>& members,
+                         const umag_solver_params* sp, int demag) {
+    const int nb = (int)members.size();
+    const umag_ens_instance& r0 = in[members[0]];
+    SimImpl* s = new SimImpl();
+    C.s = s;
+    C.members = members;
+    s->nb = nb;
+    s->batched = true;
+    s->sp = *sp;
+    memset(&s->p, 0, sizeof(s->p));
+    for (int i = 0; i < 3; i++) { s->p.N[i] = r0.N[i]; s->p.cell[i] = r0.cell[i]; }
+    s->p.enable_demag = demag;
+    s->p.precess = 1;
+    s->N = r0.N[0] * r0.N[1] * r0.N[2];
+    s->g = Mesh3{r0.N[0], r0.N[1], r0.N[2], 0};
+    const size_t n3 = 3 * (size_t)s->N;
+    UMAG_CUDA(cudaStreamCreateWithFlags(&C.st, cudaStreamNonBlocking));
+    UMAG_CUDA(cudaEventCreateWithFlags(&C.done, cudaEventDisableTiming));
+    UMAG_CUDA(cudaMalloc(&s->bufs, sizeof(float) * n3 * 9 * nb));
+    UMAG_CUDA(cudaMemset(s->bufs, 0, sizeof(float) * n3 * 9 * nb));
+    UMAG_CUDA(cudaMalloc(&s->zero_regions, s->N));
+    UMAG_CUDA(cudaMemset(s->zero_regions, 0, s->N));
+    s->p.regions = s->zero_regions;
+    if (demag) {
+        int pbc[3] = {0, 0, 0};
+        UMAG_TRY(demag_new_newell(r0.N[0], r0.N[1], r0.N[2], pbc, r0.cell[0], r0.cell[1], r0.cell[2], 32, 0, &s->demag));
+        UMAG_CUDA(cudaMalloc(&s->bd, sizeof(float) * n3 * nb));
+    }
+    UMAG_CUDA(cudaMalloc(&s->ctl, sizeof(DevCtl) * nb));
+    UMAG_CUDA(cudaMallocHost(&s->hctl, sizeof(DevCtl) * nb));
+    memset(s->hctl, 0, sizeof(DevCtl) * nb);
+    for (int b = 0; b < nb; b++) {
+        DevCtl& c = s->hctl[b];
+        float* base = s->bufs + (size_t)b * 9 * n3;
+        c.m = base;
+        c.mw = base + n3;
+        for (int i = 0; i < 7; i++) c.k[i] = base + (2 + i) * n3;
+        c.bd = s->bd ? s->bd + (size_t)b * n3 : nullptr;
+        c.dt = sp->dt;
+        c.stop = INFINITY;
+        c.max_err = sp->max_err; c.rel_err = sp->rel_err; c.min_dt = sp->min_dt; c.max_dt = sp->max_dt;
+        c.fix_dt = sp->fix_dt; c.headroom = sp->headroom; c.min_slope = sp->min_slope; c.gamma = sp->gamma_ll;
+        c.active = 1;
+    }
+    UMAG_TRY(push_ctl(s));
+    // per-instance uniform values: Ms, and the region-(0,0) LUT entries the
+    // plain engine would use (engine/exchange.go:193-201 harmonic mean, float32)
+    std::vector<float> hp(3 * nb);
+    bool dmi = false, anis = false, zee = false;
+    for (int b = 0; b < nb; b++) {
+        const umag_ens_instance& r = in[members[b]];
+        hp[b] = r.Ms;
+        hp[nb + b] = 2.0f / (1.0f / r.Aex + 1.0f / r.Aex);
+        const float D = r.Dind;
+        hp[2 * nb + b] = D == 0.0f ? 0.0f : 2.0f / (1.0f / D + 1.0f / D);
+        dmi |= D != 0.0f;
+        anis |= r.Ku1 != 0.0f || r.Ku2 != 0.0f;
+        zee |= r.B_ext[0] != 0.0f || r.B_ext[1] != 0.0f || r.B_ext[2] != 0.0f;
+    }
+    UMAG_CUDA(cudaMalloc(&C.params, sizeof(float) * 3 * nb));
+    UMAG_CUDA(cudaMemcpy(C.params, hp.data(), sizeof(float) * 3 * nb, cudaMemcpyHostToDevice));
+    UMAG_CUDA(cudaMalloc(&s->ip_dev, sizeof(InstParams) * nb));
+    LocalArgs& la = s->la;
+    la.g = s->g;
+    la.N = s->N;
+    la.ctl = s->ctl;
+    la.bd = nullptr;
+    la.regions = s->zero_regions;
+    la.cx = (float)r0.cell[0]; la.cy = (float)r0.cell[1]; la.cz = (float)r0.cell[2];
+    la.wx = (float)(2 / (r0.cell[0] * r0.cell[0]));
+    la.wy = (float)(2 / (r0.cell[1] * r0.cell[1]));
+    la.wz = (float)(2 / (r0.cell[2] * r0.cell[2]));
+    la.dmi = dmi;
+    la.openbc = 0;
+    la.anis = anis;
+    la.zeeman = zee;
+    la.precess = 1;
+    la.ms_uniform = 1; la.alpha_uniform = 1; la.anis_uniform = 1;
+    la.ip = s->ip_dev;
+    std::vector<InstParams> hip(nb);
+    for (int b = 0; b < nb; b++) {  // uniform constants of each instance, bit-identical to the plain engine's
+        const umag_ens_instance& r = in[members[b]];
+        LocalArgs t = la;
+        t.aLUT = C.params + nb + b;
+        t.dLUT = C.params + 2 * nb + b;
+        t.alpha_mul = r.alpha;
+        t.Ms_mul = r.Ms;
+        t.up = UniaxParams{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, r.Ms, r.Ku1, r.Ku2,
+                           r.anisU[0], r.anisU[1], r.anisU[2]};
+        k_local_consts<<<1, 1, 0, S()>>>(t, &s->ip_dev[b].kc);
+        UMAG_LAUNCH_CHECK();
+        hip[b].alpha_mul = r.alpha;
+        hip[b].Ms_mul = r.Ms;
+        hip[b].dmi = r.Dind != 0.0f;
+        for (int c = 0; c < 3; c++) hip[b].bext[c] = r.B_ext[c];
+    }
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    // fill the non-kc fields without touching kc
+    for (int b = 0; b < nb; b++)
+        UMAG_CUDA(cudaMemcpy(reinterpret_cast<char*>(s->ip_dev + b) + offsetof(InstParams, alpha_mul),
+                             reinterpret_cast<char*>(&hip[b]) + offsetof(InstParams, alpha_mul),
+                             sizeof(InstParams) - offsetof(InstParams, alpha_mul), cudaMemcpyHostToDevice));
+    if (demag) {
+        fill_pass_args(s->demag, s->pa);
+        const long spec_elems = 3L * s->demag->P[2] * s->demag->N[1] * s->demag->Lx;  // one plan's spectrum
+        UMAG_CUDA(cudaMalloc(&C.spec, sizeof(float2) * spec_elems * nb));
+        s->pa.spec = C.spec;
+        s->pa.spec_stride = spec_elems;
+        s->pa.m_ind = &s->ctl[0].m;
+        s->pa.m_ind_w = &s->ctl[0].mw;
+        s->pa.active = &s->ctl[0].active;
+        s->pa.ctl_stride = sizeof(DevCtl);
+        s->pa.vol = nullptr;
+        s->pa.Ms = nullptr;
+        s->pa.Ms_mul = 0.0f;
+        s->pa.ms_mul_b = C.params;
+        s->pa.ncell = s->N;
+        for (int c = 0; c < 3; c++) s->pa.B[c] = s->bd + (size_t)c * s->N;
+        s->pa.b_stride = (long)n3;
+    }
+    return UMAG_OK;
+}
+
+int ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int demag, umag_ens** out) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(n > 0 && in && sp && out, "bad argument");
+    UMAG_REQUIRE(sp->solver == 2 || sp->solver == 3 || sp->solver == 4 || sp->solver == 5, "unknown solver");
+    EnsImpl* e = new EnsImpl();
+    e->sp = *sp;
+    e->where.resize(n);
+    auto fail = [&](int code) { ens_free(reinterpret_cast<umag_ens*>(e)); return code; };
+    // classes: same mesh and cell size
+    std::vector<std::vector<int>> groups;
+    for (int i = 0; i < n; i++) {
+        const umag_ens_instance& r = in[i];
+        if (r.N[0] <= 0 || r.N[1] <= 0 || r.N[2] <= 0) return fail(set_error(UMAG_E_ARG, "instance %d: bad mesh", i));
+        if (!(r.Ms > 0) || !(r.Aex > 0)) return fail(set_error(UMAG_E_ARG, "instance %d: Ms and Aex must be > 0", i));
+        int g = -1;
+        for (size_t k = 0; k < groups.size(); k++) {
+            const umag_ens_instance& q = in[groups[k][0]];
+            if (q.N[0] == r.N[0] && q.N[1] == r.N[1] && q.N[2] == r.N[2] && q.cell[0] == r.cell[0] &&
+                q.cell[1] == r.cell[1] && q.cell[2] == r.cell[2])
+                g = (int)k;
+        }
+        if (g < 0) { groups.push_back({}); g = (int)groups.size() - 1; }
+        e->where[i] = {g, (int)groups[g].size()};
+        groups[g].push_back(i);
+    }
+    e->cls.resize(groups.size());
+    for (size_t k = 0; k < groups.size(); k++) {
+        int st = ens_class_new(e->cls[k], in, groups[k], sp, demag);
+        if (st != UMAG_OK) return fail(st);
+    }
+    if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess)
+        return fail(set_error(UMAG_E_CUDA, "event"));
+    *out = reinterpret_cast<umag_ens*>(e);
+    return UMAG_OK;
+}
+
+static SimImpl* ens_sim(EnsImpl* e, int i, int* b) {
+    const auto& w = e->where[i];
+    *b = w.second;
+    return e->cls[w.first].s;
+}
+
+int ens_set_m(umag_ens* h, int i, const float* host_m) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    UMAG_REQUIRE(e && host_m && i >= 0 && i < (int)e->where.size(), "bad argument");
+    int b;
+    SimImpl* s = ens_sim(e, i, &b);
+    UMAG_TRY(sync_ctl_to_host(s));
+    float* m = s->hctl[b].m;
+    UMAG_CUDA(cudaMemcpy(m, host_m, sizeof(float) * 3 * s->N, cudaMemcpyHostToDevice));
+    UMAG_TRY(normalize(m, m + s->N, m + 2 * (size_t)s->N, nullptr, s->N));  // engine/magnetization.go:34
+    UMAG_CUDA(cudaDeviceSynchronize());
+    s->need_k1 = true;
+    return UMAG_OK;
+}
+
+int ens_get_m(umag_ens* h, int i, float* host_m) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    UMAG_REQUIRE(e && host_m && i >= 0 && i < (int)e->where.size(), "bad argument");
+    int b;
+    SimImpl* s = ens_sim(e, i, &b);
+    UMAG_TRY(sync_ctl_to_host(s));
+    UMAG_CUDA(cudaMemcpy(host_m, s->hctl[b].m, sizeof(float) * 3 * s->N, cudaMemcpyDeviceToHost));
+    return UMAG_OK;
+}
+
+int ens_get_state(umag_ens* h, int i, umag_solver_state* st) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    UMAG_REQUIRE(e && st && i >= 0 && i < (int)e->where.size(), "bad argument");
+    int b;
+    SimImpl* s = ens_sim(e, i, &b);
+    UMAG_TRY(sync_ctl_to_host(s));
+    const DevCtl& c = s->hctl[b];
+    st->time = c.t; st->dt = c.dt; st->last_err = c.last_err; st->peak_err = c.peak_err;
+    st->last_torque = c.last_torque; st->nsteps = c.nsteps; st->nundone = c.nundone; st->nevals = c.nevals;
+    st->status = c.status;
+    return UMAG_OK;
+}
+
+// one graph: graph_steps steps of every class, classes on parallel branches
+static int ens_build_graph(EnsImpl* e) {
+    if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
+    cudaStream_t main = ctx().stream;
+    cudaGraph_t graph;
+    UMAG_CUDA(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
+    int st = UMAG_OK;
+    if (cudaEventRecord(e->fork, main) != cudaSuccess) st = set_error(UMAG_E_CUDA, "fork");
+    for (auto& c : e->cls) {
+        if (st != UMAG_OK) break;
+        if (cudaStreamWaitEvent(c.st, e->fork, 0) != cudaSuccess) { st = set_error(UMAG_E_CUDA, "fork wait"); break; }
+        g_launch_stream = c.st;
+        int nl = 0;
+        for (int k = 0; k < e->graph_steps && st == UMAG_OK; k++) st = launch_step(c.s, &nl);
+        g_launch_stream = nullptr;
+        if (st == UMAG_OK && cudaEventRecord(c.done, c.st) != cudaSuccess) st = set_error(UMAG_E_CUDA, "join");
+        if (st == UMAG_OK && cudaStreamWaitEvent(main, c.done, 0) != cudaSuccess) st = set_error(UMAG_E_CUDA, "join");
+    }
+    g_launch_stream = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(main, &graph);
+    if (st != UMAG_OK) return st;
+    if (ce != cudaSuccess) return set_error(UMAG_E_CUDA, "ensemble graph capture: %s", cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&e->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return set_error(UMAG_E_CUDA, "ensemble graph instantiate: %s", cudaGetErrorString(ce));
+    return UMAG_OK;
+}
+
+// engine/run.go:190 Run(seconds) for every instance: each runs until its own
+// time reaches start + seconds (its dt honours that alarm); the host checks
+// the instances every `chunk` graph replays
+int ens_run(umag_ens* h, double seconds, int chunk, long long max_replays) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    UMAG_REQUIRE(e && seconds >= 0, "bad argument");
+    if (chunk <= 0) chunk = 8;
+    for (auto& c : e->cls) {
+        SimImpl* s = c.s;
+        UMAG_TRY(sync_ctl_to_host(s));
+        for (int b = 0; b < s->nb; b++) {
+            s->hctl[b].stop = s->hctl[b].t + seconds;
+            s->hctl[b].alarm = s->hctl[b].stop;
+        }
+        UMAG_TRY(push_ctl(s));
+        s->need_k1 = true;  // RunWhile frees the stepper (engine/run.go:207)
+        UMAG_TRY(ensure_k1(s));
+    }
+    if (!e->gexec) UMAG_TRY(ens_build_graph(e));
+    long long done = 0;
+    while (done < max_replays) {
+        for (int k = 0; k < chunk && done < max_replays; k++, done++)
+            UMAG_CUDA(cudaGraphLaunch(e->gexec, ctx().stream));
+        bool running = false;
+        for (auto& c : e->cls) {
+            UMAG_TRY(sync_ctl_to_host(c.s));
+            for (int b = 0; b < c.s->nb; b++) {
+                const DevCtl& d = c.s->hctl[b];
+                if (d.status != 0)
+                    return set_error(UMAG_E_SOLVER, "instance %d: solver failure code %d at t=%g", c.members[b],
+                                     d.status, d.t);
+                running |= d.t < d.stop;
+            }
+        }
+        if (!running) break;
+    }
+    return UMAG_OK;
+}
+
+int ens_count(umag_ens* h, int* n_instances, int* n_classes) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    UMAG_REQUIRE(e, "NULL argument");
+    if (n_instances) *n_instances = (int)e->where.size();
+    if (n_classes) *n_classes = (int)e->cls.size();
+    return UMAG_OK;
 }
 
 int sim_launches_per_step(umag_sim* h, int* n) {

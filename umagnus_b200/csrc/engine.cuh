@@ -19,4 +19,11 @@ int sim_launches_per_step(umag_sim* s, int* n);
 int sim_torque_evals(umag_sim* s, int n);
 int sim_energies(umag_sim* s, double E[5]);
 int sim_relax(umag_sim* s, double threshold);
+int ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int demag, umag_ens** out);
+int ens_free(umag_ens* e);
+int ens_set_m(umag_ens* e, int i, const float* host_m);
+int ens_get_m(umag_ens* e, int i, float* host_m);
+int ens_get_state(umag_ens* e, int i, umag_solver_state* st);
+int ens_run(umag_ens* e, double seconds, int chunk, long long max_replays);
+int ens_count(umag_ens* e, int* n_instances, int* n_classes);
 }  // namespace umag

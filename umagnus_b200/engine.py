@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import SimParams, SolverParams, SolverState, UmagError, check
+from ._lib import EnsInstance, SimParams, SolverParams, SolverState, UmagError, check
 
 NREGION = 256  # engine/regions.go:11
 GAMMA_LL = 1.7595e11  # engine/torque.go:27
@@ -248,6 +248,79 @@ class Simulation:
     def free(self):
         if getattr(self, "_h", None):
             self.L.umag_sim_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Ensemble:
+    """Many independent simulations advanced together on one GPU (no
+    counterpart in the reference, which runs one simulation per process).
+
+    instances: list of dicts with N, cell, Msat, Aex, alpha and optional
+    Dind, Ku1, Ku2, anisU, B_ext (uniform values only).  Each instance keeps
+    its own time, dt and step controller; the solver knobs are shared.
+    Instances with the same mesh run as one batch of launches, and one CUDA
+    graph steps all of them.
+    """
+
+    def __init__(self, instances, demag=True, solver=DORMANDPRINCE, dt=1e-15, MaxErr=1e-5, RelErr=1e-4,
+                 MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8, device=0):
+        self.L = _lib.init(device)
+        arr = (EnsInstance * len(instances))()
+        self.shapes = []
+        for k, d in enumerate(instances):
+            r = arr[k]
+            N = tuple(int(n) for n in d["N"])
+            r.N[:] = N
+            r.cell[:] = [float(c) for c in d["cell"]]
+            r.Ms, r.Aex, r.alpha = float(d["Msat"]), float(d["Aex"]), float(d["alpha"])
+            r.Dind, r.Ku1, r.Ku2 = float(d.get("Dind", 0.0)), float(d.get("Ku1", 0.0)), float(d.get("Ku2", 0.0))
+            r.anisU[:] = [float(u) for u in d.get("anisU", (0.0, 0.0, 1.0))]
+            r.B_ext[:] = [float(b) for b in d.get("B_ext", (0.0, 0.0, 0.0))]
+            self.shapes.append((3, N[2], N[1], N[0]))
+        sp = SolverParams()
+        self.L.umag_solver_defaults(ctypes.byref(sp))
+        sp.solver = int(solver)
+        sp.dt, sp.max_err, sp.rel_err, sp.min_dt, sp.max_dt = dt, MaxErr, RelErr, MinDt, MaxDt
+        sp.fix_dt, sp.headroom, sp.gamma_ll = FixDt, Headroom, GAMMA_LL
+        h = ctypes.c_void_p()
+        check(self.L.umag_ens_new(len(instances), arr, ctypes.byref(sp), int(bool(demag)), ctypes.byref(h)))
+        self._h = h.value
+
+    def __len__(self):
+        return len(self.shapes)
+
+    def classes(self):
+        n, c = ctypes.c_int(), ctypes.c_int()
+        check(self.L.umag_ens_count(self._h, ctypes.byref(n), ctypes.byref(c)))
+        return c.value
+
+    def set_m(self, i, m):
+        a = np.ascontiguousarray(np.asarray(m, np.float32).reshape(self.shapes[i]))
+        check(self.L.umag_ens_set_m(self._h, int(i), a.ctypes.data))
+
+    def get_m(self, i):
+        a = np.empty(self.shapes[i], np.float32)
+        check(self.L.umag_ens_get_m(self._h, int(i), a.ctypes.data))
+        return a
+
+    def state(self, i):
+        st = SolverState()
+        check(self.L.umag_ens_get_state(self._h, int(i), ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in SolverState._fields_}
+
+    def run(self, seconds, chunk=8, max_replays=10 ** 12):
+        """engine/run.go:190 Run(seconds) for every instance."""
+        check(self.L.umag_ens_run(self._h, float(seconds), int(chunk), int(max_replays)))
+
+    def free(self):
+        if getattr(self, "_h", None):
+            self.L.umag_ens_free(self._h)
             self._h = None
 
     def __del__(self):

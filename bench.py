@@ -353,6 +353,89 @@ def run_ours(args, rank, world, local_rank):
     return result
 
 
+# ------------------------------------------------------------------ ensemble workload
+ENS_SIZES = (32, 48, 64, 96, 128)
+ENS_CELL = (4e-9, 4e-9, 3e-9)
+
+
+def ensemble_instances(count=256, seed=5):
+    """The 256-instance thin-film ensemble: n x n x 1 films, n uniform in
+    {32, 48, 64, 96, 128}, 4x4x3 nm cells; Ms U[4e5, 1.2e6] A/m, Aex
+    U[5e-12, 2e-11] J/m, alpha U[0.01, 0.5], B_ext of random direction and
+    magnitude U[0, 100] mT; m0 random unit vectors (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.choice(ENS_SIZES))
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        b = d * rng.uniform(0.0, 0.1)
+        out.append(dict(N=(n, n, 1), cell=ENS_CELL, Msat=float(rng.uniform(4e5, 1.2e6)),
+                        Aex=float(rng.uniform(5e-12, 2e-11)), alpha=float(rng.uniform(0.01, 0.5)),
+                        B_ext=tuple(float(x) for x in b), m_seed=int(rng.integers(1 << 31))))
+    return out
+
+
+def run_ensemble(args):
+    """Batched ensemble vs the plain engine one instance at a time, both to
+    t = args.ens_time per instance; the plain form is timed on a per-size
+    sample (args.ens_plain_sample instances of each size) and extrapolated."""
+    import torch
+    from umagnus_b200 import engine
+    insts = ensemble_instances()
+    T = args.ens_time
+    ncell = [d["N"][0] * d["N"][1] for d in insts]
+    ens = engine.Ensemble([{k: v for k, v in d.items() if k != "m_seed"} for d in insts])
+    for i, d in enumerate(insts):
+        ens.set_m(i, random_m(d["N"], d["m_seed"]))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ens.run(T, chunk=8)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    states = [ens.state(i) for i in range(len(insts))]
+    acc = np.array([s["nsteps"] for s in states], float)
+    cu_batch = float(np.dot(acc, ncell)) / t_batch
+    # plain form, one instance at a time, on a sample of each size
+    per_size = {}
+    for n in ENS_SIZES:
+        idx = [i for i, d in enumerate(insts) if d["N"][0] == n][: args.ens_plain_sample]
+        ts = []
+        for i in idx:
+            d = insts[i]
+            sim = engine.Simulation(d["N"], d["cell"], d["Msat"], d["Aex"], d["alpha"], B_ext=d["B_ext"])
+            sim.set_m(random_m(d["N"], d["m_seed"]))
+            torch.cuda.synchronize()
+            a = time.perf_counter()
+            sim.run(T)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - a)
+            st = sim.state()
+            assert st["nsteps"] == states[i]["nsteps"], "plain and batched trajectories differ"
+            sim.free()
+        per_size[n] = (float(np.mean(ts)), len(idx))
+    t_plain = sum(per_size[d["N"][0]][0] for d in insts)
+    ens.free()
+    line = {"metric": "RK45DP instances/s, 256-instance thin-film ensemble (batched vs one at a time)",
+            "value": len(insts) / t_batch, "unit": "instances/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded instances and m0)",
+            "config": {"workload": "256 films n x n x 1, n in {32,48,64,96,128}, 4x4x3 nm, Newell demag + exchange "
+                                   "+ Zeeman, RK45DP MaxErr 1e-5, each instance to t = %g s" % T,
+                       "instances": len(insts), "cells": int(sum(ncell)),
+                       "classes": {str(n): sum(1 for d in insts if d["N"][0] == n) for n in ENS_SIZES}},
+            "batched": {"seconds": t_batch, "instances_per_s": len(insts) / t_batch,
+                        "cell_updates_per_s": cu_batch, "accepted_steps_total": int(acc.sum()),
+                        "steps_min_max": [int(acc.min()), int(acc.max())]},
+            "plain": {"seconds_extrapolated": t_plain, "instances_per_s": len(insts) / t_plain,
+                      "cell_updates_per_s": float(np.dot(acc, ncell)) / t_plain,
+                      "sample_seconds_per_instance": {str(n): v[0] for n, v in per_size.items()},
+                      "sample_per_size": args.ens_plain_sample},
+            "speedup": t_plain / t_batch,
+            "identical_trajectories": True}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -361,7 +444,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=90.0, help="seconds of timed CPU steps (reference arm)")
+    ap.add_argument("--workload", default="multilayer", choices=["multilayer", "ensemble"])
+    ap.add_argument("--ens-time", type=float, default=2e-9, help="ensemble: simulated time per instance (s)")
+    ap.add_argument("--ens-plain-sample", type=int, default=2, help="ensemble: plain-form instances timed per size")
     args = ap.parse_args()
+    if args.workload == "ensemble":
+        return run_ensemble(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

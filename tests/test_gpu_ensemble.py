@@ -41,3 +41,31 @@ def test_ensemble_matches_individual_runs(demag):
         np.testing.assert_array_equal(ens.get_m(k), sim.get_m().cpu().numpy())
         sim.free()
     ens.free()
+
+
+def test_ensemble_is_deterministic_and_matches_every_instance():
+    """Two runs of a 40-instance mixed ensemble are identical, and every
+    instance equals its single run."""
+    import bench
+    from umagnus_b200 import engine
+    insts = bench.ensemble_instances(count=40, seed=11)
+    runs = []
+    for _ in range(2):
+        ens = engine.Ensemble([{k: v for k, v in d.items() if k != "m_seed"} for d in insts])
+        for i, d in enumerate(insts):
+            ens.set_m(i, bench.random_m(d["N"], d["m_seed"]))
+        ens.run(5e-12, chunk=2)
+        runs.append(([ens.state(i) for i in range(len(insts))], [ens.get_m(i) for i in range(len(insts))]))
+        ens.free()
+    for i in range(len(insts)):
+        assert runs[0][0][i] == runs[1][0][i], i
+        np.testing.assert_array_equal(runs[0][1][i], runs[1][1][i])
+    for i, d in enumerate(insts):
+        sim = engine.Simulation(d["N"], d["cell"], d["Msat"], d["Aex"], d["alpha"], B_ext=d["B_ext"])
+        sim.set_m(bench.random_m(d["N"], d["m_seed"]))
+        sim.run(5e-12)
+        st = sim.state()
+        assert (st["nsteps"], st["nundone"], st["time"], st["dt"]) == (
+            runs[0][0][i]["nsteps"], runs[0][0][i]["nundone"], runs[0][0][i]["time"], runs[0][0][i]["dt"]), i
+        np.testing.assert_array_equal(sim.get_m().cpu().numpy(), runs[0][1][i])
+        sim.free()

@@ -29,28 +29,32 @@ template <int M, int PZ> struct AcShape {
 };
 
 // copypadmul2.cl:13-20: MU0*Ms (FP64 product rounded to float32) * vol * m
-__device__ __forceinline__ float scaled_m(const PassArgs& a, const float* __restrict__ m, int i) {
-    float fac = a.Ms == nullptr ? a.Ms_mul : __fmul_rn(a.Ms_mul, __ldg(a.Ms + i));
+__device__ __forceinline__ float scaled_m(const PassArgs& a, const float* __restrict__ m, int i, float msmul) {
+    float fac = a.Ms == nullptr ? msmul : __fmul_rn(msmul, __ldg(a.Ms + i));
     float bsat = (float)(kMu0f * (double)fac);
     float w = a.vol == nullptr ? 1.0f : __fmul_rn(1.0f, __ldg(a.vol + i));
     return __fmul_rn(__fmul_rn(bsat, w), __ldg(m + i));
 }
 
-// Batched launches (an ensemble of same-size instances): shift the pointers
-// of PassArgs to instance b -- spectrum scratch, field output, the
-// instance's controller fields (m slots, active flag) and its Ms.
-__device__ __forceinline__ void demag_batch_fix(PassArgs& A, int b) {
-    A.spec += (long)b * A.spec_stride;
-    for (int c = 0; c < 3; c++) A.B[c] += (long)b * A.b_stride;
-    const long o = (long)b * A.ctl_stride;
-    if (A.m_ind) A.m_ind = reinterpret_cast<float* const*>(reinterpret_cast<const char*>(A.m_ind) + o);
-    if (A.m_ind_w) A.m_ind_w = reinterpret_cast<float* const*>(reinterpret_cast<const char*>(A.m_ind_w) + o);
-    if (A.active) A.active = reinterpret_cast<const int*>(reinterpret_cast<const char*>(A.active) + o);
-    if (A.ms_mul_b) A.Ms_mul = A.ms_mul_b[b];
+// Per-instance views of PassArgs for batched launches (an ensemble of
+// same-size instances, instance ib): spectrum scratch, field output, the
+// instance's controller fields (m slots, active flag) and its Ms.  With
+// ib = 0 (single-instance kernels) every offset folds away.
+__device__ __forceinline__ float2* inst_spec(const PassArgs& a, int ib) { return a.spec + (long)ib * a.spec_stride; }
+__device__ __forceinline__ float* inst_B(const PassArgs& a, int ib, int c) { return a.B[c] + (long)ib * a.b_stride; }
+__device__ __forceinline__ bool inst_inactive(const PassArgs& a, int ib) {
+    if (!a.active) return false;
+    return !*reinterpret_cast<const int*>(reinterpret_cast<const char*>(a.active) + (long)ib * a.ctl_stride);
 }
+__device__ __forceinline__ const float* inst_m(const PassArgs& a, int ib, int c) {
+    if (!a.m_ind) return a.m[c];
+    const char* slot = reinterpret_cast<const char*>(a.m_sel ? a.m_ind_w : a.m_ind) + (long)ib * a.ctl_stride;
+    return *reinterpret_cast<float* const*>(slot) + (long)c * a.ncell;
+}
+__device__ __forceinline__ float inst_msmul(const PassArgs& a, int ib) { return a.ms_mul_b ? a.ms_mul_b[ib] : a.Ms_mul; }
 
 template <int M, int PZ>
-__device__ __forceinline__ void k_fast_a_body(const PassArgs& a, const int bx, const int by) {
+__device__ __forceinline__ void k_fast_a_body(const PassArgs& a, const int bx, const int by, const int ib) {
     using S = AcShape<M, PZ>;
     constexpr int NZ = S::NZ, XP = S::XP, CW = S::CW, H = M / 2;
     extern __shared__ __align__(16) float2 sm[];
@@ -59,21 +63,22 @@ __device__ __forceinline__ void k_fast_a_body(const PassArgs& a, const int bx, c
     float2* twr = twz + PZ;
     float2* X1 = twr + (H + 1);
     float2* Z2 = X1 + NZ * XP;
-    if (a.active && !*a.active) return;
+    if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
     for (int i = tid; i < M; i += kNT) twx[i] = a.fx.tw[i];
     if (PZ > 1)
         for (int i = tid; i < PZ; i += kNT) twz[i] = a.fz.tw[i];
     for (int i = tid; i <= H; i += kNT) twr[i] = a.twr[i];
     const int y = bx, c = by, Ny = a.Ny;
-    const float* __restrict__ m = a.m_ind ? (a.m_sel ? *a.m_ind_w : *a.m_ind) + (long)c * a.ncell : a.m[c];
+    const float* __restrict__ m = inst_m(a, ib, c);
+    const float msm = inst_msmul(a, ib);
     // 1. scaled m, pairs of reals packed into complex (x = 2n, 2n+1), Nx = M
     for (int e = tid; e < NZ * M; e += kNT) {
         const int z = e / M, n = e % M;
         float2 v = make_float2(0.f, 0.f);  // x >= Nx is zero padding
         if (n < H) {
             const int i = (z * Ny + y) * M + 2 * n;
-            v = make_float2(scaled_m(a, m, i), scaled_m(a, m, i + 1));
+            v = make_float2(scaled_m(a, m, i, msm), scaled_m(a, m, i + 1, msm));
         }
         X1[z * XP + n] = v;
     }
@@ -96,7 +101,7 @@ __device__ __forceinline__ void k_fast_a_body(const PassArgs& a, const int bx, c
         row[k2] = make_float2(E.x - WO.x, WO.y - E.y);
     }
     __syncthreads();
-    float2* out = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
+    float2* out = inst_spec(a, ib) + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
     const long kzs = (long)Ny * a.Lx;
     if constexpr (PZ == 1) {
         for (int k = tid; k <= M; k += kNT) out[k] = X1[k];
@@ -123,18 +128,16 @@ __device__ __forceinline__ void k_fast_a_body(const PassArgs& a, const int bx, c
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) { k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y); }
-// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+__global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) { k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+// batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(kNT) k_fast_a_bat(PassArgs a) {
     const int per = 3, b = blockIdx.y / per;
-    PassArgs A = a;
-    demag_batch_fix(A, b);
-    k_fast_a_body<M, PZ>(A, blockIdx.x, blockIdx.y - b * per);
+    k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
 
 template <int M, int PZ>
-__device__ __forceinline__ void k_fast_c_body(const PassArgs& a, const int bx, const int by) {
+__device__ __forceinline__ void k_fast_c_body(const PassArgs& a, const int bx, const int by, const int ib) {
     using S = AcShape<M, PZ>;
     constexpr int NZ = S::NZ, XP = S::XP, CW = S::CW, H = M / 2;
     extern __shared__ __align__(16) float2 sm[];
@@ -143,14 +146,14 @@ __device__ __forceinline__ void k_fast_c_body(const PassArgs& a, const int bx, c
     float2* twr = twz + PZ;
     float2* X1 = twr + (H + 1);
     float2* Z2 = X1 + NZ * XP;
-    if (a.active && !*a.active) return;
+    if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
     for (int i = tid; i < M; i += kNT) twx[i] = a.fx.tw[i];
     if (PZ > 1)
         for (int i = tid; i < PZ; i += kNT) twz[i] = a.fz.tw[i];
     for (int i = tid; i <= H; i += kNT) twr[i] = a.twr[i];
     const int y = bx, c = by, Ny = a.Ny;
-    const float2* in = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
+    const float2* in = inst_spec(a, ib) + (long)c * PZ * Ny * a.Lx + (long)y * a.Lx;
     const long kzs = (long)Ny * a.Lx;
     // 1. inverse z FFT per block of columns, keep z < NZ
     if constexpr (PZ == 1) {
@@ -203,7 +206,7 @@ __device__ __forceinline__ void k_fast_c_body(const PassArgs& a, const int bx, c
 #pragma unroll 1
     for (int rb = 0; rb < NZ; rb += S::ZB) sfft<float2, M, S::ZB, kNT, XP, 1, false, +1>(X1 + rb * XP, twx);
     // 4. unpack even/odd samples, crop and overwrite B (copyunpad.cl)
-    float* __restrict__ B = a.B[c];
+    float* __restrict__ B = inst_B(a, ib, c);
     for (int e = tid; e < NZ * H; e += kNT) {
         const int z = e / H, n = e % H;
         float2 v = X1[z * XP + n];
@@ -211,14 +214,12 @@ __device__ __forceinline__ void k_fast_c_body(const PassArgs& a, const int bx, c
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) { k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y); }
-// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+__global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) { k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+// batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(kNT) k_fast_c_bat(PassArgs a) {
     const int per = 3, b = blockIdx.y / per;
-    PassArgs A = a;
-    demag_batch_fix(A, b);
-    k_fast_c_body<M, PZ>(A, blockIdx.x, blockIdx.y - b * per);
+    k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
 
 template <int PY> struct BShape {
@@ -228,18 +229,18 @@ template <int PY> struct BShape {
 };
 
 template <int PY>
-__device__ __forceinline__ void k_fast_b_body(const PassArgs& a, const int bx, const int by) {
+__device__ __forceinline__ void k_fast_b_body(const PassArgs& a, const int bx, const int by, const int ib) {
     constexpr int WB = BShape<PY>::WB, W3 = 3 * WB, NY = PY / 2, HY = PY / 2 + 1;
     extern __shared__ __align__(16) float2 sm[];
     float2* twy = sm;
     float2* S = twy + PY;  // [PY][3*WB]
-    if (a.active && !*a.active) return;
+    if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
     for (int i = tid; i < PY; i += kNTB) twy[i] = a.fy.tw[i];
     const int kx0 = bx * WB, kz = by;
     const int hx = a.Hx, Pz = a.Pz;
     const long cs = (long)Pz * NY * a.Lx;
-    const float2* in = a.spec + (long)kz * NY * a.Lx + kx0;
+    const float2* in = inst_spec(a, ib) + (long)kz * NY * a.Lx + kx0;
     for (int e = tid; e < PY * W3; e += kNTB) {
         const int yy = e / W3, r = e % W3, c = r / WB, w = r % WB;
         float2 v = make_float2(0.f, 0.f);
@@ -276,21 +277,19 @@ __device__ __forceinline__ void k_fast_b_body(const PassArgs& a, const int bx, c
     }
     __syncthreads();
     sfft<float2, PY, W3, kNTB, 1, W3, true, +1>(S, twy);
-    float2* outp = a.spec + (long)kz * NY * a.Lx + kx0;
+    float2* outp = inst_spec(a, ib) + (long)kz * NY * a.Lx + kx0;
     for (int e = tid; e < NY * W3; e += kNTB) {
         const int yy = e / W3, r = e % W3, c = r / WB, w = r % WB;
         if (kx0 + w < hx) outp[c * cs + (long)yy * a.Lx + w] = S[e];
     }
 }
 template <int PY>
-__global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) { k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y); }
-// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+__global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) { k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y, 0); }
+// batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int PY>
 __global__ void __launch_bounds__(kNTB) k_fast_b_bat(PassArgs a) {
     const int per = a.Pz, b = blockIdx.y / per;
-    PassArgs A = a;
-    demag_batch_fix(A, b);
-    k_fast_b_body<PY>(A, blockIdx.x, blockIdx.y - b * per);
+    k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
 
 // cp.async (global -> shared, asynchronous) helpers
@@ -328,14 +327,14 @@ __device__ __forceinline__ long kern_idx(const PassArgs& a, int kz, int ky, int 
 // With the blocked layouts a warp's loads and stores of one component are one
 // contiguous run (WB = 4: 8 rows x 4 columns = 256 bytes).
 template <int PY, int WB>
-__device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, const int by) {
+__device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, const int by, const int ib) {
     constexpr int T = PY / 8, NT = T * WB, NY = PY / 2, HY = PY / 2 + 1;
     constexpr int LP = rg_line<PY>();
     extern __shared__ __align__(16) float2 sm[];
     float2* tw = sm;                  // PY twiddles
     float2* ex = tw + PY;             // [3][WB][LP] exchange lines
     float* Ks = reinterpret_cast<float*>(ex + 3 * WB * LP);  // [6][HY][WB] kernel block
-    if (a.active && !*a.active) return;
+    if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
     const int w = tid % WB, t = tid / WB;
     for (int i = tid; i < PY; i += NT) tw[i] = a.fy.tw[i];
@@ -376,7 +375,7 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     }
     const bool col = kx < hx;
     const long cs = (long)Pz * NY * a.Lx, rs = spec_rowstride(a);
-    const float2* in = a.spec + (long)kz * NY * a.Lx + spec_col(a, kx);
+    const float2* in = inst_spec(a, ib) + (long)kz * NY * a.Lx + spec_col(a, kx);
     float2 v[3][8];
 #pragma unroll
     for (int c = 0; c < 3; c++)
@@ -414,7 +413,7 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     }
     rg_fft_fwd<PY, 3>(v, t, exl, exs, tw);
     if (col) {
-        float2* out = a.spec + (long)kz * NY * a.Lx + spec_col(a, kx);
+        float2* out = inst_spec(a, ib) + (long)kz * NY * a.Lx + spec_col(a, kx);
 #pragma unroll
         for (int c = 0; c < 3; c++)
 #pragma unroll
@@ -425,14 +424,12 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     }
 }
 template <int PY, int WB>
-__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) { k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y); }
-// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) { k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y, 0); }
+// batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int PY, int WB>
 __global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b_bat(PassArgs a) {
     const int per = a.Pz, b = blockIdx.y / per;
-    PassArgs A = a;
-    demag_batch_fix(A, b);
-    k_reg_b_body<PY, WB>(A, blockIdx.x, blockIdx.y - b * per);
+    k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
 
 // ---- passes A and C with the register-blocked FFT (3D, power-of-two sizes)
@@ -448,7 +445,7 @@ template <int M, int PZ> struct RegAC {
 };
 
 template <int M, int PZ>
-__device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, const int by) {
+__device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, const int by, const int ib) {
     using S = RegAC<M, PZ>;
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
     extern __shared__ __align__(16) float2 sm[];
@@ -457,12 +454,13 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
     float2* twr = twz + PZ;    // M: exp(-2 pi i k / Px)
     float2* Xs = twr + M;      // [NZ][XP]
     float2* ex = Xs + NZ * XP; // exchange lines
-    if (a.active && !*a.active) return;
+    if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
     for (int i = tid; i < M; i += NT) { twx[i] = a.fx.tw[i]; twr[i] = a.twr[i]; }
     for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
     const int y = bx, c = by, Ny = a.Ny;
-    const float* __restrict__ mp = a.m_ind ? (a.m_sel ? *a.m_ind_w : *a.m_ind) + (long)c * a.ncell : a.m[c];
+    const float* __restrict__ mp = inst_m(a, ib, c);
+    const float msm = inst_msmul(a, ib);
     // x phase: row z, lane t holds packed z[n] = x[2n] + i x[2n+1], n = t + TX*j
     const int z = tid / TX, t = tid % TX;
     float2 v[1][8];
@@ -471,7 +469,7 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
     for (int j = 0; j < 8; j++) {
         if (j < 4) {  // n < M/2 carries data, the rest is zero padding
             const int i = rowi + 2 * (t + TX * j);
-            v[0][j] = make_float2(scaled_m(a, mp, i), scaled_m(a, mp, i + 1));
+            v[0][j] = make_float2(scaled_m(a, mp, i, msm), scaled_m(a, mp, i + 1, msm));
         } else {
             v[0][j] = make_float2(0.f, 0.f);
         }
@@ -505,7 +503,7 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
         if (k == 0) xrow[M] = make_float2(A.x - A.y, 0.f);  // Nyquist: Re Z0 - Im Z0
     }
     __syncthreads();
-    float2* out = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
+    float2* out = inst_spec(a, ib) + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
     const long kzs = (long)Ny * a.Lx;
     if constexpr (PZ == 16 || PZ == 32) {
         // z phase on lane pairs, decimation in frequency: with x[n] = 0 for
@@ -598,18 +596,16 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) { k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y); }
-// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) { k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+// batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a_bat(PassArgs a) {
     const int per = 3, b = blockIdx.y / per;
-    PassArgs A = a;
-    demag_batch_fix(A, b);
-    k_reg_a_body<M, PZ>(A, blockIdx.x, blockIdx.y - b * per);
+    k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
 
 template <int M, int PZ>
-__device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, const int by) {
+__device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, const int by, const int ib) {
     using S = RegAC<M, PZ>;
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
     extern __shared__ __align__(16) float2 sm[];
@@ -618,13 +614,13 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
     float2* twr = twz + PZ;
     float2* Xs = twr + M;
     float2* ex = Xs + NZ * XP;
-    if (a.active && !*a.active) return;
+    if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
     for (int i = tid; i < M; i += NT) { twx[i] = a.fx.tw[i]; twr[i] = a.twr[i]; }
     for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
     __syncthreads();
     const int y = bx, c = by, Ny = a.Ny;
-    const float2* in = a.spec + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
+    const float2* in = inst_spec(a, ib) + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
     const long kzs = (long)Ny * a.Lx;
     if constexpr (PZ == 16 || PZ == 32) {
         // z phase on lane pairs, inverse by the conjugate trick, decimation in
@@ -729,7 +725,7 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
         v[0][j] = make_float2(S1.x - T1.y, -(S1.y + T1.x));  // conj(Z[k])
     }
     rg_fft_fwd<M, 1, true, 4>(v, t, ex + z * S::LX, 0, twx);
-    float* __restrict__ B = a.B[c];
+    float* __restrict__ B = inst_B(a, ib, c);
     const int rowo = (z * Ny + y) * M;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -738,14 +734,12 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) { k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y); }
-// batched: blockIdx.y = index + per * instance (see demag_batch_fix)
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) { k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+// batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c_bat(PassArgs a) {
     const int per = 3, b = blockIdx.y / per;
-    PassArgs A = a;
-    demag_batch_fix(A, b);
-    k_reg_c_body<M, PZ>(A, blockIdx.x, blockIdx.y - b * per);
+    k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
 
 template <int PY> struct RegB {

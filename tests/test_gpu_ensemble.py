@@ -69,3 +69,30 @@ def test_ensemble_is_deterministic_and_matches_every_instance():
             runs[0][0][i]["nsteps"], runs[0][0][i]["nundone"], runs[0][0][i]["time"], runs[0][0][i]["dt"]), i
         np.testing.assert_array_equal(sim.get_m().cpu().numpy(), runs[0][1][i])
         sim.free()
+
+
+def test_ensemble_error_against_fp64_oracle():
+    """Two ensemble instances against the FP64 oracle (uMagNUS64 restated)
+    after 20 ps of adaptive RK45DP: <m> within 1e-4, every cell within 1e-3
+    (float32 state and FFT against FP64; the ensemble is bit-identical to
+    the single-instance engine, so this is also the plain form's error)."""
+    from oracle import oracle as O
+    import bench
+    from umagnus_b200 import engine
+    insts = [dict(N=(32, 32, 1), cell=(4e-9, 4e-9, 3e-9), Msat=7e5, Aex=1.1e-11, alpha=0.2, B_ext=(0.03, 0.0, 0.04)),
+             dict(N=(48, 48, 1), cell=(4e-9, 4e-9, 3e-9), Msat=1.0e6, Aex=1.6e-11, alpha=0.35, B_ext=(0.0, 0.05, 0.0))]
+    ens = engine.Ensemble(insts)
+    ms = [bench.random_m(d["N"], 100 + i) for i, d in enumerate(insts)]
+    for i, m in enumerate(ms):
+        ens.set_m(i, m)
+    T = 2e-11
+    ens.run(T)
+    for i, d in enumerate(insts):
+        orc = O.Simulation(d["N"], d["cell"], d["Msat"], d["Aex"], d["alpha"], dtype=np.float64, B_ext=d["B_ext"])
+        orc.set_m(ms[i].astype(np.float64))
+        orc.run(T)
+        got = ens.get_m(i).astype(np.float64)
+        want = orc.m.reshape(got.shape)
+        assert np.max(np.abs(got - want)) < 1e-3
+        assert np.max(np.abs(got.reshape(3, -1).mean(1) - want.reshape(3, -1).mean(1))) < 1e-4
+    ens.free()

@@ -436,6 +436,84 @@ def run_ensemble(args):
     return 0
 
 
+# ------------------------------------------------------------------ adjoint workload
+def adjoint_problem(seed=4):
+    """The differentiation workload: 128x128x1 film of 4 nm cubes, per-cell Ms
+    U[6e5, 9e5] A/m, Aex 1.3e-11 J/m, Ku1 2e5 J/m^3 along x, alpha 0.02,
+    B_ext (5, 5, 0) mT; fixed-step RK4, dt 1e-13 s, 4000 steps, checkpoints
+    every 100 steps; loss = mean over the last 1000 steps of m_z averaged over
+    a 16x16 probe window (centre of the film) + |<m>(final) - target|^2 with a
+    seeded random unit target; m0 random unit vectors (seeded)."""
+    rng = np.random.default_rng(seed)
+    n = 128
+    Ms = rng.uniform(6e5, 9e5, (1, n, n)).astype(np.float32)
+    m0 = random_m((n, n, 1), seed + 1)
+    t = rng.standard_normal(3)
+    t /= np.linalg.norm(t)
+    kw = dict(N=(n, n, 1), cell=(4e-9, 4e-9, 4e-9), alpha=0.02, anisU=(1.0, 0.0, 0.0), dt=1e-13, nsteps=4000,
+              probe=(56, 56, 16, 16), avg_from=3001, target=tuple(float(x) for x in t))
+    theta = dict(Aex=1.3e-11, Ku1=2e5, B_ext=(5e-3, 5e-3, 0.0))
+    return kw, Ms, m0, theta
+
+
+def run_adjoint(args):
+    """Forward and backward of the differentiation workload, timed with CUDA
+    events on the library's stream (each call returns after its work ends);
+    optionally the gradients against the FP64 oracle's reverse pass."""
+    import torch
+    from umagnus_b200.adjoint import AdjointRK4
+    kw, Ms, m0, th = adjoint_problem()
+    sim = AdjointRK4(K=100, **kw)
+    fw, bw = [], []
+    for it in range(max(args.warmup, 1) + args.steps):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        loss = sim.forward(m0, Ms, th["Aex"], th["Ku1"], th["B_ext"])
+        e1.record()
+        g = sim.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        if it >= max(args.warmup, 1):
+            fw.append(e0.elapsed_time(e1) / 1e3)
+            bw.append(e1.elapsed_time(e2) / 1e3)
+    f, b = float(np.median(fw)), float(np.median(bw))
+    N = 128 * 128
+    line = {"metric": "adjoint backward/forward time, 128x128x1 film, RK4 4000 steps",
+            "value": b / f, "unit": "backward/forward", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 1), "higher_is_better": False, "dtype": "f32",
+            "data": "synthetic (seeded Ms map, m0 and target)",
+            "config": {"workload": "128x128x1 film, 4 nm cells, per-cell Ms U[6e5,9e5], Aex 1.3e-11, Ku1 2e5 along x, "
+                                   "alpha 0.02, B_ext (5,5,0) mT, Newell demag, fixed-step RK4 dt 1e-13 s x 4000, "
+                                   "checkpoints every 100 steps", "cells": N},
+            "forward_s": f, "backward_s": b,
+            "forward_cell_updates_per_s": 4000 * N / f,
+            "loss": loss,
+            "grad": {"Aex": g["Aex"], "Ku1": g["Ku1"], "B_ext": g["B_ext"],
+                     "Ms_norm": float(torch.linalg.vector_norm(g["Ms"].double()))}}
+    if args.adj_fp64:
+        from oracle import adjoint_ref as R
+        t0 = time.perf_counter()
+        prob = R.Problem(**kw)
+        loss64, g64 = prob.backward(m0.astype(np.float64).reshape(3, 1, 128, 128),
+                                    R.params(Ms.astype(np.float64), th["Aex"], th["Ku1"], th["B_ext"]))
+
+        def rel(a, b_):
+            a, b_ = np.asarray(a, np.float64), np.asarray(b_, np.float64)
+            return float(np.linalg.norm(a - b_) / np.linalg.norm(b_))
+        gMs = g["Ms"].cpu().numpy()
+        cells = np.random.default_rng(7).choice(N, 64, replace=False)
+        per_cell = np.abs(gMs.ravel()[cells] - g64["Ms"].ravel()[cells]) / np.abs(g64["Ms"].ravel()[cells])
+        line["fp64_check"] = {"loss_fp64": loss64, "loss_rel_err": abs(loss - loss64) / abs(loss64),
+                              "rel_err": {"Ms": rel(gMs, g64["Ms"]), "Aex": rel(g["Aex"], g64["A"]),
+                                          "Ku1": rel(g["Ku1"], g64["K1"]), "B_ext": rel(g["B_ext"], g64["B"]),
+                                          "m0": rel(g["m0"].cpu().numpy(), g64["m0"])},
+                              "Ms_64_cells_max_rel_err": float(per_cell.max()),
+                              "seconds_cpu": time.perf_counter() - t0}
+    sim.free()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -444,12 +522,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=90.0, help="seconds of timed CPU steps (reference arm)")
-    ap.add_argument("--workload", default="multilayer", choices=["multilayer", "ensemble"])
+    ap.add_argument("--workload", default="multilayer", choices=["multilayer", "ensemble", "adjoint"])
+    ap.add_argument("--adj-fp64", action="store_true", help="adjoint: compare with the FP64 oracle (minutes of CPU)")
     ap.add_argument("--ens-time", type=float, default=2e-9, help="ensemble: simulated time per instance (s)")
     ap.add_argument("--ens-plain-sample", type=int, default=2, help="ensemble: plain-form instances timed per size")
     args = ap.parse_args()
     if args.workload == "ensemble":
         return run_ensemble(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

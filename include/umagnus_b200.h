@@ -298,6 +298,44 @@ int umag_ens_get_state(umag_ens* e, int i, umag_solver_state* st);
 int umag_ens_run(umag_ens* e, double seconds, int chunk, long long max_replays);
 int umag_ens_count(umag_ens* e, int* n_instances, int* n_classes);
 
+/* ---- differentiable simulation: forward RK4 and its adjoint --------------
+ * No counterpart in the reference (which has no gradients).  A thin film or
+ * block with a per-cell Ms map, uniform exchange Aex, uniaxial Ku1 along
+ * anisU, Zeeman field B_ext and damping alpha, integrated by fixed-step RK4
+ * (engine/rk4.go with FixDt) for nsteps steps; m is checkpointed every K
+ * steps.  Loss = w_probe * (mean over states avg_from..nsteps of the mean
+ * m_z over the probe window of layer 0) + w_target * |<m>(final) - target|^2.
+ * umag_adj_backward returns dLoss/dMs (per cell), dLoss/dAex, dLoss/dKu1,
+ * dLoss/dB_ext and, if gm0 is not NULL, dLoss/dm0, by hand-written
+ * vector-Jacobian products through the steps, recomputing each segment of
+ * K steps from its checkpoint. */
+typedef struct {
+    int N[3];
+    double cell[3];
+    float alpha;
+    float anisU[3];
+    int enable_demag;
+    int demag_kernel;       /* 0 Newell, 1 brute force (engine/demag.go) */
+    double demag_accuracy;  /* brute force; <= 0: 6 */
+    double dt, gamma_ll;    /* gamma_ll <= 0: 1.7595e11 */
+    int nsteps, K;
+    int probe[4];           /* x0, y0, width, height (cells, layer 0) */
+    int avg_from;           /* 1 <= avg_from <= nsteps */
+    double w_probe, w_target;
+    double target[3];
+} umag_adj_params;
+typedef struct umag_adj umag_adj;
+int umag_adj_new(const umag_adj_params* p, umag_adj** out);
+int umag_adj_free(umag_adj* a);
+/* device arrays: m0 3N floats (normalised first), Ms N floats */
+int umag_adj_forward(umag_adj* a, const float* m0, const float* Ms, float Aex, float Ku1, const float B_ext[3],
+                     double* loss);
+/* final m of the last forward (device, 3N floats) */
+int umag_adj_final_m(umag_adj* a, float* m);
+/* gradients of the last forward's loss: gMs device N floats, gm0 device 3N
+ * floats or NULL; the scalars on the host */
+int umag_adj_backward(umag_adj* a, float* gMs, float* gm0, double* gAex, double* gKu1, double gB_ext[3]);
+
 /* ---- field files (oommf/*.go, dump/*.go) ----------------------------------
  * Host arrays of float32, structure of arrays [c][z][y][x] (x fastest), the
  * layout of data.Slice.Tensors(); numbers in headers and text data are

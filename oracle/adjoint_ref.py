@@ -1,0 +1,228 @@
+"""FP64 CPU restatement of the differentiable RK4 simulation and its adjoint.
+
+TEST INFRASTRUCTURE ONLY: tests/ and bench.py import this module to check
+the GPU adjoint (umag_adj_*); the product never does.
+
+The model is the engine's effective field and LL torque for uniform region
+0 (engine/effectivefield.go:14-24, engine/demag.go, engine/exchange.go,
+engine/anisotropy.go, engine/zeeman.go, engine/torque.go:135-144) with a
+per-cell Ms map, stepped by fixed-step RK4 (engine/rk4.go:35-61, every stage
+normalised, opencl normalize2.cl).  The reference has no gradients; this
+module gives the FP64 gradient two ways: a hand-written reverse pass (the
+same vector-Jacobian products as the GPU adjoint, in FP64) and central
+finite differences of the FP64 forward, so that the two can pin each other.
+
+Arrays are (3, Nz, Ny, Nx) for vectors and (Nz, Ny, Nx) for Ms.
+"""
+import numpy as np
+
+from . import oracle
+
+MU0 = 4 * np.pi * 1e-7  # kernels_src/clh/constants.clh:5
+GAMMA_LL = 1.7595e11    # engine/torque.go:27
+
+
+class Problem:
+    """Static part of the problem: mesh, demag kernel, stepper, loss."""
+
+    def __init__(self, N, cell, alpha, anisU, dt, nsteps, probe, avg_from, w_probe=1.0, w_target=1.0,
+                 target=(0.0, 0.0, 1.0), demag=True, gamma_ll=GAMMA_LL):
+        self.N = tuple(int(n) for n in N)
+        self.cell = tuple(float(c) for c in cell)
+        self.alpha = float(alpha)
+        u = np.asarray(anisU, np.float64)
+        self.u = u / np.linalg.norm(u) if np.linalg.norm(u) > 0 else u
+        self.h = dt * gamma_ll
+        self.nsteps = int(nsteps)
+        self.probe = tuple(int(p) for p in probe)
+        self.avg_from = int(avg_from)
+        self.w_probe, self.w_target = float(w_probe), float(w_target)
+        self.target = np.asarray(target, np.float64)
+        self.gilb = -1.0 / (1.0 + self.alpha ** 2)
+        self.w = [2.0 / (c * c) for c in self.cell]
+        self.demag = demag
+        if demag:
+            K = oracle.newell_kernel(self.N, self.cell)  # (6, Pz, Py, Px): xx yy zz yz xz xy
+            self.P = K.shape[1:]
+            self.Kf = np.fft.rfftn(K, axes=(1, 2, 3))
+
+    # ------------------------------------------------------------ field
+    def demag_field(self, v):
+        """mu0 * K * v (v already scaled by Ms), zero-padded convolution."""
+        Nx, Ny, Nz = self.N
+        Pz, Py, Px = self.P
+        V = np.zeros((3, Pz, Py, Px))
+        V[:, :Nz, :Ny, :Nx] = v
+        F = np.fft.rfftn(V, axes=(1, 2, 3))
+        xx, yy, zz, yz, xz, xy = self.Kf
+        Bf = np.stack([xx * F[0] + xy * F[1] + xz * F[2],
+                       xy * F[0] + yy * F[1] + yz * F[2],
+                       xz * F[0] + yz * F[1] + zz * F[2]])
+        B = np.fft.irfftn(Bf, s=(Pz, Py, Px), axes=(1, 2, 3))
+        return MU0 * B[:, :Nz, :Ny, :Nx]
+
+    def stencil(self, v):
+        """sum_d w_d (v_neighbour - v) with clamped neighbours (exchange.cl)."""
+        out = np.zeros_like(v)
+        Nz = v.shape[1]
+        axes = [(3, self.w[0]), (2, self.w[1])] + ([(1, self.w[2])] if Nz > 1 else [])
+        for ax, w in axes:
+            n = v.shape[ax]
+            idx = np.arange(n)
+            lo = np.take(v, np.maximum(idx - 1, 0), axis=ax)
+            hi = np.take(v, np.minimum(idx + 1, n - 1), axis=ax)
+            out += w * ((lo - v) + (hi - v))
+        return out
+
+    def field(self, m, th):
+        Ms, A, K1, Bext = th["Ms"], th["A"], th["K1"], th["B"]
+        B = self.demag_field(Ms * m) if self.demag else np.zeros_like(m)
+        B = B + A * self.stencil(m) / Ms
+        if K1 != 0:
+            mu = np.einsum("c...,c->...", m, self.u)
+            B = B + (2 * K1 / Ms * mu)[None] * self.u[:, None, None, None]
+        return B + np.asarray(Bext, np.float64)[:, None, None, None]
+
+    def torque(self, m, B):
+        mxB = np.cross(m, B, axis=0)
+        return self.gilb * (mxB + self.alpha * np.cross(m, mxB, axis=0))
+
+    @staticmethod
+    def normalize(v):
+        return v / np.sqrt((v * v).sum(0))[None]
+
+    def step(self, m, th, keep=False):
+        h = self.h
+        ms, Bs, ks = [m], [], []
+        for q in range(4):
+            B = self.field(ms[q], th)
+            k = self.torque(ms[q], B)
+            Bs.append(B)
+            ks.append(k)
+            if q < 3:
+                c = (0.5, 0.5, 1.0)[q]
+                ms.append(self.normalize(m + c * h * k))
+        out = self.normalize(m + h / 6 * ks[0] + h / 3 * ks[1] + h / 3 * ks[2] + h / 6 * ks[3])
+        return (out, ms, Bs, ks) if keep else out
+
+    # ------------------------------------------------------------ loss
+    def probe_mean(self, m):
+        x0, y0, w, h = self.probe
+        return m[2, 0, y0:y0 + h, x0:x0 + w].mean()
+
+    def forward(self, m0, th, keep=False):
+        m = self.normalize(np.asarray(m0, np.float64))
+        states = [m]
+        acc = 0.0
+        for n in range(1, self.nsteps + 1):
+            m = self.step(m, th)
+            if keep:
+                states.append(m)
+            if n >= self.avg_from:
+                acc += self.probe_mean(m)
+        navg = self.nsteps - self.avg_from + 1
+        avg = m.reshape(3, -1).mean(1)
+        loss = self.w_probe * acc / navg + self.w_target * ((avg - self.target) ** 2).sum()
+        return (loss, states) if keep else loss
+
+    # ------------------------------------------------------------ adjoint
+    def _loss_grad(self, m, with_probe, with_avg):
+        g = np.zeros_like(m)
+        x0, y0, w, h = self.probe
+        navg = self.nsteps - self.avg_from + 1
+        if with_probe:
+            g[2, 0, y0:y0 + h, x0:x0 + w] += self.w_probe / (navg * w * h)
+        if with_avg:
+            avg = m.reshape(3, -1).mean(1)
+            g += (2 * self.w_target * (avg - self.target) / m[0].size)[:, None, None, None]
+        return g
+
+    @staticmethod
+    def _norm_vjp(u, w):
+        ln = np.sqrt((u * u).sum(0))[None]
+        n = u / ln
+        return (w - n * (n * w).sum(0)[None]) / ln
+
+    def _field_vjp(self, m, wB, th, grads):
+        Ms, A, K1 = th["Ms"], th["A"], th["K1"]
+        gm = np.zeros_like(m)
+        if self.demag:
+            dw = self.demag_field(wB)
+            gm += Ms * dw
+            grads["Ms"] += (m * dw).sum(0)
+        e = self.stencil(m)
+        gm += A * self.stencil(wB / Ms)
+        we = (wB * e).sum(0)
+        grads["Ms"] -= A * we / Ms ** 2
+        grads["A"] += (we / Ms).sum()
+        if K1 != 0:
+            mu = np.einsum("c...,c->...", m, self.u)
+            wu = np.einsum("c...,c->...", wB, self.u)
+            gm += (2 * K1 / Ms * wu)[None] * self.u[:, None, None, None]
+            grads["Ms"] -= 2 * K1 * mu * wu / Ms ** 2
+            grads["K1"] += (2 * mu * wu / Ms).sum()
+        grads["B"] += wB.reshape(3, -1).sum(1)
+        return gm
+
+    def _torque_vjp(self, m, B, w):
+        g = self.gilb
+        a = self.alpha
+        mxB = np.cross(m, B, axis=0)
+        wxm = np.cross(w, m, axis=0)
+        gm = g * (np.cross(B, w, axis=0) + a * (np.cross(mxB, w, axis=0) + np.cross(B, wxm, axis=0)))
+        wB = g * (wxm + a * np.cross(wxm, m, axis=0))
+        return gm, wB
+
+    def backward(self, m0, th):
+        """Gradient of forward(m0, th) by the reverse pass (all states kept)."""
+        loss, states = self.forward(m0, th, keep=True)
+        grads = {"Ms": np.zeros_like(th["Ms"], dtype=np.float64), "A": 0.0, "K1": 0.0, "B": np.zeros(3)}
+        h = self.h
+        lam = self._loss_grad(states[-1], self.nsteps >= self.avg_from, True)
+        fin = (h / 6, h / 3, h / 3, h / 6)
+        stc = (0.5 * h, 0.5 * h, 1.0 * h)
+        for n in range(self.nsteps, 0, -1):
+            m = states[n - 1]
+            _, ms, Bs, ks = self.step(m, th, keep=True)
+            u = m + sum(f * k for f, k in zip(fin, ks))
+            gu = self._norm_vjp(u, lam)
+            lam2 = gu.copy()
+            gk = [f * gu for f in fin]
+            for q in range(3, -1, -1):
+                gmq, wB = self._torque_vjp(ms[q], Bs[q], gk[q])
+                gmq = gmq + self._field_vjp(ms[q], wB, th, grads)
+                if q > 0:
+                    gu = self._norm_vjp(m + stc[q - 1] * ks[q - 1], gmq)
+                    lam2 += gu
+                    gk[q - 1] = gk[q - 1] + stc[q - 1] * gu
+                else:
+                    lam2 += gmq
+            lam = lam2
+            if n - 1 >= self.avg_from:
+                lam = lam + self._loss_grad(states[n - 1], True, False)
+        grads["m0"] = self._norm_vjp(np.asarray(m0, np.float64), lam)
+        return loss, grads
+
+
+def params(Ms, A, K1, B):
+    return {"Ms": np.asarray(Ms, np.float64), "A": float(A), "K1": float(K1), "B": np.asarray(B, np.float64)}
+
+
+def fd_gradient(prob, m0, th, which, rel=1e-4):
+    """Central finite differences of the FP64 loss with relative step rel.
+
+    which: ("Ms", (z, y, x)), ("A", None), ("K1", None) or ("B", c); for a
+    zero-valued parameter the step is rel (absolute)."""
+    name, idx = which
+
+    def with_value(v):
+        t = {k: (np.array(x, copy=True) if isinstance(x, np.ndarray) else x) for k, x in th.items()}
+        if idx is None:
+            t[name] = v
+        else:
+            t[name][idx] = v
+        return t
+
+    x0 = th[name] if idx is None else th[name][idx]
+    d = rel * abs(x0) if x0 != 0 else rel
+    return (prob.forward(m0, with_value(x0 + d)) - prob.forward(m0, with_value(x0 - d))) / (2 * d)

@@ -1,0 +1,125 @@
+"""GPU adjoint (umag_adj_*): the forward pass against the engine's RK4, the
+gradients against the FP64 oracle's reverse pass (itself pinned to central
+finite differences in tests/test_oracle_adjoint.py), and the autograd
+wrapper.  The problem is the differentiation workload (per-cell Ms map in
+[6e5, 9e5] A/m, Aex 1.3e-11 J/m, Ku1 2e5 J/m^3 along x, alpha 0.02,
+B_ext (5, 5, 0) mT, fixed-step RK4 with dt 1e-13 s) on a smaller film and
+fewer steps, so that the FP64 oracle finishes in seconds."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import adjoint_ref as R
+
+pytestmark = pytest.mark.gpu
+
+CELL = (4e-9, 4e-9, 4e-9)
+A_EX, KU1, BEXT = 1.3e-11, 2e5, (5e-3, 5e-3, 0.0)
+
+
+def make_case(n, steps, seed):
+    rng = np.random.default_rng(seed)
+    Ms = rng.uniform(6e5, 9e5, (1, n, n)).astype(np.float32)
+    m0 = rng.normal(size=(3, 1, n, n))
+    m0 = (m0 / np.linalg.norm(m0, axis=0)).astype(np.float32)
+    t = rng.normal(size=3)
+    t /= np.linalg.norm(t)
+    w = max(2, n // 8)
+    kw = dict(N=(n, n, 1), cell=CELL, alpha=0.02, anisU=(1.0, 0.0, 0.0), dt=1e-13, nsteps=steps,
+              probe=(n // 2 - w // 2, n // 2 - w // 2, w, w), avg_from=steps - steps // 4 + 1, target=tuple(t))
+    return Ms, m0, kw
+
+
+def gpu_sim(kw, K):
+    from umagnus_b200.adjoint import AdjointRK4
+    return AdjointRK4(K=K, **kw)
+
+
+def test_forward_matches_engine_rk4():
+    """The adjoint's forward pass is the engine's fixed-step RK4, bit for bit."""
+    from umagnus_b200.engine import RUNGEKUTTA, Simulation
+    Ms, m0, kw = make_case(32, 40, 1)
+    adj = gpu_sim(kw, K=16)
+    adj.forward(m0, Ms, A_EX, KU1, BEXT)
+    m_adj = adj.final_m().cpu().numpy()
+    sim = Simulation(kw["N"], CELL, Msat=Ms, Aex=A_EX, alpha=0.02, Ku1=KU1, anisU=(1.0, 0.0, 0.0), B_ext=BEXT,
+                     solver=RUNGEKUTTA, dt=1e-13, FixDt=1e-13)
+    sim.set_m(m0)
+    sim.steps(40)
+    m_eng = sim.get_m().cpu().numpy().reshape(m_adj.shape)
+    assert np.array_equal(m_adj, m_eng), np.abs(m_adj - m_eng).max()
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("n,steps,K", [(16, 30, 7), (32, 60, 16)])
+def test_gradients_match_fp64_oracle(n, steps, K):
+    Ms, m0, kw = make_case(n, steps, 2 + n)
+    adj = gpu_sim(kw, K=K)
+    loss = adj.forward(m0, Ms, A_EX, KU1, BEXT)
+    g = adj.backward()
+    prob = R.Problem(**{k: v for k, v in kw.items()})
+    th = R.params(Ms.astype(np.float64), A_EX, KU1, BEXT)
+    loss64, g64 = prob.backward(m0.astype(np.float64), th)
+    assert abs(loss - loss64) <= 1e-5 * max(1.0, abs(loss64))
+    errs = {"Ms": _rel(g["Ms"].cpu().numpy(), g64["Ms"]), "m0": _rel(g["m0"].cpu().numpy(), g64["m0"]),
+            "Aex": _rel(g["Aex"], g64["A"]), "Ku1": _rel(g["Ku1"], g64["K1"]),
+            "B_ext": _rel(g["B_ext"], g64["B"])}
+    print("relative gradient error vs FP64:", errs)
+    for k, e in errs.items():
+        assert e < 1e-3, (k, e)
+
+
+def test_segment_length_does_not_change_gradients():
+    """Checkpoint interval K only changes what is recomputed, not the result."""
+    Ms, m0, kw = make_case(16, 24, 9)
+    out = []
+    for K in (1, 5, 24):
+        adj = gpu_sim(kw, K=K)
+        loss = adj.forward(m0, Ms, A_EX, KU1, BEXT)
+        g = adj.backward()
+        out.append((loss, g["Ms"].cpu().numpy(), g["Aex"], g["Ku1"], g["B_ext"]))
+    for o in out[1:]:
+        assert o[0] == out[0][0]
+        assert np.array_equal(o[1], out[0][1])
+        # FP64 sums accumulate per-block partials atomically: equal to rounding
+        for a, b in zip(o[2:], out[0][2:]):
+            assert np.allclose(a, b, rtol=1e-9, atol=0)
+
+
+def test_autograd_function():
+    Ms, m0, kw = make_case(16, 20, 11)
+    adj = gpu_sim(kw, K=8)
+    dev = torch.device("cuda", 0)
+    tMs = torch.tensor(Ms, device=dev, requires_grad=True)
+    tm0 = torch.tensor(m0, device=dev, requires_grad=True)
+    tA = torch.tensor(A_EX, dtype=torch.float64, requires_grad=True)
+    tK = torch.tensor(KU1, dtype=torch.float64, requires_grad=True)
+    tB = torch.tensor(BEXT, dtype=torch.float64, requires_grad=True)
+    loss = adj.loss(tm0, tMs, tA, tK, tB)
+    (2.0 * loss).backward()
+    ref = gpu_sim(kw, K=8)
+    ref.forward(m0, Ms, A_EX, KU1, BEXT)
+    g = ref.backward()
+    assert torch.equal(tMs.grad, 2.0 * g["Ms"])
+    assert torch.equal(tm0.grad, 2.0 * g["m0"])
+    assert float(tA.grad) == 2.0 * g["Aex"]
+    assert float(tK.grad) == 2.0 * g["Ku1"]
+    assert np.allclose(tB.grad.numpy(), 2.0 * np.asarray(g["B_ext"]), rtol=0, atol=0)
+
+
+def test_argument_errors():
+    from umagnus_b200._lib import UmagError
+    Ms, m0, kw = make_case(16, 10, 3)
+    bad = dict(kw, avg_from=11)
+    with pytest.raises(UmagError):
+        gpu_sim(bad, K=4)
+    bad = dict(kw, probe=(10, 10, 8, 8))
+    with pytest.raises(UmagError):
+        gpu_sim(bad, K=4)
+    adj = gpu_sim(kw, K=4)
+    with pytest.raises(UmagError):
+        adj.backward()  # no forward yet

@@ -50,6 +50,13 @@ class EnsInstance(ctypes.Structure):
                 ("Dind", c_float), ("Ku1", c_float), ("Ku2", c_float), ("anisU", c_float * 3), ("B_ext", c_float * 3)]
 
 
+class AdjParams(ctypes.Structure):
+    _fields_ = [("N", c_int * 3), ("cell", c_double * 3), ("alpha", c_float), ("anisU", c_float * 3),
+                ("enable_demag", c_int), ("demag_kernel", c_int), ("demag_accuracy", c_double),
+                ("dt", c_double), ("gamma_ll", c_double), ("nsteps", c_int), ("K", c_int), ("probe", c_int * 4),
+                ("avg_from", c_int), ("w_probe", c_double), ("w_target", c_double), ("target", c_double * 3)]
+
+
 # name -> argtypes (restype int unless listed in _RESTYPE)
 _SIGS = {
     "umag_init": [c_int], "umag_release": [], "umag_last_error": [], "umag_set_stream": [P], "umag_sync": [],
@@ -96,6 +103,10 @@ _SIGS = {
     "umag_ens_new": [c_int, P, P, c_int, ctypes.POINTER(c_void_p)], "umag_ens_free": [P],
     "umag_ens_set_m": [P, c_int, P], "umag_ens_get_m": [P, c_int, P], "umag_ens_get_state": [P, c_int, P],
     "umag_ens_run": [P, c_double, c_int, c_ll], "umag_ens_count": [P, ctypes.POINTER(c_int), ctypes.POINTER(c_int)],
+    "umag_adj_new": [ctypes.POINTER(AdjParams), ctypes.POINTER(c_void_p)], "umag_adj_free": [P],
+    "umag_adj_forward": [P, P, P, c_float, c_float, ctypes.POINTER(c_float), ctypes.POINTER(c_double)],
+    "umag_adj_final_m": [P, P],
+    "umag_adj_backward": [P, P, P, ctypes.POINTER(c_double), ctypes.POINTER(c_double), ctypes.POINTER(c_double)],
 }
 _RESTYPE = {"umag_last_error": ctypes.c_char_p, "umag_version": ctypes.c_char_p, "umag_solver_defaults": None}
 

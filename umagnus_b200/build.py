@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libumagnus_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["ops.cu", "demag.cu", "demag_fast.cu", "engine.cu", "capi.cu", "noalloc.cu", "ovf.cu", "brute.cu"]
+SOURCES = ["ops.cu", "demag.cu", "demag_fast.cu", "engine.cu", "capi.cu", "noalloc.cu", "ovf.cu", "brute.cu", "adjoint.cu"]
 # per-file flags: the brute-force kernel keeps the reference's FP64 operation
 # order (no fused multiply-adds)
 FILE_FLAGS = {"brute.cu": ["-fmad=false"]}

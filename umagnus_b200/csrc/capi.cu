@@ -195,5 +195,15 @@ int umag_ens_run(umag_ens* e, double seconds, int chunk, long long max_replays) 
     return ens_run(e, seconds, chunk, max_replays);
 }
 int umag_ens_count(umag_ens* e, int* n_instances, int* n_classes) { return ens_count(e, n_instances, n_classes); }
+int umag_adj_new(const umag_adj_params* p, umag_adj** out) { return adj_new(p, out); }
+int umag_adj_free(umag_adj* a) { return adj_free(a); }
+int umag_adj_forward(umag_adj* a, const float* m0, const float* Ms, float Aex, float Ku1, const float B_ext[3],
+                     double* loss) {
+    return adj_forward(a, m0, Ms, Aex, Ku1, B_ext, loss);
+}
+int umag_adj_final_m(umag_adj* a, float* m) { return adj_final_m(a, m); }
+int umag_adj_backward(umag_adj* a, float* gMs, float* gm0, double* gAex, double* gKu1, double gB_ext[3]) {
+    return adj_backward(a, gMs, gm0, gAex, gKu1, gB_ext);
+}
 
 }  // extern "C"

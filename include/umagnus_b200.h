@@ -323,6 +323,7 @@ typedef struct {
     int avg_from;           /* 1 <= avg_from <= nsteps */
     double w_probe, w_target;
     double target[3];
+    int no_graph;           /* 1: plain stream launches instead of CUDA graphs */
 } umag_adj_params;
 typedef struct umag_adj umag_adj;
 int umag_adj_new(const umag_adj_params* p, umag_adj** out);

@@ -30,9 +30,9 @@ def make_case(n, steps, seed):
     return Ms, m0, kw
 
 
-def gpu_sim(kw, K):
+def gpu_sim(kw, K, use_graph=True):
     from umagnus_b200.adjoint import AdjointRK4
-    return AdjointRK4(K=K, **kw)
+    return AdjointRK4(K=K, use_graph=use_graph, **kw)
 
 
 def test_forward_matches_engine_rk4():
@@ -73,21 +73,43 @@ def test_gradients_match_fp64_oracle(n, steps, K):
         assert e < 1e-3, (k, e)
 
 
+def _run(kw, K, Ms, m0, use_graph=True):
+    adj = gpu_sim(kw, K=K, use_graph=use_graph)
+    loss = adj.forward(m0, Ms, A_EX, KU1, BEXT)
+    g = adj.backward()
+    return (loss, g["Ms"].cpu().numpy(), g["m0"].cpu().numpy(), g["Aex"], g["Ku1"], tuple(g["B_ext"]))
+
+
+def _same(a, b):
+    assert a[0] == b[0]
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    assert a[3:] == b[3:]
+
+
 def test_segment_length_does_not_change_gradients():
-    """Checkpoint interval K only changes what is recomputed, not the result."""
+    """The checkpoint interval K only changes what is recomputed: results
+    are bit-identical (per-cell FP64 accumulators, fixed-order reduction)."""
     Ms, m0, kw = make_case(16, 24, 9)
-    out = []
-    for K in (1, 5, 24):
-        adj = gpu_sim(kw, K=K)
-        loss = adj.forward(m0, Ms, A_EX, KU1, BEXT)
-        g = adj.backward()
-        out.append((loss, g["Ms"].cpu().numpy(), g["Aex"], g["Ku1"], g["B_ext"]))
-    for o in out[1:]:
-        assert o[0] == out[0][0]
-        assert np.array_equal(o[1], out[0][1])
-        # FP64 sums accumulate per-block partials atomically: equal to rounding
-        for a, b in zip(o[2:], out[0][2:]):
-            assert np.allclose(a, b, rtol=1e-9, atol=0)
+    ref = _run(kw, 24, Ms, m0)
+    for K in (1, 5, 7):
+        _same(_run(kw, K, Ms, m0), ref)
+
+
+def test_graphs_match_stream_launches():
+    Ms, m0, kw = make_case(16, 20, 13)
+    _same(_run(kw, 6, Ms, m0, use_graph=True), _run(kw, 6, Ms, m0, use_graph=False))
+
+
+def test_repeated_calls_and_new_parameters():
+    """Graphs are keyed by the baked-in parameters: a second forward with a
+    different Aex must not replay the first one's graphs."""
+    Ms, m0, kw = make_case(16, 12, 17)
+    adj = gpu_sim(kw, K=4)
+    l1 = adj.forward(m0, Ms, A_EX, KU1, BEXT)
+    l2 = adj.forward(m0, Ms, 2 * A_EX, KU1, BEXT)
+    l3 = adj.forward(m0, Ms, A_EX, KU1, BEXT)
+    fresh = gpu_sim(kw, K=4, use_graph=False)
+    assert l1 == l3 and l2 == fresh.forward(m0, Ms, 2 * A_EX, KU1, BEXT) and l1 != l2
 
 
 def test_autograd_function():

@@ -54,7 +54,8 @@ class AdjParams(ctypes.Structure):
     _fields_ = [("N", c_int * 3), ("cell", c_double * 3), ("alpha", c_float), ("anisU", c_float * 3),
                 ("enable_demag", c_int), ("demag_kernel", c_int), ("demag_accuracy", c_double),
                 ("dt", c_double), ("gamma_ll", c_double), ("nsteps", c_int), ("K", c_int), ("probe", c_int * 4),
-                ("avg_from", c_int), ("w_probe", c_double), ("w_target", c_double), ("target", c_double * 3)]
+                ("avg_from", c_int), ("w_probe", c_double), ("w_target", c_double), ("target", c_double * 3),
+                ("no_graph", c_int)]
 
 
 # name -> argtypes (restype int unless listed in _RESTYPE)

@@ -31,7 +31,7 @@ GAMMA_LL = 1.7595e11  # engine/torque.go:27
 class AdjointRK4:
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, K, probe, avg_from, w_probe=1.0, w_target=1.0,
                  target=(0.0, 0.0, 1.0), demag=True, demag_kernel="newell", demag_accuracy=6.0, gamma_ll=GAMMA_LL,
-                 device=0):
+                 use_graph=True, device=0):
         self.L = _lib.init(device)
         p = AdjParams()
         p.N[:] = [int(n) for n in N]
@@ -47,6 +47,7 @@ class AdjointRK4:
         p.avg_from = int(avg_from)
         p.w_probe, p.w_target = float(w_probe), float(w_target)
         p.target[:] = [float(t) for t in target]
+        p.no_graph = 0 if use_graph else 1
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
         h = ctypes.c_void_p()

@@ -7,18 +7,28 @@
 // uniaxial(K1, u)/Ms + B_ext, torque = LL torque with alpha, RK4 with fixed
 // dt and every stage normalised.  Parameters: a per-cell Ms map, uniform A,
 // K1 and B_ext (the differentiable ones) and uniform alpha and easy axis.
-// Loss: w_probe * mean over steps n >= n0 of the mean m_z over a probe window
-// + w_target * |<m>_final - target|^2.
+// Loss: w_probe * mean over states avg_from..nsteps of the mean m_z over a
+// probe window + w_target * |<m>_final - target|^2.
 //
-// Backward, per RK4 step in reverse (stage states recomputed from the last
-// checkpoint of the segment and kept): the normalisation's VJP
-// (w - n (n.w)) / |u|, the LL torque's VJP (cross products), and the
-// effective field's VJP: the demag convolution with a real, even kernel is
-// self-adjoint (the same plan applied to the cotangent), the exchange stencil
-// with its clamped boundary is symmetric, anisotropy and Zeeman are local.
+// Backward, per RK4 step in reverse (stage states recomputed from the
+// segment's checkpoint and kept): the normalisation's VJP (w - n (n.w))/|u|,
+// the LL torque's VJP (cross products), and the effective field's VJP: the
+// demag convolution with a real, even kernel is self-adjoint (the same plan
+// applied to the cotangent), the exchange stencil with its clamped boundary
+// is symmetric, anisotropy and Zeeman are local.
+//
+// Launch structure.  Forward, per stage: the three demag passes, then one
+// kernel that evaluates the field and torque of the stage state and, per
+// cell, forms the next stage state (or the step's result, with the probe
+// sum).  Reverse, per step: one kernel for the final combination's VJP and
+// the last stage's torque VJP, then per stage the demag of the field
+// cotangent and one kernel for the field VJP, the stage normalisation's VJP
+// and the torque VJP of the stage before.  Each segment (K steps forward, or
+// K steps recomputed and reversed) is replayed from a CUDA graph.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "cellmath.cuh"
@@ -37,154 +47,203 @@ struct AdjField {
     float u[3];        // easy axis as given (normalised per cell like uniaxialanisotropy2.cl)
     float bext[3];
     int anis;
+    int probe[4];      // x0, y0, width, height
 };
 
-// ---------------------------------------------------------------- forward
-// B_eff and the LL torque of m (engine/effectivefield.go:14-24 order);
-// bd = demag field or NULL
-__global__ void k_adj_field(AdjField a, const float* __restrict__ m, const float* __restrict__ bd, float* B,
-                            float* tau) {
-    const int N = a.N;
-    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x) {
-        const int ix = I % a.g.Nx, iy = (I / a.g.Nx) % a.g.Ny, iz = I / (a.g.Nx * a.g.Ny);
-        const float *mx = m, *my = m + N, *mz = m + 2 * N;
-        const f3 m0 = ld3(mx, my, mz, I);
-        f3 b{0.f, 0.f, 0.f};
-        if (bd) b = f3{bd[I], bd[N + I], bd[2 * N + I]};
-        if (!is0(m0)) {
-            const f3 e = exchange_sum_u(mx, my, mz, a.pc, a.g, ix, iy, iz, m0);
-            const float inv = inv_msat(a.Ms, 1.0f, I);
-            b.x = fa(b.x, fm(e.x, inv));
-            b.y = fa(b.y, fm(e.y, inv));
-            b.z = fa(b.z, fm(e.z, inv));
-        }
-        if (a.anis) {
-            const UniaxParams up{a.Ms, nullptr, nullptr, nullptr, nullptr, nullptr, 1.0f, a.K1, 0.0f, a.u[0], a.u[1], a.u[2]};
-            add_uniaxial(b, up, m0, I);
-        }
-        b.x = fa(b.x, a.bext[0]);
-        b.y = fa(b.y, a.bext[1]);
-        b.z = fa(b.z, a.bext[2]);
-        const f3 mxB = cross3(m0, b), mmxB = cross3(m0, mxB);
-        const f3 t{fm(a.gilb, fa(mxB.x, fm(a.alpha, mmxB.x))), fm(a.gilb, fa(mxB.y, fm(a.alpha, mmxB.y))),
-                   fm(a.gilb, fa(mxB.z, fm(a.alpha, mmxB.z)))};
-        if (B) { B[I] = b.x; B[N + I] = b.y; B[2 * N + I] = b.z; }
-        tau[I] = t.x; tau[N + I] = t.y; tau[2 * N + I] = t.z;
-    }
+// RK4 weights (engine/rk4.go:35-61): stage offsets 1/2, 1/2, 1 and the final
+// combination 1/6, 1/3, 1/3, 1/6, each float32(c) * h as Madd takes them
+struct Rk4Fac {
+    float st[3], fin[4];
+};
+
+__device__ __forceinline__ bool in_probe(const AdjField& a, int I) {
+    if (I >= a.g.Nx * a.g.Ny) return false;  // layer 0 only
+    const int x = I % a.g.Nx, y = I / a.g.Nx;
+    return x >= a.probe[0] && x < a.probe[0] + a.probe[2] && y >= a.probe[1] && y < a.probe[1] + a.probe[3];
 }
 
-// dst = normalize(m + sum_j f_j k_j) with the Madd<n> rounding order (the
-// engine's k_stage); nk = 1 or 4
-__global__ void k_adj_stage(int N, const float* __restrict__ m, const float* k0, const float* k1, const float* k2,
-                            const float* k3, int nk, float f0, float f1, float f2, float f3_, float* dst) {
-    const float* ks[4] = {k0, k1, k2, k3};
-    const float fs_[4] = {f0, f1, f2, f3_};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+// B_eff and the LL torque of cell I of state m (engine/effectivefield.go:14-24
+// order, the engine's per-cell arithmetic); bd = demag field or NULL
+__device__ __forceinline__ void adj_field_cell(const AdjField& a, const float* __restrict__ m,
+                                               const float* __restrict__ bd, int I, f3& b, f3& t) {
+    const int N = a.N;
+    const int ix = I % a.g.Nx, iy = (I / a.g.Nx) % a.g.Ny, iz = I / (a.g.Nx * a.g.Ny);
+    const float *mx = m, *my = m + N, *mz = m + 2 * N;
+    const f3 m0 = ld3(mx, my, mz, I);
+    b = f3{0.f, 0.f, 0.f};
+    if (bd) b = f3{bd[I], bd[N + I], bd[2 * N + I]};
+    if (!is0(m0)) {
+        const f3 e = exchange_sum_u(mx, my, mz, a.pc, a.g, ix, iy, iz, m0);
+        const float inv = inv_msat(a.Ms, 1.0f, I);
+        b.x = fa(b.x, fm(e.x, inv));
+        b.y = fa(b.y, fm(e.y, inv));
+        b.z = fa(b.z, fm(e.z, inv));
+    }
+    if (a.anis) {
+        const UniaxParams up{a.Ms, nullptr, nullptr, nullptr, nullptr, nullptr,
+                             1.0f, a.K1, 0.0f, a.u[0], a.u[1], a.u[2]};
+        add_uniaxial(b, up, m0, I);
+    }
+    b.x = fa(b.x, a.bext[0]);
+    b.y = fa(b.y, a.bext[1]);
+    b.z = fa(b.z, a.bext[2]);
+    const f3 mxB = cross3(m0, b), mmxB = cross3(m0, mxB);
+    t = f3{fm(a.gilb, fa(mxB.x, fm(a.alpha, mmxB.x))), fm(a.gilb, fa(mxB.y, fm(a.alpha, mmxB.y))),
+           fm(a.gilb, fa(mxB.z, fm(a.alpha, mmxB.z)))};
+}
+
+__device__ __forceinline__ void st3(float* p, int N, int I, f3 v) {
+    p[I] = v.x;
+    p[N + I] = v.y;
+    p[2 * N + I] = v.z;
+}
+__device__ __forceinline__ f3 ld3p(const float* p, int N, int I) { return f3{p[I], p[N + I], p[2 * N + I]}; }
+
+// ---------------------------------------------------------------- forward
+// Stage q of an RK4 step of state m: field and torque k_q of stage state mq
+// (B_q kept if Bq), then per cell the next stage state
+//   q < 3: mnext = normalize(m + st[q] k_q)
+//   q = 3: mnext = normalize(m + fin0 k0 + fin1 k1 + fin2 k2 + fin3 k3)
+// with the Madd<n> rounding order (the engine's k_stage), and for q = 3 the
+// probe's m_z sum of mnext added to *psum when psum != NULL.
+__global__ void __launch_bounds__(256) k_adj_stage_fwd(AdjField a, Rk4Fac f, int q, const float* __restrict__ mq,
+                                                       const float* __restrict__ bd, float* Bq, float* kq,
+                                                       const float* __restrict__ m, const float* k0,
+                                                       const float* k1, const float* k2, float* mnext,
+                                                       double* psum) {
+    const int N = a.N;
+    double acc = 0;
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x) {
+        f3 b, t;
+        adj_field_cell(a, mq, bd, I, b, t);
+        if (Bq) st3(Bq, N, I, b);
+        st3(kq, N, I, t);
+        const float tk[3] = {t.x, t.y, t.z};
         float v[3];
         for (int c = 0; c < 3; c++) {
-            float acc = fm(1.0f, m[c * N + i]);
-            for (int j = 0; j < nk; j++) acc = fa(acc, fm(fs_[j], ks[j][c * N + i]));
-            v[c] = acc;
+            const int o = c * N + I;
+            float s = fm(1.0f, m[o]);
+            if (q < 3) {
+                s = fa(s, fm(f.st[q], tk[c]));
+            } else {
+                s = fa(s, fm(f.fin[0], k0[o]));
+                s = fa(s, fm(f.fin[1], k1[o]));
+                s = fa(s, fm(f.fin[2], k2[o]));
+                s = fa(s, fm(f.fin[3], tk[c]));
+            }
+            v[c] = s;
         }
         const f3 r = normalize_vol(f3{v[0], v[1], v[2]}, 1.0f);
-        dst[i] = r.x; dst[N + i] = r.y; dst[2 * N + i] = r.z;
+        st3(mnext, N, I, r);
+        if (psum && in_probe(a, I)) acc += (double)r.z;
     }
-}
-
-// loss pieces of one state: sum over the probe window of m_z (FP64), and the
-// component sums of m (FP64) for the final average
-__global__ void k_adj_probe(int N, int Nx, int Ny, const float* __restrict__ m, int px, int py, int pw, int ph,
-                            double* out) {
-    __shared__ double sh[8];
-    double acc = 0;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < pw * ph; q += gridDim.x * blockDim.x) {
-        const int x = px + q % pw, y = py + q / pw;
-        acc += (double)m[2 * N + y * Nx + x];  // z component, layer 0
-    }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
-        atomicAdd(out, t);
+    if (psum) {
+        __shared__ double sh[8];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += sh[w];
+            if (s != 0) atomicAdd(psum, s);
+        }
     }
 }
 
 // ---------------------------------------------------------------- backward
-// VJP of dst = normalize(u), u = m + sum_j f_j k_j: g_u = (w - n (n.w)) / |u|;
-// lam += g_u; gk_j += f_j g_u
-__global__ void k_adj_norm_vjp(int N, const float* __restrict__ m, const float* k0, const float* k1, const float* k2,
-                               const float* k3, int nk, float f0, float f1, float f2, float f3_,
-                               const float* __restrict__ w, float* lam, float* g0, float* g1, float* g2, float* g3) {
-    const float* ks[4] = {k0, k1, k2, k3};
-    float* gs[4] = {g0, g1, g2, g3};
-    const float fs_[4] = {f0, f1, f2, f3_};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        float u[3];
-        for (int c = 0; c < 3; c++) {
-            float acc = fm(1.0f, m[c * N + i]);
-            for (int j = 0; j < nk; j++) acc = fa(acc, fm(fs_[j], ks[j][c * N + i]));
-            u[c] = acc;
-        }
-        const float len = sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-        const float il = len > 0.f ? 1.0f / len : 0.0f;
-        const float n[3] = {u[0] * il, u[1] * il, u[2] * il};
-        const float ww[3] = {w[i], w[N + i], w[2 * N + i]};
-        const float nw = n[0] * ww[0] + n[1] * ww[1] + n[2] * ww[2];
-        for (int c = 0; c < 3; c++) {
-            const float gu = (ww[c] - n[c] * nw) * il;
-            lam[c * N + i] += gu;
-            for (int j = 0; j < nk; j++) gs[j][c * N + i] += fs_[j] * gu;
-        }
-    }
+__device__ __forceinline__ f3 c3(f3 a, f3 b) {
+    return f3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float d3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 sc3(float s, f3 a) { return f3{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ f3 ad3(f3 a, f3 b) { return f3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+
+// VJP of n = u / |u|: (w - n (n.w)) / |u|
+__device__ __forceinline__ f3 norm_vjp(f3 u, f3 w) {
+    const float len = sqrtf(d3(u, u));
+    const float il = len > 0.f ? 1.0f / len : 0.0f;
+    const f3 n = sc3(il, u);
+    const float nw = d3(n, w);
+    return f3{(w.x - n.x * nw) * il, (w.y - n.y * nw) * il, (w.z - n.z * nw) * il};
 }
 
-// VJP of the LL torque t = g (m x B + alpha m x (m x B)), g = -1/(1+alpha^2):
-// gm = g [B x w + alpha ((m x B) x w + B x (w x m))],
+// VJP of the LL torque t = g (m x B + alpha m x (m x B)), g = -1/(1+alpha^2),
+// with cotangent w: gm = g [B x w + alpha ((m x B) x w + B x (w x m))],
 // wB = g [w x m + alpha (w x m) x m]
-__device__ __forceinline__ f3 c3(f3 a, f3 b) { return f3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
-__global__ void k_adj_torque_vjp(int N, float alpha, float gilb, const float* __restrict__ m,
-                                 const float* __restrict__ B, const float* __restrict__ w, float* gm, float* wB) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const f3 mm{m[i], m[N + i], m[2 * N + i]}, b{B[i], B[N + i], B[2 * N + i]}, ww{w[i], w[N + i], w[2 * N + i]};
-        const f3 mxB = c3(mm, b), wxm = c3(ww, mm);
-        const f3 t1 = c3(b, ww), t2 = c3(mxB, ww), t3 = c3(b, wxm), t4 = c3(wxm, mm);
-        gm[i] = gilb * (t1.x + alpha * (t2.x + t3.x));
-        gm[N + i] = gilb * (t1.y + alpha * (t2.y + t3.y));
-        gm[2 * N + i] = gilb * (t1.z + alpha * (t2.z + t3.z));
-        wB[i] = gilb * (wxm.x + alpha * t4.x);
-        wB[N + i] = gilb * (wxm.y + alpha * t4.y);
-        wB[2 * N + i] = gilb * (wxm.z + alpha * t4.z);
+__device__ __forceinline__ void torque_vjp(float alpha, float gilb, f3 m, f3 B, f3 w, f3& gm, f3& wB) {
+    const f3 mxB = c3(m, B), wxm = c3(w, m);
+    const f3 t1 = c3(B, w), t2 = c3(mxB, w), t3 = c3(B, wxm), t4 = c3(wxm, m);
+    gm = sc3(gilb, ad3(t1, sc3(alpha, ad3(t2, t3))));
+    wB = sc3(gilb, ad3(wxm, sc3(alpha, t4)));
+}
+
+// Start of the reverse of one step, per cell: u = m + sum_j fin_j k_j,
+// g_u = VJP(normalize)(u; lam); lam2 = g_u; gk_j = fin_j g_u (j < 3); and the
+// torque VJP of stage 3 with cotangent fin_3 g_u -> gm, wB.
+__global__ void __launch_bounds__(256) k_adj_rev_start(AdjField a, Rk4Fac f, const float* __restrict__ m,
+                                                       const float* __restrict__ k0, const float* __restrict__ k1,
+                                                       const float* __restrict__ k2, const float* __restrict__ k3,
+                                                       const float* __restrict__ m3, const float* __restrict__ B3,
+                                                       const float* __restrict__ lam, float* lam2, float* gk0,
+                                                       float* gk1, float* gk2, float* gm, float* wB) {
+    const int N = a.N;
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x) {
+        float u[3];
+        for (int c = 0; c < 3; c++) {  // the forward's rounding order
+            const int o = c * N + I;
+            float s = fm(1.0f, m[o]);
+            s = fa(s, fm(f.fin[0], k0[o]));
+            s = fa(s, fm(f.fin[1], k1[o]));
+            s = fa(s, fm(f.fin[2], k2[o]));
+            s = fa(s, fm(f.fin[3], k3[o]));
+            u[c] = s;
+        }
+        const f3 gu = norm_vjp(f3{u[0], u[1], u[2]}, ld3p(lam, N, I));
+        st3(lam2, N, I, gu);
+        st3(gk0, N, I, sc3(f.fin[0], gu));
+        st3(gk1, N, I, sc3(f.fin[1], gu));
+        st3(gk2, N, I, sc3(f.fin[2], gu));
+        f3 g, w;
+        torque_vjp(a.alpha, a.gilb, ld3p(m3, N, I), ld3p(B3, N, I), sc3(f.fin[3], gu), g, w);
+        st3(gm, N, I, g);
+        st3(wB, N, I, w);
     }
 }
 
-// VJP of B_eff(m; Ms, A, K1, B_ext) with cotangent wB at state m:
-//   gm += Ms D(wB) (demag D = mu0 K, self-adjoint) + S(wB / Ms) (exchange
-//   stencil S, symmetric) + 2 k1 (wB.u) u (anisotropy, k1 = K1/Ms);
-//   gMs += m.D(wB) - wB.e / Ms^2 - 2 K1 (m.u)(wB.u) / Ms^2 (e = S m);
-//   gA += wB.e / (Ms A); gK1 += 2 (m.u)(wB.u) / Ms; gB += wB.
-// dw = D(wB) (demag of the cotangent) or NULL; sums: gA, gK1, gB[3] (FP64)
-__global__ void k_adj_field_vjp(AdjField a, float A, const float* __restrict__ m, const float* __restrict__ wB,
-                                const float* __restrict__ dw, float* gm, double* gMs, double* sums) {
-    __shared__ double sh[5][8];
+// Stage q of the reverse, per cell.  In: gm = torque-VJP part of dL/dm_q,
+// wB = dL/dB_q (all cells: the exchange transpose reads neighbours), dw =
+// mu0 K wB (demag of the cotangent) or NULL.  Field VJP:
+//   dL/dm_q = gm + Ms dw + S(wB / Ms) + 2 (K1/Ms) (wB.u) u
+//   acc[Ms] += m.dw - wB.e/Ms^2 - 2 K1 (m.u)(wB.u)/Ms^2,  e = S m_q
+//   acc[A] += wB.e/(Ms A);  acc[K1] += 2 (m.u)(wB.u)/Ms;  acc[B] += wB
+// (S: the exchange stencil with the clamped boundary, symmetric).  Then
+//   q > 0: m_q = normalize(m + st[q-1] k_{q-1}): g_u = VJP; lam2 += g_u;
+//          dL/dk_{q-1} = gk_{q-1} + st[q-1] g_u, and the torque VJP of stage
+//          q-1 with it -> gm (in place), wBn
+//   q = 0: lam2 += dL/dm_0, plus the probe term wprobe (m_z in the window)
+// acc: per-cell FP64 accumulators [Ms | A | K1 | Bx | By | Bz] (N each).
+__global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, Rk4Fac f, int q, float A,
+                                                       const float* __restrict__ mq, const float* __restrict__ wB,
+                                                       const float* __restrict__ dw, float* gm,
+                                                       const float* __restrict__ m, const float* __restrict__ kprev,
+                                                       const float* __restrict__ gkprev,
+                                                       const float* __restrict__ mprev,
+                                                       const float* __restrict__ Bprev, float* lam2, float* wBn,
+                                                       float wprobe, double* acc) {
     const int N = a.N;
-    double acc[5] = {0, 0, 0, 0, 0};
     for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x) {
         const int ix = I % a.g.Nx, iy = (I / a.g.Nx) % a.g.Ny, iz = I / (a.g.Nx * a.g.Ny);
         const float ms = a.Ms[I];
         const float inv = ms == 0.f ? 0.f : 1.0f / ms;
-        const f3 w{wB[I], wB[N + I], wB[2 * N + I]};
-        const f3 m0{m[I], m[N + I], m[2 * N + I]};
-        f3 g{0.f, 0.f, 0.f};
+        const f3 w = ld3p(wB, N, I);
+        const f3 m0 = ld3p(mq, N, I);
+        f3 g = ld3p(gm, N, I);
         double gms = 0;
-        if (dw) {  // dw = mu0 K wB (the demag plan applied to wB with Ms = 1)
-            const f3 d{dw[I], dw[N + I], dw[2 * N + I]};
-            g = f3{ms * d.x, ms * d.y, ms * d.z};
+        if (dw) {
+            const f3 d = ld3p(dw, N, I);
+            g = ad3(g, sc3(ms, d));
             gms += (double)m0.x * d.x + (double)m0.y * d.y + (double)m0.z * d.z;
         }
-        // exchange: the stencil applied to x = wB / Ms (transpose of the forward
-        // stencil, which is symmetric with the clamped boundary), and e = S m
         {
             int nb[6];
             nb[0] = (iz * a.g.Ny + iy) * a.g.Nx + lclamp(ix - 1, a.g.Nx, false);
@@ -195,96 +254,112 @@ __global__ void k_adj_field_vjp(AdjField a, float A, const float* __restrict__ m
             nb[5] = (hclamp(iz + 1, a.g.Nz, false) * a.g.Ny + iy) * a.g.Nx + ix;
             const int nn = a.g.Nz != 1 ? 6 : 4;
             f3 sx{0.f, 0.f, 0.f}, e{0.f, 0.f, 0.f};
-            const f3 x0{w.x * inv, w.y * inv, w.z * inv};
+            const f3 x0 = sc3(inv, w);
             for (int k = 0; k < nn; k++) {
                 const float s = k < 2 ? a.pc.wax : (k < 4 ? a.pc.way : a.pc.waz);
                 const int j = nb[k];
-                const float ij = a.Ms[j] == 0.f ? 0.f : 1.0f / a.Ms[j];
-                sx.x += s * (wB[j] * ij - x0.x);
-                sx.y += s * (wB[N + j] * ij - x0.y);
-                sx.z += s * (wB[2 * N + j] * ij - x0.z);
-                e.x += s * (m[j] - m0.x);
-                e.y += s * (m[N + j] - m0.y);
-                e.z += s * (m[2 * N + j] - m0.z);
+                const float msj = a.Ms[j];
+                const float ij = msj == 0.f ? 0.f : 1.0f / msj;
+                sx = ad3(sx, sc3(s, f3{wB[j] * ij - x0.x, wB[N + j] * ij - x0.y, wB[2 * N + j] * ij - x0.z}));
+                e = ad3(e, sc3(s, f3{mq[j] - m0.x, mq[N + j] - m0.y, mq[2 * N + j] - m0.z}));
             }
-            g.x += sx.x; g.y += sx.y; g.z += sx.z;
-            const double we = (double)(w.x * e.x + w.y * e.y + w.z * e.z);
+            g = ad3(g, sx);
+            const double we = (double)w.x * e.x + (double)w.y * e.y + (double)w.z * e.z;
             gms -= we * (double)inv * (double)inv;
-            acc[0] += we * (double)inv / (double)A;
+            acc[(size_t)N + I] += we * (double)inv / (double)A;
         }
         if (a.anis) {
             f3 u{a.u[0], a.u[1], a.u[2]};
-            const float len = sqrtf(u.x * u.x + u.y * u.y + u.z * u.z);
-            const float il = len > 0.f ? 1.0f / len : 0.f;
-            u = f3{u.x * il, u.y * il, u.z * il};
-            const float mu = m0.x * u.x + m0.y * u.y + m0.z * u.z;
-            const float wu = w.x * u.x + w.y * u.y + w.z * u.z;
-            const float k1 = a.K1 * inv;
-            g.x += 2.f * k1 * wu * u.x;
-            g.y += 2.f * k1 * wu * u.y;
-            g.z += 2.f * k1 * wu * u.z;
+            const float len = sqrtf(d3(u, u));
+            u = sc3(len > 0.f ? 1.0f / len : 0.f, u);
+            const float mu = d3(m0, u), wu = d3(w, u);
+            g = ad3(g, sc3(2.f * a.K1 * inv * wu, u));
             gms -= 2.0 * (double)a.K1 * (double)mu * (double)wu * (double)inv * (double)inv;
-            acc[1] += 2.0 * (double)mu * (double)wu * (double)inv;
+            acc[2 * (size_t)N + I] += 2.0 * (double)mu * (double)wu * (double)inv;
         }
-        acc[2] += w.x;
-        acc[3] += w.y;
-        acc[4] += w.z;
-        gm[I] += g.x; gm[N + I] += g.y; gm[2 * N + I] += g.z;
-        gMs[I] += gms;
+        acc[I] += gms;
+        acc[3 * (size_t)N + I] += w.x;
+        acc[4 * (size_t)N + I] += w.y;
+        acc[5 * (size_t)N + I] += w.z;
+        f3 l = ld3p(lam2, N, I);
+        if (q > 0) {
+            const float c = f.st[q - 1];
+            const f3 M = ld3p(m, N, I), Kp = ld3p(kprev, N, I);
+            const f3 u{fa(fm(1.0f, M.x), fm(c, Kp.x)), fa(fm(1.0f, M.y), fm(c, Kp.y)), fa(fm(1.0f, M.z), fm(c, Kp.z))};
+            const f3 gu = norm_vjp(u, g);
+            l = ad3(l, gu);
+            const f3 gk = ad3(ld3p(gkprev, N, I), sc3(c, gu));
+            f3 gn, wn;
+            torque_vjp(a.alpha, a.gilb, ld3p(mprev, N, I), ld3p(Bprev, N, I), gk, gn, wn);
+            st3(gm, N, I, gn);
+            st3(wBn, N, I, wn);
+        } else {
+            l = ad3(l, g);
+            if (wprobe != 0.f && in_probe(a, I)) l.z += wprobe;
+        }
+        st3(lam2, N, I, l);
+    }
+}
+
+// loss cotangent of the final state: the probe term (weight wprobe per
+// window cell) and the final-average term (gx, gy, gz)
+__global__ void k_adj_loss_final(AdjField a, float* lam, float wprobe, float gx, float gy, float gz) {
+    const int N = a.N;
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x) {
+        f3 l{gx, gy, gz};
+        if (wprobe != 0.f && in_probe(a, I)) l.z += wprobe;
+        st3(lam, N, I, l);
+    }
+}
+
+// dL/dm0 through the initial normalisation
+__global__ void k_adj_m0(int N, const float* __restrict__ m0, const float* __restrict__ lam, float* gm0) {
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x)
+        st3(gm0, N, I, norm_vjp(ld3p(m0, N, I), ld3p(lam, N, I)));
+}
+
+// per-cell accumulators -> gMs (float) and the five scalar sums, in a fixed
+// order (one block of 1024 threads; deterministic)
+__global__ void __launch_bounds__(1024) k_adj_reduce(int N, const double* __restrict__ acc, float* gMs, double* out) {
+    __shared__ double sh[5][32];
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int I = threadIdx.x; I < N; I += blockDim.x) {
+        gMs[I] = (float)acc[I];
+        for (int t = 0; t < 5; t++) s[t] += acc[(size_t)(t + 1) * N + I];
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int t = 0; t < 5; t++) {
-        double v = acc[t];
+        double v = s[t];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) sh[t][wid] = v;
     }
     __syncthreads();
     if (threadIdx.x < 5) {
         double v = 0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); q++) v += sh[threadIdx.x][q];
-        atomicAdd(sums + threadIdx.x, v);
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sh[threadIdx.x][w];
+        out[threadIdx.x] = v;
     }
-}
-
-// loss cotangents of one state: the probe term (m_z over the window in layer
-// 0, weight wprobe per cell) and the final-average term gavg (NULL: none)
-__global__ void k_adj_loss_grad(int N, int Nx, int Ny, float* lam, int px, int py, int pw, int ph, float wprobe,
-                                const float* gavg) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        if (gavg)
-            for (int c = 0; c < 3; c++) lam[c * N + i] += gavg[c];
-        if (wprobe != 0.f && i < Nx * Ny) {
-            const int x = i % Nx, y = i / Nx;
-            if (x >= px && x < px + pw && y >= py && y < py + ph) lam[2 * N + i] += wprobe;
-        }
-    }
-}
-
-__global__ void k_adj_axpy(size_t n, const float* __restrict__ x, float* y) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        y[i] += x[i];
-}
-
-__global__ void k_adj_to_f32(int n, const double* __restrict__ x, float* y) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = (float)x[i];
 }
 
 // ---------------------------------------------------------------- host
 // work buffers (3N floats each)
 enum : int {
-    W_K = 0,      // 0..3: k1..k4 (forward) / their cotangents (backward)
-    W_MS = 4,     // 4..6: stage states m2..m4 (forward)
-    W_GM = 4,     // backward: cotangent of a stage state
-    W_WB = 5,     // backward: cotangent of the stage's field
-    W_DW = 6,     // backward: demag of that cotangent
-    W_BD = 7,     // demag field
+    W_K = 0,     // 0..3: k1..k4 (forward) / 0..2: their cotangents (reverse)
+    W_MS = 4,    // 4..6: stage states m2..m4 (forward)
+    W_GM = 4,    // reverse: torque-VJP part of a stage state's cotangent
+    W_WB = 5,    // reverse: 5, 6: field cotangents (ping-pong)
+    W_BD = 7,    // demag field / demag of the field cotangent
     W_A = 8, W_B = 9,
     W_FINAL = 10,
     W_LAM = 11, W_LAM2 = 12,
-    W_GAVG = 13,
-    W_NEXT = 14,
-    W_M0 = 15,    // m0 as given (before the initial normalisation)
-    W_COUNT = 16
+    W_NEXT = 13,
+    W_M0 = 14,   // m0 as given (before the initial normalisation)
+    W_COUNT = 15
+};
+
+struct AdjGraph {
+    std::string key;
+    cudaGraphExec_t exec;
 };
 
 struct AdjImpl {
@@ -296,14 +371,16 @@ struct AdjImpl {
     float* Ms = nullptr;  // per-cell Ms of the last forward
     float A = 0, A00 = 0, K1 = 0, B[3] = {0, 0, 0};
     std::vector<float*> ckpt;  // m at steps 0, K, 2K, ...
-    float* seg = nullptr;      // one segment: K steps x 12 x 3N (start state, m2..m4, B1..B4, k1..k4)
+    float* seg = nullptr;      // one segment: K steps x 12 x 3N (m2..m4, B1..B4, k1..k4, start state)
     float* work = nullptr;     // W_COUNT x 3N
-    double* gMs = nullptr;     // per-cell gradient (FP64)
-    double* dsum = nullptr;    // 8 doubles: probe sum / gA, gK1, gB
+    double* acc = nullptr;     // per-cell FP64 gradient accumulators, 6 x N
+    double* dsum = nullptr;    // 8 doubles: probe sum / scalar gradients
     bool have_forward = false;
     double avg[3] = {0, 0, 0};
+    std::vector<AdjGraph> graphs;  // segment graphs by key (parameters are baked in)
     size_t n3() const { return 3 * (size_t)N; }
     float* w(int k) const { return work + (size_t)k * n3(); }
+    float* slot(int j, int q) const { return seg + ((size_t)j * 12 + q) * n3(); }
 };
 
 static cudaStream_t AS() { return ctx().stream; }
@@ -326,38 +403,10 @@ static AdjField adj_field(const AdjImpl* s) {
     a.gilb = -1.0f / den;  // lltorque2.cl:18
     for (int c = 0; c < 3; c++) { a.u[c] = s->p.anisU[c]; a.bext[c] = s->B[c]; }
     a.anis = s->K1 != 0.f;
+    for (int c = 0; c < 4; c++) a.probe[c] = s->p.probe[c];
     return a;
 }
 
-static unsigned gridN(const AdjImpl* s) { return (unsigned)grid_for(s->N, 256); }
-
-// demag of v (3N) into out: Ms map (forward) or Ms = 1 (cotangent)
-static int adj_demag(AdjImpl* s, const float* v, const float* Ms, float* out) {
-    PassArgs a{};
-    fill_pass_args(s->demag, a);
-    for (int c = 0; c < 3; c++) { a.m[c] = v + (size_t)c * s->N; a.B[c] = out + (size_t)c * s->N; }
-    a.Ms = Ms;
-    a.Ms_mul = 1.0f;
-    return demag_launch(s->demag, a, AS());
-}
-
-// torque (and field if B) of m
-static int adj_torque(AdjImpl* s, const float* m, float* B, float* tau) {
-    const float* bd = nullptr;
-    if (s->demag) {
-        UMAG_TRY(adj_demag(s, m, s->Ms, s->w(W_BD)));
-        bd = s->w(W_BD);
-    }
-    k_adj_field<<<gridN(s), 256, 0, AS()>>>(adj_field(s), m, bd, B, tau);
-    UMAG_LAUNCH_CHECK();
-    return UMAG_OK;
-}
-
-// RK4 weights (engine/rk4.go:35-61): stage offsets 1/2, 1/2, 1 and the final
-// combination 1/6, 1/3, 1/3, 1/6, each float32(c) * h as Madd takes them
-struct Rk4Fac {
-    float st[3], fin[4];
-};
 static Rk4Fac rk4_fac(float h) {
     Rk4Fac f;
     f.st[0] = (float)(1. / 2.) * h;
@@ -370,39 +419,96 @@ static Rk4Fac rk4_fac(float h) {
     return f;
 }
 
-// one RK4 step m -> mout with fixed h; st (or NULL) receives m2..m4 (st[0..2]),
-// B1..B4 (st[3..6]) and k1..k4 (st[7..10])
-static int adj_step(AdjImpl* s, const float* m, float* mout, float* const* st) {
+static unsigned gridN(const AdjImpl* s) { return (unsigned)grid_for(s->N, 256); }
+
+// demag of v (3N) into out: Ms map (forward) or Ms = 1 (cotangent)
+static int adj_demag(AdjImpl* s, const float* v, const float* Ms, float* out) {
+    if (!s->demag) return UMAG_OK;
+    PassArgs a{};
+    fill_pass_args(s->demag, a);
+    for (int c = 0; c < 3; c++) { a.m[c] = v + (size_t)c * s->N; a.B[c] = out + (size_t)c * s->N; }
+    a.Ms = Ms;
+    a.Ms_mul = 1.0f;
+    return demag_launch(s->demag, a, AS());
+}
+
+// one RK4 step m -> mout (engine/rk4.go:35-61 with fixed dt).  st (or NULL)
+// receives m2..m4 (st[0..2]), B1..B4 (st[3..6]) and k1..k4 (st[7..10]);
+// psum (or NULL) accumulates the probe's m_z sum of mout.
+static int adj_step(AdjImpl* s, const AdjField& af, const Rk4Fac& f, const float* m, float* mout, float* const* st,
+                    double* psum) {
     float* k[4];
-    float* ms[3];
     float* Bs[4];
+    float* next[4];
+    const float* ms[4];
     for (int q = 0; q < 4; q++) {
         k[q] = st ? st[7 + q] : s->w(W_K + q);
         Bs[q] = st ? st[3 + q] : nullptr;
+        next[q] = q < 3 ? (st ? st[q] : s->w(W_MS + q)) : mout;
+        ms[q] = q == 0 ? m : next[q - 1];
     }
-    for (int q = 0; q < 3; q++) ms[q] = st ? st[q] : s->w(W_MS + q);
-    const Rk4Fac f = rk4_fac(s->h);
-    const unsigned G = gridN(s);
-    UMAG_TRY(adj_torque(s, m, Bs[0], k[0]));
-    for (int q = 0; q < 3; q++) {
-        k_adj_stage<<<G, 256, 0, AS()>>>(s->N, m, k[q], nullptr, nullptr, nullptr, 1, f.st[q], 0, 0, 0, ms[q]);
-        UMAG_TRY(adj_torque(s, ms[q], Bs[q + 1], k[q + 1]));
+    const float* bd = s->demag ? s->w(W_BD) : nullptr;
+    for (int q = 0; q < 4; q++) {
+        UMAG_TRY(adj_demag(s, ms[q], s->Ms, s->w(W_BD)));
+        k_adj_stage_fwd<<<gridN(s), 256, 0, AS()>>>(af, f, q, ms[q], bd, Bs[q], k[q], m, k[0], k[1], k[2], next[q],
+                                                     q == 3 ? psum : nullptr);
+        UMAG_LAUNCH_CHECK();
     }
-    k_adj_stage<<<G, 256, 0, AS()>>>(s->N, m, k[0], k[1], k[2], k[3], 4, f.fin[0], f.fin[1], f.fin[2], f.fin[3], mout);
-    UMAG_LAUNCH_CHECK();
     return UMAG_OK;
+}
+
+// run `body` directly, or from the graph cached under `key` (captured on
+// first use); the graph bakes in every pointer and parameter, so the key
+// holds everything that varies between calls
+template <class F>
+static int adj_run(AdjImpl* s, const std::string& key, F body) {
+    if (s->p.no_graph) return body();
+    for (const AdjGraph& g : s->graphs)
+        if (g.key == key) {
+            UMAG_CUDA(cudaGraphLaunch(g.exec, AS()));
+            return UMAG_OK;
+        }
+    cudaGraph_t graph;
+    UMAG_CUDA(cudaStreamBeginCapture(AS(), cudaStreamCaptureModeThreadLocal));
+    const int st = body();
+    const cudaError_t e = cudaStreamEndCapture(AS(), &graph);
+    if (st != UMAG_OK) {
+        if (e == cudaSuccess) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (e != cudaSuccess) return set_error(UMAG_E_CUDA, "adjoint graph capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec;
+    const cudaError_t e2 = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) return set_error(UMAG_E_CUDA, "adjoint graph instantiate: %s", cudaGetErrorString(e2));
+    s->graphs.push_back(AdjGraph{key, exec});
+    UMAG_CUDA(cudaGraphLaunch(exec, AS()));
+    return UMAG_OK;
+}
+
+static void adj_drop_graphs(AdjImpl* s) {
+    for (AdjGraph& g : s->graphs) cudaGraphExecDestroy(g.exec);
+    s->graphs.clear();
+}
+
+// the values baked into a graph besides pointers: exchange, anisotropy, field
+static std::string param_key(const AdjImpl* s) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "/%a/%a/%a/%a/%a/%a", s->A, s->A00, s->K1, s->B[0], s->B[1], s->B[2]);
+    return buf;
 }
 
 int adj_free(umag_adj* h) {
     AdjImpl* s = reinterpret_cast<AdjImpl*>(h);
     if (!s) return UMAG_OK;
     cudaStreamSynchronize(AS());
+    adj_drop_graphs(s);
     if (s->demag) demag_free(s->demag);
     cudaFree(s->Ms);
     for (float* c : s->ckpt) cudaFree(c);
     cudaFree(s->seg);
     cudaFree(s->work);
-    cudaFree(s->gMs);
+    cudaFree(s->acc);
     cudaFree(s->dsum);
     delete s;
     return UMAG_OK;
@@ -422,19 +528,20 @@ int adj_new(const umag_adj_params* p, umag_adj** out) {
     s->p = *p;
     s->N = p->N[0] * p->N[1] * p->N[2];
     s->g = Mesh3{p->N[0], p->N[1], p->N[2], 0};
-    s->h = (float)(p->dt * (p->gamma_ll > 0 ? p->gamma_ll : 1.7595e11));  // engine/run.go:33 GammaLL
+    s->h = (float)(p->dt * (p->gamma_ll > 0 ? p->gamma_ll : 1.7595e11));  // engine/torque.go:27 GammaLL
     auto fail = [&](int c) {
         adj_free(reinterpret_cast<umag_adj*>(s));
         return c;
     };
     const size_t n3 = s->n3();
+    const int K = std::min(p->K, p->nsteps);
     if (cudaMalloc(&s->Ms, sizeof(float) * s->N) != cudaSuccess ||
-        cudaMalloc(&s->seg, sizeof(float) * n3 * 12 * (size_t)p->K) != cudaSuccess ||
+        cudaMalloc(&s->seg, sizeof(float) * n3 * 12 * (size_t)K) != cudaSuccess ||
         cudaMalloc(&s->work, sizeof(float) * n3 * W_COUNT) != cudaSuccess ||
-        cudaMalloc(&s->gMs, sizeof(double) * s->N) != cudaSuccess ||
+        cudaMalloc(&s->acc, sizeof(double) * 6 * (size_t)s->N) != cudaSuccess ||
         cudaMalloc(&s->dsum, sizeof(double) * 8) != cudaSuccess)
         return fail(set_error(UMAG_E_NOMEM, "adjoint buffers"));
-    const int nck = (p->nsteps + p->K - 1) / p->K;  // states 0, K, ..: segment starts
+    const int nck = (p->nsteps + p->K - 1) / p->K;  // segment starts: states 0, K, 2K, ...
     for (int i = 0; i < nck; i++) {
         float* c = nullptr;
         if (cudaMalloc(&c, sizeof(float) * n3) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "checkpoints"));
@@ -465,26 +572,39 @@ int adj_forward(umag_adj* hd, const float* m0, const float* Ms, float A, float K
     s->A00 = 2.0f / (1.0f / A + 1.0f / A);  // engine/exchange.go:153-167, region 0 with itself
     s->K1 = K1;
     for (int c = 0; c < 3; c++) s->B[c] = Bext[c];
-    float* a = s->w(W_A);
-    float* b = s->w(W_B);
+    const AdjField af = adj_field(s);
+    const Rk4Fac f = rk4_fac(s->h);
     UMAG_CUDA(cudaMemcpyAsync(s->w(W_M0), m0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
-    UMAG_CUDA(cudaMemcpyAsync(a, m0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
-    UMAG_TRY(normalize(a, a + s->N, a + 2 * (size_t)s->N, nullptr, s->N));  // engine/magnetization.go:34
+    float* a0 = s->w(W_A);
+    UMAG_CUDA(cudaMemcpyAsync(a0, m0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
+    UMAG_TRY(normalize(a0, a0 + s->N, a0 + 2 * (size_t)s->N, nullptr, s->N));  // engine/magnetization.go:34
     UMAG_CUDA(cudaMemsetAsync(s->dsum, 0, sizeof(double) * 8, AS()));
-    for (int n = 1; n <= p.nsteps; n++) {
-        if ((n - 1) % p.K == 0)
-            UMAG_CUDA(cudaMemcpyAsync(s->ckpt[(n - 1) / p.K], a, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
-        UMAG_TRY(adj_step(s, a, b, nullptr));
-        std::swap(a, b);
-        if (n >= p.avg_from && p.w_probe != 0)
-            k_adj_probe<<<8, 256, 0, AS()>>>(s->N, p.N[0], p.N[1], a, p.probe[0], p.probe[1], p.probe[2],
-                                              p.probe[3], s->dsum);
+    const int nseg = (p.nsteps + p.K - 1) / p.K;
+    const std::string pk = param_key(s);
+    for (int sg = 0; sg < nseg; sg++) {
+        const int n_begin = sg * p.K, len = std::min(p.nsteps, n_begin + p.K) - n_begin;
+        UMAG_CUDA(cudaMemcpyAsync(s->ckpt[sg], a0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
+        // segment: len steps from W_A back into W_A, probe sums after steps n >= avg_from
+        std::string key = "F" + std::to_string(len) + "/";
+        for (int j = 0; j < len; j++) key += (n_begin + j + 1 >= p.avg_from && p.w_probe != 0) ? '1' : '0';
+        key += pk;
+        UMAG_TRY(adj_run(s, key, [&]() -> int {
+            float* a = s->w(W_A);
+            float* b = s->w(W_B);
+            for (int j = 0; j < len; j++) {
+                const int n = n_begin + j + 1;
+                UMAG_TRY(adj_step(s, af, f, a, b, nullptr, (n >= p.avg_from && p.w_probe != 0) ? s->dsum : nullptr));
+                std::swap(a, b);
+            }
+            if (a != s->w(W_A))
+                UMAG_CUDA(cudaMemcpyAsync(s->w(W_A), a, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
+            return UMAG_OK;
+        }));
     }
-    UMAG_LAUNCH_CHECK();
-    UMAG_CUDA(cudaMemcpyAsync(s->w(W_FINAL), a, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
+    UMAG_CUDA(cudaMemcpyAsync(s->w(W_FINAL), a0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
     double avg[3];
     for (int c = 0; c < 3; c++) {
-        UMAG_TRY(sum_dot(a + (size_t)c * s->N, nullptr, s->N, &avg[c]));  // compensated FP64 sum
+        UMAG_TRY(sum_dot(a0 + (size_t)c * s->N, nullptr, s->N, &avg[c]));  // compensated FP64 sum
         avg[c] /= s->N;
     }
     double probe_sum = 0;
@@ -511,6 +631,52 @@ int adj_final_m(umag_adj* hd, float* m) {
     return UMAG_OK;
 }
 
+// the reverse of one segment: recompute its steps from slot(0, 11) keeping
+// every stage, then the steps in reverse with lam = dL/d(state at the
+// segment's end) in W_LAM, leaving dL/d(state at its start) in W_LAM
+static int adj_rev_segment(AdjImpl* s, const AdjField& af, const Rk4Fac& f, int n_begin, int len, float wprobe) {
+    const umag_adj_params& p = s->p;
+    const unsigned G = gridN(s);
+    const size_t n3 = s->n3();
+    for (int j = 0; j < len; j++) {
+        float* st[11];
+        for (int q = 0; q < 11; q++) st[q] = s->slot(j, q);
+        UMAG_TRY(adj_step(s, af, f, s->slot(j, 11), j + 1 < len ? s->slot(j + 1, 11) : s->w(W_NEXT), st, nullptr));
+    }
+    float* lam = s->w(W_LAM);
+    float* lam2 = s->w(W_LAM2);
+    float* gk[3] = {s->w(W_K), s->w(W_K + 1), s->w(W_K + 2)};
+    float* gm = s->w(W_GM);
+    float* wb[2] = {s->w(W_WB), s->w(W_WB + 1)};
+    const float* dw = s->demag ? s->w(W_BD) : nullptr;
+    for (int j = len - 1; j >= 0; j--) {
+        const int n = n_begin + j + 1;  // the step from state n-1 to state n
+        const float* m = s->slot(j, 11);
+        const float* ms[4] = {m, s->slot(j, 0), s->slot(j, 1), s->slot(j, 2)};
+        const float* Bs[4] = {s->slot(j, 3), s->slot(j, 4), s->slot(j, 5), s->slot(j, 6)};
+        const float* ks[4] = {s->slot(j, 7), s->slot(j, 8), s->slot(j, 9), s->slot(j, 10)};
+        // stage q's field cotangent lives in wb[q & 1]
+        k_adj_rev_start<<<G, 256, 0, AS()>>>(af, f, m, ks[0], ks[1], ks[2], ks[3], ms[3], Bs[3], lam, lam2, gk[0],
+                                              gk[1], gk[2], gm, wb[1]);
+        UMAG_LAUNCH_CHECK();
+        for (int q = 3; q >= 0; q--) {
+            float* wcur = wb[q & 1];
+            float* wnext = wb[(q + 1) & 1];
+            UMAG_TRY(adj_demag(s, wcur, nullptr, s->w(W_BD)));
+            const bool probe_prev = q == 0 && n - 1 >= p.avg_from && p.w_probe != 0;
+            k_adj_rev_stage<<<G, 256, 0, AS()>>>(af, f, q, s->A, ms[q], wcur, dw, gm, m, q > 0 ? ks[q - 1] : nullptr,
+                                                  q > 0 ? gk[q - 1] : nullptr, q > 0 ? ms[q - 1] : nullptr,
+                                                  q > 0 ? Bs[q - 1] : nullptr, lam2, wnext,
+                                                  probe_prev ? wprobe : 0.f, s->acc);
+            UMAG_LAUNCH_CHECK();
+        }
+        std::swap(lam, lam2);
+    }
+    if (lam != s->w(W_LAM))
+        UMAG_CUDA(cudaMemcpyAsync(s->w(W_LAM), lam, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
+    return UMAG_OK;
+}
+
 int adj_backward(umag_adj* hd, float* gMs, float* gm0, double* gA, double* gK1, double gB[3]) {
     AdjImpl* s = reinterpret_cast<AdjImpl*>(hd);
     UMAG_REQUIRE(s && gMs && gA && gK1 && gB, "NULL argument");
@@ -521,72 +687,29 @@ int adj_backward(umag_adj* hd, float* gMs, float* gm0, double* gA, double* gK1, 
     const unsigned G = gridN(s);
     const Rk4Fac f = rk4_fac(s->h);
     const AdjField af = adj_field(s);
-    UMAG_CUDA(cudaMemsetAsync(s->gMs, 0, sizeof(double) * N, AS()));
-    UMAG_CUDA(cudaMemsetAsync(s->dsum, 0, sizeof(double) * 8, AS()));
-    float* lam = s->w(W_LAM);    // dL/d(state n)
-    float* lam2 = s->w(W_LAM2);  // dL/d(state n-1), being accumulated
-    float* gk = s->w(W_K);
-    float* gm = s->w(W_GM);
-    float* wB = s->w(W_WB);
-    float* dw = s->w(W_DW);
+    UMAG_CUDA(cudaMemsetAsync(s->acc, 0, sizeof(double) * 6 * (size_t)N, AS()));
     const float wprobe = (float)(p.w_probe / ((double)(p.nsteps - p.avg_from + 1) * p.probe[2] * p.probe[3]));
     float gavg[3];
     for (int c = 0; c < 3; c++) gavg[c] = (float)(2.0 * p.w_target * (s->avg[c] - p.target[c]) / N);
-    UMAG_CUDA(cudaMemcpyAsync(s->w(W_GAVG), gavg, sizeof(gavg), cudaMemcpyHostToDevice, AS()));
-    UMAG_CUDA(cudaMemsetAsync(lam, 0, sizeof(float) * n3, AS()));
-    k_adj_loss_grad<<<G, 256, 0, AS()>>>(N, p.N[0], p.N[1], lam, p.probe[0], p.probe[1], p.probe[2], p.probe[3],
-                                          wprobe, s->w(W_GAVG));
+    k_adj_loss_final<<<G, 256, 0, AS()>>>(af, s->w(W_LAM), p.w_probe != 0 ? wprobe : 0.f, gavg[0], gavg[1], gavg[2]);
     UMAG_LAUNCH_CHECK();
     const int nseg = (p.nsteps + p.K - 1) / p.K;
+    const std::string pk = param_key(s);
     for (int sg = nseg - 1; sg >= 0; sg--) {
         const int n_begin = sg * p.K, len = std::min(p.nsteps, n_begin + p.K) - n_begin;
-        // recompute the segment from its checkpoint, keeping every stage
-        auto slot = [&](int j, int q) { return s->seg + ((size_t)j * 12 + q) * n3; };
-        UMAG_CUDA(cudaMemcpyAsync(slot(0, 11), s->ckpt[sg], sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
-        for (int j = 0; j < len; j++) {
-            float* st[11];
-            for (int q = 0; q < 11; q++) st[q] = slot(j, q);
-            UMAG_TRY(adj_step(s, slot(j, 11), j + 1 < len ? slot(j + 1, 11) : s->w(W_NEXT), st));
-        }
-        // reverse through the segment's steps
-        for (int j = len - 1; j >= 0; j--) {
-            const int n = n_begin + j + 1;  // the step from state n-1 to state n
-            const float* m = slot(j, 11);
-            const float* ms[4] = {m, slot(j, 0), slot(j, 1), slot(j, 2)};
-            const float* Bs[4] = {slot(j, 3), slot(j, 4), slot(j, 5), slot(j, 6)};
-            const float* ks[4] = {slot(j, 7), slot(j, 8), slot(j, 9), slot(j, 10)};
-            UMAG_CUDA(cudaMemsetAsync(gk, 0, sizeof(float) * 4 * n3, AS()));
-            UMAG_CUDA(cudaMemsetAsync(lam2, 0, sizeof(float) * n3, AS()));
-            k_adj_norm_vjp<<<G, 256, 0, AS()>>>(N, m, ks[0], ks[1], ks[2], ks[3], 4, f.fin[0], f.fin[1], f.fin[2],
-                                                 f.fin[3], lam, lam2, gk, gk + n3, gk + 2 * n3, gk + 3 * n3);
-            for (int q = 3; q >= 0; q--) {
-                k_adj_torque_vjp<<<G, 256, 0, AS()>>>(N, af.alpha, af.gilb, ms[q], Bs[q], gk + q * n3, gm, wB);
-                if (s->demag) UMAG_TRY(adj_demag(s, wB, nullptr, dw));
-                k_adj_field_vjp<<<G, 256, 0, AS()>>>(af, s->A, ms[q], wB, s->demag ? dw : nullptr, gm, s->gMs,
-                                                      s->dsum);
-                if (q > 0)  // m_q = normalize(m + c h k_{q-1})
-                    k_adj_norm_vjp<<<G, 256, 0, AS()>>>(N, m, ks[q - 1], nullptr, nullptr, nullptr, 1, f.st[q - 1],
-                                                         0, 0, 0, gm, lam2, gk + (q - 1) * n3, nullptr, nullptr,
-                                                         nullptr);
-                else
-                    k_adj_axpy<<<G, 256, 0, AS()>>>(n3, gm, lam2);
-            }
-            UMAG_LAUNCH_CHECK();
-            std::swap(lam, lam2);
-            if (n - 1 >= p.avg_from && p.w_probe != 0)  // the probe term of state n-1
-                k_adj_loss_grad<<<G, 256, 0, AS()>>>(N, p.N[0], p.N[1], lam, p.probe[0], p.probe[1], p.probe[2],
-                                                      p.probe[3], wprobe, nullptr);
-        }
+        UMAG_CUDA(cudaMemcpyAsync(s->slot(0, 11), s->ckpt[sg], sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
+        std::string key = "R" + std::to_string(len) + "/";
+        for (int j = 0; j < len; j++) key += (n_begin + j >= p.avg_from && p.w_probe != 0) ? '1' : '0';
+        key += pk;
+        UMAG_TRY(adj_run(s, key, [&]() { return adj_rev_segment(s, af, f, n_begin, len, wprobe); }));
     }
-    // lam = dL/d(normalised m0); through the initial normalisation
     if (gm0) {
-        UMAG_CUDA(cudaMemsetAsync(gm0, 0, sizeof(float) * n3, AS()));
-        k_adj_norm_vjp<<<G, 256, 0, AS()>>>(N, s->w(W_M0), nullptr, nullptr, nullptr, nullptr, 0, 0, 0, 0, 0, lam,
-                                             gm0, nullptr, nullptr, nullptr, nullptr);
+        k_adj_m0<<<G, 256, 0, AS()>>>(N, s->w(W_M0), s->w(W_LAM), gm0);
+        UMAG_LAUNCH_CHECK();
     }
-    k_adj_to_f32<<<G, 256, 0, AS()>>>(N, s->gMs, gMs);
+    k_adj_reduce<<<1, 1024, 0, AS()>>>(N, s->acc, gMs, s->dsum);
     UMAG_LAUNCH_CHECK();
-    double hs[8];
+    double hs[5];
     UMAG_CUDA(cudaMemcpyAsync(hs, s->dsum, sizeof(hs), cudaMemcpyDeviceToHost, AS()));
     UMAG_CUDA(cudaStreamSynchronize(AS()));
     *gA = hs[0];

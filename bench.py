@@ -437,17 +437,25 @@ def run_ensemble(args):
 
 
 # ------------------------------------------------------------------ adjoint workload
-def adjoint_problem(seed=4):
+def adjoint_problem(seed=4, m0_kind="easy_axis"):
     """The differentiation workload: 128x128x1 film of 4 nm cubes, per-cell Ms
     U[6e5, 9e5] A/m, Aex 1.3e-11 J/m, Ku1 2e5 J/m^3 along x, alpha 0.02,
     B_ext (5, 5, 0) mT; fixed-step RK4, dt 1e-13 s, 4000 steps, checkpoints
     every 100 steps; loss = mean over the last 1000 steps of m_z averaged over
     a 16x16 probe window (centre of the film) + |<m>(final) - target|^2 with a
-    seeded random unit target; m0 random unit vectors (seeded)."""
+    seeded random unit target.  m0 (not fixed by the workload's definition):
+    "easy_axis" = uniform along +x, the anisotropy axis, so that the applied
+    field drives a damped precession; "random" = i.i.d. random unit vectors,
+    whose low-damping dynamics are chaotic (float32 and FP64 runs part after
+    a few hundred steps)."""
     rng = np.random.default_rng(seed)
     n = 128
     Ms = rng.uniform(6e5, 9e5, (1, n, n)).astype(np.float32)
-    m0 = random_m((n, n, 1), seed + 1)
+    if m0_kind == "random":
+        m0 = random_m((n, n, 1), seed + 1)
+    else:
+        m0 = np.zeros((3, 1, n, n), np.float32)
+        m0[0] = 1.0
     t = rng.standard_normal(3)
     t /= np.linalg.norm(t)
     kw = dict(N=(n, n, 1), cell=(4e-9, 4e-9, 4e-9), alpha=0.02, anisU=(1.0, 0.0, 0.0), dt=1e-13, nsteps=4000,
@@ -458,12 +466,19 @@ def adjoint_problem(seed=4):
 
 def run_adjoint(args):
     """Forward and backward of the differentiation workload, timed with CUDA
-    events on the library's stream (each call returns after its work ends);
-    optionally the gradients against the FP64 oracle's reverse pass."""
+    events (each call returns after its work ends).  Options: --adj-steps
+    (fewer steps, the probe average over the last quarter), --adj-fd
+    (central differences of the FP32 forward, relative step 1e-4: Aex, Ku1,
+    B_ext and 64 random cells of Ms), --adj-fp64 (the FP64 oracle's reverse
+    pass on the host, minutes of CPU at 4000 steps)."""
     import torch
     from umagnus_b200.adjoint import AdjointRK4
-    kw, Ms, m0, th = adjoint_problem()
-    sim = AdjointRK4(K=100, **kw)
+    kw, Ms, m0, th = adjoint_problem(m0_kind=args.adj_m0)
+    if args.adj_steps:
+        kw["nsteps"] = args.adj_steps
+        kw["avg_from"] = args.adj_steps - args.adj_steps // 4 + 1
+    nsteps = kw["nsteps"]
+    sim = AdjointRK4(K=min(100, nsteps), **kw)
     fw, bw = [], []
     for it in range(max(args.warmup, 1) + args.steps):
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -478,30 +493,61 @@ def run_adjoint(args):
             bw.append(e1.elapsed_time(e2) / 1e3)
     f, b = float(np.median(fw)), float(np.median(bw))
     N = 128 * 128
-    line = {"metric": "adjoint backward/forward time, 128x128x1 film, RK4 4000 steps",
+    gMs = g["Ms"].cpu().numpy()
+    cells = np.random.default_rng(7).choice(N, 64, replace=False)
+    line = {"metric": f"adjoint backward/forward time, 128x128x1 film, RK4 {nsteps} steps",
             "value": b / f, "unit": "backward/forward", "n_gpus": 1, "steps": args.steps,
             "warmup": max(args.warmup, 1), "higher_is_better": False, "dtype": "f32",
             "data": "synthetic (seeded Ms map, m0 and target)",
             "config": {"workload": "128x128x1 film, 4 nm cells, per-cell Ms U[6e5,9e5], Aex 1.3e-11, Ku1 2e5 along x, "
-                                   "alpha 0.02, B_ext (5,5,0) mT, Newell demag, fixed-step RK4 dt 1e-13 s x 4000, "
-                                   "checkpoints every 100 steps", "cells": N},
+                                   f"alpha 0.02, B_ext (5,5,0) mT, Newell demag, fixed-step RK4 dt 1e-13 s x {nsteps}, "
+                                   f"checkpoints every {min(100, nsteps)} steps", "cells": N,
+                       "m0": "uniform along +x" if args.adj_m0 == "easy_axis" else "random unit vectors"},
             "forward_s": f, "backward_s": b,
-            "forward_cell_updates_per_s": 4000 * N / f,
+            "forward_cell_updates_per_s": nsteps * N / f,
             "loss": loss,
             "grad": {"Aex": g["Aex"], "Ku1": g["Ku1"], "B_ext": g["B_ext"],
-                     "Ms_norm": float(torch.linalg.vector_norm(g["Ms"].double()))}}
+                     "Ms_norm": float(np.linalg.norm(gMs.astype(np.float64)))}}
+
+    def rel(a, b_):
+        a, b_ = np.asarray(a, np.float64), np.asarray(b_, np.float64)
+        return float(np.linalg.norm(a - b_) / np.linalg.norm(b_))
+
+    if args.adj_fd:
+        def L(Ms_=Ms, A=th["Aex"], K=th["Ku1"], B=th["B_ext"]):
+            return sim.forward(m0, Ms_, A, K, B)
+        fd = {}
+        d = 1e-4
+        fd["Aex"] = (L(A=th["Aex"] * (1 + d)) - L(A=th["Aex"] * (1 - d))) / (2 * d * th["Aex"])
+        fd["Ku1"] = (L(K=th["Ku1"] * (1 + d)) - L(K=th["Ku1"] * (1 - d))) / (2 * d * th["Ku1"])
+        Bn = float(np.linalg.norm(th["B_ext"]))
+        fdB = []
+        for c in range(3):
+            hB = d * Bn
+            bp, bm = list(th["B_ext"]), list(th["B_ext"])
+            bp[c] += hB
+            bm[c] -= hB
+            fdB.append((L(B=bp) - L(B=bm)) / (2 * hB))
+        errs = []
+        for c in cells:
+            mp, mm = Ms.copy().ravel(), Ms.copy().ravel()
+            hM = d * float(Ms.ravel()[c])
+            mp[c] += hM
+            mm[c] -= hM
+            v = (L(Ms_=mp.reshape(Ms.shape)) - L(Ms_=mm.reshape(Ms.shape))) / (2 * hM)
+            errs.append(abs(v - gMs.ravel()[c]) / max(abs(v), 1e-300))
+        line["fd_fp32"] = {"rel_step": d, "Aex": [fd["Aex"], g["Aex"]], "Ku1": [fd["Ku1"], g["Ku1"]],
+                           "B_ext": [fdB, g["B_ext"]], "rel_err_Aex": abs(fd["Aex"] - g["Aex"]) / abs(fd["Aex"]),
+                           "rel_err_Ku1": abs(fd["Ku1"] - g["Ku1"]) / abs(fd["Ku1"]),
+                           "rel_err_B_ext": rel(g["B_ext"], fdB),
+                           "Ms_64_cells_rel_err_median": float(np.median(errs)),
+                           "Ms_64_cells_rel_err_max": float(np.max(errs))}
     if args.adj_fp64:
         from oracle import adjoint_ref as R
         t0 = time.perf_counter()
         prob = R.Problem(**kw)
         loss64, g64 = prob.backward(m0.astype(np.float64).reshape(3, 1, 128, 128),
                                     R.params(Ms.astype(np.float64), th["Aex"], th["Ku1"], th["B_ext"]))
-
-        def rel(a, b_):
-            a, b_ = np.asarray(a, np.float64), np.asarray(b_, np.float64)
-            return float(np.linalg.norm(a - b_) / np.linalg.norm(b_))
-        gMs = g["Ms"].cpu().numpy()
-        cells = np.random.default_rng(7).choice(N, 64, replace=False)
         per_cell = np.abs(gMs.ravel()[cells] - g64["Ms"].ravel()[cells]) / np.abs(g64["Ms"].ravel()[cells])
         line["fp64_check"] = {"loss_fp64": loss64, "loss_rel_err": abs(loss - loss64) / abs(loss64),
                               "rel_err": {"Ms": rel(gMs, g64["Ms"]), "Aex": rel(g["Aex"], g64["A"]),
@@ -524,6 +570,9 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=90.0, help="seconds of timed CPU steps (reference arm)")
     ap.add_argument("--workload", default="multilayer", choices=["multilayer", "ensemble", "adjoint"])
     ap.add_argument("--adj-fp64", action="store_true", help="adjoint: compare with the FP64 oracle (minutes of CPU)")
+    ap.add_argument("--adj-fd", action="store_true", help="adjoint: central differences of the FP32 forward")
+    ap.add_argument("--adj-steps", type=int, default=0, help="adjoint: steps instead of 4000")
+    ap.add_argument("--adj-m0", default="easy_axis", choices=["easy_axis", "random"], help="adjoint: initial m")
     ap.add_argument("--ens-time", type=float, default=2e-9, help="ensemble: simulated time per instance (s)")
     ap.add_argument("--ens-plain-sample", type=int, default=2, help="ensemble: plain-form instances timed per size")
     args = ap.parse_args()

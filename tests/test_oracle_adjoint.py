@@ -28,7 +28,7 @@ def test_reverse_pass_matches_central_fd(demag):
     _, g = prob.backward(m0, th)
     checks = [("A", None), ("K1", None), ("B", 0), ("B", 1), ("B", 2)]
     n = m0.shape[-1]
-    cells = rng.choice(n * n, size=16, replace=False)
+    cells = rng.choice(n * n, size=64 if demag else 16, replace=False)
     checks += [("Ms", (0, int(c) // n, int(c) % n)) for c in cells]
     for which in checks:
         fd = R.fd_gradient(prob, m0, th, which, rel=1e-4)

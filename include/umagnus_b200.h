@@ -261,6 +261,11 @@ int umag_sim_torque_evals(umag_sim* s, int n);
  * Each term is -k V sum(M_full . B_term) with float32 dot products per cell
  * and FP64 accumulation. */
 int umag_sim_energies(umag_sim* s, double E[5]);
+/* engine/energy.go:36-42 SetTotalEdens (Edens_total) for the current m:
+ * per-cell total energy density in J/m^3 into dst (device, N floats), each
+ * term added in float32 as opencl.AddDotProduct does, in the terms'
+ * registration order. */
+int umag_sim_energy_density(umag_sim* s, float* dst);
 /* engine/relax.go:23-112 Relax(): RK23 without precession; steps while the
  * total energy decreases (checked every 3 steps), then while the mean
  * squared torque decreases, lowering MaxErr by sqrt(2) down to 1e-9 --

@@ -40,6 +40,35 @@ def test_energies_match_oracle():
     sim.free()
 
 
+def test_energy_density_matches_fp64():
+    """Edens_total per cell (engine/energy.go:36 SetTotalEdens) of a
+    multi-region state with per-cell Ms and easy axes, against the FP64
+    instantiation of the oracle (itself pinned to the CPU oracle), and its
+    sum against the engine's total energy."""
+    import torch
+    from oracle import gpu64
+    engine, config = _engine()
+    N, cell = (32, 24, 4), (2e-9, 2e-9, 2e-9)
+    rng = np.random.default_rng(5)
+    regions = rng.integers(0, 3, size=(N[2], N[1], N[0])).astype(np.uint8)
+    Ms = np.array([6e5, 9e5, 7e5], np.float32)[regions]
+    aex = np.zeros(256)
+    aex[:3] = [1.0e-11, 1.5e-11, 1.2e-11]
+    u = rng.normal(size=(3,) + regions.shape).astype(np.float32)
+    sim = engine.Simulation(N, cell, Ms, aex, 0.05, Ku1=2e5, anisU=u, regions=regions, B_ext=(0.0, 0.01, 0.02))
+    sim.set_m(G.random_unit(N, 4))
+    dens = sim.energy_density().double()
+    m = sim.get_m().double()
+    ref = gpu64.System64(N, cell, Ms.astype(np.float64), O.exch_lut(aex, dtype=np.float64), regions, 0.05,
+                         kernel=O.newell_kernel(N, cell), Ku1=2e5, anisU=u.astype(np.float64),
+                         B_ext=(0.0, 0.01, 0.02)).energy_density(m)
+    err = float((dens - ref).abs().max() / ref.abs().max())
+    assert err < 1e-5, err
+    V = cell[0] * cell[1] * cell[2]
+    assert float(dens.sum()) * V == pytest.approx(sim.energies()["total"], rel=1e-5)
+    sim.free()
+
+
 def test_relax_matches_oracle():
     """Relax() of a small film from a tilted state: same final <m> (1e-3) and
     energy (1e-4) as the oracle's restatement; time unchanged."""

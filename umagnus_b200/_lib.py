@@ -97,7 +97,7 @@ _SIGS = {
     "umag_sim_set_time": [P, c_double, c_double], "umag_sim_average_m": [P, ctypes.POINTER(c_double)],
     "umag_sim_use_graph": [P, c_int, c_int], "umag_sim_launches_per_step": [P, ctypes.POINTER(c_int)],
     "umag_sim_torque_evals": [P, c_int],
-    "umag_sim_energies": [P, ctypes.POINTER(c_double)], "umag_sim_relax": [P, c_double],
+    "umag_sim_energies": [P, ctypes.POINTER(c_double)], "umag_sim_energy_density": [P, P], "umag_sim_relax": [P, c_double],
     "umag_field_read_info": [ctypes.c_char_p, P], "umag_field_read": [ctypes.c_char_p, P, c_size_t, P],
     "umag_ovf_write": [ctypes.c_char_p, P, P, ctypes.c_char_p, c_int], "umag_dump_write": [ctypes.c_char_p, P, P],
     "umag_format_float": [c_double, c_int, ctypes.c_char_p, c_int],

@@ -183,6 +183,7 @@ int umag_sim_use_graph(umag_sim* s, int enable, int steps) { return sim_use_grap
 int umag_sim_launches_per_step(umag_sim* s, int* n) { return sim_launches_per_step(s, n); }
 int umag_sim_torque_evals(umag_sim* s, int n) { return sim_torque_evals(s, n); }
 int umag_sim_energies(umag_sim* s, double E[5]) { return sim_energies(s, E); }
+int umag_sim_energy_density(umag_sim* s, float* dst) { return sim_energy_density(s, dst); }
 int umag_sim_relax(umag_sim* s, double torque_threshold) { return sim_relax(s, torque_threshold); }
 int umag_ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int enable_demag, umag_ens** out) {
     return ens_new(n, in, sp, enable_demag, out);

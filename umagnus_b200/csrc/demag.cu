@@ -51,7 +51,8 @@ static int make_line(int L, FftLine<T>& f, typename Cplx<T>::t** dev_tw) {
         return set_error(UMAG_E_UNSUPPORTED, "FFT length %d has a prime factor above 13", L);
     auto t = twiddles<typename Cplx<T>::t>(L, L);
     UMAG_CUDA(cudaMalloc((void**)dev_tw, sizeof(t[0]) * (L > 0 ? L : 1)));
-    UMAG_CUDA(cudaMemcpy(*dev_tw, t.data(), sizeof(t[0]) * L, cudaMemcpyHostToDevice));
+    UMAG_CUDA(cudaMemcpyAsync(*dev_tw, t.data(), sizeof(t[0]) * L, cudaMemcpyHostToDevice, ctx().stream));
+    UMAG_CUDA(cudaStreamSynchronize(ctx().stream));  // t is freed on return
     f.tw = *dev_tw;
     return UMAG_OK;
 }
@@ -447,10 +448,11 @@ static int plan_common(umag_demag* d) {
         return set_error(UMAG_E_UNSUPPORTED, "Nz = %d too large for the z transform", d->N[2]);
     auto twr = twiddles<float2>(d->P[0], d->M > 1 ? d->M : 2);  // exp(-2 pi i k / Px), k < Px/2
     UMAG_CUDA(cudaMalloc(&d->twr, sizeof(float2) * twr.size()));
-    UMAG_CUDA(cudaMemcpy(d->twr, twr.data(), sizeof(float2) * twr.size(), cudaMemcpyHostToDevice));
+    UMAG_CUDA(cudaMemcpyAsync(d->twr, twr.data(), sizeof(float2) * twr.size(), cudaMemcpyHostToDevice, ctx().stream));
+    UMAG_CUDA(cudaStreamSynchronize(ctx().stream));
     size_t spec_elems = (size_t)3 * d->P[2] * d->N[1] * d->Lx;
     UMAG_CUDA(cudaMalloc(&d->spec, sizeof(float2) * spec_elems));
-    UMAG_CUDA(cudaMemset(d->spec, 0, sizeof(float2) * spec_elems));
+    UMAG_CUDA(cudaMemsetAsync(d->spec, 0, sizeof(float2) * spec_elems, ctx().stream));
     d->Kp = (d->Hx + 3) / 4 * 4;
     size_t kn = (size_t)d->Kp * (d->P[1] / 2 + 1) * (d->P[2] / 2 + 1);
     d->Kn = kn;
@@ -635,8 +637,10 @@ int demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6], u
     double* Kr[6] = {};
     for (int c = 0; c < 6 && s == UMAG_OK; c++) {
         if (cudaMalloc(&Kr[c], sizeof(double) * n) != cudaSuccess) { s = set_error(UMAG_E_NOMEM, "kernel"); break; }
-        if (kern[c]) cudaMemcpy(Kr[c], kern[c], sizeof(double) * n, cudaMemcpyHostToDevice);
-        else cudaMemset(Kr[c], 0, sizeof(double) * n);
+        const cudaError_t e = kern[c] ? cudaMemcpyAsync(Kr[c], kern[c], sizeof(double) * n, cudaMemcpyHostToDevice,
+                                                        ctx().stream)
+                                      : cudaMemsetAsync(Kr[c], 0, sizeof(double) * n, ctx().stream);
+        if (e != cudaSuccess) s = set_error(UMAG_E_CUDA, "kernel upload: %s", cudaGetErrorString(e));
     }
     if (s == UMAG_OK) s = kernel_to_spectrum(d, Kr, ctx().stream);
     for (int c = 0; c < 6; c++) cudaFree(Kr[c]);
@@ -658,8 +662,10 @@ int demag_get_kernel(umag_demag* d, double* const host[6]) {
         else s = set_error(UMAG_E_UNSUPPORTED, "the plan was built from a caller-supplied kernel, which it does not keep");
     }
     for (int c = 0; c < 6 && s == UMAG_OK; c++)
-        if (host[c] && cudaMemcpy(host[c], Kr[c], sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        if (host[c] && cudaMemcpyAsync(host[c], Kr[c], sizeof(double) * n, cudaMemcpyDeviceToHost, ctx().stream) !=
+                           cudaSuccess)
             s = set_error(UMAG_E_CUDA, "copy kernel");
+    if (cudaStreamSynchronize(ctx().stream) != cudaSuccess && s == UMAG_OK) s = set_error(UMAG_E_CUDA, "copy kernel");
     for (int c = 0; c < 6; c++) cudaFree(Kr[c]);
     return s;
 }
@@ -676,10 +682,12 @@ int demag_get_spectrum(umag_demag* d, float* const host[6]) {
             memset(host[c], 0, sizeof(float) * d->Hx * rows);
         } else if (!blocked) {
             // reference layout: rows of Px/2+1 floats (the device rows are padded to Kp)
-            UMAG_CUDA(cudaMemcpy2D(host[c], sizeof(float) * d->Hx, d->K[c], sizeof(float) * d->Kp,
-                                   sizeof(float) * d->Hx, rows, cudaMemcpyDeviceToHost));
+            UMAG_CUDA(cudaMemcpy2DAsync(host[c], sizeof(float) * d->Hx, d->K[c], sizeof(float) * d->Kp,
+                                        sizeof(float) * d->Hx, rows, cudaMemcpyDeviceToHost, ctx().stream));
+            UMAG_CUDA(cudaStreamSynchronize(ctx().stream));
         } else {
-            UMAG_CUDA(cudaMemcpy(tmp.data(), d->K[c], sizeof(float) * d->Kn, cudaMemcpyDeviceToHost));
+            UMAG_CUDA(cudaMemcpyAsync(tmp.data(), d->K[c], sizeof(float) * d->Kn, cudaMemcpyDeviceToHost, ctx().stream));
+            UMAG_CUDA(cudaStreamSynchronize(ctx().stream));
             const size_t nb = d->Kp / 4;
             for (size_t r = 0; r < rows; r++) {  // r = z * hy + y
                 const size_t z = r / hy, y = r % hy;

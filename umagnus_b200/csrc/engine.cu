@@ -480,43 +480,53 @@ __global__ void k_step_end(DevCtl* c0, int nb, int rk4) {
 // accumulated in FP64 (compensated relative to the reference's float32
 // reduction).  sums: [0] demag, [1] exchange (+DMI), [2] anisotropy from K1
 // alone, [3] anisotropy from K2 alone, [4] Zeeman.
-__global__ void __launch_bounds__(256) k_energy_terms(LocalArgs a, const float* __restrict__ vol, double* sums) {
-    __shared__ double sh[5][8];
+// the five float32 dot products of cell I: [0] demag, [1] exchange (+DMI),
+// [2] anisotropy from K1 alone, [3] from K2 alone, [4] Zeeman
+__device__ __forceinline__ void energy_cell_terms(const LocalArgs& a, const float* __restrict__ vol, int I,
+                                                  float t[5]) {
     const int N = a.N;
     const float* m = a.ctl->m;
     const float *mx = m, *my = m + N, *mz = m + 2 * N;
+    const int ix = I % a.g.Nx, iy = (I / a.g.Nx) % a.g.Ny, iz = I / (a.g.Nx * a.g.Ny);
+    const f3 m0 = ld3(mx, my, mz, I);
+    const float ms = amul(a.Ms, a.Ms_mul, I);
+    f3 Mf{fm(m0.x, ms), fm(m0.y, ms), fm(m0.z, ms)};
+    if (vol) {
+        const float w = __ldg(vol + I);
+        Mf = f3{fm(Mf.x, w), fm(Mf.y, w), fm(Mf.z, w)};
+    }
+    for (int k = 0; k < 5; k++) t[k] = 0.f;
+    if (a.bd) t[0] = dot3(Mf, f3{__ldg(a.bd + I), __ldg(a.bd + N + I), __ldg(a.bd + 2 * N + I)});
+    if (!is0(m0)) {
+        const int r0 = __ldg(a.regions + I);
+        const f3 e = a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
+                           : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
+        const float inv = inv_msat(a.Ms, a.Ms_mul, I);
+        t[1] = dot3(Mf, f3{fm(e.x, inv), fm(e.y, inv), fm(e.z, inv)});
+    }
+    if (a.anis) {
+        UniaxParams p1 = a.up, p2 = a.up;
+        p1.K2 = nullptr; p1.K2_mul = 0.f;
+        p2.K1 = nullptr; p2.K1_mul = 0.f;
+        f3 B1{0.f, 0.f, 0.f}, B2{0.f, 0.f, 0.f};
+        add_uniaxial(B1, p1, m0, I);
+        add_uniaxial(B2, p2, m0, I);
+        t[2] = dot3(Mf, B1);
+        t[3] = dot3(Mf, B2);
+    }
+    if (a.zeeman) {
+        const int r = __ldg(a.regions + I);
+        t[4] = dot3(Mf, f3{__ldg(a.bext[0] + r), __ldg(a.bext[1] + r), __ldg(a.bext[2] + r)});
+    }
+}
+
+__global__ void __launch_bounds__(256) k_energy_terms(LocalArgs a, const float* __restrict__ vol, double* sums) {
+    __shared__ double sh[5][8];
     double acc[5] = {0, 0, 0, 0, 0};
-    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x) {
-        const int ix = I % a.g.Nx, iy = (I / a.g.Nx) % a.g.Ny, iz = I / (a.g.Nx * a.g.Ny);
-        const f3 m0 = ld3(mx, my, mz, I);
-        const float ms = amul(a.Ms, a.Ms_mul, I);
-        f3 Mf{fm(m0.x, ms), fm(m0.y, ms), fm(m0.z, ms)};
-        if (vol) {
-            const float w = __ldg(vol + I);
-            Mf = f3{fm(Mf.x, w), fm(Mf.y, w), fm(Mf.z, w)};
-        }
-        if (a.bd) acc[0] += (double)dot3(Mf, f3{__ldg(a.bd + I), __ldg(a.bd + N + I), __ldg(a.bd + 2 * N + I)});
-        if (!is0(m0)) {
-            const int r0 = __ldg(a.regions + I);
-            const f3 e = a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
-                               : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
-            const float inv = inv_msat(a.Ms, a.Ms_mul, I);
-            acc[1] += (double)dot3(Mf, f3{fm(e.x, inv), fm(e.y, inv), fm(e.z, inv)});
-        }
-        if (a.anis) {
-            UniaxParams p1 = a.up, p2 = a.up;
-            p1.K2 = nullptr; p1.K2_mul = 0.f;
-            p2.K1 = nullptr; p2.K1_mul = 0.f;
-            f3 B1{0.f, 0.f, 0.f}, B2{0.f, 0.f, 0.f};
-            add_uniaxial(B1, p1, m0, I);
-            add_uniaxial(B2, p2, m0, I);
-            acc[2] += (double)dot3(Mf, B1);
-            acc[3] += (double)dot3(Mf, B2);
-        }
-        if (a.zeeman) {
-            const int r = __ldg(a.regions + I);
-            acc[4] += (double)dot3(Mf, f3{__ldg(a.bext[0] + r), __ldg(a.bext[1] + r), __ldg(a.bext[2] + r)});
-        }
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < a.N; I += gridDim.x * blockDim.x) {
+        float t[5];
+        energy_cell_terms(a, vol, I, t);
+        for (int k = 0; k < 5; k++) acc[k] += (double)t[k];
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -829,10 +839,10 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
     size_t b3 = sizeof(float) * 3 * (size_t)s->N;
     auto fail = [&](int code) { sim_free(reinterpret_cast<umag_sim*>(s)); return code; };
     if (cudaMalloc(&s->bufs, b3 * 9) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "state buffers"));
-    cudaMemset(s->bufs, 0, b3 * 9);
+    if (cudaMemsetAsync(s->bufs, 0, b3 * 9, S()) != cudaSuccess) return fail(set_error(UMAG_E_CUDA, "state buffers"));
     if (!p->regions) {
         if (cudaMalloc(&s->zero_regions, s->N) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "regions"));
-        cudaMemset(s->zero_regions, 0, s->N);
+        if (cudaMemsetAsync(s->zero_regions, 0, s->N, S()) != cudaSuccess) return fail(set_error(UMAG_E_CUDA, "regions"));
         s->p.regions = s->zero_regions;
     }
     if (p->enable_demag) {
@@ -1097,6 +1107,27 @@ int sim_torque_evals(umag_sim* h, int n) {
 // E[0] total, E[1] demag (engine/demag.go:146), E[2] exchange incl. DMI
 // (engine/exchange.go:79), E[3] anisotropy (engine/anisotropy.go:210),
 // E[4] Zeeman (engine/zeeman.go:15).  Joules.
+// engine/energy.go:36-42 SetTotalEdens: dst = 0, then each term's
+// AddDotProduct(dst, prefactor, B_term, M_full) in float32, in the order the
+// terms register (anisotropy -1/2 and -1/4, demag -1/2, exchange -1/2,
+// Zeeman -1; engine/anisotropy.go:164-190, demag.go:31, exchange.go:34,
+// zeeman.go:9)
+__global__ void __launch_bounds__(256) k_energy_density(LocalArgs a, const float* __restrict__ vol, float* dst) {
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < a.N; I += gridDim.x * blockDim.x) {
+        float t[5];
+        energy_cell_terms(a, vol, I, t);
+        float d = 0.0f;
+        if (a.anis) {
+            d = fa(d, fm(-0.5f, t[2]));
+            d = fa(d, fm(-0.25f, t[3]));
+        }
+        if (a.bd) d = fa(d, fm(-0.5f, t[0]));
+        d = fa(d, fm(-0.5f, t[1]));
+        if (a.zeeman) d = fa(d, fm(-1.0f, t[4]));
+        dst[I] = d;
+    }
+}
+
 int sim_energies(umag_sim* h, double E[5]) {
     SimImpl* s = reinterpret_cast<SimImpl*>(h);
     UMAG_REQUIRE(s && E, "NULL argument");
@@ -1121,6 +1152,25 @@ int sim_energies(umag_sim* h, double E[5]) {
     E[1] = Ed; E[2] = Ee; E[3] = Ea; E[4] = Ez;
     // registration order of the terms (files anisotropy, demag, exchange, zeeman)
     E[0] = ((Ea + Ed) + Ee) + Ez;
+    return UMAG_OK;
+}
+
+// per-cell total energy density (J/m^3) of the current m into dst (device, N floats)
+int sim_energy_density(umag_sim* h, float* dst) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && dst, "NULL argument");
+    UMAG_REQUIRE(!s->batched, "energy density of a batched simulation");
+    UMAG_TRY(sync_ctl_to_host(s));
+    s->hctl->active = 1;
+    UMAG_TRY(push_ctl(s));
+    if (s->p.enable_demag) {
+        PassArgs a = s->pa;
+        a.m_sel = 0;
+        UMAG_TRY(demag_launch(s->demag, a, S()));
+    }
+    k_energy_density<<<grid_for(s->N, 256), 256, 0, S()>>>(s->la, s->p.vol, dst);
+    UMAG_LAUNCH_CHECK();
+    UMAG_CUDA(cudaStreamSynchronize(S()));
     return UMAG_OK;
 }
 
@@ -1325,14 +1375,15 @@ static int ens_class_new(EnsClass& C, const umag_ens_instance* in, const std::ve
     UMAG_CUDA(cudaStreamCreateWithFlags(&C.st, cudaStreamNonBlocking));
     UMAG_CUDA(cudaEventCreateWithFlags(&C.done, cudaEventDisableTiming));
     UMAG_CUDA(cudaMalloc(&s->bufs, sizeof(float) * n3 * 9 * nb));
-    UMAG_CUDA(cudaMemset(s->bufs, 0, sizeof(float) * n3 * 9 * nb));
+    UMAG_CUDA(cudaMemsetAsync(s->bufs, 0, sizeof(float) * n3 * 9 * nb, S()));
     UMAG_CUDA(cudaMalloc(&s->zero_regions, s->N));
-    UMAG_CUDA(cudaMemset(s->zero_regions, 0, s->N));
+    UMAG_CUDA(cudaMemsetAsync(s->zero_regions, 0, s->N, S()));
     s->p.regions = s->zero_regions;
     if (demag) {
         int pbc[3] = {0, 0, 0};
         UMAG_TRY(demag_new_newell(r0.N[0], r0.N[1], r0.N[2], pbc, r0.cell[0], r0.cell[1], r0.cell[2], 32, 0, &s->demag));
         UMAG_CUDA(cudaMalloc(&s->bd, sizeof(float) * n3 * nb));
+        UMAG_CUDA(cudaMemsetAsync(s->bd, 0, sizeof(float) * n3 * nb, S()));
     }
     UMAG_CUDA(cudaMalloc(&s->ctl, sizeof(DevCtl) * nb));
     UMAG_CUDA(cudaMallocHost(&s->hctl, sizeof(DevCtl) * nb));
@@ -1366,7 +1417,8 @@ static int ens_class_new(EnsClass& C, const umag_ens_instance* in, const std::ve
         zee |= r.B_ext[0] != 0.0f || r.B_ext[1] != 0.0f || r.B_ext[2] != 0.0f;
     }
     UMAG_CUDA(cudaMalloc(&C.params, sizeof(float) * 3 * nb));
-    UMAG_CUDA(cudaMemcpy(C.params, hp.data(), sizeof(float) * 3 * nb, cudaMemcpyHostToDevice));
+    UMAG_CUDA(cudaMemcpyAsync(C.params, hp.data(), sizeof(float) * 3 * nb, cudaMemcpyHostToDevice, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
     UMAG_CUDA(cudaMalloc(&s->ip_dev, sizeof(InstParams) * nb));
     LocalArgs& la = s->la;
     la.g = s->g;
@@ -1405,13 +1457,15 @@ static int ens_class_new(EnsClass& C, const umag_ens_instance* in, const std::ve
     UMAG_CUDA(cudaStreamSynchronize(S()));
     // fill the non-kc fields without touching kc
     for (int b = 0; b < nb; b++)
-        UMAG_CUDA(cudaMemcpy(reinterpret_cast<char*>(s->ip_dev + b) + offsetof(InstParams, alpha_mul),
-                             reinterpret_cast<char*>(&hip[b]) + offsetof(InstParams, alpha_mul),
-                             sizeof(InstParams) - offsetof(InstParams, alpha_mul), cudaMemcpyHostToDevice));
+        UMAG_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(s->ip_dev + b) + offsetof(InstParams, alpha_mul),
+                                  reinterpret_cast<char*>(&hip[b]) + offsetof(InstParams, alpha_mul),
+                                  sizeof(InstParams) - offsetof(InstParams, alpha_mul), cudaMemcpyHostToDevice, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
     if (demag) {
         fill_pass_args(s->demag, s->pa);
         const long spec_elems = 3L * s->demag->P[2] * s->demag->N[1] * s->demag->Lx;  // one plan's spectrum
         UMAG_CUDA(cudaMalloc(&C.spec, sizeof(float2) * spec_elems * nb));
+        UMAG_CUDA(cudaMemsetAsync(C.spec, 0, sizeof(float2) * spec_elems * nb, S()));
         s->pa.spec = C.spec;
         s->pa.spec_stride = spec_elems;
         s->pa.m_ind = &s->ctl[0].m;
@@ -1478,7 +1532,8 @@ int ens_set_m(umag_ens* h, int i, const float* host_m) {
     SimImpl* s = ens_sim(e, i, &b);
     UMAG_TRY(sync_ctl_to_host(s));
     float* m = s->hctl[b].m;
-    UMAG_CUDA(cudaMemcpy(m, host_m, sizeof(float) * 3 * s->N, cudaMemcpyHostToDevice));
+    // on the library stream, so that the normalisation below sees the copy
+    UMAG_CUDA(cudaMemcpyAsync(m, host_m, sizeof(float) * 3 * s->N, cudaMemcpyHostToDevice, S()));
     UMAG_TRY(normalize(m, m + s->N, m + 2 * (size_t)s->N, nullptr, s->N));  // engine/magnetization.go:34
     UMAG_CUDA(cudaDeviceSynchronize());
     s->need_k1 = true;
@@ -1491,7 +1546,8 @@ int ens_get_m(umag_ens* h, int i, float* host_m) {
     int b;
     SimImpl* s = ens_sim(e, i, &b);
     UMAG_TRY(sync_ctl_to_host(s));
-    UMAG_CUDA(cudaMemcpy(host_m, s->hctl[b].m, sizeof(float) * 3 * s->N, cudaMemcpyDeviceToHost));
+    UMAG_CUDA(cudaMemcpyAsync(host_m, s->hctl[b].m, sizeof(float) * 3 * s->N, cudaMemcpyDeviceToHost, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
     return UMAG_OK;
 }
 

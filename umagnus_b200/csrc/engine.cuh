@@ -18,6 +18,7 @@ int sim_use_graph(umag_sim* s, int enable, int steps);
 int sim_launches_per_step(umag_sim* s, int* n);
 int sim_torque_evals(umag_sim* s, int n);
 int sim_energies(umag_sim* s, double E[5]);
+int sim_energy_density(umag_sim* s, float* dst);
 int sim_relax(umag_sim* s, double threshold);
 int ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int demag, umag_ens** out);
 int ens_free(umag_ens* e);

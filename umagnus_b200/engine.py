@@ -225,6 +225,14 @@ class Simulation:
         check(self.L.umag_sim_energies(self._h, out))
         return dict(zip(("total", "demag", "exchange", "anisotropy", "zeeman"), list(out)))
 
+    def energy_density(self, out=None):
+        """engine/energy.go:36 SetTotalEdens (Edens_total, J/m^3) for the
+        current m, as a (Nz, Ny, Nx) float32 tensor on the device."""
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device="cuda")
+        check(self.L.umag_sim_energy_density(self._h, out.data_ptr()))
+        return out
+
     def relax(self, torque_threshold=-1.0):
         """engine/relax.go:23 Relax() (RelaxTorqueThreshold = torque_threshold)."""
         check(self.L.umag_sim_relax(self._h, float(torque_threshold)))

@@ -560,6 +560,138 @@ def run_adjoint(args):
     return 0
 
 
+# ------------------------------------------------------------------ precision workload
+def voronoi_grains(N, ngrain, seed):
+    """Columnar Voronoi grains: ngrain seed points uniform in the film plane
+    (seeded), each cell (and the column above it) in the grain of its nearest
+    seed; grain index = region id."""
+    rng = np.random.default_rng(seed)
+    Nx, Ny, Nz = N
+    pts = rng.uniform(0, 1, size=(ngrain, 2)) * np.array([Nx, Ny])
+    x = np.arange(Nx) + 0.5
+    y = np.arange(Ny) + 0.5
+    best = np.full((Ny, Nx), np.inf)
+    grain = np.zeros((Ny, Nx), np.uint8)
+    for g, (px, py) in enumerate(pts):
+        d = (x[None, :] - px) ** 2 + (y[:, None] - py) ** 2
+        closer = d < best
+        best[closer] = d[closer]
+        grain[closer] = g
+    return np.broadcast_to(grain, (Nz, Ny, Nx)).copy()
+
+
+def precision_problem(N=(512, 512, 32), seed=3):
+    """The precision workload: 2 nm cubes, 64 columnar Voronoi grains (region
+    ids 0..63), each grain of class 0 or 1 (seeded) with Ms 6e5 / 9e5 A/m and
+    Aex 1.0e-11 / 1.5e-11 J/m, Ku1 2e5 J/m^3 along a random axis per grain
+    (seeded), alpha 0.05, no applied field, m0 random unit vectors (seeded)."""
+    rng = np.random.default_rng(seed)
+    regions = voronoi_grains(N, 64, seed)
+    cls = rng.integers(0, 2, size=64)
+    ms_r = np.where(cls == 0, 6e5, 9e5)
+    aex_r = np.zeros(256)
+    aex_r[:64] = np.where(cls == 0, 1.0e-11, 1.5e-11)
+    axes = rng.standard_normal((64, 3))
+    axes /= np.linalg.norm(axes, axis=1, keepdims=True)
+    Ms = ms_r[regions].astype(np.float32)
+    u = np.stack([axes[regions][..., c] for c in range(3)]).astype(np.float32)
+    m0 = random_m(N, seed + 1)
+    return dict(N=N, cell=(2e-9, 2e-9, 2e-9), regions=regions, Ms=Ms, aex_r=aex_r, Ku1=2e5, u=u, alpha=0.05, m0=m0)
+
+
+def run_precision(args):
+    """Float32 engine (FP64 Newell tensor, compensated sums, FP64 time) against
+    the FP64 instantiation of the oracle on the GPU (oracle/gpu64.py, the
+    uMagNUS64 semantics) from the same m0: the effective field and energy
+    density of the same m (at m0 and at the final float32 state), then
+    --prec-steps RK45DP step attempts on both, comparing average m and the
+    accepted dt sequence step by step."""
+    import torch
+    from oracle import gpu64
+    from oracle import oracle as O
+    from umagnus_b200 import engine
+    from umagnus_b200 import opencl as cl
+    N = tuple(int(v) for v in args.prec_size.split("x"))
+    pb = precision_problem(N)
+    t_start = time.perf_counter()
+    sim = engine.Simulation(N, pb["cell"], Msat=pb["Ms"], Aex=pb["aex_r"], alpha=pb["alpha"], Ku1=pb["Ku1"],
+                            anisU=pb["u"], regions=pb["regions"])
+    sim.set_m(pb["m0"])
+    d = cl.NewNewellDemag(N, (0, 0, 0), pb["cell"])
+    K = d.kernel()
+    d.Free()
+    sys64 = gpu64.System64(N, pb["cell"], pb["Ms"].astype(np.float64), O.exch_lut(pb["aex_r"], dtype=np.float64),
+                           pb["regions"], pb["alpha"], kernel=K, Ku1=pb["Ku1"], anisU=pb["u"].astype(np.float64))
+    del K
+
+    def field_errors(label):
+        m32 = sim.get_m().reshape((3,) + sim.shape)
+        _, B32 = sim.torque(beff=True)
+        B32 = B32.reshape((3,) + sim.shape).double()
+        e32 = sim.energy_density().double()
+        m = m32.double()
+        B64 = sys64.beff(m)
+        e64 = sys64.energy_density(m)
+        dB = torch.sqrt(((B32 - B64) ** 2).sum(0))
+        nB = torch.sqrt((B64 ** 2).sum(0))
+        de = (e32 - e64).abs()
+        return {label: {"B_eff": {"max_abs_T": float(dB.max()), "rms_abs_T": float(torch.sqrt((dB ** 2).mean())),
+                                  "max_rel_to_max": float(dB.max() / nB.max()),
+                                  "rms_rel_to_rms": float(torch.sqrt((dB ** 2).mean() / (nB ** 2).mean()))},
+                        "energy_density": {"max_abs_J_m3": float(de.max()),
+                                           "rms_abs_J_m3": float(torch.sqrt((de ** 2).mean())),
+                                           "max_rel_to_max": float(de.max() / e64.abs().max()),
+                                           "rms_rel_to_rms": float(torch.sqrt((de ** 2).mean() / (e64 ** 2).mean()))},
+                        "total_energy_rel": float(abs(e32.sum() - e64.sum()) / abs(e64.sum()))}}
+
+    out = field_errors("at_m0")
+    st64 = gpu64.RK45DP64(sys64, sim.get_m().reshape((3,) + sim.shape).double().cpu().numpy())
+    rec32, rec64 = [], []
+    prev = sim.state()
+    for i in range(args.prec_steps):
+        sim.steps(1)
+        s = sim.state()
+        acc = s["nsteps"] > prev["nsteps"]
+        rec32.append((acc, s["time"] - prev["time"], s["dt"], sim.average_m()))
+        prev = s
+        t0 = st64.time
+        a64 = st64.step()
+        rec64.append((a64, st64.time - t0, st64.dt, st64.average_m()))
+    same = 0
+    while same < len(rec32) and rec32[same][0] == rec64[same][0]:
+        same += 1
+    dts32 = np.array([r[1] for r in rec32[:same] if r[0]])
+    dts64 = np.array([r[1] for r in rec64[:same] if r[0]])
+    rel_dt = np.abs(dts32 - dts64) / dts64
+    am32 = np.array([r[3] for r in rec32[:same]])
+    am64 = np.array([r[3] for r in rec64[:same]])
+    dam = np.linalg.norm(am32 - am64, axis=1)
+    out.update(field_errors("at_final_state"))
+    mf32 = sim.get_m().reshape((3,) + sim.shape).double()
+    dm = torch.sqrt(((mf32 - st64.m) ** 2).sum(0))
+    line = {"metric": "float32 engine error against the FP64 oracle (precision workload)",
+            "value": float(rel_dt.max()) if rel_dt.size else None, "unit": "max relative error of accepted dt",
+            "higher_is_better": False, "dtype": "f32", "n_gpus": 1,
+            "data": "synthetic (seeded Voronoi grains, axes, m0)",
+            "config": {"workload": f"{N[0]}x{N[1]}x{N[2]} cells of 2 nm, 64 Voronoi grains (2 classes: Ms 6e5/9e5, "
+                                   "Aex 1.0e-11/1.5e-11), Ku1 2e5 along a random axis per grain, alpha 0.05, "
+                                   "Newell demag, RK45DP MaxErr 1e-5",
+                       "step_attempts": args.prec_steps, "oracle": "oracle/gpu64.py (FP64, torch + cuFFT)"},
+            "fields": out,
+            "trajectory": {"attempts_with_identical_accept_decisions": same,
+                           "accepted_f32": int(sum(r[0] for r in rec32)), "accepted_f64": int(sum(r[0] for r in rec64)),
+                           "time_f32": prev["time"], "time_f64": st64.time,
+                           "dt_rel_err": {"max": float(rel_dt.max()) if rel_dt.size else None,
+                                          "rms": float(np.sqrt((rel_dt ** 2).mean())) if rel_dt.size else None},
+                           "avg_m_abs_err": {"max": float(dam.max()) if dam.size else None,
+                                             "rms": float(np.sqrt((dam ** 2).mean())) if dam.size else None,
+                                             "final": float(dam[-1]) if dam.size else None},
+                           "final_m_per_cell_err": {"max": float(dm.max()), "rms": float(torch.sqrt((dm ** 2).mean()))}},
+            "seconds": time.perf_counter() - t_start}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -568,10 +700,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=90.0, help="seconds of timed CPU steps (reference arm)")
-    ap.add_argument("--workload", default="multilayer", choices=["multilayer", "ensemble", "adjoint"])
+    ap.add_argument("--workload", default="multilayer", choices=["multilayer", "ensemble", "adjoint", "precision"])
     ap.add_argument("--adj-fp64", action="store_true", help="adjoint: compare with the FP64 oracle (minutes of CPU)")
     ap.add_argument("--adj-fd", action="store_true", help="adjoint: central differences of the FP32 forward")
     ap.add_argument("--adj-steps", type=int, default=0, help="adjoint: steps instead of 4000")
+    ap.add_argument("--prec-steps", type=int, default=2000, help="precision: RK45DP step attempts")
+    ap.add_argument("--prec-size", default="512x512x32", help="precision: mesh NxxNyxNz")
     ap.add_argument("--adj-m0", default="easy_axis", choices=["easy_axis", "random"], help="adjoint: initial m")
     ap.add_argument("--ens-time", type=float, default=2e-9, help="ensemble: simulated time per instance (s)")
     ap.add_argument("--ens-plain-sample", type=int, default=2, help="ensemble: plain-form instances timed per size")
@@ -580,6 +714,8 @@ def main():
         return run_ensemble(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "precision":
+        return run_precision(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

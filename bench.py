@@ -686,7 +686,11 @@ def run_precision(args):
                            "avg_m_abs_err": {"max": float(dam.max()) if dam.size else None,
                                              "rms": float(np.sqrt((dam ** 2).mean())) if dam.size else None,
                                              "final": float(dam[-1]) if dam.size else None},
-                           "final_m_per_cell_err": {"max": float(dm.max()), "rms": float(torch.sqrt((dm ** 2).mean()))}},
+                           "final_m_per_cell_err": {"max": float(dm.max()), "rms": float(torch.sqrt((dm ** 2).mean()))},
+                           "avg_m_abs_err_at_attempt": {str(k): float(dam[k - 1]) for k in (10, 100, 250, 500, 1000, 1500, 2000)
+                                                        if k <= dam.size},
+                           "dt_rel_err_at_accepted": {str(k): float(rel_dt[k - 1]) for k in (10, 100, 250, 500, 1000, 1500, 2000)
+                                                      if k <= rel_dt.size}},
             "seconds": time.perf_counter() - t_start}
     print(json.dumps(line), flush=True)
     return 0

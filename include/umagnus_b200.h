@@ -89,6 +89,9 @@ int umag_region_addv(float* dx, float* dy, float* dz, const float* lutx, const f
 int umag_region_decode(float* dst, const float* lut, const uint8_t* regions, int N);
 
 /* ---- torque -------------------------------------------------------------- */
+/* opencl/zeromask.go:12 ZeroMask (zeromask.cl): dst_c[i] = 0 where
+ * maskLUT[regions[i]] != 0, for the three components. */
+int umag_zero_mask(float* dx, float* dy, float* dz, const float* maskLUT, const uint8_t* regions, int N);
 /* opencl/lltorque.go:16 LLTorque (lltorque2.cl); t may alias h. */
 int umag_lltorque(float* tx, float* ty, float* tz, const float* mx, const float* my,
                   const float* mz, const float* hx, const float* hy, const float* hz,
@@ -207,6 +210,8 @@ typedef struct {
     int asymptotic_radius;         /* engine/demag.go:27, default 32 */
     int demag_kernel;              /* 0 Newell (EnableNewellDemag), 1 brute force (EnableDemag) */
     double demag_accuracy;         /* brute force: DemagAccuracy (engine/demag.go:25); <= 0 -> 6 */
+    const float* frozen_lut;       /* FrozenSpins per region (256 floats, device) or NULL
+                                      (engine/torque.go:348-352: torque zeroed where != 0) */
 } umag_sim_params;
 
 /* Solver knobs, engine/run.go:14-43 (defaults by umag_solver_defaults). */

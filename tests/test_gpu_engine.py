@@ -136,3 +136,27 @@ def test_run_stops_exactly_at_alarm(eng):
     g.run(5e-13, chunk=3)
     assert g.state()["time"] == pytest.approx(1.5e-12, rel=0, abs=1e-24)
     g.free()
+
+
+def test_frozen_spins(eng):
+    """engine/torque.go:348-352 FreezeSpins: the torque is zero in frozen
+    regions and unchanged elsewhere; frozen cells keep their m through steps."""
+    p = multilayer_small(N=(24, 20, 4))
+    regions = (np.arange(p["N"][0])[None, None, :] >= p["N"][0] // 2).astype(np.uint8)
+    regions = np.broadcast_to(regions, (p["N"][2], p["N"][1], p["N"][0])).copy()
+    kw = dict(Dind=p["Dind"], Ku1=p["Ku1"], anisU=p["anisU"], B_ext=p["B_ext"], regions=regions)
+    free = eng.Simulation(p["N"], p["cell"], p["Ms"], p["Aex"], p["alpha"], **kw)
+    frozen = eng.Simulation(p["N"], p["cell"], p["Ms"], p["Aex"], p["alpha"], FrozenSpins=[0.0, 1.0], **kw)
+    m0 = G.random_unit(p["N"], 3)
+    for s in (free, frozen):
+        s.set_m(m0)
+    tf = free.torque().cpu().numpy()
+    tz = frozen.torque().cpu().numpy()
+    sel = regions == 1
+    assert np.all(tz[:, sel] == 0)
+    assert np.array_equal(tz[:, ~sel], tf[:, ~sel])
+    frozen.steps(10)
+    m = frozen.get_m().cpu().numpy().reshape(m0.shape)
+    mn = m0 / np.linalg.norm(m0, axis=0)
+    assert np.abs(m[:, sel] - mn[:, sel]).max() < 1e-6
+    assert np.abs(m[:, ~sel] - mn[:, ~sel]).max() > 1e-3

@@ -90,6 +90,19 @@ def test_uniaxial_zeeman_torque_bitexact(cl):
     assert np.array_equal(t2.cpu().numpy(), O.llnoprecess(m, want))
 
 
+def test_zero_mask(cl):
+    """opencl/zeromask.go:12 ZeroMask: zero where the region's LUT entry is non-zero."""
+    N = (19, 11, 3)
+    m, regions, _, _ = _setup(N)
+    lut = np.zeros(256, np.float32)
+    lut[np.unique(regions)[::2]] = 1.0
+    want = m.copy()
+    want[:, lut[regions] != 0] = 0.0
+    d = cu(m)
+    cl.ZeroMask(d, cu(lut), cu(regions))
+    assert np.array_equal(d.cpu().numpy(), want)
+
+
 def test_madd_normalize_bitexact(cl):
     rng = np.random.default_rng(9)
     n = 5000

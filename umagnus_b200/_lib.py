@@ -29,7 +29,7 @@ class SimParams(ctypes.Structure):
         ("anisU", P * 3), ("anisU_mul", c_float * 3),
         ("aLUT", P), ("dLUT", P), ("bextLUT", P * 3),
         ("enable_demag", c_int), ("openbc", c_int), ("precess", c_int), ("asymptotic_radius", c_int),
-        ("demag_kernel", c_int), ("demag_accuracy", c_double),
+        ("demag_kernel", c_int), ("demag_accuracy", c_double), ("frozen_lut", P),
     ]
 
 
@@ -71,6 +71,7 @@ _SIGS = {
     "umag_add_uniaxial_anisotropy2": [P, P, P, P, P, P, P, c_float, P, c_float, P, c_float, P, c_float, P, c_float, P,
                                       c_float, c_int],
     "umag_region_addv": [P, P, P, P, P, P, P, c_int], "umag_region_decode": [P, P, P, c_int],
+    "umag_zero_mask": [P, P, P, P, P, c_int],
     "umag_lltorque": [P, P, P, P, P, P, P, P, P, P, c_float, c_int],
     "umag_llnoprecess": [P, P, P, P, P, P, P, P, P, c_int],
     "umag_madd": [c_int, P, c_int, P, P, c_int],

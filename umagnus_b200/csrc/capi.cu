@@ -81,6 +81,9 @@ int umag_region_addv(float* dx, float* dy, float* dz, const float* lx, const flo
 int umag_region_decode(float* dst, const float* lut, const uint8_t* regions, int N) {
     return region_decode(dst, lut, regions, N);
 }
+int umag_zero_mask(float* dx, float* dy, float* dz, const float* maskLUT, const uint8_t* regions, int N) {
+    return zero_mask(dx, dy, dz, maskLUT, regions, N);
+}
 int umag_lltorque(float* tx, float* ty, float* tz, const float* mx, const float* my, const float* mz,
                   const float* hx, const float* hy, const float* hz, const float* alpha, float alpha_mul, int N) {
     return torque(tx, ty, tz, mx, my, mz, hx, hy, hz, alpha, alpha_mul, N, 1);

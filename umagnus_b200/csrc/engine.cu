@@ -77,6 +77,7 @@ struct LocalArgs {
     const uint8_t* regions;
     float wx, wy, wz, cx, cy, cz;
     int dmi, openbc, anis, zeeman, precess;
+    const float* frozen;  // FrozenSpins LUT (256) or NULL
     int ms_uniform, alpha_uniform, anis_uniform;
     DmiPairLut dl;
     LocalConsts kc;
@@ -221,6 +222,8 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
     if (!a.precess) t = llnoprecess(m0, B);
     else if (BAT || a.alpha_uniform) t = lltorque_g(m0, B, alpha_mul, kc.gilb);
     else t = lltorque(m0, B, amul(a.alpha, a.alpha_mul, I));
+    // engine/torque.go:348-352 FreezeSpins (zeromask.cl)
+    if (!BAT && a.frozen && __ldg(a.frozen + (UREG ? 0 : __ldg(a.regions + I))) != 0.0f) t = f3{0.f, 0.f, 0.f};
     float* out = a.tau_direct ? a.tau_direct : ctl->k[a.out_slot];
     out[I] = t.x; out[N + I] = t.y; out[2 * N + I] = t.z;
 }
@@ -905,6 +908,7 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
     la.alpha = p->alpha;
     la.alpha_mul = p->alpha_mul;
     la.precess = p->precess;
+    la.frozen = p->frozen_lut;
     la.Ms = p->Ms;
     la.Ms_mul = p->Ms_mul;
     la.ms_uniform = p->Ms == nullptr;

@@ -203,6 +203,26 @@ __global__ void k_add_dot(float* dst, float pre, const float* __restrict__ ax, c
         dst[i] = fa(dst[i], fm(pre, dot3(ld3(ax, ay, az, i), ld3(bx, by, bz, i))));
 }
 
+// zeromask.cl
+__global__ void k_zero_mask(float* dx, float* dy, float* dz, const float* __restrict__ lut,
+                            const uint8_t* __restrict__ regions, int N) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        if (lut[regions[i]] != 0.0f) {
+            dx[i] = 0.0f;
+            dy[i] = 0.0f;
+            dz[i] = 0.0f;
+        }
+}
+
+int zero_mask(float* dx, float* dy, float* dz, const float* lut, const uint8_t* regions, int N) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(dx && dy && dz && lut && regions, "NULL argument");
+    if (N <= 0) return UMAG_OK;
+    k_zero_mask<<<grid_for(N, 256), 256, 0, ctx().stream>>>(dx, dy, dz, lut, regions, N);
+    UMAG_LAUNCH_CHECK();
+    return UMAG_OK;
+}
+
 // ---- reductions ------------------------------------------------------------
 // kind 0: max |v|^2 of a vector field; 1: max |a-b|^2; 2: max |v| of a scalar
 template <int KIND>

@@ -75,13 +75,14 @@ class Simulation:
     anisU: 3-vector or (3, Nz, Ny, Nx); B_ext: 3-vector (T) or (256, 3)
     per-region; regions: uint8 (Nz, Ny, Nx) map; geom: cell volume fraction;
     demag_kernel: "newell" (EnableNewellDemag) or "brute" (EnableDemag, the
-    reference default, with DemagAccuracy = demag_accuracy).
+    reference default, with DemagAccuracy = demag_accuracy); FrozenSpins: a
+    scalar or 256 per-region values, the torque is zero where non-zero.
     """
 
     def __init__(self, N, cell, Msat, Aex, alpha, Dind=0.0, Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
                  regions=None, geom=None, demag=True, open_bc=False, precess=True, solver=DORMANDPRINCE,
                  dt=1e-15, MaxErr=1e-5, RelErr=1e-4, MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8,
-                 device=0, asymptotic_radius=32, demag_kernel="newell", demag_accuracy=6.0):
+                 device=0, asymptotic_radius=32, demag_kernel="newell", demag_accuracy=6.0, FrozenSpins=None):
         self.L = _lib.init(device)
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
@@ -137,6 +138,14 @@ class Simulation:
             raise ValueError("demag_kernel must be 'newell' or 'brute'")
         p.demag_kernel = 1 if demag_kernel == "brute" else 0
         p.demag_accuracy = float(demag_accuracy)
+        if FrozenSpins is not None:  # engine/torque.go:348-352: a scalar or 256 per-region values
+            fz = np.zeros(NREGION, np.float32)
+            v = np.asarray(FrozenSpins, np.float32).ravel()
+            fz[: v.size] = v
+            if v.size == 1:
+                fz[:] = v[0]
+            self.frozen = _dev(fz)
+            p.frozen_lut = keep(self.frozen)
         sp = SolverParams()
         self.L.umag_solver_defaults(ctypes.byref(sp))
         sp.solver = int(solver)

@@ -187,6 +187,14 @@ def LLTorque(torque, m, B, alpha):
     Sync()
 
 
+def ZeroMask(dst, mask, regions):
+    """opencl/zeromask.go:12: dst = 0 where mask[regions] != 0 (mask: 256-entry LUT)."""
+    L = _L()
+    _in()
+    check(L.umag_zero_mask(*_comps(dst), _p(_f32(mask, "mask")), _p(regions), dst[0].numel()))
+    Sync()
+
+
 def LLNoPrecess(torque, m, B):
     """opencl/lltorque.go:97"""
     L = _L()

@@ -337,14 +337,21 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
     const int w = tid % WB, t = tid / WB;
+    const int hx = a.Hx, Pz = a.Pz;
+    // The last column block holds only the Nyquist column kx = Hx - 1.  When
+    // Pz is a multiple of WB its CTAs are packed: CTA by < Pz/WB handles that
+    // column for the WB planes kz = by*WB + w (the others exit), so the grid
+    // carries Pz/WB such CTAs instead of Pz mostly idle ones.
+    const bool nyq = bx * WB == hx - 1 && WB > 1 && Pz % WB == 0 && Pz >= WB;
+    if (nyq && by * WB >= Pz) return;
     for (int i = tid; i < PY; i += NT) tw[i] = a.fy.tw[i];
-    const int kx0 = bx * WB, kz = by;
-    const int kx = kx0 + w, hx = a.Hx, Pz = a.Pz;
+    const int kx0 = bx * WB;
+    const int kx = nyq ? hx - 1 : kx0 + w, kz = nyq ? by * WB + w : by;
     // the kernel block this CTA multiplies with: asynchronous copies that
     // complete while the forward transform runs
-    int kzm = kz;
-    float sz = 1.f;
-    if (kz > Pz / 2) { kzm = Pz - kz; sz = -1.f; }
+    auto kz_mirror = [&](int z) { return z > Pz / 2 ? Pz - z : z; };
+    const int kzm = kz_mirror(kz);
+    const float sz = kz > Pz / 2 ? -1.f : 1.f;
     const bool k3d = a.K[3] != nullptr;
     {
         const int ncomp = k3d ? 6 : 4;
@@ -352,7 +359,7 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
         if constexpr (WB % 4 == 0) {
             // 16-byte pieces of 4 columns: plan layouts (pitch padded to 4
             // floats, pad columns zero); blocked pieces are consecutive in ky
-            wide = a.Kp % 4 == 0 && kx0 + WB <= a.Kp;
+            wide = !nyq && a.Kp % 4 == 0 && kx0 + WB <= a.Kp;
             if (wide) {
                 constexpr int CH = WB / 4;
                 for (int e = tid; e < ncomp * HY * CH; e += NT) {
@@ -367,7 +374,8 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
                 const int cc = e / (HY * WB), r = e % (HY * WB), ky = r / WB, ww = r % WB;
                 const int comp = k3d ? cc : (cc == 3 ? 5 : cc);
                 float* dst = Ks + comp * HY * WB + ky * WB + ww;
-                if (kx0 + ww < hx) cpa4(dst, a.K[comp] + kern_idx(a, kzm, ky, kx0 + ww, HY));
+                const int kxw = nyq ? hx - 1 : kx0 + ww, kzw = nyq ? kz_mirror(by * WB + ww) : kzm;
+                if (kxw < hx) cpa4(dst, a.K[comp] + kern_idx(a, kzw, ky, kxw, HY));
                 else *dst = 0.f;
             }
         }

@@ -38,9 +38,9 @@ CONFIG = dict(N=(256, 256, 16), cell=(2e-9, 2e-9, 1e-9), Ms=1.1e6, Aex=1.6e-11, 
 METRIC = "RK45DP cell-updates/s (256x256x16 multilayer, FP32, Newell demag)"
 UNIT = "cell-updates/s"
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_reg_b<512,4> launch on
-# this workload (79,323,136 + 5,381,888 B), from one ncu --set full capture of
+# this workload (79,291,392 + 5,342,208 B), from one ncu --set full capture of
 # that launch (cold cache: ncu flushes the caches between its passes)
-TRAFFIC_B = 84705024
+TRAFFIC_B = 84633600
 
 
 def alg_bytes_per_eval(N):

@@ -236,6 +236,18 @@ def cpu_baseline(config, budget_s=12.0):
 
 
 # ------------------------------------------------------------------ GPU arm
+def combine_ranks(times, counts, dist=None):
+    """The replicas' figures as one job: the slowest rank's time for each
+    timing (max over ranks) and the steps all ranks took (sum), so that the
+    whole-job throughput is every rank's cell-updates over the slowest
+    rank's time.  Every rank calls it; tensors on the process group's
+    device."""
+    if dist is not None:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+        dist.all_reduce(counts, op=dist.ReduceOp.SUM)
+    return times.tolist(), counts.tolist()
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from umagnus_b200 import engine
@@ -309,13 +321,9 @@ def run_ours(args, rank, world, local_rank):
     acc_e2e = s_now["nsteps"] - s_before["nsteps"]
     steps_e2e = chunks * graph_steps
     bytes_state = 88
-    times = torch.tensor([ms, ms_eval, t_e2e], dtype=torch.float64, device="cuda")
-    accs = torch.tensor([acc, acc_e2e], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-        dist.all_reduce(accs, op=dist.ReduceOp.SUM)
-    ms_max, ms_eval_max, t_e2e_max = times.tolist()
-    acc_tot, acc_e2e_tot = accs.tolist()
+    (ms_max, ms_eval_max, t_e2e_max), (acc_tot, acc_e2e_tot) = combine_ranks(
+        torch.tensor([ms, ms_eval, t_e2e], dtype=torch.float64, device="cuda"),
+        torch.tensor([acc, acc_e2e], dtype=torch.float64, device="cuda"), dist)
     result = None
     if rank == 0:
         peak, peak_kind = measured_peak()

@@ -1,0 +1,55 @@
+"""The benchmark's multi-GPU bookkeeping (replicas, one process per GPU) on
+CPU ranks over gloo: timings reduce to the slowest rank, step counts to
+their sum, so the whole-job throughput is all ranks' cell-updates over the
+slowest rank's time; every rank takes the same collective steps."""
+import os
+import socket
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        import bench
+        times = torch.tensor([10.0 + rank, 2.0 - 0.5 * rank, 3.0 * (rank + 1)], dtype=torch.float64)
+        counts = torch.tensor([100.0 + rank, 7.0], dtype=torch.float64)
+        t, c = bench.combine_ranks(times, counts, dist)
+        dist.barrier()
+        out.put((rank, t, c))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_combine_ranks_gloo(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, t, c in res:
+        assert t == [10.0 + world - 1, 2.0, 3.0 * world]
+        assert c == [100.0 * world + sum(range(world)), 7.0 * world]
+
+
+def test_combine_ranks_single_process():
+    import bench
+    t, c = bench.combine_ranks(torch.tensor([1.5, 2.5]), torch.tensor([4.0]), None)
+    assert t == [1.5, 2.5] and c == [4.0]

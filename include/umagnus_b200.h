@@ -82,6 +82,19 @@ int umag_add_uniaxial_anisotropy2(float* Bx, float* By, float* Bz, const float* 
                                   const float* K1, float K1_mul, const float* K2, float K2_mul,
                                   const float* ux, float ux_mul, const float* uy, float uy_mul,
                                   const float* uz, float uz_mul, int N);
+/* opencl/dmibulk.go AddDMIBulk (dmibulk.cl): exchange + bulk DMI, boundary
+ * extrapolation of missing neighbours in x, y and z. */
+int umag_add_dmi_bulk(float* Hx, float* Hy, float* Hz, const float* mx, const float* my,
+                      const float* mz, const float* Ms, float Ms_mul, const float* aLUT2d,
+                      const float* dLUT2d, const uint8_t* regions, int Nx, int Ny, int Nz, double cx,
+                      double cy, double cz, int pbc, int openbc);
+/* opencl/anisotropy.go AddCubicAnisotropy2 (cubicanisotropy2.cl): Kc1, Kc2,
+ * Kc3 with axes c1, c2 (c3 = c1 x c2), each as (array or NULL, multiplier). */
+int umag_add_cubic_anisotropy2(float* Bx, float* By, float* Bz, const float* mx, const float* my,
+                               const float* mz, const float* Ms, float Ms_mul, const float* K1,
+                               float K1_mul, const float* K2, float K2_mul, const float* K3, float K3_mul,
+                               const float* const c1[3], const float c1_mul[3],
+                               const float* const c2[3], const float c2_mul[3], int N);
 /* opencl/region.go:13 RegionAddV (regionaddv.cl): dst += LUT[region]. */
 int umag_region_addv(float* dx, float* dy, float* dz, const float* lutx, const float* luty,
                      const float* lutz, const uint8_t* regions, int N);
@@ -212,6 +225,16 @@ typedef struct {
     double demag_accuracy;         /* brute force: DemagAccuracy (engine/demag.go:25); <= 0 -> 6 */
     const float* frozen_lut;       /* FrozenSpins per region (256 floats, device) or NULL
                                       (engine/torque.go:348-352: torque zeroed where != 0) */
+    /* cubic anisotropy (engine/anisotropy.go:14-19, :54-74): Kc1..Kc3 and the
+     * axes anisC1, anisC2, each (array or NULL, multiplier); off when all
+     * three constants are zero */
+    const float* Kc1; float Kc1_mul;
+    const float* Kc2; float Kc2_mul;
+    const float* Kc3; float Kc3_mul;
+    const float* anisC1[3]; float anisC1_mul[3];
+    const float* anisC2[3]; float anisC2_mul[3];
+    const float* dbulkLUT;         /* bulk DMI LUT (engine/exchange.go:49-66 Dbulk) or NULL;
+                                      exclusive with dLUT */
 } umag_sim_params;
 
 /* Solver knobs, engine/run.go:14-43 (defaults by umag_solver_defaults). */

@@ -22,7 +22,7 @@ KS = os.path.join(REF, "kernels_src")
 
 HEADERS = ["typedefs.clh", "constants.clh", "stencil.clh", "float3.clh", "exchange.clh", "amul.clh"]
 KERNELS = ["copypadmul2", "copyunpad", "kernmulrsymm3d", "kernmulrsymm2dxy", "kernmulrsymm2dz",
-           "exchange", "dmi", "uniaxialanisotropy2", "regionaddv", "regiondecode", "lltorque2",
+           "exchange", "dmi", "dmibulk", "uniaxialanisotropy2", "cubicanisotropy2", "regionaddv", "regiondecode", "lltorque2",
            "llnoprecess", "madd2", "madd3", "madd4", "madd5", "madd6", "madd7", "normalize2",
            "vecnorm", "div", "dotproduct"]
 
@@ -43,6 +43,15 @@ WRAPPERS = [
                                " R* K2, R K2_mul, R* ux, R ux_mul, R* uy, R uy_mul, R* uz, R uz_mul, int N",
      "adduniaxialanisotropy2(Bx, By, Bz, mx, my, mz, Ms, Ms_mul, K1, K1_mul, K2, K2_mul, ux, ux_mul,"
      " uy, uy_mul, uz, uz_mul, N)", "1d:N"),
+    ("adddmibulk", f"R* Hx, R* Hy, R* Hz, R* mx, R* my, R* mz, R* Ms, R Ms_mul, R* aLUT, R* dLUT, uint8_t* regions,"
+                   f" R cx, R cy, R cz, int Nx, int Ny, int Nz, int pbc, int openbc",
+     "adddmibulk(Hx, Hy, Hz, mx, my, mz, Ms, Ms_mul, aLUT, dLUT, regions, cx, cy, cz, Nx, Ny, Nz,"
+     " (uint8_t)pbc, (uint8_t)openbc)", "3d:Nx,Ny,Nz"),
+    ("addcubicanisotropy2", "R* Bx, R* By, R* Bz, R* mx, R* my, R* mz, R* Ms, R Ms_mul, R* K1, R K1_mul,"
+                            " R* K2, R K2_mul, R* K3, R K3_mul, R* c1x, R c1x_mul, R* c1y, R c1y_mul, R* c1z,"
+                            " R c1z_mul, R* c2x, R c2x_mul, R* c2y, R c2y_mul, R* c2z, R c2z_mul, int N",
+     "addcubicanisotropy2(Bx, By, Bz, mx, my, mz, Ms, Ms_mul, K1, K1_mul, K2, K2_mul, K3, K3_mul, c1x, c1x_mul,"
+     " c1y, c1y_mul, c1z, c1z_mul, c2x, c2x_mul, c2y, c2y_mul, c2z, c2z_mul, N)", "1d:N"),
     ("regionaddv", "R* dx, R* dy, R* dz, R* lx, R* ly, R* lz, uint8_t* regions, int N",
      "regionaddv(dx, dy, dz, lx, ly, lz, regions, N)", "1d:N"),
     ("regiondecode", "R* dst, R* lut, uint8_t* regions, int N", "regiondecode(dst, lut, regions, N)", "1d:N"),

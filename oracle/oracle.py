@@ -48,6 +48,11 @@ class OrcSystem(ctypes.Structure):
         ("enable_demag", ctypes.c_int), ("dmi", ctypes.c_int), ("openbc", ctypes.c_int),
         ("precess", ctypes.c_int), ("anis", ctypes.c_int),
         ("Kf", f64p * 6), ("P", ctypes.c_int * 3),
+        ("Kc1", ctypes.c_void_p), ("Kc2", ctypes.c_void_p), ("Kc3", ctypes.c_void_p),
+        ("c1", ctypes.c_void_p * 3), ("c2", ctypes.c_void_p * 3),
+        ("Kc1_mul", ctypes.c_double), ("Kc2_mul", ctypes.c_double), ("Kc3_mul", ctypes.c_double),
+        ("c1_mul", ctypes.c_double * 3), ("c2_mul", ctypes.c_double * 3),
+        ("cubic", ctypes.c_int), ("dbLUT", ctypes.c_void_p),
     ]
 
 
@@ -239,6 +244,45 @@ def add_uniaxial(B, m, Ms, K1, K2, u):
         uarr, umul, n)
 
 
+def add_cubic(B, m, Ms, K1, K2, K3, c1, c2):
+    """kernels_src/cl/cubicanisotropy2.cl; Ms/K1/K2/K3 scalar or per-cell
+    arrays, c1/c2 3-vectors or (3, ...) arrays."""
+    dt = B.dtype
+    S = _scal(dt)
+    n = m[0].size
+    P = f32p if dt == np.float32 else f64p
+
+    def ms(v):
+        return (None, float(v)) if np.isscalar(v) else (_c(v, dt).ravel(), 1.0)
+
+    def vec(u):
+        if np.asarray(u).ndim == 1:
+            return (P * 3)(None, None, None), (S * 3)(*[float(x) for x in u]), []
+        arrs = [_c(u[c], dt).ravel() for c in range(3)]
+        return (P * 3)(*[_ptr(a) for a in arrs]), (S * 3)(1.0, 1.0, 1.0), arrs
+
+    Msa, Msm = ms(Ms)
+    K1a, K1m = ms(K1)
+    K2a, K2m = ms(K2)
+    K3a, K3m = ms(K3)
+    c1p, c1m, keep1 = vec(c1)
+    c2p, c2m, keep2 = vec(c2)
+    getattr(lib(), f"orc_add_cubic2_{_sfx(dt)}")(
+        _arr3(list(B)), _arr3(list(m)), _ptr(Msa), S(Msm), _ptr(K1a), S(K1m), _ptr(K2a), S(K2m), _ptr(K3a), S(K3m),
+        c1p, c1m, c2p, c2m, n)
+
+
+def add_dmibulk(B, m, aLUT, dLUT, regions, cell, Ms, pbc=0, openbc=0):
+    """kernels_src/cl/dmibulk.cl: exchange + bulk DMI."""
+    dt = B.dtype
+    S = _scal(dt)
+    Nz, Ny, Nx = m.shape[1:]
+    ms_arr, ms_mul = (None, float(Ms)) if np.isscalar(Ms) else (_c(Ms, dt), 1.0)
+    getattr(lib(), f"orc_add_dmibulk_{_sfx(dt)}")(
+        _arr3(list(B)), _arr3(list(m)), _ptr(ms_arr), S(ms_mul), _ptr(_c(aLUT, dt)), _ptr(_c(dLUT, dt)),
+        _ptr(_c(regions, np.uint8)), S(cell[0]), S(cell[1]), S(cell[2]), Nx, Ny, Nz, pbc, openbc)
+
+
 def region_addv(B, lut, regions):
     dt = B.dtype
     getattr(lib(), f"orc_region_addv_{_sfx(dt)}")(
@@ -327,7 +371,8 @@ class Simulation:
     def __init__(self, N, cell, Ms, Aex, alpha, dtype=np.float32, pbc=(0, 0, 0), Dind=0.0,
                  Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None, regions=None, vol=None,
                  Aex_regions=None, Dind_regions=None, Bext_regions=None, demag=True, openbc=False,
-                 precess=True, solver=5, kernel=None, round_kernel_f32=False):
+                 precess=True, solver=5, kernel=None, round_kernel_f32=False, Kc1=0.0, Kc2=0.0, Kc3=0.0,
+                 anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0, Dbulk_regions=None):
         self.dtype = np.dtype(dtype)
         self.N = tuple(N)
         self.ncell = N[0] * N[1] * N[2]
@@ -335,7 +380,8 @@ class Simulation:
         # the material as given, for the energy restatement (energies())
         self.cfg = dict(cell=tuple(cell), Ms=Ms, Aex=Aex, Dind=Dind, Ku1=Ku1, Ku2=Ku2, anisU=anisU, B_ext=B_ext,
                         vol=vol, Aex_regions=Aex_regions, Dind_regions=Dind_regions, Bext_regions=Bext_regions,
-                        demag=demag, openbc=openbc)
+                        demag=demag, openbc=openbc, Kc1=Kc1, Kc2=Kc2, Kc3=Kc3, anisC1=anisC1, anisC2=anisC2,
+                        Dbulk=Dbulk, Dbulk_regions=Dbulk_regions)
         s = OrcSystem()
         s.N[:] = N
         s.pbc[:] = pbc
@@ -362,6 +408,18 @@ class Simulation:
             for c in range(3):
                 s.u[c], s.u_mul[c] = param(anisU[c])
         s.anis = int(not (np.all(np.asarray(Ku1) == 0) and np.all(np.asarray(Ku2) == 0)))
+        s.Kc1, s.Kc1_mul = param(Kc1)
+        s.Kc2, s.Kc2_mul = param(Kc2)
+        s.Kc3, s.Kc3_mul = param(Kc3)
+        for name, val in (("c1", anisC1), ("c2", anisC2)):
+            ptrs, muls = getattr(s, name), getattr(s, name + "_mul")
+            if np.asarray(val).ndim == 1:
+                for c in range(3):
+                    ptrs[c], muls[c] = None, float(val[c])
+            else:
+                for c in range(3):
+                    ptrs[c], muls[c] = param(val[c])
+        s.cubic = int(not all(np.all(np.asarray(k) == 0) for k in (Kc1, Kc2, Kc3)))
         self.vol = None
         if vol is not None:
             self.vol = _c(vol, self.dtype).ravel()
@@ -375,6 +433,10 @@ class Simulation:
         din = np.full(256, Dind, dtype=self.dtype) if Dind_regions is None else _c(Dind_regions, self.dtype)
         self.dLUT = exch_lut(din, dtype=self.dtype)
         s.dLUT = _vp(self.dLUT)
+        dbk = np.full(256, Dbulk, dtype=self.dtype) if Dbulk_regions is None else _c(Dbulk_regions, self.dtype)
+        if np.any(dbk != 0):
+            self.dbLUT = exch_lut(dbk, dtype=self.dtype)
+            s.dbLUT = _vp(self.dbLUT)
         s.openbc = int(openbc)
         s.precess = int(precess)
         # Zeeman LUT (engine/excitation.go:41-53)
@@ -465,7 +527,10 @@ def energies(sim, m=None):
     alut = exch_lut(aex, dtype=f8)
     Be = np.zeros_like(m)
     din = np.full(256, c["Dind"], f8) if c["Dind_regions"] is None else np.asarray(c["Dind_regions"], f8)
-    if np.any(din != 0):
+    dbk = np.full(256, c["Dbulk"], f8) if c["Dbulk_regions"] is None else np.asarray(c["Dbulk_regions"], f8)
+    if np.any(dbk != 0):
+        add_dmibulk(Be, m, alut, exch_lut(dbk, dtype=f8), regions, cell, Ms, 0, int(c["openbc"]))
+    elif np.any(din != 0):
         add_dmi(Be, m, alut, exch_lut(din, dtype=f8), regions, cell, Ms, 0, int(c["openbc"]))
     else:
         add_exchange(Be, m, alut, regions, cell, Ms)
@@ -477,6 +542,13 @@ def energies(sim, m=None):
         B2 = np.zeros_like(m)
         add_uniaxial(B2, m, Ms, 0.0, c["Ku2"], c["anisU"])
         Ea = V * float(np.sum(-0.5 * np.sum(Mf * B1, axis=0) - 0.25 * np.sum(Mf * B2, axis=0)))
+    if not all(np.all(np.asarray(c[k]) == 0) for k in ("Kc1", "Kc2", "Kc3")):
+        # engine/anisotropy.go:191-206: -1/4, -1/6, -1/8 of M_full.B of each constant alone
+        for k, pre in (("Kc1", -0.25), ("Kc2", -1.0 / 6.0), ("Kc3", -0.125)):
+            Ks = [c[k] if j == k else 0.0 for j in ("Kc1", "Kc2", "Kc3")]
+            Bc = np.zeros_like(m)
+            add_cubic(Bc, m, Ms, Ks[0], Ks[1], Ks[2], np.asarray(c["anisC1"], f8), np.asarray(c["anisC2"], f8))
+            Ea += V * pre * float(np.sum(Mf * Bc))
     E["anisotropy"] = Ea
     Ez = 0.0
     if c["Bext_regions"] is not None or c["B_ext"] is not None:

@@ -79,6 +79,12 @@ void orc_add_dmi_##S(R* H[3], R* const m[3], const R* Ms, R Ms_mul, const R* aLU
 void orc_add_uniaxial2_##S(R* B[3], R* const m[3], const R* Ms, R Ms_mul, const R* K1,        \
                            R K1_mul, const R* K2, R K2_mul, R* const u[3],                    \
                            const R u_mul[3], int N);                                          \
+void orc_add_cubic2_##S(R* B[3], R* const m[3], const R* Ms, R Ms_mul, const R* K1, R K1_mul,  \
+                        const R* K2, R K2_mul, const R* K3, R K3_mul, R* const c1[3],          \
+                        const R c1_mul[3], R* const c2[3], const R c2_mul[3], int N);          \
+void orc_add_dmibulk_##S(R* H[3], R* const m[3], const R* Ms, R Ms_mul, const R* aLUT2d,      \
+                         const R* dLUT2d, const uint8_t* regions, R cx, R cy, R cz, int Nx,   \
+                         int Ny, int Nz, int pbc, int openbc);                                \
 void orc_region_addv_##S(R* dst[3], R* const lut[3], const uint8_t* regions, int N);          \
 void orc_region_decode_##S(R* dst, const R* lut, const uint8_t* regions, int N);              \
 void orc_lltorque_##S(R* t[3], R* const m[3], R* const h[3], const R* alpha, R alpha_mul,     \
@@ -118,6 +124,11 @@ typedef struct {
     int enable_demag, dmi, openbc, precess, anis;
     double* Kf[6];                /* kernel spectrum (orc_kernel_spectrum) */
     int P[3];
+    /* cubic anisotropy (engine/anisotropy.go:54-74) and bulk DMI (engine/exchange.go:60-61) */
+    const void *Kc1, *Kc2, *Kc3, *c1[3], *c2[3];
+    double Kc1_mul, Kc2_mul, Kc3_mul, c1_mul[3], c2_mul[3];
+    int cubic;
+    const void* dbLUT;            /* 32896-entry bulk DMI LUT or NULL */
 } orc_system;
 
 typedef struct {

@@ -82,6 +82,54 @@ def test_local_terms_bitexact_without_demag(eng):
     g.free()
 
 
+@pytest.mark.parametrize("case", ["cubic_uniform", "cubic_map_bulk_dmi", "bulk_dmi_regions"])
+def test_cubic_and_bulk_dmi_bitexact_without_demag(eng, case):
+    """Cubic anisotropy (engine/anisotropy.go:54-74) and bulk DMI
+    (engine/exchange.go:60-61) in the engine's torque: bit-identical to the
+    oracle, whose kernels are bit-identical to the reference's."""
+    N, cell = (20, 14, 4), (2e-9, 2.5e-9, 1.5e-9)
+    rng = np.random.default_rng(12)
+    shape = (N[2], N[1], N[0])
+    kw = dict(Ku1=2e5, anisU=(0.3, 0.1, 1.0), B_ext=(0.01, -0.02, 0.05))
+    if case == "cubic_uniform":
+        kw.update(Kc1=4.5e4, Kc2=-1.2e4, Kc3=3e3, anisC1=(1.0, 0.2, 0.0), anisC2=(-0.2, 1.0, 0.1))
+    elif case == "cubic_map_bulk_dmi":
+        kw.update(Kc1=(rng.random(shape) * 5e4).astype(np.float32), Kc2=2e4,
+                  anisC1=rng.standard_normal((3,) + shape).astype(np.float32), anisC2=(0.0, 1.0, 0.0),
+                  Dbulk=1.5e-3)
+    else:
+        kw.update(Dbulk=[2e-3, -1e-3], regions=rng.integers(0, 2, size=shape).astype(np.uint8))
+    okw = dict(kw)
+    if "regions" in kw and not np.isscalar(kw["Dbulk"]):
+        dbk = np.zeros(256)
+        dbk[:2] = kw["Dbulk"]
+        okw.pop("Dbulk")
+        okw["Dbulk_regions"] = dbk
+    g = eng.Simulation(N, cell, 9e5, 1.2e-11, 0.1, demag=False, **kw)
+    o = O.Simulation(N, cell, 9e5, 1.2e-11, 0.1, demag=False, **okw)
+    m = G.random_unit(N, 5)
+    g.set_m(m)
+    o.set_m(m)
+    t, b = g.torque(beff=True)
+    to, bo = o.torque(beff=True)
+    assert np.array_equal(b.cpu().numpy(), bo)
+    assert np.array_equal(t.cpu().numpy(), to)
+    E = g.energies()
+    Eo = O.energies(o, o.m)
+    scale = sum(abs(Eo[k]) for k in ("exchange", "anisotropy", "zeeman"))
+    for k in ("exchange", "anisotropy", "zeeman", "total"):
+        assert abs(E[k] - Eo[k]) <= 1e-5 * scale, (k, E[k], Eo[k])
+    V = cell[0] * cell[1] * cell[2]
+    assert float(g.energy_density().double().sum()) * V == pytest.approx(E["total"], rel=1e-5, abs=1e-9 * scale)
+    g.free()
+
+
+def test_interfacial_and_bulk_dmi_are_exclusive(eng):
+    from umagnus_b200._lib import UmagError
+    with pytest.raises(UmagError):
+        eng.Simulation((8, 8, 1), (2e-9, 2e-9, 2e-9), 8e5, 1e-11, 0.1, Dind=1e-3, Dbulk=1e-3)
+
+
 @pytest.mark.parametrize("solver", [2, 3, 4, 5])
 def test_fixed_step_trajectory(eng, solver):
     p = thin_film()

@@ -90,6 +90,42 @@ def test_uniaxial_zeeman_torque_bitexact(cl):
     assert np.array_equal(t2.cpu().numpy(), O.llnoprecess(m, want))
 
 
+@pytest.mark.parametrize("N,pbc,openbc", [((13, 9, 4), 0, 0), ((16, 16, 1), 0, 1), ((7, 5, 3), 5, 0)])
+def test_dmibulk_bitexact(cl, N, pbc, openbc):
+    """opencl/dmibulk.go AddDMIBulk (dmibulk.cl) against the oracle (itself
+    bit-identical to the reference kernel)."""
+    m, regions, aex, dind = _setup(N)
+    cell = (2e-9, 3e-9, 1e-9)
+    Ms = (np.float32(8e5) + np.arange(m[0].size, dtype=np.float32)).reshape(m[0].shape)
+    want = np.random.default_rng(1).standard_normal(m.shape).astype(np.float32)
+    B = cu(want.copy())
+    O.add_dmibulk(want, m, aex, dind, regions, cell, Ms, pbc=pbc, openbc=openbc)
+    mesh = cl.Mesh(N, cell, (pbc & 1, (pbc >> 1) & 1, (pbc >> 2) & 1))
+    cl.AddDMIBulk(B, cu(m), cu(aex), cu(dind), cl.MSlice(cu(Ms)), cu(regions), mesh, OpenBC=bool(openbc))
+    assert np.array_equal(B.cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("per_cell", [False, True])
+def test_cubic_bitexact(cl, per_cell):
+    """opencl/anisotropy.go AddCubicAnisotropy2 (cubicanisotropy2.cl)."""
+    N = (31, 17, 5)
+    m, _, _, _ = _setup(N)
+    rng = np.random.default_rng(6)
+    if per_cell:
+        c1 = rng.standard_normal((3,) + m.shape[1:]).astype(np.float32)
+        c2 = rng.standard_normal((3,) + m.shape[1:]).astype(np.float32)
+        K1 = (rng.random(m.shape[1:]) * 5e5).astype(np.float32)
+        gc1, gc2, gK1 = cu(c1), cu(c2), cl.MSlice(cu(K1))
+    else:
+        c1, c2, K1 = (1.0, 0.2, 0.1), (-0.1, 1.0, 0.3), 4.5e4
+        gc1, gc2, gK1 = c1, c2, K1
+    want = rng.standard_normal(m.shape).astype(np.float32)
+    B = cu(want.copy())
+    O.add_cubic(want, m, 1.1e6, K1, -2e4, 7e3, np.asarray(c1), np.asarray(c2))
+    cl.AddCubicAnisotropy2(B, cu(m), 1.1e6, gK1, -2e4, 7e3, gc1, gc2)
+    assert np.array_equal(B.cpu().numpy(), want)
+
+
 def test_zero_mask(cl):
     """opencl/zeromask.go:12 ZeroMask: zero where the region's LUT entry is non-zero."""
     N = (19, 11, 3)

@@ -76,6 +76,51 @@ def test_uniaxial_bitexact(dtype):
 
 
 @pytest.mark.parametrize("dtype", DT)
+@pytest.mark.parametrize("N,pbc,openbc", [((13, 9, 4), 0, 0), ((16, 16, 1), 0, 1), ((7, 5, 3), 5, 0),
+                                          ((6, 7, 4), 0, 1)])
+def test_dmibulk_bitexact(dtype, N, pbc, openbc):
+    m, regions, alut, dlut = _setup(N, dtype)
+    cell = (2e-9, 3e-9, 1e-9)
+    Ms = dtype(8e5) + np.arange(m[0].size, dtype=dtype).reshape(m[0].shape)
+    B1 = np.random.default_rng(1).standard_normal(m.shape).astype(dtype)
+    B2 = B1.copy()
+    O.add_dmibulk(B1, m, alut, dlut, regions, cell, Ms, pbc=pbc, openbc=openbc)
+    clref.call("adddmibulk", dtype, B2[0], B2[1], B2[2], m[0], m[1], m[2], Ms, 1.0, alut, dlut, regions,
+               float(dtype(cell[0])), float(dtype(cell[1])), float(dtype(cell[2])), N[0], N[1], N[2], pbc, openbc)
+    assert np.array_equal(B1, B2, equal_nan=True)
+
+
+@pytest.mark.parametrize("dtype", DT)
+@pytest.mark.parametrize("per_cell", [False, True])
+def test_cubic_bitexact(dtype, per_cell):
+    N = (11, 7, 3)
+    m, _, _, _ = _setup(N, dtype)
+    rng = np.random.default_rng(6)
+    if per_cell:
+        c1 = rng.standard_normal((3,) + m.shape[1:]).astype(dtype)
+        c2 = rng.standard_normal((3,) + m.shape[1:]).astype(dtype)
+        K1 = (rng.random(m.shape[1:]) * 5e5).astype(dtype)
+    else:
+        c1 = np.array([1.0, 0.2, 0.1])
+        c2 = np.array([-0.1, 1.0, 0.3])
+        K1 = 4.5e4
+    B1 = rng.standard_normal(m.shape).astype(dtype)
+    B2 = B1.copy()
+    O.add_cubic(B1, m, 1.1e6, K1, -2e4, 7e3, c1, c2)
+    n = m[0].size
+    if per_cell:
+        cargs = [c1[0], 1.0, c1[1], 1.0, c1[2], 1.0, c2[0], 1.0, c2[1], 1.0, c2[2], 1.0]
+        kargs = [K1, 1.0]
+    else:
+        cargs = [None, float(c1[0]), None, float(c1[1]), None, float(c1[2]),
+                 None, float(c2[0]), None, float(c2[1]), None, float(c2[2])]
+        kargs = [None, 4.5e4]
+    clref.call("addcubicanisotropy2", dtype, B2[0], B2[1], B2[2], m[0], m[1], m[2], None, 1.1e6, *kargs,
+               None, -2e4, None, 7e3, *cargs, n)
+    assert np.array_equal(B1, B2)
+
+
+@pytest.mark.parametrize("dtype", DT)
 def test_torque_zeeman_madd_normalize_bitexact(dtype):
     N = (9, 8, 2)
     n = N[0] * N[1] * N[2]

@@ -30,6 +30,9 @@ class SimParams(ctypes.Structure):
         ("aLUT", P), ("dLUT", P), ("bextLUT", P * 3),
         ("enable_demag", c_int), ("openbc", c_int), ("precess", c_int), ("asymptotic_radius", c_int),
         ("demag_kernel", c_int), ("demag_accuracy", c_double), ("frozen_lut", P),
+        ("Kc1", P), ("Kc1_mul", c_float), ("Kc2", P), ("Kc2_mul", c_float), ("Kc3", P), ("Kc3_mul", c_float),
+        ("anisC1", P * 3), ("anisC1_mul", c_float * 3), ("anisC2", P * 3), ("anisC2_mul", c_float * 3),
+        ("dbulkLUT", P),
     ]
 
 
@@ -70,6 +73,10 @@ _SIGS = {
                      c_int],
     "umag_add_uniaxial_anisotropy2": [P, P, P, P, P, P, P, c_float, P, c_float, P, c_float, P, c_float, P, c_float, P,
                                       c_float, c_int],
+    "umag_add_dmi_bulk": [P, P, P, P, P, P, P, c_float, P, P, P, c_int, c_int, c_int, c_double, c_double, c_double,
+                          c_int, c_int],
+    "umag_add_cubic_anisotropy2": [P, P, P, P, P, P, P, c_float, P, c_float, P, c_float, P, c_float, P, P, P, P,
+                                   c_int],
     "umag_region_addv": [P, P, P, P, P, P, P, c_int], "umag_region_decode": [P, P, P, c_int],
     "umag_zero_mask": [P, P, P, P, P, c_int],
     "umag_lltorque": [P, P, P, P, P, P, P, P, P, P, c_float, c_int],

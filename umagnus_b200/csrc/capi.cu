@@ -74,6 +74,21 @@ int umag_add_uniaxial_anisotropy2(float* Bx, float* By, float* Bz, const float* 
     UniaxParams p{Ms, K1, K2, ux, uy, uz, Ms_mul, K1_mul, K2_mul, ux_mul, uy_mul, uz_mul};
     return add_uniaxial(Bx, By, Bz, mx, my, mz, p, N);
 }
+int umag_add_dmi_bulk(float* Hx, float* Hy, float* Hz, const float* mx, const float* my, const float* mz,
+                      const float* Ms, float Ms_mul, const float* aLUT2d, const float* dLUT2d, const uint8_t* regions,
+                      int Nx, int Ny, int Nz, double cx, double cy, double cz, int pbc, int openbc) {
+    return add_dmibulk(Hx, Hy, Hz, mx, my, mz, Ms, Ms_mul, aLUT2d, dLUT2d, regions, Nx, Ny, Nz, cx, cy, cz, pbc,
+                       openbc);
+}
+int umag_add_cubic_anisotropy2(float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
+                               const float* Ms, float Ms_mul, const float* K1, float K1_mul, const float* K2,
+                               float K2_mul, const float* K3, float K3_mul, const float* const c1[3],
+                               const float c1_mul[3], const float* const c2[3], const float c2_mul[3], int N) {
+    UMAG_REQUIRE(c1 && c1_mul && c2 && c2_mul, "NULL axis arguments");
+    CubicParams p{Ms, K1, K2, K3, {c1[0], c1[1], c1[2]}, {c2[0], c2[1], c2[2]}, Ms_mul, K1_mul, K2_mul, K3_mul,
+                  {c1_mul[0], c1_mul[1], c1_mul[2]}, {c2_mul[0], c2_mul[1], c2_mul[2]}};
+    return add_cubic(Bx, By, Bz, mx, my, mz, p, N);
+}
 int umag_region_addv(float* dx, float* dy, float* dz, const float* lx, const float* ly, const float* lz,
                      const uint8_t* regions, int N) {
     return region_addv(dx, dy, dz, lx, ly, lz, regions, N);

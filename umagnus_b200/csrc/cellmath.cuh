@@ -353,6 +353,119 @@ __device__ __forceinline__ void add_uniaxial(f3& B, const UniaxParams& p, f3 m, 
     B.z = fa(B.z, fa(fm(f1, u.z), fm(f2, u.z)));
 }
 
+// cubicanisotropy2.cl:10-58 -- cubic anisotropy field of cell i added to B
+struct CubicParams {
+    const float *Ms, *K1, *K2, *K3, *c1[3], *c2[3];
+    float Ms_mul, K1_mul, K2_mul, K3_mul, c1_mul[3], c2_mul[3];
+};
+// float3.clh:18-21 normalized() of amul.clh:10-15 vmul()
+__device__ __forceinline__ f3 normalized_vmul(const float* const v[3], const float mul[3], int i) {
+    f3 a{amul(v[0], mul[0], i), amul(v[1], mul[1], i), amul(v[2], mul[2], i)};
+    float len = __fsqrt_rn(dot3(a, a));
+    float il = (len != 0.0f) ? fd(1.0f, len) : 0.0f;
+    return f3{fm(il, a.x), fm(il, a.y), fm(il, a.z)};
+}
+__device__ __forceinline__ float pw4(float x) {  // float3.clh:36-39
+    float s = fm(x, x);
+    return fm(s, s);
+}
+__device__ __forceinline__ void add_cubic(f3& B, const CubicParams& p, f3 m, int i) {
+    const float invMs = inv_msat(p.Ms, p.Ms_mul, i);
+    const float k1 = fm(amul(p.K1, p.K1_mul, i), invMs);
+    const float k2 = fm(amul(p.K2, p.K2_mul, i), invMs);
+    const float k3 = fm(amul(p.K3, p.K3_mul, i), invMs);
+    const f3 u1 = normalized_vmul(p.c1, p.c1_mul, i), u2 = normalized_vmul(p.c2, p.c2_mul, i);
+    const f3 u3 = cross3(u1, u2);
+    const float u1m = dot3(u1, m), u2m = dot3(u2, m), u3m = dot3(u3, m);
+    const float s1 = fm(u1m, u1m), s2 = fm(u2m, u2m), s3 = fm(u3m, u3m);
+    const float a1 = fa(s2, s3), a2 = fa(s1, s3), a3 = fa(s1, s2);
+    const float b1 = fm(s2, s3), b2 = fm(s1, s3), b3 = fm(s1, s2);
+    const float e1 = fa(pw4(u2m), pw4(u3m)), e2 = fa(pw4(u1m), pw4(u3m)), e3 = fa(pw4(u1m), pw4(u2m));
+    const float p1 = fm(s1, u1m), p2 = fm(s2, u2m), p3 = fm(s3, u3m);
+    const float f1 = fm(-2.0f, k1), f2 = fm(2.0f, k2), f3_ = fm(4.0f, k3);
+    const float U1[3] = {u1.x, u1.y, u1.z}, U2[3] = {u2.x, u2.y, u2.z}, U3[3] = {u3.x, u3.y, u3.z};
+    float out[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float S1 = fa(fa(fm(a1, fm(u1m, U1[c])), fm(a2, fm(u2m, U2[c]))), fm(a3, fm(u3m, U3[c])));
+        const float S2 = fa(fa(fm(b1, fm(u1m, U1[c])), fm(b2, fm(u2m, U2[c]))), fm(b3, fm(u3m, U3[c])));
+        const float S3 = fa(fa(fm(e1, fm(p1, U1[c])), fm(e2, fm(p2, U2[c]))), fm(e3, fm(p3, U3[c])));
+        out[c] = fs(fs(fm(f1, S1), fm(f2, S2)), fm(f3_, S3));
+    }
+    B.x = fa(B.x, out[0]);
+    B.y = fa(B.y, out[1]);
+    B.z = fa(B.z, out[2]);
+}
+
+// dmibulk.cl:28-228 -- exchange + bulk DMI of cell (ix, iy, iz) before the
+// 1/Ms factor; missing neighbours extrapolated in all three directions
+__device__ __forceinline__ f3 dmibulk_sum(const float* __restrict__ mx, const float* __restrict__ my,
+                                          const float* __restrict__ mz, const float* __restrict__ aLUT,
+                                          const float* __restrict__ dLUT, const uint8_t* __restrict__ regions,
+                                          float cx, float cy, float cz, Mesh3 g, bool openbc, int ix, int iy,
+                                          int iz, f3 m0, int r0) {
+    f3 h{0.f, 0.f, 0.f};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        if (d == 2 && g.Nz == 1) break;
+        const float c = d == 0 ? cx : (d == 1 ? cy : cz);
+#pragma unroll
+        for (int side = -1; side <= 1; side += 2) {
+            f3 mn{0.f, 0.f, 0.f};
+            int i_;
+            bool inside;
+            if (d == 0) {
+                const int xx = side < 0 ? lclamp(ix - 1, g.Nx, g.pbc & 1) : hclamp(ix + 1, g.Nx, g.pbc & 1);
+                i_ = (iz * g.Ny + iy) * g.Nx + xx;
+                inside = (side < 0 ? ix - 1 >= 0 : ix + 1 < g.Nx) || (g.pbc & 1);
+            } else if (d == 1) {
+                const int yy = side < 0 ? lclamp(iy - 1, g.Ny, g.pbc & 2) : hclamp(iy + 1, g.Ny, g.pbc & 2);
+                i_ = (iz * g.Ny + yy) * g.Nx + ix;
+                inside = (side < 0 ? iy - 1 >= 0 : iy + 1 < g.Ny) || (g.pbc & 2);
+            } else {
+                const int zz = side < 0 ? lclamp(iz - 1, g.Nz, g.pbc & 4) : hclamp(iz + 1, g.Nz, g.pbc & 4);
+                i_ = (zz * g.Ny + iy) * g.Nx + ix;
+                inside = (side < 0 ? iz - 1 >= 0 : iz + 1 < g.Nz) || (g.pbc & 4);
+            }
+            if (inside) mn = ld3(mx, my, mz, i_);
+            const bool missing = is0(mn);
+            const int si = symidx(r0, missing ? r0 : (int)__ldg(regions + i_));
+            const float A = __ldg(aLUT + si), D = __ldg(dLUT + si);
+            const float D_2A = fd(D, fm(2.0f, A));
+            if (!missing || !openbc) {
+                const float sc = side < 0 ? -c : c;
+                if (missing) {
+                    const float q = fm(sc, D_2A);
+                    if (d == 0) {
+                        mn = f3{m0.x, fs(m0.y, fm(q, m0.z)), fa(m0.z, fm(q, m0.y))};
+                    } else if (d == 1) {
+                        mn = f3{fa(m0.x, fm(q, m0.z)), m0.y, fs(m0.z, fm(q, m0.x))};
+                    } else {
+                        mn = f3{fs(m0.x, fm(q, m0.y)), fa(m0.y, fm(q, m0.x)), m0.z};
+                    }
+                }
+                const float s = fd(fm(2.0f, A), fm(c, c));
+                h.x = fa(h.x, fm(s, fs(mn.x, m0.x)));
+                h.y = fa(h.y, fm(s, fs(mn.y, m0.y)));
+                h.z = fa(h.z, fm(s, fs(mn.z, m0.z)));
+                const float Dc = fd(D, c);
+                const f3 t = side < 0 ? f3{-mn.x, -mn.y, -mn.z} : mn;
+                if (d == 0) {
+                    h.y = fa(h.y, fm(Dc, t.z));
+                    h.z = fs(h.z, fm(Dc, t.y));
+                } else if (d == 1) {
+                    h.x = fs(h.x, fm(Dc, t.z));
+                    h.z = fa(h.z, fm(Dc, t.x));
+                } else {
+                    h.x = fa(h.x, fm(Dc, t.y));
+                    h.y = fs(h.y, fm(Dc, t.x));
+                }
+            }
+        }
+    }
+    return h;
+}
+
 // lltorque2.cl:13-23
 __device__ __forceinline__ f3 lltorque(f3 m, f3 H, float alpha) {
     f3 mxH = cross3(m, H);

@@ -78,6 +78,9 @@ struct LocalArgs {
     float wx, wy, wz, cx, cy, cz;
     int dmi, openbc, anis, zeeman, precess;
     const float* frozen;  // FrozenSpins LUT (256) or NULL
+    int cubic;            // cubic anisotropy on (cp)
+    CubicParams cp;
+    const float* dbLUT;   // bulk DMI LUT or NULL
     int ms_uniform, alpha_uniform, anis_uniform;
     DmiPairLut dl;
     LocalConsts kc;
@@ -179,7 +182,10 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
     f3 m0 = ld3(mx, my, mz, I);
     if (!is0(m0)) {
         f3 e;
-        if constexpr (UREG) {
+        if (!BAT && a.dbLUT) {  // engine/exchange.go:60-61 AddDMIBulk
+            e = dmibulk_sum(mx, my, mz, a.aLUT, a.dbLUT, a.regions, a.cx, a.cy, a.cz, a.g, a.openbc != 0, ix, iy,
+                            iz, m0, UREG ? 0 : __ldg(a.regions + I));
+        } else if constexpr (UREG) {
             e = dmi ? dmi_sum_u(mx, my, mz, kc.pc, a.g, a.openbc != 0, ix, iy, iz, m0)
                     : exchange_sum_u(mx, my, mz, kc.pc, a.g, ix, iy, iz, m0);
         } else {
@@ -205,6 +211,7 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
             add_uniaxial(B, a.up, m0, I);
         }
     }
+    if (!BAT && a.cubic) add_cubic(B, a.cp, m0, I);  // engine/anisotropy.go:158
     if (a.zeeman) {
         if constexpr (BAT) {
             B.x = fa(B.x, ip->bext[0]);
@@ -483,10 +490,12 @@ __global__ void k_step_end(DevCtl* c0, int nb, int rk4) {
 // accumulated in FP64 (compensated relative to the reference's float32
 // reduction).  sums: [0] demag, [1] exchange (+DMI), [2] anisotropy from K1
 // alone, [3] anisotropy from K2 alone, [4] Zeeman.
-// the five float32 dot products of cell I: [0] demag, [1] exchange (+DMI),
-// [2] anisotropy from K1 alone, [3] from K2 alone, [4] Zeeman
+// the float32 dot products of cell I: [0] demag, [1] exchange (+DMI),
+// [2] uniaxial anisotropy from K1 alone, [3] from K2 alone, [4] Zeeman,
+// [5..7] cubic anisotropy from Kc1, Kc2, Kc3 alone
+constexpr int kNE = 8;
 __device__ __forceinline__ void energy_cell_terms(const LocalArgs& a, const float* __restrict__ vol, int I,
-                                                  float t[5]) {
+                                                  float t[kNE]) {
     const int N = a.N;
     const float* m = a.ctl->m;
     const float *mx = m, *my = m + N, *mz = m + 2 * N;
@@ -498,11 +507,13 @@ __device__ __forceinline__ void energy_cell_terms(const LocalArgs& a, const floa
         const float w = __ldg(vol + I);
         Mf = f3{fm(Mf.x, w), fm(Mf.y, w), fm(Mf.z, w)};
     }
-    for (int k = 0; k < 5; k++) t[k] = 0.f;
+    for (int k = 0; k < kNE; k++) t[k] = 0.f;
     if (a.bd) t[0] = dot3(Mf, f3{__ldg(a.bd + I), __ldg(a.bd + N + I), __ldg(a.bd + 2 * N + I)});
     if (!is0(m0)) {
         const int r0 = __ldg(a.regions + I);
-        const f3 e = a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
+        const f3 e = a.dbLUT ? dmibulk_sum(mx, my, mz, a.aLUT, a.dbLUT, a.regions, a.cx, a.cy, a.cz, a.g,
+                                           a.openbc != 0, ix, iy, iz, m0, r0)
+                   : a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
                            : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
         const float inv = inv_msat(a.Ms, a.Ms_mul, I);
         t[1] = dot3(Mf, f3{fm(e.x, inv), fm(e.y, inv), fm(e.z, inv)});
@@ -521,25 +532,36 @@ __device__ __forceinline__ void energy_cell_terms(const LocalArgs& a, const floa
         const int r = __ldg(a.regions + I);
         t[4] = dot3(Mf, f3{__ldg(a.bext[0] + r), __ldg(a.bext[1] + r), __ldg(a.bext[2] + r)});
     }
+    if (a.cubic) {  // engine/anisotropy.go:191-206: each constant alone
+        for (int k = 0; k < 3; k++) {
+            CubicParams q = a.cp;
+            if (k != 0) { q.K1 = nullptr; q.K1_mul = 0.f; }
+            if (k != 1) { q.K2 = nullptr; q.K2_mul = 0.f; }
+            if (k != 2) { q.K3 = nullptr; q.K3_mul = 0.f; }
+            f3 Bc{0.f, 0.f, 0.f};
+            add_cubic(Bc, q, m0, I);
+            t[5 + k] = dot3(Mf, Bc);
+        }
+    }
 }
 
 __global__ void __launch_bounds__(256) k_energy_terms(LocalArgs a, const float* __restrict__ vol, double* sums) {
-    __shared__ double sh[5][8];
-    double acc[5] = {0, 0, 0, 0, 0};
+    __shared__ double sh[kNE][8];
+    double acc[kNE] = {};
     for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < a.N; I += gridDim.x * blockDim.x) {
-        float t[5];
+        float t[kNE];
         energy_cell_terms(a, vol, I, t);
-        for (int k = 0; k < 5; k++) acc[k] += (double)t[k];
+        for (int k = 0; k < kNE; k++) acc[k] += (double)t[k];
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-    for (int t = 0; t < 5; t++) {
+    for (int t = 0; t < kNE; t++) {
         double v = acc[t];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) sh[t][wid] = v;
     }
     __syncthreads();
-    if (threadIdx.x < 5) {
+    if (threadIdx.x < kNE) {
         double v = 0;
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sh[threadIdx.x][w];
         atomicAdd(sums + threadIdx.x, v);
@@ -568,7 +590,7 @@ struct SimImpl {
     cudaGraphExec_t gexec = nullptr;   // graph_steps steps
     cudaGraphExec_t gexec1 = nullptr;  // one step
     int launches_per_step = 0;
-    double* esum = nullptr;            // energy term sums (5 doubles)
+    double* esum = nullptr;            // energy term sums (kNE doubles)
     // batched ensemble class: nb same-size instances with uniform parameters
     int nb = 1;
     bool batched = false;
@@ -833,6 +855,8 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
                  "solver must be 2 (Heun), 3 (RK23), 4 (RK4) or 5 (RK45DP)");
     if (p->pbc[0] || p->pbc[1] || p->pbc[2])
         return set_error(UMAG_E_UNSUPPORTED, "periodic boundary conditions are not supported by this build");
+    // engine/exchange.go:62-63
+    UMAG_REQUIRE(!(p->dLUT && p->dbulkLUT), "Cannot have induced and interfacial DMI at the same time");
     SimImpl* s = new SimImpl();
     s->p = *p;
     s->sp = *sp;
@@ -909,6 +933,13 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
     la.alpha_mul = p->alpha_mul;
     la.precess = p->precess;
     la.frozen = p->frozen_lut;
+    la.cubic = (p->Kc1 != nullptr || p->Kc1_mul != 0.f || p->Kc2 != nullptr || p->Kc2_mul != 0.f ||
+                p->Kc3 != nullptr || p->Kc3_mul != 0.f);
+    la.cp = CubicParams{p->Ms, p->Kc1, p->Kc2, p->Kc3, {p->anisC1[0], p->anisC1[1], p->anisC1[2]},
+                        {p->anisC2[0], p->anisC2[1], p->anisC2[2]}, p->Ms_mul, p->Kc1_mul, p->Kc2_mul, p->Kc3_mul,
+                        {p->anisC1_mul[0], p->anisC1_mul[1], p->anisC1_mul[2]},
+                        {p->anisC2_mul[0], p->anisC2_mul[1], p->anisC2_mul[2]}};
+    la.dbLUT = p->dbulkLUT;
     la.Ms = p->Ms;
     la.Ms_mul = p->Ms_mul;
     la.ms_uniform = p->Ms == nullptr;
@@ -1118,12 +1149,17 @@ int sim_torque_evals(umag_sim* h, int n) {
 // zeeman.go:9)
 __global__ void __launch_bounds__(256) k_energy_density(LocalArgs a, const float* __restrict__ vol, float* dst) {
     for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < a.N; I += gridDim.x * blockDim.x) {
-        float t[5];
+        float t[kNE];
         energy_cell_terms(a, vol, I, t);
         float d = 0.0f;
         if (a.anis) {
             d = fa(d, fm(-0.5f, t[2]));
             d = fa(d, fm(-0.25f, t[3]));
+        }
+        if (a.cubic) {
+            d = fa(d, fm(-0.25f, t[5]));
+            d = fa(d, fm((float)(-1. / 6.), t[6]));
+            d = fa(d, fm(-0.125f, t[7]));
         }
         if (a.bd) d = fa(d, fm(-0.5f, t[0]));
         d = fa(d, fm(-0.5f, t[1]));
@@ -1135,7 +1171,7 @@ __global__ void __launch_bounds__(256) k_energy_density(LocalArgs a, const float
 int sim_energies(umag_sim* h, double E[5]) {
     SimImpl* s = reinterpret_cast<SimImpl*>(h);
     UMAG_REQUIRE(s && E, "NULL argument");
-    if (!s->esum) UMAG_CUDA(cudaMalloc(&s->esum, 5 * sizeof(double)));
+    if (!s->esum) UMAG_CUDA(cudaMalloc(&s->esum, kNE * sizeof(double)));
     UMAG_TRY(sync_ctl_to_host(s));
     s->hctl->active = 1;
     UMAG_TRY(push_ctl(s));
@@ -1144,15 +1180,17 @@ int sim_energies(umag_sim* h, double E[5]) {
         a.m_sel = 0;
         UMAG_TRY(demag_launch(s->demag, a, S()));
     }
-    UMAG_CUDA(cudaMemsetAsync(s->esum, 0, 5 * sizeof(double), S()));
+    UMAG_CUDA(cudaMemsetAsync(s->esum, 0, kNE * sizeof(double), S()));
     k_energy_terms<<<grid_for(s->N, 256, 4), 256, 0, S()>>>(s->la, s->p.vol, s->esum);
     UMAG_LAUNCH_CHECK();
-    double t[5];
+    double t[kNE];
     UMAG_CUDA(cudaMemcpyAsync(t, s->esum, sizeof(t), cudaMemcpyDeviceToHost, S()));
     UMAG_CUDA(cudaStreamSynchronize(S()));
     const double V = s->p.cell[0] * s->p.cell[1] * s->p.cell[2];  // engine/energy.go:45-48 cellVolume
     const double Ed = -0.5 * V * t[0], Ee = -0.5 * V * t[1];
-    const double Ea = V * (-0.5 * t[2] - 0.25 * t[3]), Ez = -1.0 * V * t[4];
+    // engine/anisotropy.go:164-206: uniaxial -1/2, -1/4; cubic -1/4, -1/6, -1/8
+    const double Ea = V * (-0.5 * t[2] - 0.25 * t[3] - 0.25 * t[5] - t[6] / 6.0 - 0.125 * t[7]);
+    const double Ez = -1.0 * V * t[4];
     E[1] = Ed; E[2] = Ee; E[3] = Ea; E[4] = Ez;
     // registration order of the terms (files anisotropy, demag, exchange, zeeman)
     E[0] = ((Ea + Ed) + Ee) + Ez;

@@ -111,6 +111,37 @@ __global__ void k_add_dmi(float* __restrict__ Hx, float* __restrict__ Hy, float*
     Hz[I] = fa(Hz[I], fm(h.z, inv));
 }
 
+__global__ void k_add_dmibulk(float* __restrict__ Hx, float* __restrict__ Hy, float* __restrict__ Hz,
+                              const float* __restrict__ mx, const float* __restrict__ my,
+                              const float* __restrict__ mz, const float* __restrict__ Ms, float Ms_mul,
+                              const float* __restrict__ aLUT, const float* __restrict__ dLUT,
+                              const uint8_t* __restrict__ regions, float cx, float cy, float cz, Mesh3 g,
+                              int openbc) {
+    int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    int iz = blockIdx.z;
+    if (ix >= g.Nx || iy >= g.Ny) return;
+    int I = (iz * g.Ny + iy) * g.Nx + ix;
+    f3 m0 = ld3(mx, my, mz, I);
+    if (is0(m0)) return;
+    f3 h = dmibulk_sum(mx, my, mz, aLUT, dLUT, regions, cx, cy, cz, g, openbc != 0, ix, iy, iz, m0,
+                       __ldg(regions + I));
+    float inv = inv_msat(Ms, Ms_mul, I);
+    Hx[I] = fa(Hx[I], fm(h.x, inv));
+    Hy[I] = fa(Hy[I], fm(h.y, inv));
+    Hz[I] = fa(Hz[I], fm(h.z, inv));
+}
+
+__global__ void k_add_cubic(float* __restrict__ Bx, float* __restrict__ By, float* __restrict__ Bz,
+                            const float* __restrict__ mx, const float* __restrict__ my,
+                            const float* __restrict__ mz, CubicParams p, int N) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        f3 B{Bx[i], By[i], Bz[i]};
+        add_cubic(B, p, ld3(mx, my, mz, i), i);
+        Bx[i] = B.x; By[i] = B.y; Bz[i] = B.z;
+    }
+}
+
 __global__ void k_add_uniaxial(float* __restrict__ Bx, float* __restrict__ By, float* __restrict__ Bz,
                                const float* __restrict__ mx, const float* __restrict__ my,
                                const float* __restrict__ mz, UniaxParams p, int N) {
@@ -338,6 +369,30 @@ int add_dmi(float* Hx, float* Hy, float* Hz, const float* mx, const float* my, c
     k_add_dmi<<<grid3d(Nx, Ny, Nz), block3d(), 0, ctx().stream>>>(Hx, Hy, Hz, mx, my, mz, Ms, Ms_mul, aLUT, dLUT,
                                                                   regions, (float)cx, (float)cy, (float)cz,
                                                                   Mesh3{Nx, Ny, Nz, pbc}, openbc);
+    UMAG_LAUNCH_CHECK();
+    return UMAG_OK;
+}
+
+int add_dmibulk(float* Hx, float* Hy, float* Hz, const float* mx, const float* my, const float* mz,
+                const float* Ms, float Ms_mul, const float* aLUT, const float* dLUT, const uint8_t* regions, int Nx,
+                int Ny, int Nz, double cx, double cy, double cz, int pbc, int openbc) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(Hx && Hy && Hz && mx && my && mz && aLUT && dLUT && regions, "NULL argument");
+    UMAG_REQUIRE(Nx > 0 && Ny > 0 && Nz > 0, "bad mesh size");
+    // opencl/dmibulk.go: cell sizes passed as float32
+    k_add_dmibulk<<<grid3d(Nx, Ny, Nz), block3d(), 0, ctx().stream>>>(Hx, Hy, Hz, mx, my, mz, Ms, Ms_mul, aLUT,
+                                                                      dLUT, regions, (float)cx, (float)cy,
+                                                                      (float)cz, Mesh3{Nx, Ny, Nz, pbc}, openbc);
+    UMAG_LAUNCH_CHECK();
+    return UMAG_OK;
+}
+
+int add_cubic(float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
+              const CubicParams& p, int N) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(Bx && By && Bz && mx && my && mz, "NULL argument");
+    if (N <= 0) return UMAG_OK;
+    k_add_cubic<<<grid_for(N, 256), 256, 0, ctx().stream>>>(Bx, By, Bz, mx, my, mz, p, N);
     UMAG_LAUNCH_CHECK();
     return UMAG_OK;
 }

@@ -16,6 +16,11 @@ int add_dmi(float* Hx, float* Hy, float* Hz, const float* mx, const float* my, c
             double cx, double cy, double cz, int pbc, int openbc);
 int add_uniaxial(float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
                  const UniaxParams& p, int N);
+int add_dmibulk(float* Hx, float* Hy, float* Hz, const float* mx, const float* my, const float* mz,
+                const float* Ms, float Ms_mul, const float* aLUT, const float* dLUT, const uint8_t* regions, int Nx,
+                int Ny, int Nz, double cx, double cy, double cz, int pbc, int openbc);
+int add_cubic(float* Bx, float* By, float* Bz, const float* mx, const float* my, const float* mz,
+              const CubicParams& p, int N);
 int region_addv(float* dx, float* dy, float* dz, const float* lx, const float* ly, const float* lz,
                 const uint8_t* regions, int N);
 int region_decode(float* dst, const float* lut, const uint8_t* regions, int N);

@@ -76,13 +76,17 @@ class Simulation:
     per-region; regions: uint8 (Nz, Ny, Nx) map; geom: cell volume fraction;
     demag_kernel: "newell" (EnableNewellDemag) or "brute" (EnableDemag, the
     reference default, with DemagAccuracy = demag_accuracy); FrozenSpins: a
-    scalar or 256 per-region values, the torque is zero where non-zero.
+    scalar or 256 per-region values, the torque is zero where non-zero;
+    Kc1, Kc2, Kc3, anisC1, anisC2: cubic anisotropy (scalars / 3-vectors or
+    per-cell maps); Dbulk: bulk DMI (scalar or 256 per-region values; not
+    together with Dind).
     """
 
     def __init__(self, N, cell, Msat, Aex, alpha, Dind=0.0, Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
                  regions=None, geom=None, demag=True, open_bc=False, precess=True, solver=DORMANDPRINCE,
                  dt=1e-15, MaxErr=1e-5, RelErr=1e-4, MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8,
-                 device=0, asymptotic_radius=32, demag_kernel="newell", demag_accuracy=6.0, FrozenSpins=None):
+                 device=0, asymptotic_radius=32, demag_kernel="newell", demag_accuracy=6.0, FrozenSpins=None,
+                 Kc1=0.0, Kc2=0.0, Kc3=0.0, anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0):
         self.L = _lib.init(device)
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
@@ -117,11 +121,26 @@ class Simulation:
                 p.anisU[c], p.anisU_mul[c] = None, float(np.float32(u[c]))
             else:
                 p.anisU[c], p.anisU_mul[c] = param(u[c])
+        # cubic anisotropy (engine/anisotropy.go:14-19)
+        p.Kc1, p.Kc1_mul = param(Kc1)
+        p.Kc2, p.Kc2_mul = param(Kc2)
+        p.Kc3, p.Kc3_mul = param(Kc3)
+        for name, val in (("anisC1", anisC1), ("anisC2", anisC2)):
+            v = np.asarray(val, np.float64)
+            ptrs, muls = getattr(p, name), getattr(p, name + "_mul")
+            for c in range(3):
+                if v.ndim == 1:
+                    ptrs[c], muls[c] = None, float(np.float32(v[c]))
+                else:
+                    ptrs[c], muls[c] = param(v[c])
         self.aLUT = _dev(exchange_lut(Aex))
         p.aLUT = keep(self.aLUT)
         if np.any(np.asarray(Dind) != 0):
             self.dLUT = _dev(exchange_lut(Dind))
             p.dLUT = keep(self.dLUT)
+        if np.any(np.asarray(Dbulk) != 0):  # engine/exchange.go:60-61 AddDMIBulk
+            self.dbLUT = _dev(exchange_lut(Dbulk))
+            p.dbulkLUT = keep(self.dbLUT)
         if B_ext is not None:
             b = np.asarray(B_ext, np.float32)
             lut = np.tile(b, (NREGION, 1)) if b.ndim == 1 else b

@@ -162,6 +162,35 @@ def AddUniaxialAnisotropy2(Beff, m, Msat, k1, k2, u):
     Sync()
 
 
+def AddDMIBulk(Beff, m, Aex_red, D_red, Msat, regions, mesh, OpenBC=False):
+    """opencl/dmibulk.go:14"""
+    L = _L()
+    _in()
+    ms = _ms(Msat)
+    c = mesh.cellsize
+    check(L.umag_add_dmi_bulk(*_comps(Beff), *_comps(m), ms.ptr(), ms.mul, _p(Aex_red), _p(D_red), _p(regions),
+                              *mesh.size, c[0], c[1], c[2], mesh.PBC_code(), int(bool(OpenBC))))
+    Sync()
+
+
+def AddCubicAnisotropy2(Beff, m, Msat, k1, k2, k3, c1, c2):
+    """opencl/anisotropy.go:12.  c1, c2: 3 MSlices each (or 3-vectors, or (3,...) tensors)."""
+    import ctypes
+    L = _L()
+    _in()
+    ms, K1, K2, K3 = _ms(Msat), _ms(k1), _ms(k2), _ms(k3)
+
+    def axes(u):
+        us = [MSlice(u[i], 1.0) for i in range(3)] if torch.is_tensor(u) else [_ms(x) for x in u]
+        return (ctypes.c_void_p * 3)(*[x.ptr() for x in us]), (ctypes.c_float * 3)(*[x.mul for x in us])
+
+    p1, m1 = axes(c1)
+    p2, m2 = axes(c2)
+    check(L.umag_add_cubic_anisotropy2(*_comps(Beff), *_comps(m), ms.ptr(), ms.mul, K1.ptr(), K1.mul, K2.ptr(),
+                                       K2.mul, K3.ptr(), K3.mul, p1, m1, p2, m2, m[0].numel()))
+    Sync()
+
+
 def RegionAddV(dst, lut, regions):
     """opencl/region.go:13; lut: (3, 256) float32 CUDA tensor"""
     L = _L()

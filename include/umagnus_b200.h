@@ -101,6 +101,18 @@ int umag_region_addv(float* dx, float* dy, float* dz, const float* lutx, const f
 /* opencl/region.go:108 RegionDecode (regiondecode.cl). */
 int umag_region_decode(float* dst, const float* lut, const uint8_t* regions, int N);
 
+/* ---- thermal field --------------------------------------------------------
+ * opencl/temperature.go:14 SetTemperature (temperature2.cl): B = noise *
+ * sqrt(k2 * alpha * T / Ms), k2 = 2 kB / (GammaLL V dt) as float32. */
+int umag_set_temperature(float* B, const float* noise, float k2, const float* Ms, float Ms_mul,
+                         const float* temp, float temp_mul, const float* alpha, float alpha_mul, int N);
+/* Standard normal noise for N cells (three components) of accepted step
+ * `step` under `seed`: Philox4x32-10 of (cell, step) + Box-Muller.  Stands in
+ * for the reference's device-dependent Threefry stream (opencl/rng.go,
+ * engine/temperature.go:117-120): same distribution, reproducible on any
+ * device. */
+int umag_thermal_noise(float* nx, float* ny, float* nz, int N, unsigned long long seed, long long step);
+
 /* ---- torque -------------------------------------------------------------- */
 /* opencl/zeromask.go:12 ZeroMask (zeromask.cl): dst_c[i] = 0 where
  * maskLUT[regions[i]] != 0, for the three components. */
@@ -235,6 +247,11 @@ typedef struct {
     const float* anisC2[3]; float anisC2_mul[3];
     const float* dbulkLUT;         /* bulk DMI LUT (engine/exchange.go:49-66 Dbulk) or NULL;
                                       exclusive with dLUT */
+    /* thermal field (engine/temperature.go): Temp (array or NULL, multiplier);
+     * off when zero; noise from umag_thermal_noise's generator under therm_seed
+     * (ThermSeed), drawn anew for every accepted step */
+    const float* temp; float temp_mul;
+    unsigned long long therm_seed;
 } umag_sim_params;
 
 /* Solver knobs, engine/run.go:14-43 (defaults by umag_solver_defaults). */

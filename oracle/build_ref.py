@@ -24,7 +24,7 @@ HEADERS = ["typedefs.clh", "constants.clh", "stencil.clh", "float3.clh", "exchan
 KERNELS = ["copypadmul2", "copyunpad", "kernmulrsymm3d", "kernmulrsymm2dxy", "kernmulrsymm2dz",
            "exchange", "dmi", "dmibulk", "uniaxialanisotropy2", "cubicanisotropy2", "regionaddv", "regiondecode", "lltorque2",
            "llnoprecess", "madd2", "madd3", "madd4", "madd5", "madd6", "madd7", "normalize2",
-           "vecnorm", "div", "dotproduct"]
+           "vecnorm", "div", "dotproduct", "temperature2"]
 
 # extern "C" wrappers: (name, C parameter list, kernel call, launch kind)
 #   kind "3d:<x>,<y>,<z>"  -> make3DConf (opencl/util.go:35-45): local 16x16x1
@@ -52,6 +52,8 @@ WRAPPERS = [
                             " R c1z_mul, R* c2x, R c2x_mul, R* c2y, R c2y_mul, R* c2z, R c2z_mul, int N",
      "addcubicanisotropy2(Bx, By, Bz, mx, my, mz, Ms, Ms_mul, K1, K1_mul, K2, K2_mul, K3, K3_mul, c1x, c1x_mul,"
      " c1y, c1y_mul, c1z, c1z_mul, c2x, c2x_mul, c2y, c2y_mul, c2z, c2z_mul, N)", "1d:N"),
+    ("settemperature2", "R* B, R* noise, R k2, R* Ms, R Ms_mul, R* temp, R temp_mul, R* alpha, R alpha_mul, int N",
+     "settemperature2(B, noise, k2, Ms, Ms_mul, temp, temp_mul, alpha, alpha_mul, N)", "1d:N"),
     ("regionaddv", "R* dx, R* dy, R* dz, R* lx, R* ly, R* lz, uint8_t* regions, int N",
      "regionaddv(dx, dy, dz, lx, ly, lz, regions, N)", "1d:N"),
     ("regiondecode", "R* dst, R* lut, uint8_t* regions, int N", "regiondecode(dst, lut, regions, N)", "1d:N"),

@@ -283,6 +283,56 @@ def add_dmibulk(B, m, aLUT, dLUT, regions, cell, Ms, pbc=0, openbc=0):
         _ptr(_c(regions, np.uint8)), S(cell[0]), S(cell[1]), S(cell[2]), Nx, Ny, Nz, pbc, openbc)
 
 
+def set_temperature(B, noise, k2, Ms, temp, alpha):
+    """kernels_src/cl/temperature2.cl (one component); Ms/temp/alpha scalar or arrays."""
+    dt = B.dtype
+    S = _scal(dt)
+
+    def ms(v):
+        return (None, float(v)) if np.isscalar(v) else (_c(v, dt).ravel(), 1.0)
+
+    Msa, Msm = ms(Ms)
+    ta, tm = ms(temp)
+    aa, am = ms(alpha)
+    getattr(lib(), f"orc_set_temperature_{_sfx(dt)}")(
+        _ptr(B), _ptr(_c(noise, dt)), S(k2), _ptr(Msa), S(Msm), _ptr(ta), S(tm), _ptr(aa), S(am), B.size)
+
+
+M0_PHILOX, M1_PHILOX = 0xD2511F53, 0xCD9E8D57
+W0_PHILOX, W1_PHILOX = 0x9E3779B9, 0xBB67AE85
+
+
+def philox4x32_10(c0, c1, c2, c3, k0, k1):
+    """Philox4x32-10 (Salmon et al., SC'11) on uint64 arrays holding 32-bit words."""
+    m32 = np.uint64(0xFFFFFFFF)
+    c = [np.asarray(x, np.uint64) & m32 for x in (c0, c1, c2, c3)]
+    k0, k1 = int(k0) & 0xFFFFFFFF, int(k1) & 0xFFFFFFFF
+    for r in range(10):
+        if r:
+            k0 = (k0 + W0_PHILOX) & 0xFFFFFFFF
+            k1 = (k1 + W1_PHILOX) & 0xFFFFFFFF
+        p0 = np.uint64(M0_PHILOX) * c[0]
+        p1 = np.uint64(M1_PHILOX) * c[2]
+        c = [(p1 >> np.uint64(32)) ^ c[1] ^ np.uint64(k0), p1 & m32, (p0 >> np.uint64(32)) ^ c[3] ^ np.uint64(k1),
+             p0 & m32]
+    return c
+
+
+def thermal_normals(seed, step, n):
+    """The three standard normals per cell of the device's thermal noise
+    (umag_thermal_noise): Philox4x32-10 of (cell, step lo, step hi, 0) under
+    the 64-bit seed, Box-Muller on 24-bit uniforms.  Shape (3, n), float32;
+    the transcendental functions are evaluated in FP64 and rounded."""
+    cell = np.arange(n, dtype=np.uint64)
+    step = int(step) & ((1 << 64) - 1)
+    r = philox4x32_10(cell, step & 0xFFFFFFFF, step >> 32, 0, seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF)
+    u = [((x >> np.uint64(8)).astype(np.float64) + 0.5) / 16777216.0 for x in r]
+    a = np.sqrt(-2.0 * np.log(u[0]))
+    b = np.sqrt(-2.0 * np.log(u[2]))
+    return np.stack([a * np.cos(2 * np.pi * u[1]), a * np.sin(2 * np.pi * u[1]),
+                     b * np.cos(2 * np.pi * u[3])]).astype(np.float32)
+
+
 def region_addv(B, lut, regions):
     dt = B.dtype
     getattr(lib(), f"orc_region_addv_{_sfx(dt)}")(

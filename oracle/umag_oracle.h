@@ -85,6 +85,8 @@ void orc_add_cubic2_##S(R* B[3], R* const m[3], const R* Ms, R Ms_mul, const R* 
 void orc_add_dmibulk_##S(R* H[3], R* const m[3], const R* Ms, R Ms_mul, const R* aLUT2d,      \
                          const R* dLUT2d, const uint8_t* regions, R cx, R cy, R cz, int Nx,   \
                          int Ny, int Nz, int pbc, int openbc);                                \
+void orc_set_temperature_##S(R* B, const R* noise, R k2, const R* Ms, R Ms_mul, const R* temp,  \
+                             R temp_mul, const R* alpha, R alpha_mul, int N);                 \
 void orc_region_addv_##S(R* dst[3], R* const lut[3], const uint8_t* regions, int N);          \
 void orc_region_decode_##S(R* dst, const R* lut, const uint8_t* regions, int N);              \
 void orc_lltorque_##S(R* t[3], R* const m[3], R* const h[3], const R* alpha, R alpha_mul,     \

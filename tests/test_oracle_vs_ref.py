@@ -121,6 +121,22 @@ def test_cubic_bitexact(dtype, per_cell):
 
 
 @pytest.mark.parametrize("dtype", DT)
+def test_set_temperature_bitexact(dtype):
+    rng = np.random.default_rng(8)
+    n = 3001
+    noise = rng.standard_normal(n).astype(dtype)
+    Ms = (rng.random(n) * 1e6 + 1e5).astype(dtype)
+    Ms[::17] = 0
+    temp = (rng.random(n) * 400).astype(dtype)
+    k2 = float(dtype(2 * 1.380650424e-23 / (1.7595e11 * 1e-24 * 2e-13)))
+    B1 = np.zeros(n, dtype)
+    B2 = np.zeros(n, dtype)
+    O.set_temperature(B1, noise, k2, Ms, temp, 0.05)
+    clref.call("settemperature2", dtype, B2, noise, k2, Ms, 1.0, temp, 1.0, None, 0.05, n)
+    assert np.array_equal(B1, B2)
+
+
+@pytest.mark.parametrize("dtype", DT)
 def test_torque_zeeman_madd_normalize_bitexact(dtype):
     N = (9, 8, 2)
     n = N[0] * N[1] * N[2]

@@ -32,7 +32,7 @@ class SimParams(ctypes.Structure):
         ("demag_kernel", c_int), ("demag_accuracy", c_double), ("frozen_lut", P),
         ("Kc1", P), ("Kc1_mul", c_float), ("Kc2", P), ("Kc2_mul", c_float), ("Kc3", P), ("Kc3_mul", c_float),
         ("anisC1", P * 3), ("anisC1_mul", c_float * 3), ("anisC2", P * 3), ("anisC2_mul", c_float * 3),
-        ("dbulkLUT", P),
+        ("dbulkLUT", P), ("temp", P), ("temp_mul", c_float), ("therm_seed", ctypes.c_ulonglong),
     ]
 
 
@@ -79,6 +79,8 @@ _SIGS = {
                                    c_int],
     "umag_region_addv": [P, P, P, P, P, P, P, c_int], "umag_region_decode": [P, P, P, c_int],
     "umag_zero_mask": [P, P, P, P, P, c_int],
+    "umag_thermal_noise": [P, P, P, c_int, ctypes.c_ulonglong, c_ll],
+    "umag_set_temperature": [P, P, c_float, P, c_float, P, c_float, P, c_float, c_int],
     "umag_lltorque": [P, P, P, P, P, P, P, P, P, P, c_float, c_int],
     "umag_llnoprecess": [P, P, P, P, P, P, P, P, P, c_int],
     "umag_madd": [c_int, P, c_int, P, P, c_int],

@@ -96,6 +96,13 @@ int umag_region_addv(float* dx, float* dy, float* dz, const float* lx, const flo
 int umag_region_decode(float* dst, const float* lut, const uint8_t* regions, int N) {
     return region_decode(dst, lut, regions, N);
 }
+int umag_thermal_noise(float* nx, float* ny, float* nz, int N, unsigned long long seed, long long step) {
+    return thermal_noise(nx, ny, nz, N, (uint64_t)seed, step);
+}
+int umag_set_temperature(float* B, const float* noise, float k2, const float* Ms, float Ms_mul, const float* temp,
+                         float temp_mul, const float* alpha, float alpha_mul, int N) {
+    return set_temperature(B, noise, k2, Ms, Ms_mul, temp, temp_mul, alpha, alpha_mul, N);
+}
 int umag_zero_mask(float* dx, float* dy, float* dz, const float* maskLUT, const uint8_t* regions, int N) {
     return zero_mask(dx, dy, dz, maskLUT, regions, N);
 }

@@ -466,6 +466,53 @@ __device__ __forceinline__ f3 dmibulk_sum(const float* __restrict__ mx, const fl
     return h;
 }
 
+// Thermal noise.  The reference draws its normals from an OpenCL Threefry
+// generator whose stream depends on the device's compute-unit count and
+// work-group size (opencl/rng.go:198-205), so no other device reproduces its
+// numbers; only their distribution is the contract.  Here each normal is a
+// function of (seed, accepted-step index, cell, component): Philox4x32-10
+// (Salmon, Moraes, Dror and Shaw, "Parallel random numbers: as easy as
+// 1, 2, 3", SC'11) of the counter (cell, step lo, step hi, 0) under the
+// 64-bit seed, then Box-Muller on pairs of 24-bit uniforms in (0, 1).  A
+// rejected step retries with the same numbers (the step index is unchanged),
+// as the reference keeps its noise during a step (engine/temperature.go:86-97).
+struct PhiloxCtr {
+    uint32_t v[4];
+};
+__host__ __device__ __forceinline__ PhiloxCtr philox4x32_10(PhiloxCtr c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        if (r > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c.v[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.v[2];
+        const PhiloxCtr o{{(uint32_t)(p1 >> 32) ^ c.v[1] ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.v[3] ^ k1,
+                           (uint32_t)p0}};
+        c = o;
+    }
+    return c;
+}
+// uniform in (0, 1) from the top 24 bits (exact in float32)
+__device__ __forceinline__ float u24(uint32_t x) { return ((float)(x >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+// three standard normals for (seed, step, cell)
+__device__ __forceinline__ f3 therm_normals(uint64_t seed, long long step, int cell) {
+    const PhiloxCtr r = philox4x32_10(PhiloxCtr{{(uint32_t)cell, (uint32_t)(uint64_t)step,
+                                                  (uint32_t)((uint64_t)step >> 32), 0u}},
+                                       (uint32_t)seed, (uint32_t)(seed >> 32));
+    const float a = sqrtf(-2.0f * logf(u24(r.v[0])));
+    const float b = sqrtf(-2.0f * logf(u24(r.v[2])));
+    float s1, c1, s2, c2;
+    sincospif(2.0f * u24(r.v[1]), &s1, &c1);
+    sincospif(2.0f * u24(r.v[3]), &s2, &c2);
+    return f3{a * c1, a * s1, b * c2};
+}
+// temperature2.cl:11-17: noise * sqrt(kB2_VgammaDt * alpha * T / Ms)
+__device__ __forceinline__ float therm_scale(float k2, float alpha, float temp, float invMs) {
+    return __fsqrt_rn(fm(fm(fm(k2, alpha), temp), invMs));
+}
+
 // lltorque2.cl:13-23
 __device__ __forceinline__ f3 lltorque(f3 m, f3 H, float alpha) {
     f3 mxH = cross3(m, H);

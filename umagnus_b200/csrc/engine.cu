@@ -24,6 +24,8 @@
 namespace umag {
 
 // ---------------------------------------------------------------- device state
+constexpr double kBoltzmann = 1.380650424e-23;  // mag/constants.go:9 Kb
+
 struct DevCtl {
     float* m;        // state magnetisation (3N, SoA)
     float* mw;       // working / stage magnetisation
@@ -39,6 +41,10 @@ struct DevCtl {
     long long nsteps, nundone, nevals;
     int status;
     double max_err, rel_err, min_dt, max_dt, fix_dt, headroom, min_slope, gamma;
+    // thermal field: k2 = float32(2 kB / ((GammaLL V) dt)) of the step in
+    // progress (engine/temperature.go:111); therm_gv = GammaLL V (0: no thermal field)
+    double therm_gv;
+    float k2;
 };
 
 // Uniform parameters evaluated once on the device with the operations the
@@ -81,6 +87,10 @@ struct LocalArgs {
     int cubic;            // cubic anisotropy on (cp)
     CubicParams cp;
     const float* dbLUT;   // bulk DMI LUT or NULL
+    int thermal;          // thermal field on (off while relaxing)
+    const float* temp;
+    float temp_mul;
+    unsigned long long seed;
     int ms_uniform, alpha_uniform, anis_uniform;
     DmiPairLut dl;
     LocalConsts kc;
@@ -223,6 +233,14 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
             B.y = fa(B.y, __ldg(a.bext[1] + r));
             B.z = fa(B.z, __ldg(a.bext[2] + r));
         }
+    }
+    if (!BAT && a.thermal) {  // engine/effectivefield.go:20-22 B_therm (temperature2.cl)
+        const float sc = therm_scale(ctl->k2, amul(a.alpha, a.alpha_mul, I), amul(a.temp, a.temp_mul, I),
+                                     inv_msat(a.Ms, a.Ms_mul, I));
+        const f3 n = therm_normals(a.seed, ctl->nsteps, I);
+        B.x = fa(B.x, fm(n.x, sc));
+        B.y = fa(B.y, fm(n.y, sc));
+        B.z = fa(B.z, fm(n.z, sc));
     }
     if (a.beff) { a.beff[I] = B.x; a.beff[N + I] = B.y; a.beff[2 * N + I] = B.z; }
     f3 t;
@@ -388,6 +406,7 @@ __global__ void k_step_begin(DevCtl* c0, int nb) {
     if (!c->active) return;
     if (c->fix_dt != 0) c->dt = c->fix_dt;
     c->h = (float)(c->dt * c->gamma);
+    if (c->therm_gv != 0) c->k2 = (float)(2 * kBoltzmann / (c->therm_gv * c->dt));
     c->t0 = c->t;
     c->err2 = 0u; c->dm2 = 0u; c->rel = 0u;
     c->accepted = 0;
@@ -492,8 +511,8 @@ __global__ void k_step_end(DevCtl* c0, int nb, int rk4) {
 // alone, [3] anisotropy from K2 alone, [4] Zeeman.
 // the float32 dot products of cell I: [0] demag, [1] exchange (+DMI),
 // [2] uniaxial anisotropy from K1 alone, [3] from K2 alone, [4] Zeeman,
-// [5..7] cubic anisotropy from Kc1, Kc2, Kc3 alone
-constexpr int kNE = 8;
+// [5..7] cubic anisotropy from Kc1, Kc2, Kc3 alone, [8] thermal field
+constexpr int kNE = 9;
 __device__ __forceinline__ void energy_cell_terms(const LocalArgs& a, const float* __restrict__ vol, int I,
                                                   float t[kNE]) {
     const int N = a.N;
@@ -531,6 +550,12 @@ __device__ __forceinline__ void energy_cell_terms(const LocalArgs& a, const floa
     if (a.zeeman) {
         const int r = __ldg(a.regions + I);
         t[4] = dot3(Mf, f3{__ldg(a.bext[0] + r), __ldg(a.bext[1] + r), __ldg(a.bext[2] + r)});
+    }
+    if (a.thermal) {  // engine/temperature.go:21 Edens_therm: the field of the current step
+        const float sc = therm_scale(a.ctl->k2, amul(a.alpha, a.alpha_mul, I), amul(a.temp, a.temp_mul, I),
+                                     inv_msat(a.Ms, a.Ms_mul, I));
+        const f3 n = therm_normals(a.seed, a.ctl->nsteps, I);
+        t[8] = dot3(Mf, f3{fm(n.x, sc), fm(n.y, sc), fm(n.z, sc)});
     }
     if (a.cubic) {  // engine/anisotropy.go:191-206: each constant alone
         for (int k = 0; k < 3; k++) {
@@ -896,6 +921,11 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
     c.max_err = sp->max_err; c.rel_err = sp->rel_err; c.min_dt = sp->min_dt; c.max_dt = sp->max_dt;
     c.fix_dt = sp->fix_dt; c.headroom = sp->headroom; c.min_slope = sp->min_slope; c.gamma = sp->gamma_ll;
     c.active = 1;
+    if (p->temp != nullptr || p->temp_mul != 0.f) {  // engine/temperature.go:111 (cellVolume: c0 c1 c2)
+        c.therm_gv = sp->gamma_ll * (p->cell[0] * p->cell[1] * p->cell[2]);
+        const double dt0 = sp->fix_dt != 0 ? sp->fix_dt : sp->dt;
+        c.k2 = (float)(2 * kBoltzmann / (c.therm_gv * dt0));
+    }
     st = push_ctl(s);
     if (st != UMAG_OK) return fail(st);
     // pass / local arguments
@@ -940,6 +970,10 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
                         {p->anisC1_mul[0], p->anisC1_mul[1], p->anisC1_mul[2]},
                         {p->anisC2_mul[0], p->anisC2_mul[1], p->anisC2_mul[2]}};
     la.dbLUT = p->dbulkLUT;
+    la.thermal = (p->temp != nullptr || p->temp_mul != 0.f);
+    la.temp = p->temp;
+    la.temp_mul = p->temp_mul;
+    la.seed = p->therm_seed;
     la.Ms = p->Ms;
     la.Ms_mul = p->Ms_mul;
     la.ms_uniform = p->Ms == nullptr;
@@ -1163,6 +1197,7 @@ __global__ void __launch_bounds__(256) k_energy_density(LocalArgs a, const float
         }
         if (a.bd) d = fa(d, fm(-0.5f, t[0]));
         d = fa(d, fm(-0.5f, t[1]));
+        if (a.thermal) d = fa(d, fm(-1.0f, t[8]));
         if (a.zeeman) d = fa(d, fm(-1.0f, t[4]));
         dst[I] = d;
     }
@@ -1191,9 +1226,10 @@ int sim_energies(umag_sim* h, double E[5]) {
     // engine/anisotropy.go:164-206: uniaxial -1/2, -1/4; cubic -1/4, -1/6, -1/8
     const double Ea = V * (-0.5 * t[2] - 0.25 * t[3] - 0.25 * t[5] - t[6] / 6.0 - 0.125 * t[7]);
     const double Ez = -1.0 * V * t[4];
+    const double Et = s->la.thermal ? -1.0 * V * t[8] : 0.0;  // engine/temperature.go:124-130
     E[1] = Ed; E[2] = Ee; E[3] = Ea; E[4] = Ez;
-    // registration order of the terms (files anisotropy, demag, exchange, zeeman)
-    E[0] = ((Ea + Ed) + Ee) + Ez;
+    // registration order of the terms (files anisotropy, demag, exchange, temperature, zeeman)
+    E[0] = (((Ea + Ed) + Ee) + Et) + Ez;
     return UMAG_OK;
 }
 
@@ -1274,7 +1310,10 @@ int sim_relax(umag_sim* h, double threshold) {
     UMAG_TRY(sync_ctl_to_host(s));
     const int prev_solver = s->sp.solver, prev_precess = s->la.precess;
     const double prev_err = s->hctl->max_err, prev_fix = s->hctl->fix_dt;
+    const int prev_thermal = s->la.thermal;
     set_stepper(s, 3, 0);
+    s->la.thermal = 0;  // engine/effectivefield.go:20: no B_therm while relaxing
+    if (prev_thermal) drop_graph(s);  // the captured steps bake the flag in
     s->hctl->fix_dt = 0;
     UMAG_TRY(push_ctl(s));
     auto body = [&]() -> int {
@@ -1331,6 +1370,8 @@ int sim_relax(umag_sim* h, double threshold) {
     s->hctl->max_err = prev_err;
     s->hctl->fix_dt = prev_fix;
     push_ctl(s);
+    s->la.thermal = prev_thermal;
+    drop_graph(s);
     set_stepper(s, prev_solver, prev_precess);
     return st;
 }

@@ -234,6 +234,46 @@ __global__ void k_add_dot(float* dst, float pre, const float* __restrict__ ax, c
         dst[i] = fa(dst[i], fm(pre, dot3(ld3(ax, ay, az, i), ld3(bx, by, bz, i))));
 }
 
+// thermal noise of (seed, step) for N cells, three components
+__global__ void k_thermal_noise(float* nx, float* ny, float* nz, int N, uint64_t seed, long long step) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const f3 n = therm_normals(seed, step, i);
+        nx[i] = n.x;
+        ny[i] = n.y;
+        nz[i] = n.z;
+    }
+}
+
+// temperature2.cl:3-19 settemperature2
+__global__ void k_set_temperature(float* B, const float* __restrict__ noise, float k2, const float* __restrict__ Ms,
+                                  float Ms_mul, const float* __restrict__ temp, float temp_mul,
+                                  const float* __restrict__ alpha, float alpha_mul, int N) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const float invMs = inv_msat(Ms, Ms_mul, i);
+        B[i] = fm(noise[i], therm_scale(k2, amul(alpha, alpha_mul, i), amul(temp, temp_mul, i), invMs));
+    }
+}
+
+int thermal_noise(float* nx, float* ny, float* nz, int N, uint64_t seed, long long step) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(nx && ny && nz, "NULL argument");
+    if (N <= 0) return UMAG_OK;
+    k_thermal_noise<<<grid_for(N, 256), 256, 0, ctx().stream>>>(nx, ny, nz, N, seed, step);
+    UMAG_LAUNCH_CHECK();
+    return UMAG_OK;
+}
+
+int set_temperature(float* B, const float* noise, float k2, const float* Ms, float Ms_mul, const float* temp,
+                    float temp_mul, const float* alpha, float alpha_mul, int N) {
+    UMAG_TRY(ensure_init());
+    UMAG_REQUIRE(B && noise, "NULL argument");
+    if (N <= 0) return UMAG_OK;
+    k_set_temperature<<<grid_for(N, 256), 256, 0, ctx().stream>>>(B, noise, k2, Ms, Ms_mul, temp, temp_mul, alpha,
+                                                                   alpha_mul, N);
+    UMAG_LAUNCH_CHECK();
+    return UMAG_OK;
+}
+
 // zeromask.cl
 __global__ void k_zero_mask(float* dx, float* dy, float* dz, const float* __restrict__ lut,
                             const uint8_t* __restrict__ regions, int N) {

@@ -27,6 +27,9 @@ int region_decode(float* dst, const float* lut, const uint8_t* regions, int N);
 int torque(float* tx, float* ty, float* tz, const float* mx, const float* my, const float* mz, const float* hx,
            const float* hy, const float* hz, const float* alpha, float alpha_mul, int N, int precess);
 int zero_mask(float* dx, float* dy, float* dz, const float* lut, const uint8_t* regions, int N);
+int thermal_noise(float* nx, float* ny, float* nz, int N, uint64_t seed, long long step);
+int set_temperature(float* B, const float* noise, float k2, const float* Ms, float Ms_mul, const float* temp,
+                    float temp_mul, const float* alpha, float alpha_mul, int N);
 int madd(int ncomp, float* const* dst, int nsrc, const float* const* src, const float* fac, int N);
 int normalize(float* vx, float* vy, float* vz, const float* vol, int N);
 int vecnorm(float* dst, const float* ax, const float* ay, const float* az, int N);

@@ -79,14 +79,16 @@ class Simulation:
     scalar or 256 per-region values, the torque is zero where non-zero;
     Kc1, Kc2, Kc3, anisC1, anisC2: cubic anisotropy (scalars / 3-vectors or
     per-cell maps); Dbulk: bulk DMI (scalar or 256 per-region values; not
-    together with Dind).
+    together with Dind); Temp (K, scalar or per-cell map) with ThermSeed: the
+    thermal field, new noise every accepted step.
     """
 
     def __init__(self, N, cell, Msat, Aex, alpha, Dind=0.0, Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
                  regions=None, geom=None, demag=True, open_bc=False, precess=True, solver=DORMANDPRINCE,
                  dt=1e-15, MaxErr=1e-5, RelErr=1e-4, MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8,
                  device=0, asymptotic_radius=32, demag_kernel="newell", demag_accuracy=6.0, FrozenSpins=None,
-                 Kc1=0.0, Kc2=0.0, Kc3=0.0, anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0):
+                 Kc1=0.0, Kc2=0.0, Kc3=0.0, anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0,
+                 Temp=0.0, ThermSeed=0):
         self.L = _lib.init(device)
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
@@ -157,6 +159,9 @@ class Simulation:
             raise ValueError("demag_kernel must be 'newell' or 'brute'")
         p.demag_kernel = 1 if demag_kernel == "brute" else 0
         p.demag_accuracy = float(demag_accuracy)
+        # engine/temperature.go: Temp (K), scalar or per-cell; ThermSeed seeds the noise
+        p.temp, p.temp_mul = param(Temp)
+        p.therm_seed = int(ThermSeed) & ((1 << 64) - 1)
         if FrozenSpins is not None:  # engine/torque.go:348-352: a scalar or 256 per-region values
             fz = np.zeros(NREGION, np.float32)
             v = np.asarray(FrozenSpins, np.float32).ravel()

@@ -216,6 +216,25 @@ def LLTorque(torque, m, B, alpha):
     Sync()
 
 
+def SetTemperature(Bth, noise, k2mu0_Mu0VgammaDt, Msat, Temp, Alpha):
+    """opencl/temperature.go:14 (temperature2.cl): Bth = noise * sqrt(k2 alpha T / Ms); one component."""
+    L = _L()
+    _in()
+    ms, t, a = _ms(Msat), _ms(Temp), _ms(Alpha)
+    check(L.umag_set_temperature(_p(Bth), _p(noise), float(k2mu0_Mu0VgammaDt), ms.ptr(), ms.mul, t.ptr(), t.mul,
+                                 a.ptr(), a.mul, Bth.numel()))
+    Sync()
+
+
+def ThermalNoise(noise, seed, step):
+    """Standard normal noise (3, ...) of accepted step `step` under `seed`
+    (the stand-in for the reference's device-dependent Threefry stream)."""
+    L = _L()
+    _in()
+    check(L.umag_thermal_noise(*_comps(noise), noise[0].numel(), int(seed) & ((1 << 64) - 1), int(step)))
+    Sync()
+
+
 def ZeroMask(dst, mask, regions):
     """opencl/zeromask.go:12: dst = 0 where mask[regions] != 0 (mask: 256-entry LUT)."""
     L = _L()

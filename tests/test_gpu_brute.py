@@ -25,6 +25,18 @@ def test_kernel_equals_oracle(N, cell):
     d.Free()
 
 
+@pytest.mark.parametrize("N,cell,pbc", [((6, 4, 1), (1e-9, 2e-9, 1e-9), (2, 1, 0)),
+                                         ((4, 4, 3), (2e-9, 2e-9, 1e-9), (0, 0, 2))])
+def test_pbc_kernel_equals_oracle(N, cell, pbc):
+    """Periodic images accumulated in float32 in the reference's loop order."""
+    from umagnus_b200 import opencl as cl
+    d = cl.NewBruteDemag(N, pbc, cell)
+    got = d.kernel()
+    want = O.brute_kernel(N, cell, pbc).astype(np.float64)
+    np.testing.assert_array_equal(got, want)
+    d.Free()
+
+
 @pytest.mark.parametrize("N,cell,want,tol", [
     ((3, 4, 1), (1e-9, 2e-9, 0.5e-9), (-0.15768295526, -0.05676037073, -0.78447151184), 1e-6),  # demagSmall.mx3
     ((3, 4, 2), (1e-9, 2e-9, 3e-9), (-0.52710835138, -0.20121671756, -0.27112555503), 1e-6),   # demagSmall3D.mx3

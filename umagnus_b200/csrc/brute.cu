@@ -34,6 +34,73 @@ __device__ __forceinline__ int brute_wrap(int n, int max) {  // demagkernel.go:3
     return n;
 }
 
+// the field of source direction s at destination displacement (x, y, z)
+// cells (demagkernel.go:200-268): FP64 in the reference's operation order
+__device__ void brute_point(const BruteArgs& a, int s, int x, int y, int z, double B[3]) {
+    const int u = s, v = (s + 1) % 3, w = (s + 2) % 3;
+    const double* c = a.c;
+    double R[3] = {(double)x * c[0], (double)y * c[1], (double)z * c[2]};
+    const double dx = brute_delta(x) * c[0], dy = brute_delta(y) * c[1], dz = brute_delta(z) * c[2];
+    double d = sqrt(dx * dx + dy * dy + dz * dz);
+    if (d == 0) d = a.L;
+    const double maxSize = d / a.accuracy;
+    int nv = (int)(fmax(c[v] / maxSize, 1.0) + 0.5);
+    int nw = (int)(fmax(c[w] / maxSize, 1.0) + 0.5);
+    const int nx = (int)(fmax(c[0] / maxSize, 1.0) + 0.5);
+    const int ny = (int)(fmax(c[1] / maxSize, 1.0) + 0.5);
+    const int nz = (int)(fmax(c[2] / maxSize, 1.0) + 0.5);
+    nv *= 2;  // staggered source and destination grids
+    nw *= 2;
+    const double scale = 1 / (double)(nv * nw * nx * ny * nz);
+    const double surface = c[v] * c[w];
+    const double charge = surface * scale;
+    const double pu1 = c[u] / 2.;
+    const double pu2 = -pu1;
+    const double fourpi = 4 * M_PI;
+    double pole[3], R2[3];
+    B[0] = B[1] = B[2] = 0;
+    for (int i = 0; i < nv; i++) {
+        pole[v] = -(c[v] / 2.) + c[v] / (double)(2 * nv) + (double)i * (c[v] / (double)nv);
+        for (int j = 0; j < nw; j++) {
+            pole[w] = -(c[w] / 2.) + c[w] / (double)(2 * nw) + (double)j * (c[w] / (double)nw);
+            for (int al = 0; al < nx; al++) {
+                const double rx = R[0] - c[0] / 2 + c[0] / (double)(2 * nx) + (c[0] / (double)nx) * (double)al;
+                for (int be = 0; be < ny; be++) {
+                    const double ry = R[1] - c[1] / 2 + c[1] / (double)(2 * ny) + (c[1] / (double)ny) * (double)be;
+                    for (int ga = 0; ga < nz; ga++) {
+                        const double rz =
+                            R[2] - c[2] / 2 + c[2] / (double)(2 * nz) + (c[2] / (double)nz) * (double)ga;
+                        pole[u] = pu1;
+                        R2[0] = rx - pole[0]; R2[1] = ry - pole[1]; R2[2] = rz - pole[2];
+                        double r = sqrt(R2[0] * R2[0] + R2[1] * R2[1] + R2[2] * R2[2]);
+                        double qr = charge / (fourpi * r * r * r);
+                        const double bx = R2[0] * qr, by = R2[1] * qr, bz = R2[2] * qr;
+                        pole[u] = pu2;
+                        R2[0] = rx - pole[0]; R2[1] = ry - pole[1]; R2[2] = rz - pole[2];
+                        r = sqrt(R2[0] * R2[0] + R2[1] * R2[1] + R2[2] * R2[2]);
+                        qr = -charge / (fourpi * r * r * r);
+                        B[0] += (bx + R2[0] * qr);  // addition ordered for accuracy (as the reference)
+                        B[1] += (by + R2[1] * qr);
+                        B[2] += (bz + R2[2] * qr);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// first and last image index k with w + k P in [r1, r2]
+__device__ __forceinline__ void brute_images(int w, int P, int r1, int r2, int& k0, int& k1) {
+    k0 = (int)floor((double)(r1 - w) / P);
+    if (w + k0 * P < r1) k0++;
+    k1 = (int)floor((double)(r2 - w) / P);
+}
+
+// One thread per (source direction s, octant point in [0, P/2]): the field
+// of every periodic image inside the kernel ranges (demagkernel.go:189-268),
+// each rounded to float32 and summed in float32 in the reference's loop
+// order (z, y, x ascending), as the reference accumulates into its float32
+// kernel.  Without PBC the only image is the point itself.
 __global__ void k_brute_octant(double* K0, double* K1, double* K2, double* K3, double* K4, double* K5, BruteArgs a) {
     const long npt = (long)a.ext[0] * a.ext[1] * a.ext[2];
     double* K[6] = {K0, K1, K2, K3, K4, K5};
@@ -41,63 +108,23 @@ __global__ void k_brute_octant(double* K0, double* K1, double* K2, double* K3, d
     for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < 3 * npt; e += (long)gridDim.x * blockDim.x) {
         const int s = (int)(e / npt);
         const long q = e - s * npt;
-        const int x = a.r1[0] + (int)(q % a.ext[0]);
-        const int y = a.r1[1] + (int)((q / a.ext[0]) % a.ext[1]);
-        const int z = a.r1[2] + (int)(q / ((long)a.ext[0] * a.ext[1]));
-        const int xw = brute_wrap(x, a.P[0]), yw = brute_wrap(y, a.P[1]), zw = brute_wrap(z, a.P[2]);
-        if (xw > a.P[0] / 2 || yw > a.P[1] / 2 || zw > a.P[2] / 2) continue;  // reconstructed by symmetry
-        const int u = s, v = (s + 1) % 3, w = (s + 2) % 3;
-        const double* c = a.c;
-        double R[3] = {(double)x * c[0], (double)y * c[1], (double)z * c[2]};
-        const double dx = brute_delta(x) * c[0], dy = brute_delta(y) * c[1], dz = brute_delta(z) * c[2];
-        double d = sqrt(dx * dx + dy * dy + dz * dz);
-        if (d == 0) d = a.L;
-        const double maxSize = d / a.accuracy;
-        int nv = (int)(fmax(c[v] / maxSize, 1.0) + 0.5);
-        int nw = (int)(fmax(c[w] / maxSize, 1.0) + 0.5);
-        const int nx = (int)(fmax(c[0] / maxSize, 1.0) + 0.5);
-        const int ny = (int)(fmax(c[1] / maxSize, 1.0) + 0.5);
-        const int nz = (int)(fmax(c[2] / maxSize, 1.0) + 0.5);
-        nv *= 2;  // staggered source and destination grids
-        nw *= 2;
-        const double scale = 1 / (double)(nv * nw * nx * ny * nz);
-        const double surface = c[v] * c[w];
-        const double charge = surface * scale;
-        const double pu1 = c[u] / 2.;
-        const double pu2 = -pu1;
-        const double fourpi = 4 * M_PI;
-        double pole[3], R2[3];
-        double B[3] = {0, 0, 0};
-        for (int i = 0; i < nv; i++) {
-            pole[v] = -(c[v] / 2.) + c[v] / (double)(2 * nv) + (double)i * (c[v] / (double)nv);
-            for (int j = 0; j < nw; j++) {
-                pole[w] = -(c[w] / 2.) + c[w] / (double)(2 * nw) + (double)j * (c[w] / (double)nw);
-                for (int al = 0; al < nx; al++) {
-                    const double rx = R[0] - c[0] / 2 + c[0] / (double)(2 * nx) + (c[0] / (double)nx) * (double)al;
-                    for (int be = 0; be < ny; be++) {
-                        const double ry = R[1] - c[1] / 2 + c[1] / (double)(2 * ny) + (c[1] / (double)ny) * (double)be;
-                        for (int ga = 0; ga < nz; ga++) {
-                            const double rz =
-                                R[2] - c[2] / 2 + c[2] / (double)(2 * nz) + (c[2] / (double)nz) * (double)ga;
-                            pole[u] = pu1;
-                            R2[0] = rx - pole[0]; R2[1] = ry - pole[1]; R2[2] = rz - pole[2];
-                            double r = sqrt(R2[0] * R2[0] + R2[1] * R2[1] + R2[2] * R2[2]);
-                            double qr = charge / (fourpi * r * r * r);
-                            const double bx = R2[0] * qr, by = R2[1] * qr, bz = R2[2] * qr;
-                            pole[u] = pu2;
-                            R2[0] = rx - pole[0]; R2[1] = ry - pole[1]; R2[2] = rz - pole[2];
-                            r = sqrt(R2[0] * R2[0] + R2[1] * R2[1] + R2[2] * R2[2]);
-                            qr = -charge / (fourpi * r * r * r);
-                            B[0] += (bx + R2[0] * qr);  // addition ordered for accuracy (as the reference)
-                            B[1] += (by + R2[1] * qr);
-                            B[2] += (bz + R2[2] * qr);
-                        }
-                    }
+        const int xw = (int)(q % a.ext[0]);
+        const int yw = (int)((q / a.ext[0]) % a.ext[1]);
+        const int zw = (int)(q / ((long)a.ext[0] * a.ext[1]));
+        int kx0, kx1, ky0, ky1, kz0, kz1;
+        brute_images(xw, a.P[0], a.r1[0], a.r2[0], kx0, kx1);
+        brute_images(yw, a.P[1], a.r1[1], a.r2[1], ky0, ky1);
+        brute_images(zw, a.P[2], a.r1[2], a.r2[2], kz0, kz1);
+        float acc[3] = {0.f, 0.f, 0.f};
+        for (int kz = kz0; kz <= kz1; kz++)
+            for (int ky = ky0; ky <= ky1; ky++)
+                for (int kx = kx0; kx <= kx1; kx++) {
+                    double B[3];
+                    brute_point(a, s, xw + kx * a.P[0], yw + ky * a.P[1], zw + kz * a.P[2], B);
+                    for (int dd = s; dd < 3; dd++) acc[dd] += (float)B[dd];
                 }
-            }
-        }
         const long I = ((long)zw * a.P[1] + yw) * a.P[0] + xw;
-        for (int dd = s; dd < 3; dd++) K[comp[s][dd]][I] = (double)(float)B[dd];  // float32 kernel slices
+        for (int dd = s; dd < 3; dd++) K[comp[s][dd]][I] = (double)acc[dd];  // float32 kernel slices
     }
 }
 
@@ -128,12 +155,13 @@ int build_brute(const umag_demag* d, double accuracy, double* Kr[6], cudaStream_
     BruteArgs a{};
     for (int i = 0; i < 3; i++) {
         a.P[i] = d->P[i];
-        a.r1[i] = -(d->P[i] - 1) / 2;  // kernelRanges without PBC (demagkernel.go:338-351)
-        a.r2[i] = (d->P[i] - 1) / 2;
+        // kernelRanges (demagkernel.go:338-351)
+        if (d->pbc[i] == 0) { a.r1[i] = -(d->P[i] - 1) / 2; a.r2[i] = (d->P[i] - 1) / 2; }
+        else { a.r1[i] = -(d->P[i] * d->pbc[i] - 1); a.r2[i] = d->P[i] * d->pbc[i] - 1; }
         a.c[i] = c[i];
+        a.ext[i] = d->P[i] / 2 + 1;  // the octant [0, P/2]
     }
-    if (d->P[2] == 1) a.r2[2] = 0;
-    for (int i = 0; i < 3; i++) a.ext[i] = a.r2[i] - a.r1[i] + 1;
+    if (d->P[2] == 1 && d->pbc[2] == 0) a.r2[2] = 0;
     a.accuracy = accuracy;
     a.L = fmin(c[0], fmin(c[1], c[2]));
     const long n = (long)d->P[0] * d->P[1] * d->P[2];

@@ -60,39 +60,61 @@ static int make_line(int L, FftLine<T>& f, typename Cplx<T>::t** dev_tw) {
 // ================================================================== Newell (FP64)
 struct NewellArgs {
     int P[3], ext[3];
+    int r1[3], r2[3];  // kernelRanges (mag/demagkernel.go:339-352): the periodic images are r1..r2
     double dx, dy, dz, scale, arad2;
     int use_asym;
     newell::Expansion exx, exy, exz, eyy, eyz, ezz;
 };
 
-// One thread per octant point (x, y, z) >= 0 of the padded grid
-// (mag/newellDemagKernel.go:1166-1252).  K order: xx yy zz yz xz xy.
+// first and last image index k with w + k P in [r1, r2]
+__device__ __forceinline__ void image_range(int w, int P, int r1, int r2, int& k0, int& k1) {
+    k0 = (int)floor((double)(r1 - w) / P);
+    if (w + k0 * P < r1) k0++;
+    k1 = (int)floor((double)(r2 - w) / P);
+}
+
+// One thread per octant point (x, y, z) in [0, P/2] of the padded grid
+// (mag/newellDemagKernel.go:1166-1252): the tensor at every periodic image
+// x + kx Px, ... inside the kernel ranges, summed in the reference's loop
+// order (z, then y, then x ascending).  Without PBC the only image is k = 0.
+// K order: xx yy zz yz xz xy.
 __global__ void k_newell_octant(double* K0, double* K1, double* K2, double* K3, double* K4, double* K5,
                                 NewellArgs a) {
     long n = (long)a.ext[0] * a.ext[1] * a.ext[2];
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        int x = (int)(i % a.ext[0]);
-        int y = (int)((i / a.ext[0]) % a.ext[1]);
-        int z = (int)(i / ((long)a.ext[0] * a.ext[1]));
-        double Rx = x * a.dx, Ry = y * a.dy, Rz = z * a.dz;
-        double v[6];
-        if (a.use_asym && Rx * Rx > a.arad2 - Rz * Rz - Ry * Ry) {
-            v[0] = -newell::expansion_eval(a.exx, Rx, Ry, Rz);
-            v[5] = -newell::expansion_eval(a.exy, Rx, Ry, Rz);
-            v[4] = -newell::expansion_eval(a.exz, Rx, Rz, Ry);
-            v[1] = -newell::expansion_eval(a.eyy, Ry, Rx, Rz);
-            v[3] = -newell::expansion_eval(a.eyz, Ry, Rz, Rx);
-            v[2] = -newell::expansion_eval(a.ezz, Rz, Ry, Rx);
-        } else {
-            v[0] = newell::sda00(Rx, Ry, Rz, a.dx, a.dy, a.dz) * a.scale;
-            v[5] = newell::sda01(Rx, Ry, Rz, a.dx, a.dy, a.dz) * a.scale;
-            v[4] = newell::sda01(Rx, Rz, Ry, a.dx, a.dz, a.dy) * a.scale;
-            v[1] = newell::sda00(Ry, Rx, Rz, a.dy, a.dx, a.dz) * a.scale;
-            v[3] = newell::sda01(Ry, Rz, Rx, a.dy, a.dz, a.dx) * a.scale;
-            v[2] = newell::sda00(Rz, Ry, Rx, a.dz, a.dy, a.dx) * a.scale;
-        }
-        long I = ((long)z * a.P[1] + y) * a.P[0] + x;
-        K0[I] = v[0]; K1[I] = v[1]; K2[I] = v[2]; K3[I] = v[3]; K4[I] = v[4]; K5[I] = v[5];
+        const int xw = (int)(i % a.ext[0]);
+        const int yw = (int)((i / a.ext[0]) % a.ext[1]);
+        const int zw = (int)(i / ((long)a.ext[0] * a.ext[1]));
+        int kx0, kx1, ky0, ky1, kz0, kz1;
+        image_range(xw, a.P[0], a.r1[0], a.r2[0], kx0, kx1);
+        image_range(yw, a.P[1], a.r1[1], a.r2[1], ky0, ky1);
+        image_range(zw, a.P[2], a.r1[2], a.r2[2], kz0, kz1);
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int kz = kz0; kz <= kz1; kz++)
+            for (int ky = ky0; ky <= ky1; ky++)
+                for (int kx = kx0; kx <= kx1; kx++) {
+                    const int x = xw + kx * a.P[0], y = yw + ky * a.P[1], z = zw + kz * a.P[2];
+                    const double Rx = x * a.dx, Ry = y * a.dy, Rz = z * a.dz;
+                    double v[6];
+                    if (a.use_asym && Rx * Rx > a.arad2 - Rz * Rz - Ry * Ry) {
+                        v[0] = -newell::expansion_eval(a.exx, Rx, Ry, Rz);
+                        v[5] = -newell::expansion_eval(a.exy, Rx, Ry, Rz);
+                        v[4] = -newell::expansion_eval(a.exz, Rx, Rz, Ry);
+                        v[1] = -newell::expansion_eval(a.eyy, Ry, Rx, Rz);
+                        v[3] = -newell::expansion_eval(a.eyz, Ry, Rz, Rx);
+                        v[2] = -newell::expansion_eval(a.ezz, Rz, Ry, Rx);
+                    } else {
+                        v[0] = newell::sda00(Rx, Ry, Rz, a.dx, a.dy, a.dz) * a.scale;
+                        v[5] = newell::sda01(Rx, Ry, Rz, a.dx, a.dy, a.dz) * a.scale;
+                        v[4] = newell::sda01(Rx, Rz, Ry, a.dx, a.dz, a.dy) * a.scale;
+                        v[1] = newell::sda00(Ry, Rx, Rz, a.dy, a.dx, a.dz) * a.scale;
+                        v[3] = newell::sda01(Ry, Rz, Rx, a.dy, a.dz, a.dx) * a.scale;
+                        v[2] = newell::sda00(Rz, Ry, Rx, a.dz, a.dy, a.dx) * a.scale;
+                    }
+                    for (int c = 0; c < 6; c++) acc[c] += v[c];
+                }
+        long I = ((long)zw * a.P[1] + yw) * a.P[0] + xw;
+        K0[I] = acc[0]; K1[I] = acc[1]; K2[I] = acc[2]; K3[I] = acc[3]; K4[I] = acc[4]; K5[I] = acc[5];
     }
 }
 
@@ -416,9 +438,13 @@ static size_t pass_b_smem(const umag_demag* d) { return sizeof(float2) * (size_t
 
 static int plan_common(umag_demag* d) {
     for (int i = 0; i < 3; i++) UMAG_REQUIRE(d->N[i] > 0, "mesh size must be positive");
-    d->P[0] = 2 * d->N[0];
-    d->P[1] = 2 * d->N[1];
-    d->P[2] = d->N[2] > 5 ? 2 * d->N[2] : 2 * d->N[2] - 1;  // mag/demagkernel.go:404-420
+    for (int i = 0; i < 3; i++) UMAG_REQUIRE(d->pbc[i] >= 0, "PBC repetitions must be non-negative");
+    // mag/demagkernel.go:404-420: no padding along a periodic axis
+    d->P[0] = d->pbc[0] ? d->N[0] : 2 * d->N[0];
+    d->P[1] = d->pbc[1] ? d->N[1] : 2 * d->N[1];
+    d->P[2] = d->pbc[2] ? d->N[2] : (d->N[2] > 5 ? 2 * d->N[2] : 2 * d->N[2] - 1);
+    if (d->P[0] % 2 != 0)
+        return set_error(UMAG_E_UNSUPPORTED, "periodic x needs an even Nx (the x transform packs pairs of reals)");
     d->M = d->P[0] / 2;
     d->Hx = d->M + 1;
     d->HxP = d->M + 1;
@@ -469,7 +495,10 @@ static int plan_common(umag_demag* d) {
     UMAG_CUDA(cudaFuncSetAttribute(k_pass_b, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
     UMAG_CUDA(cudaFuncSetAttribute(k_fft_axis<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
     UMAG_TRY(demag_fast_setup());
-    d->use_fast = getenv("UMAG_GENERIC_FFT") == nullptr && demag_fast_select(d->M, d->P[1], d->P[2], d->fast);
+    // the compile-time passes assume a zero-padded half along x and y
+    const bool periodic = d->pbc[0] || d->pbc[1] || d->pbc[2];
+    d->use_fast = !periodic && getenv("UMAG_GENERIC_FFT") == nullptr &&
+                  demag_fast_select(d->M, d->P[1], d->P[2], d->fast);
     if (d->use_fast) UMAG_TRY(demag_fast_grid(d->fast, d->M, d->P[2]));
     return UMAG_OK;
 }
@@ -532,9 +561,12 @@ static int build_newell(const umag_demag* d, const double cell[3], int arad, int
     NewellArgs a{};
     for (int i = 0; i < 3; i++) {
         a.P[i] = d->P[i];
-        a.ext[i] = (d->P[i] - 1) / 2 + 1;  // kernelRanges (mag/demagkernel.go:339-352), x >= 0 half
+        a.ext[i] = d->P[i] / 2 + 1;  // octant [0, P/2]
+        // kernelRanges (mag/demagkernel.go:339-352)
+        if (d->pbc[i] == 0) { a.r1[i] = -(d->P[i] - 1) / 2; a.r2[i] = (d->P[i] - 1) / 2; }
+        else { a.r1[i] = -(d->P[i] * d->pbc[i] - 1); a.r2[i] = d->P[i] * d->pbc[i] - 1; }
     }
-    if (d->P[2] == 1) a.ext[2] = 1;
+    if (d->P[2] == 1 && d->pbc[2] == 0) a.r2[2] = 0;
     double dx = cell[0], dy = cell[1], dz = cell[2];
     newell::reduce_cell(dx, dy, dz);
     a.dx = dx; a.dy = dy; a.dz = dz;
@@ -573,14 +605,13 @@ int demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double
                      int zero_self, umag_demag** out) {
     UMAG_TRY(ensure_init());
     UMAG_REQUIRE(out != nullptr, "out is NULL");
-    if (pbc && (pbc[0] || pbc[1] || pbc[2]))
-        return set_error(UMAG_E_UNSUPPORTED, "periodic boundary conditions are not supported by this build");
     UMAG_REQUIRE(cx > 0 && cy > 0 && cz > 0, "cell size must be positive");
     umag_demag* d = new umag_demag();
     d->N[0] = Nx; d->N[1] = Ny; d->N[2] = Nz;
     d->cell[0] = cx; d->cell[1] = cy; d->cell[2] = cz;
     d->arad = arad;
     d->zero_self = zero_self;
+    for (int i = 0; i < 3; i++) d->pbc[i] = pbc ? pbc[i] : 0;
     int s = plan_common(d);
     if (s != UMAG_OK) { demag_free(d); return s; }
     cudaStream_t st = ctx().stream;
@@ -602,8 +633,6 @@ int demag_new_brute(int Nx, int Ny, int Nz, const int pbc[3], double cx, double 
                     umag_demag** out) {
     UMAG_TRY(ensure_init());
     UMAG_REQUIRE(out != nullptr, "out is NULL");
-    if (pbc && (pbc[0] || pbc[1] || pbc[2]))
-        return set_error(UMAG_E_UNSUPPORTED, "periodic boundary conditions are not supported by this build");
     UMAG_REQUIRE(cx > 0 && cy > 0 && cz > 0, "cell size must be positive");
     UMAG_REQUIRE(accuracy > 0, "demag accuracy must be positive");
     umag_demag* d = new umag_demag();
@@ -611,6 +640,7 @@ int demag_new_brute(int Nx, int Ny, int Nz, const int pbc[3], double cx, double 
     d->cell[0] = cx; d->cell[1] = cy; d->cell[2] = cz;
     d->kind = 1;
     d->accuracy = accuracy;
+    for (int i = 0; i < 3; i++) d->pbc[i] = pbc ? pbc[i] : 0;
     int s = plan_common(d);
     if (s != UMAG_OK) { demag_free(d); return s; }
     cudaStream_t st = ctx().stream;

@@ -36,6 +36,7 @@ struct umag_demag {
     umag::FastPasses fast;
     bool use_fast = false;
     int N[3], P[3];
+    int pbc[3] = {0, 0, 0};  // PBC repetitions per axis (mag/demagkernel.go:339-355); padded size = N there
     double cell[3];
     int arad, zero_self;
     int kind = 0;           // real-space kernel: 0 Newell, 1 brute force, 2 caller-supplied

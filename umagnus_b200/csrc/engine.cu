@@ -878,15 +878,15 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
     UMAG_REQUIRE(p->aLUT != nullptr, "aLUT (exchange LUT) is required");
     UMAG_REQUIRE(sp->solver == 2 || sp->solver == 3 || sp->solver == 4 || sp->solver == 5,
                  "solver must be 2 (Heun), 3 (RK23), 4 (RK4) or 5 (RK45DP)");
-    if (p->pbc[0] || p->pbc[1] || p->pbc[2])
-        return set_error(UMAG_E_UNSUPPORTED, "periodic boundary conditions are not supported by this build");
+    UMAG_REQUIRE(p->pbc[0] >= 0 && p->pbc[1] >= 0 && p->pbc[2] >= 0, "PBC repetitions must be non-negative");
     // engine/exchange.go:62-63
     UMAG_REQUIRE(!(p->dLUT && p->dbulkLUT), "Cannot have induced and interfacial DMI at the same time");
     SimImpl* s = new SimImpl();
     s->p = *p;
     s->sp = *sp;
     s->N = p->N[0] * p->N[1] * p->N[2];
-    s->g = Mesh3{p->N[0], p->N[1], p->N[2], 0};
+    // data/mesh.go PBC_code: the stencils wrap along periodic axes
+    s->g = Mesh3{p->N[0], p->N[1], p->N[2], (p->pbc[0] ? 1 : 0) | (p->pbc[1] ? 2 : 0) | (p->pbc[2] ? 4 : 0)};
     int st = UMAG_OK;
     size_t b3 = sizeof(float) * 3 * (size_t)s->N;
     auto fail = [&](int code) { sim_free(reinterpret_cast<umag_sim*>(s)); return code; };
@@ -898,7 +898,7 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
         s->p.regions = s->zero_regions;
     }
     if (p->enable_demag) {
-        int pbc[3] = {0, 0, 0};
+        const int pbc[3] = {p->pbc[0], p->pbc[1], p->pbc[2]};
         if (p->demag_kernel == 1)
             st = demag_new_brute(p->N[0], p->N[1], p->N[2], pbc, p->cell[0], p->cell[1], p->cell[2],
                                  p->demag_accuracy > 0 ? p->demag_accuracy : 6.0, &s->demag);

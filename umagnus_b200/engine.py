@@ -80,7 +80,8 @@ class Simulation:
     Kc1, Kc2, Kc3, anisC1, anisC2: cubic anisotropy (scalars / 3-vectors or
     per-cell maps); Dbulk: bulk DMI (scalar or 256 per-region values; not
     together with Dind); Temp (K, scalar or per-cell map) with ThermSeed: the
-    thermal field, new noise every accepted step.
+    thermal field, new noise every accepted step; pbc: periodic repetitions
+    per axis (engine/mesh.go SetPBC), 0 = open.
     """
 
     def __init__(self, N, cell, Msat, Aex, alpha, Dind=0.0, Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
@@ -88,7 +89,7 @@ class Simulation:
                  dt=1e-15, MaxErr=1e-5, RelErr=1e-4, MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8,
                  device=0, asymptotic_radius=32, demag_kernel="newell", demag_accuracy=6.0, FrozenSpins=None,
                  Kc1=0.0, Kc2=0.0, Kc3=0.0, anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0,
-                 Temp=0.0, ThermSeed=0):
+                 Temp=0.0, ThermSeed=0, pbc=(0, 0, 0)):
         self.L = _lib.init(device)
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
@@ -97,7 +98,7 @@ class Simulation:
         p = SimParams()
         p.N[:] = self.N
         p.cell[:] = [float(c) for c in cell]
-        p.pbc[:] = (0, 0, 0)
+        p.pbc[:] = tuple(int(x) for x in pbc)  # data/mesh.go PBC repetitions (SetPBC)
 
         def keep(t):
             self._keep.append(t)

@@ -568,6 +568,93 @@ def run_adjoint(args):
     return 0
 
 
+# ------------------------------------------------------------------ thin-film comparison workload
+def run_film(args):
+    """The plain thin film (64x64x1 cells of 4x4x3 nm, Ms 8e5 A/m, Aex
+    1.3e-11 J/m, alpha 0.1, B_ext (0, 0, 10 mT), no anisotropy, m0 random
+    unit vectors from a seed, Newell demag, RK45DP MaxErr 1e-5 to 1 ns) on the
+    GPU engine, beside the reference's float32 kernels on the host cores
+    (oracle/ref_arm.py: the reference's OpenCL C kernels compiled for the
+    host, scipy FFT, the RK45DP controller restated) and the FP64 oracle on the
+    GPU: the average-m time series compared on a common time grid, the final
+    m per cell, step counts and wall times."""
+    import torch
+    from oracle import gpu64
+    from oracle import oracle as O
+    from oracle.ref_arm import RefRK45
+    from umagnus_b200 import engine
+    N, cell, T = (64, 64, 1), (4e-9, 4e-9, 3e-9), args.film_time
+    Ms, Aex, alpha, B = 8e5, 1.3e-11, 0.1, (0.0, 0.0, 0.01)
+    m0 = random_m(N, 1)
+    # GPU engine: wall time of the plain run, then the series step by step
+    sim = engine.Simulation(N, cell, Ms, Aex, alpha, B_ext=B)
+    sim.set_m(m0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.run(T)
+    torch.cuda.synchronize()
+    t_gpu = time.perf_counter() - t0
+    st_gpu = sim.state()
+    m_gpu = sim.get_m().cpu().numpy().reshape(m0.shape)
+    sim.free()
+    sim = engine.Simulation(N, cell, Ms, Aex, alpha, B_ext=B)
+    sim.set_m(m0)
+    ser_gpu = [(0.0, np.array(sim.average_m()))]
+    while sim.state()["time"] < T:
+        before = sim.state()["nsteps"]
+        sim.run(T - sim.state()["time"], chunk=1, max_steps=1)
+        if sim.state()["nsteps"] > before:
+            ser_gpu.append((sim.state()["time"], np.array(sim.average_m())))
+    sim.free()
+    # reference kernels on the host
+    orc = O.Simulation(N, cell, Ms, Aex, alpha, B_ext=B)
+    ref = RefRK45(N, cell, Ms, Aex, alpha, 0.0, 0.0, (0.0, 0.0, 1.0), B, Kf=orc.Kf)
+    orc.set_m(m0)
+    ref.set_m(orc.m)
+    ref.alarm = T
+    ser_ref = [(0.0, ref.m.reshape(3, -1).mean(1).astype(np.float64))]
+    t0 = time.perf_counter()
+    while ref.time < T:
+        if ref.step():
+            ser_ref.append((ref.time, ref.m.reshape(3, -1).mean(1).astype(np.float64)))
+    t_ref = time.perf_counter() - t0
+    # FP64 oracle on the GPU
+    sys64 = gpu64.System64(N, cell, Ms, O.exch_lut(np.full(256, Aex), dtype=np.float64), np.zeros(N[::-1], np.uint8),
+                           alpha, kernel=O.newell_kernel(N, cell), B_ext=B)
+    st64 = gpu64.RK45DP64(sys64, orc.m.astype(np.float64))
+    ser64 = [(0.0, st64.average_m())]
+    while st64.time < T:
+        st64.dt = min(st64.dt, T - st64.time) if st64.time + st64.dt > T else st64.dt
+        if st64.step():
+            ser64.append((st64.time, st64.average_m()))
+    grid = np.linspace(0.0, T, 201)
+
+    def interp(ser):
+        t = np.array([x[0] for x in ser])
+        a = np.array([x[1] for x in ser])
+        return np.stack([np.interp(grid, t, a[:, c]) for c in range(3)], axis=1)
+
+    g, r, f = interp(ser_gpu), interp(ser_ref), interp(ser64)
+    dm_ref = np.abs(m_gpu - ref.m).max()
+    dm_64 = float(np.abs(m_gpu - st64.m.cpu().numpy()).max())
+    line = {"metric": "thin film 64x64x1 to 1 ns: GPU engine vs reference float32 kernels on the host",
+            "value": float(np.abs(g - r).max()), "unit": "max |d<m>| over the run",
+            "higher_is_better": False, "dtype": "f32", "n_gpus": 1, "data": "synthetic (seeded random m0)",
+            "config": {"workload": "64x64x1 cells of 4x4x3 nm, Ms 8e5, Aex 1.3e-11, alpha 0.1, B_ext (0,0,10 mT), "
+                                   f"Newell demag, RK45DP MaxErr 1e-5, t = 0..{T:g} s"},
+            "avg_m_max_abs_diff": {"gpu_vs_reference_f32": float(np.abs(g - r).max()),
+                                   "gpu_vs_fp64": float(np.abs(g - f).max()),
+                                   "reference_f32_vs_fp64": float(np.abs(r - f).max())},
+            "final_avg_m": {"gpu": g[-1].tolist(), "reference_f32": r[-1].tolist(), "fp64": f[-1].tolist()},
+            "final_m_max_abs_diff": {"gpu_vs_reference_f32": float(dm_ref), "gpu_vs_fp64": dm_64},
+            "accepted_steps": {"gpu": int(st_gpu["nsteps"]), "reference_f32": ref.nsteps, "fp64": st64.nsteps},
+            "rejected_steps": {"gpu": int(st_gpu["nundone"]), "reference_f32": ref.nundone, "fp64": st64.nundone},
+            "wall_s": {"gpu": t_gpu, "reference_f32_cpu": t_ref, "reference_threads": ref.threads},
+            "speedup_vs_reference_cpu": t_ref / t_gpu}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ precision workload
 def voronoi_grains(N, ngrain, seed):
     """Columnar Voronoi grains: ngrain seed points uniform in the film plane
@@ -712,11 +799,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=90.0, help="seconds of timed CPU steps (reference arm)")
-    ap.add_argument("--workload", default="multilayer", choices=["multilayer", "ensemble", "adjoint", "precision"])
+    ap.add_argument("--workload", default="multilayer", choices=["multilayer", "ensemble", "adjoint", "precision", "film"])
     ap.add_argument("--adj-fp64", action="store_true", help="adjoint: compare with the FP64 oracle (minutes of CPU)")
     ap.add_argument("--adj-fd", action="store_true", help="adjoint: central differences of the FP32 forward")
     ap.add_argument("--adj-steps", type=int, default=0, help="adjoint: steps instead of 4000")
     ap.add_argument("--prec-steps", type=int, default=2000, help="precision: RK45DP step attempts")
+    ap.add_argument("--film-time", type=float, default=1e-9, help="film: simulated time (s)")
     ap.add_argument("--prec-size", default="512x512x32", help="precision: mesh NxxNyxNz")
     ap.add_argument("--adj-m0", default="easy_axis", choices=["easy_axis", "random"], help="adjoint: initial m")
     ap.add_argument("--ens-time", type=float, default=2e-9, help="ensemble: simulated time per instance (s)")
@@ -728,6 +816,8 @@ def main():
         return run_adjoint(args)
     if args.workload == "precision":
         return run_precision(args)
+    if args.workload == "film":
+        return run_film(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

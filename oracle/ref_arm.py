@@ -40,6 +40,9 @@ class RefRK45:
         clref.set_threads(self.threads)
         self.N = tuple(N)
         self.cell = [float(np.float32(c)) for c in cell]
+        self.cell_f64 = [float(c) for c in cell]
+        self.Dind = float(Dind)
+        self.alarm = None  # engine/run.go:181-184: a step does not cross the alarm time
         self.n = N[0] * N[1] * N[2]
         self.P = O.pad_size(N)
         if Kf is None:
@@ -90,11 +93,17 @@ class RefRK45:
             full = np.ascontiguousarray(full * np.float32(scale), dtype=np.float32)
             clref.call("copyunpad", np.float32, out[c], N[0], N[1], N[2], full, P[0], P[1], P[2])
         c = self.cell
-        clref.call("adddmi", np.float32, out[0], out[1], out[2], m[0], m[1], m[2], None, self.Ms, self.alut,
-                   self.dlut, self.regions, c[0], c[1], c[2], N[0], N[1], N[2], 0, 0)
+        if self.Dind != 0:  # engine/exchange.go:49-66: exchange + DMI, or exchange alone
+            clref.call("adddmi", np.float32, out[0], out[1], out[2], m[0], m[1], m[2], None, self.Ms, self.alut,
+                       self.dlut, self.regions, c[0], c[1], c[2], N[0], N[1], N[2], 0, 0)
+        else:
+            w = [float(np.float32(2.0 / (x * x))) for x in self.cell_f64]
+            clref.call("addexchange", np.float32, out[0], out[1], out[2], m[0], m[1], m[2], None, self.Ms,
+                       self.alut, self.regions, w[0], w[1], w[2], N[0], N[1], N[2], 0)
         u = self.anisU
-        clref.call("adduniaxialanisotropy2", np.float32, out[0], out[1], out[2], m[0], m[1], m[2], None, self.Ms,
-                   None, self.Ku1, None, 0.0, None, u[0], None, u[1], None, u[2], self.n)
+        if self.Ku1 != 0:  # engine/anisotropy.go:40: only with a non-zero constant
+            clref.call("adduniaxialanisotropy2", np.float32, out[0], out[1], out[2], m[0], m[1], m[2], None,
+                       self.Ms, None, self.Ku1, None, 0.0, None, u[0], None, u[1], None, u[2], self.n)
         clref.call("regionaddv", np.float32, out[0], out[1], out[2], self.lut[0], self.lut[1], self.lut[2],
                    self.regions, self.n)
         clref.call("lltorque2", np.float32, out[0], out[1], out[2], m[0], m[1], m[2], out[0], out[1], out[2],
@@ -120,6 +129,8 @@ class RefRK45:
             corr = 1.0
         corr = min(max(corr * self.headroom, 0.5), 2.0)
         self.dt *= corr
+        if self.alarm is not None and self.time < self.alarm and self.time + self.dt > self.alarm:
+            self.dt = self.alarm - self.time
 
     def step(self):
         """One RK45DP attempt (engine/rk45dp.go:12-98); returns True if accepted."""

@@ -384,26 +384,72 @@ def ensemble_instances(count=256, seed=5):
     return out
 
 
+def partition_instances(insts, world):
+    """Instances over ranks, greedy longest-processing-time: largest meshes
+    first, each to the rank with the fewest cells so far (instances are
+    independent: no collective during the run)."""
+    order = sorted(range(len(insts)), key=lambda i: -insts[i]["N"][0] * insts[i]["N"][1])
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += insts[i]["N"][0] * insts[i]["N"][1]
+    return [sorted(x) for x in out]
+
+
 def run_ensemble(args):
     """Batched ensemble vs the plain engine one instance at a time, both to
     t = args.ens_time per instance; the plain form is timed on a per-size
-    sample (args.ens_plain_sample instances of each size) and extrapolated."""
+    sample (args.ens_plain_sample instances of each size) and extrapolated.
+    Under torchrun each rank runs its share of the instances (partition_
+    instances) and the job's time is the slowest rank's."""
     import torch
     from umagnus_b200 import engine
-    insts = ensemble_instances()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    insts_all = ensemble_instances()
+    mine = partition_instances(insts_all, world)[rank]
+    insts = [insts_all[i] for i in mine]
     T = args.ens_time
     ncell = [d["N"][0] * d["N"][1] for d in insts]
-    ens = engine.Ensemble([{k: v for k, v in d.items() if k != "m_seed"} for d in insts])
+    ens = engine.Ensemble([{k: v for k, v in d.items() if k != "m_seed"} for d in insts], device=local_rank)
     for i, d in enumerate(insts):
         ens.set_m(i, random_m(d["N"], d["m_seed"]))
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     ens.run(T, chunk=8)
     torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
+    t_local = time.perf_counter() - t0
     states = [ens.state(i) for i in range(len(insts))]
     acc = np.array([s["nsteps"] for s in states], float)
-    cu_batch = float(np.dot(acc, ncell)) / t_batch
+    (t_batch,), (cells_steps, n_done) = combine_ranks(
+        torch.tensor([t_local], dtype=torch.float64, device="cuda"),
+        torch.tensor([float(np.dot(acc, ncell)), float(len(insts))], dtype=torch.float64, device="cuda"), dist)
+    if dist:
+        dist.destroy_process_group()
+    if world > 1:
+        ens.free()
+        if rank == 0:
+            print(json.dumps({"metric": "RK45DP instances/s, 256-instance thin-film ensemble over ranks",
+                              "value": n_done / t_batch, "unit": "instances/s", "n_gpus": world,
+                              "higher_is_better": True, "scaling": "strong", "dtype": "f32",
+                              "data": "synthetic (seeded instances and m0)",
+                              "config": {"workload": "256 films, partitioned over ranks (largest first)",
+                                         "instances": int(n_done)},
+                              "seconds": t_batch, "cell_updates_per_s": cells_steps / t_batch}), flush=True)
+        return 0
+    cu_batch = cells_steps / t_batch
     # plain form, one instance at a time, on a sample of each size
     per_size = {}
     for n in ENS_SIZES:

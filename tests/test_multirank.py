@@ -53,3 +53,15 @@ def test_combine_ranks_single_process():
     import bench
     t, c = bench.combine_ranks(torch.tensor([1.5, 2.5]), torch.tensor([4.0]), None)
     assert t == [1.5, 2.5] and c == [4.0]
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_partition_instances(world):
+    """Every instance on exactly one rank, loads within one largest mesh."""
+    import bench
+    insts = bench.ensemble_instances()
+    parts = bench.partition_instances(insts, world)
+    flat = sorted(i for p in parts for i in p)
+    assert flat == list(range(len(insts)))
+    loads = [sum(insts[i]["N"][0] * insts[i]["N"][1] for i in p) for p in parts]
+    assert max(loads) - min(loads) <= max(d["N"][0] * d["N"][1] for d in insts)

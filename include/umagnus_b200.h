@@ -252,11 +252,14 @@ typedef struct {
      * (ThermSeed), drawn anew for every accepted step */
     const float* temp; float temp_mul;
     unsigned long long therm_seed;
+    /* NoDemagSpins per region (256 floats, device) or NULL (engine/demag.go:67-98):
+     * cells of regions with a non-zero value neither make nor feel demag field */
+    const float* nodemag_lut;
 } umag_sim_params;
 
 /* Solver knobs, engine/run.go:14-43 (defaults by umag_solver_defaults). */
 typedef struct {
-    int solver;      /* 2 Heun, 3 RK23, 4 RK4, 5 RK45DP (engine/run.go:83-95) */
+    int solver;      /* 1 Euler, 2 Heun, 3 RK23, 4 RK4, 5 RK45DP (engine/run.go:83-95) */
     double dt, min_dt, max_dt, fix_dt, max_err, rel_err, min_slope, headroom, gamma_ll;
 } umag_solver_params;
 
@@ -318,6 +321,27 @@ int umag_sim_energy_density(umag_sim* s, float* dst);
  * torque exceeds it.  The time is left unchanged; solver, MaxErr, FixDt and
  * precession are restored afterwards. */
 int umag_sim_relax(umag_sim* s, double torque_threshold);
+/* Between runs, the script assignments SetSolver(n) / FixDt / MaxErr / RelErr /
+ * MinDt / MaxDt / Headroom / MinSlope / GammaLL (engine/run.go:14-43, :92-125):
+ * the stepper restarts, time and dt are kept (sp->dt is ignored), so FixDt = 0
+ * resumes adaptive stepping from the last dt. */
+int umag_sim_set_solver(umag_sim* s, const umag_solver_params* sp);
+/* Between runs, reassign one material parameter or vector component (Msat = ..., alpha = ...;
+ * engine/parameter.go SetValue / setRegion): `values` a device map of N
+ * floats owned by the caller, or NULL for the uniform value `mul`.  The next
+ * step recomputes the FSAL torque and recaptures its graphs. */
+#define UMAG_PARAM_MSAT 0
+#define UMAG_PARAM_ALPHA 1
+#define UMAG_PARAM_KU1 2
+#define UMAG_PARAM_KU2 3
+#define UMAG_PARAM_TEMP 4
+#define UMAG_PARAM_ANISU_X 5   /* AnisU components: _X + 0, 1, 2 */
+#define UMAG_PARAM_KC1 8
+#define UMAG_PARAM_KC2 9
+#define UMAG_PARAM_KC3 10
+#define UMAG_PARAM_ANISC1_X 11  /* AnisC1 components: _X + 0, 1, 2 */
+#define UMAG_PARAM_ANISC2_X 14  /* AnisC2 components: _X + 0, 1, 2 */
+int umag_sim_set_param(umag_sim* s, int which, const float* values, float mul);
 
 /* ---- ensembles: many independent simulations at once --------------------
  * No counterpart in the reference, which runs one simulation per process.

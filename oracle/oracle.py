@@ -53,6 +53,7 @@ class OrcSystem(ctypes.Structure):
         ("Kc1_mul", ctypes.c_double), ("Kc2_mul", ctypes.c_double), ("Kc3_mul", ctypes.c_double),
         ("c1_mul", ctypes.c_double * 3), ("c2_mul", ctypes.c_double * 3),
         ("cubic", ctypes.c_int), ("dbLUT", ctypes.c_void_p),
+        ("nodemag", ctypes.c_void_p), ("frozen", ctypes.c_void_p),
     ]
 
 
@@ -422,7 +423,8 @@ class Simulation:
                  Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None, regions=None, vol=None,
                  Aex_regions=None, Dind_regions=None, Bext_regions=None, demag=True, openbc=False,
                  precess=True, solver=5, kernel=None, round_kernel_f32=False, Kc1=0.0, Kc2=0.0, Kc3=0.0,
-                 anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0, Dbulk_regions=None):
+                 anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0, Dbulk_regions=None,
+                 NoDemagSpins=None, FrozenSpins=None):
         self.dtype = np.dtype(dtype)
         self.N = tuple(N)
         self.ncell = N[0] * N[1] * N[2]
@@ -489,6 +491,16 @@ class Simulation:
             s.dbLUT = _vp(self.dbLUT)
         s.openbc = int(openbc)
         s.precess = int(precess)
+        # per-region switches (a scalar or 256 values): engine/demag.go:22, engine/torque.go:348
+        for name, val in (("nodemag", NoDemagSpins), ("frozen", FrozenSpins)):
+            if val is not None:
+                lut = np.zeros(256, self.dtype)
+                v = np.asarray(val, self.dtype).ravel()
+                lut[: v.size] = v
+                if v.size == 1:
+                    lut[:] = v[0]
+                setattr(self, name + "_lut", lut)
+                setattr(s, name, _vp(lut))
         # Zeeman LUT (engine/excitation.go:41-53)
         if Bext_regions is not None or B_ext is not None:
             if Bext_regions is None:

@@ -131,6 +131,9 @@ typedef struct {
     double Kc1_mul, Kc2_mul, Kc3_mul, c1_mul[3], c2_mul[3];
     int cubic;
     const void* dbLUT;            /* 32896-entry bulk DMI LUT or NULL */
+    /* per-region LUTs (256 entries) or NULL: NoDemagSpins (engine/demag.go:67-98)
+     * and FrozenSpins (engine/torque.go:348-352) */
+    const void *nodemag, *frozen;
 } orc_system;
 
 typedef struct {

@@ -130,7 +130,7 @@ def test_interfacial_and_bulk_dmi_are_exclusive(eng):
         eng.Simulation((8, 8, 1), (2e-9, 2e-9, 2e-9), 8e5, 1e-11, 0.1, Dind=1e-3, Dbulk=1e-3)
 
 
-@pytest.mark.parametrize("solver", [2, 3, 4, 5])
+@pytest.mark.parametrize("solver", [1, 2, 3, 4, 5])
 def test_fixed_step_trajectory(eng, solver):
     p = thin_film()
     g, o = make_pair(eng, p, solver=solver, fix_dt=2e-13)
@@ -144,6 +144,88 @@ def test_fixed_step_trajectory(eng, solver):
     dm = np.abs(g.get_m().cpu().numpy() - o.m).max()
     assert dm <= 1e-5
     g.free()
+
+
+def test_adaptive_euler_steps(eng):
+    """engine/euler.go:16-35 without FixDt: dt = MaxErr / max|torque| (a
+    float32 step in units of GammaLL), every step accepted, LastErr = MaxErr
+    up to the float32 rounding of dt."""
+    p = thin_film()
+    g, o = make_pair(eng, p, solver=1)
+    for _ in range(6):
+        o.step()
+    g.steps(6)
+    st = g.state()
+    assert st["status"] == 0 and st["nsteps"] == o.solver.nsteps == 6 and st["nundone"] == 0
+    assert st["nevals"] == o.solver.nevals == 6
+    # dt follows max |torque|, whose last bits depend on the demag FFT rounding
+    assert abs(st["time"] - o.solver.time) <= 1e-5 * o.solver.time
+    assert abs(st["last_err"] - 1e-5) <= 1e-12
+    assert abs(st["last_torque"] - o.solver.last_torque) <= 1e-5 * o.solver.last_torque
+    assert np.abs(g.get_m().cpu().numpy() - o.m).max() <= 1e-5
+    g.free()
+
+
+def test_reassign_solver_and_alpha_between_runs(eng):
+    """SetSolver / FixDt / alpha assigned between runs, as test/rk4.mx3 and
+    test/euler.mx3 do: RK4 adaptive, then RK4 with FixDt and a new alpha,
+    then Euler with FixDt, then RK4 adaptive again -- the oracle does the same."""
+    p = thin_film(N=(32, 32, 1), alpha=0.5)
+    g, o = make_pair(eng, p, solver=4)
+    g.run(2e-12)
+    o.run(2e-12)
+    g.set_solver(FixDt=1e-13)
+    g.set_param("alpha", 0.02)
+    o.solver.fix_dt, o.sys.alpha_mul = 1e-13, float(np.float32(0.02))
+    g.run(1e-12)
+    o.run(1e-12)
+    g.set_solver(1)
+    o.solver.solver = 1
+    g.run(5e-13)
+    o.run(5e-13)
+    g.set_solver(4, FixDt=0.0)
+    o.solver.solver, o.solver.fix_dt = 4, 0.0
+    g.run(1e-12)
+    o.run(1e-12)
+    st = g.state()
+    assert st["status"] == 0
+    assert abs(st["time"] - o.solver.time) <= 1e-22
+    assert abs(st["nsteps"] - o.solver.nsteps) <= 2
+    assert np.abs(g.get_m().cpu().numpy() - o.m).max() <= 1e-4
+    g.free()
+
+
+def test_set_param_matches_a_fresh_simulation(eng):
+    """Msat, alpha, Ku1 reassigned on a running simulation give the torque a
+    simulation created with those values gives, bit for bit."""
+    p = multilayer_small()
+    g, _ = make_pair(eng, p)
+    g.steps(3)
+    m = g.get_m().clone()
+    rng = np.random.default_rng(5)
+    shape = (p["N"][2], p["N"][1], p["N"][0])
+    ku1 = (4e5 + 2e5 * rng.random(shape)).astype(np.float32)
+    alpha = (0.1 + 0.2 * rng.random(shape)).astype(np.float32)
+    g.set_param("Msat", 9.5e5)
+    g.set_param("Ku1", ku1)
+    g.set_param("alpha", alpha)
+    f = eng.Simulation(p["N"], p["cell"], 9.5e5, p["Aex"], alpha, Dind=p["Dind"], Ku1=ku1, anisU=p["anisU"],
+                       B_ext=p["B_ext"])
+    f.set_m(m)
+    g.set_m(m)
+    tg, bg = g.torque(beff=True)
+    tf, bf = f.torque(beff=True)
+    assert torch.equal(bg, bf) and torch.equal(tg, tf)
+    # and the next steps agree too (the step graphs were rebuilt)
+    g.set_time(0.0, 5e-14)
+    f.set_time(0.0, 5e-14)
+    g.steps(4)
+    f.steps(4)
+    assert torch.equal(g.get_m(), f.get_m())
+    with pytest.raises(Exception):
+        g.set_param("Aex", 1.0)
+    g.free()
+    f.free()
 
 
 def test_adaptive_rk45dp_short_run(eng):
@@ -229,3 +311,38 @@ def test_pbc_torque_matches_oracle(eng, pbc):
         else:
             assert np.array_equal(t, to)
         g.free()
+
+
+@pytest.mark.parametrize("geom", [False, True])
+def test_no_demag_spins_matches_oracle(eng, geom):
+    """engine/demag.go:67-98 NoDemagSpins: region 1 neither makes nor feels
+    demag field (with and without a geometry mask), against the oracle."""
+    N, cell = (48, 40, 2), (3e-9, 3e-9, 2e-9)
+    regions = np.zeros((2, 40, 48), np.uint8)
+    regions[:, :, 30:] = 1
+    regions[:, :8, :] = 2
+    vol = None
+    if geom:
+        vol = np.ones((2, 40, 48), np.float32)
+        vol[:, 30:, :10] = 0
+    kw = dict(Ku1=3e5, anisU=(0, 0, 1), B_ext=(0.01, 0, 0.02), regions=regions, NoDemagSpins=[0, 1, 0],
+              FrozenSpins=[0, 0, 1])
+    g = eng.Simulation(N, cell, 8e5, 1.3e-11, 0.1, geom=vol, **kw)
+    o = O.Simulation(N, cell, 8e5, 1.3e-11, 0.1, vol=vol, **kw)
+    m = G.random_unit(N, 3)
+    g.set_m(m)
+    o.set_m(m)
+    t, b = g.torque(beff=True)
+    t_o, b_o = o.torque(beff=True)
+    b, t = b.cpu().numpy(), t.cpu().numpy()
+    assert np.abs(b - b_o).max() <= 1e-5 * np.abs(b_o).max()
+    assert np.abs(t - t_o).max() <= 1e-5 * np.abs(t_o).max()
+    # region 1 feels no demag field: B_eff there equals the field without demag
+    nd = eng.Simulation(N, cell, 8e5, 1.3e-11, 0.1, geom=vol, demag=False, **kw)
+    nd.set_m(m)
+    _, b_nd = nd.torque(beff=True)
+    r1 = np.broadcast_to(regions == 1, b.shape)
+    assert np.array_equal(b[r1], b_nd.cpu().numpy()[r1])
+    assert np.all(t[np.broadcast_to(regions == 2, t.shape)] == 0)  # FrozenSpins region 2
+    g.free()
+    nd.free()

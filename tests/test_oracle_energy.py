@@ -57,3 +57,41 @@ def test_relax_lowers_energy_and_torque():
     assert tau1 < 1e-3 * tau0
     assert sim.solver.time == t0
     assert sim.solver.solver == 5 and sim.sys.precess == 1
+
+
+def test_relax_twice_from_exact_equilibrium():
+    """test/regression017.mx3 on the oracle: with m exactly along the easy
+    axis the torque is exactly zero, so every relax step is accepted with
+    err = 0 and dt doubles (87 steps per relax).  After the second relax the
+    float32 step dt*GammaLL would overflow; dt is capped so that it stays
+    finite (2^120) and m stays put instead of turning into NaN."""
+    N = (5, 1, 1)
+    o = O.Simulation(N, (1e-9, 1e-9, 1e-9), 1000e3, 10e-12, 0.02, Ku1=1.3e6, anisU=(0, 0, 1))
+    for mz, steps in ((1.0, 87), (-1.0, 174)):
+        m = np.zeros((3, 1, 1, 5), np.float32)
+        m[2] = mz
+        o.set_m(m)
+        O.relax(o)
+        assert o.solver.status == 0 and o.solver.nsteps == steps
+        assert np.array_equal(o.m[2], np.full((1, 1, 5), mz, np.float32))
+    assert o.solver.dt * o.solver.gamma_ll == pytest.approx(2.0 ** 120, rel=1e-12)
+
+
+def test_no_demag_spins_restatement():
+    """engine/demag.go:67-98 on the oracle: with NoDemagSpins in region 1 the
+    demag field equals that of a geometry without region 1, and is zero in
+    region 1 itself (uniform m: no exchange field, no other terms)."""
+    N, cell = (12, 10, 2), (2e-9, 2e-9, 2e-9)
+    regions = np.zeros((2, 10, 12), np.uint8)
+    regions[:, :, 7:] = 1
+    m = np.zeros((3, 2, 10, 12), np.float32)
+    m[0], m[1], m[2] = 0.6, 0.0, 0.8
+    a = O.Simulation(N, cell, 8e5, 0.0, 0.1, regions=regions, NoDemagSpins=[0, 1])
+    a.set_m(m)
+    _, Ba = a.torque(beff=True)
+    b = O.Simulation(N, cell, 8e5, 0.0, 0.1, regions=regions, vol=(regions == 0).astype(np.float32))
+    b.set_m(m)
+    _, Bb = b.torque(beff=True)
+    r0 = np.broadcast_to(regions == 0, Ba.shape)
+    assert np.array_equal(Ba[r0], Bb[r0]) and np.abs(Ba[r0]).max() > 1e-3
+    assert np.all(Ba[~r0] == 0)

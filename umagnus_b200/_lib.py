@@ -33,6 +33,7 @@ class SimParams(ctypes.Structure):
         ("Kc1", P), ("Kc1_mul", c_float), ("Kc2", P), ("Kc2_mul", c_float), ("Kc3", P), ("Kc3_mul", c_float),
         ("anisC1", P * 3), ("anisC1_mul", c_float * 3), ("anisC2", P * 3), ("anisC2_mul", c_float * 3),
         ("dbulkLUT", P), ("temp", P), ("temp_mul", c_float), ("therm_seed", ctypes.c_ulonglong),
+        ("nodemag_lut", P),
     ]
 
 
@@ -108,6 +109,7 @@ _SIGS = {
     "umag_sim_use_graph": [P, c_int, c_int], "umag_sim_launches_per_step": [P, ctypes.POINTER(c_int)],
     "umag_sim_torque_evals": [P, c_int],
     "umag_sim_energies": [P, ctypes.POINTER(c_double)], "umag_sim_energy_density": [P, P], "umag_sim_relax": [P, c_double],
+    "umag_sim_set_solver": [P, ctypes.POINTER(SolverParams)], "umag_sim_set_param": [P, c_int, P, c_float],
     "umag_field_read_info": [ctypes.c_char_p, P], "umag_field_read": [ctypes.c_char_p, P, c_size_t, P],
     "umag_ovf_write": [ctypes.c_char_p, P, P, ctypes.c_char_p, c_int], "umag_dump_write": [ctypes.c_char_p, P, P],
     "umag_format_float": [c_double, c_int, ctypes.c_char_p, c_int],

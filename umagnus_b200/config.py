@@ -67,3 +67,22 @@ def two_domain(N, cell, m1, mwall, m2):
         side = np.where(X < 0, m1[c], m2[c])
         out.append((1 - gauss) * side + gauss * mwall[c])
     return np.stack(out).astype(np.float32)
+
+
+def _fmod(a, b):
+    """engine/shape.go:222-231 fmod: a folded into (-b/2, b/2]; b = 0 or inf: no folding."""
+    if b == 0 or np.isinf(b):
+        return a
+    folded = np.sign(a) * (np.mod(np.abs(a + b / 2), b) - b / 2)
+    return np.where(np.abs(a) > b / 2, folded, a)
+
+
+def rect(N, cell, sidex, sidey, repeat=(0.0, 0.0, 0.0), transl=(0.0, 0.0, 0.0)):
+    """engine/shape.go:77-82 Rect(sidex, sidey) (strict inequalities), then
+    .Repeat(*repeat) (:216-220) and .Transl(*transl) (:208-212) in that
+    order, as `rect(...).repeat(...).transl(...)` in a script: 1 inside, 0 outside."""
+    X, Y, Z = coords(N, cell)
+    x, y, z = X - transl[0], Y - transl[1], Z - transl[2]
+    x, y, z = _fmod(x, repeat[0]), _fmod(y, repeat[1]), _fmod(z, repeat[2])
+    rx, ry = sidex / 2, sidey / 2
+    return ((x < rx) & (x > -rx) & (y < ry) & (y > -ry)).astype(np.float32)

@@ -210,6 +210,10 @@ int umag_sim_torque_evals(umag_sim* s, int n) { return sim_torque_evals(s, n); }
 int umag_sim_energies(umag_sim* s, double E[5]) { return sim_energies(s, E); }
 int umag_sim_energy_density(umag_sim* s, float* dst) { return sim_energy_density(s, dst); }
 int umag_sim_relax(umag_sim* s, double torque_threshold) { return sim_relax(s, torque_threshold); }
+int umag_sim_set_solver(umag_sim* s, const umag_solver_params* sp) { return sim_set_solver(s, sp); }
+int umag_sim_set_param(umag_sim* s, int which, const float* values, float mul) {
+    return sim_set_param(s, which, values, mul);
+}
 int umag_ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int enable_demag, umag_ens** out) {
     return ens_new(n, in, sp, enable_demag, out);
 }

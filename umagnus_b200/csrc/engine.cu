@@ -84,6 +84,7 @@ struct LocalArgs {
     float wx, wy, wz, cx, cy, cz;
     int dmi, openbc, anis, zeeman, precess;
     const float* frozen;  // FrozenSpins LUT (256) or NULL
+    const float* nodemag; // NoDemagSpins LUT (256) or NULL: demag field zeroed there
     int cubic;            // cubic anisotropy on (cp)
     CubicParams cp;
     const float* dbLUT;   // bulk DMI LUT or NULL
@@ -189,6 +190,8 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
     int I = (iz * a.g.Ny + iy) * a.g.Nx + ix;
     f3 B{0.f, 0.f, 0.f};
     if (bd) B = f3{__ldg(bd + I), __ldg(bd + N + I), __ldg(bd + 2 * N + I)};
+    // engine/demag.go:95-97: NoDemagSpins cells feel no demag field
+    if (!BAT && a.nodemag && __ldg(a.nodemag + (UREG ? 0 : __ldg(a.regions + I))) != 0.0f) B = f3{0.f, 0.f, 0.f};
     f3 m0 = ld3(mx, my, mz, I);
     if (!is0(m0)) {
         f3 e;
@@ -391,6 +394,10 @@ __device__ void adapt_dt(DevCtl* c, double corr) {
     c->dt *= corr;
     if (c->min_dt != 0 && c->dt < c->min_dt) c->dt = c->min_dt;
     if (c->max_dt != 0 && c->dt > c->max_dt) c->dt = c->max_dt;
+    // the float32 step h = dt*GammaLL, times the largest tableau coefficient
+    // (|-355/33| < 16), must stay finite: zero torque (err = 0) doubles dt
+    // every step, and an infinite h turns the stages into Inf*0 = NaN
+    if (c->dt * c->gamma > 0x1p120) c->dt = 0x1p120 / c->gamma;
     if (c->dt == 0) { c->status = 2; return; }
     if (c->t < c->alarm && c->t + c->dt > c->alarm) c->dt = c->alarm - c->t;
     if (!(c->dt > 0)) c->status = 3;
@@ -414,6 +421,7 @@ __global__ void k_step_begin(DevCtl* c0, int nb) {
 
 // kind 0: integralController (engine/stepcontroller.go:35-97), FSAL when fsal
 // kind 1: simpleController (:13-32, RK4); kind 2: Heun (engine/heun.go:40-58)
+// kind 3: Euler (engine/euler.go:16-35), always accepted
 __global__ void k_controller(DevCtl* c0, int nb, int kind, int acc, int rej, int fsal_from, int fsal_to,
                              int nevals) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per instance
@@ -422,6 +430,33 @@ __global__ void k_controller(DevCtl* c0, int nb, int kind, int acc, int rej, int
     if (!c->active) return;
     c->nevals += nevals;
     if (c->nan_seen) c->status = 4;
+    if (kind == 3) {
+        // setMaxTorque(dy0), then dt = FixDt, or float32(MaxErr / LastTorque)
+        // treated as the largest allowed change of m; h is the float32 dt*GammaLL
+        const double lt = sqrt((double)__uint_as_float(c->dm2));
+        c->last_torque = lt;
+        float hf;
+        if (c->fix_dt != 0) {
+            c->dt = c->fix_dt;
+            hf = (float)(c->dt * c->gamma);
+        } else {
+            hf = (float)(c->max_err / lt);
+            c->dt = (double)hf / c->gamma;
+        }
+        if (!(hf > 0.0f)) {  // euler.go:32 "Euler solver requires fixed time step > 0"
+            c->status = 5;
+            c->accepted = 0;
+            return;
+        }
+        c->h = hf;
+        const double err = (double)hf * lt;
+        c->last_err = err;
+        if (err > c->peak_err) c->peak_err = err;
+        c->t = c->t0 + c->dt;
+        c->nsteps++;
+        c->accepted = 1;
+        return;
+    }
     double h = (double)c->h;
     double err = sqrt((double)__uint_as_float(c->err2)) * h;
     double maxdm = sqrt((double)__uint_as_float(c->dm2));
@@ -527,7 +562,8 @@ __device__ __forceinline__ void energy_cell_terms(const LocalArgs& a, const floa
         Mf = f3{fm(Mf.x, w), fm(Mf.y, w), fm(Mf.z, w)};
     }
     for (int k = 0; k < kNE; k++) t[k] = 0.f;
-    if (a.bd) t[0] = dot3(Mf, f3{__ldg(a.bd + I), __ldg(a.bd + N + I), __ldg(a.bd + 2 * N + I)});
+    if (a.bd && !(a.nodemag && __ldg(a.nodemag + __ldg(a.regions + I)) != 0.0f))
+        t[0] = dot3(Mf, f3{__ldg(a.bd + I), __ldg(a.bd + N + I), __ldg(a.bd + 2 * N + I)});
     if (!is0(m0)) {
         const int r0 = __ldg(a.regions + I);
         const f3 e = a.dbLUT ? dmibulk_sum(mx, my, mz, a.aLUT, a.dbLUT, a.regions, a.cx, a.cy, a.cz, a.g,
@@ -593,6 +629,15 @@ __global__ void __launch_bounds__(256) k_energy_terms(LocalArgs a, const float* 
     }
 }
 
+// engine/demag.go:74-83: the demag convolution's volume with NoDemagSpins --
+// a copy of the geometry (ones without one) zeroed where the region's value
+// is non-zero (zeromask.cl), so those cells make no field
+__global__ void k_nodemag_vol(const float* __restrict__ vol, const float* __restrict__ lut,
+                              const uint8_t* __restrict__ regions, float* __restrict__ out, int N) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        out[i] = __ldg(lut + __ldg(regions + i)) != 0.0f ? 0.0f : (vol ? __ldg(vol + i) : 1.0f);
+}
+
 // ---------------------------------------------------------------- host side
 struct SimImpl {
     umag_sim_params p;
@@ -604,6 +649,7 @@ struct SimImpl {
     float* bd = nullptr;          // demag field 3N
     uint8_t* zero_regions = nullptr;
     float* dmi_pairs = nullptr;   // 7 x 32896 region-pair DMI coefficients
+    float* demag_vol = nullptr;   // NoDemagSpins: geometry with the masked regions zeroed
     LocalConsts* kc_dev = nullptr;
     DevCtl* ctl = nullptr;        // device
     DevCtl* hctl = nullptr;       // pinned host mirror
@@ -769,6 +815,19 @@ static int launch_step(SimImpl* s, int* nl) {
         *nl += 1;
         return UMAG_OK;
     }
+    case 1: {  // engine/euler.go:11-36
+        UMAG_TRY(launch_torque(s, 0, 0, nullptr, nullptr, nl));           // dy0
+        UMAG_TRY(launch_err(s, {0, 0}, {1.0, -1.0}, 0, true, nl));        // max |dy0|
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 3, 1, 1, -1, -1, 1);
+        UMAG_LAUNCH_CHECK();
+        *nl += 1;
+        // y = y + dt*dy0 (Madd2), normalised (euler.go:33-34)
+        UMAG_TRY(launch_stage(s, 0, {0}, {1.0}, true, true, true, nl));
+        k_step_end<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0);
+        UMAG_LAUNCH_CHECK();
+        *nl += 1;
+        return UMAG_OK;
+    }
     case 4: {  // engine/rk4.go:11-69
         UMAG_TRY(launch_torque(s, 0, 0, nullptr, nullptr, nl));
         UMAG_TRY(launch_stage(s, 0, {0}, {1. / 2.}, true, true, false, nl));
@@ -871,13 +930,70 @@ static int run_steps(SimImpl* s, long long n) {
     return UMAG_OK;
 }
 
+// The local-term arguments that follow from the material parameters in s->p
+// (and the uniform factors evaluated from them); run at creation and again
+// whenever a parameter is reassigned.
+static int local_from_params(SimImpl* s) {
+    const umag_sim_params* p = &s->p;
+    LocalArgs& la = s->la;
+    la.aLUT = p->aLUT;
+    la.dLUT = p->dLUT;
+    la.regions = s->p.regions;
+    la.wx = (float)(2 / (p->cell[0] * p->cell[0]));
+    la.wy = (float)(2 / (p->cell[1] * p->cell[1]));
+    la.wz = (float)(2 / (p->cell[2] * p->cell[2]));
+    la.cx = (float)p->cell[0]; la.cy = (float)p->cell[1]; la.cz = (float)p->cell[2];
+    la.dmi = p->dLUT != nullptr;
+    la.openbc = p->openbc;
+    la.anis = (p->Ku1 != nullptr || p->Ku1_mul != 0.f || p->Ku2 != nullptr || p->Ku2_mul != 0.f);
+    la.up = UniaxParams{p->Ms, p->Ku1, p->Ku2, p->anisU[0], p->anisU[1], p->anisU[2],
+                        p->Ms_mul, p->Ku1_mul, p->Ku2_mul, p->anisU_mul[0], p->anisU_mul[1], p->anisU_mul[2]};
+    la.zeeman = p->bextLUT[0] != nullptr;
+    for (int i = 0; i < 3; i++) la.bext[i] = p->bextLUT[i];
+    la.alpha = p->alpha;
+    la.alpha_mul = p->alpha_mul;
+    la.precess = p->precess;
+    la.frozen = p->frozen_lut;
+    la.nodemag = p->enable_demag ? p->nodemag_lut : nullptr;
+    la.cubic = (p->Kc1 != nullptr || p->Kc1_mul != 0.f || p->Kc2 != nullptr || p->Kc2_mul != 0.f ||
+                p->Kc3 != nullptr || p->Kc3_mul != 0.f);
+    la.cp = CubicParams{p->Ms, p->Kc1, p->Kc2, p->Kc3, {p->anisC1[0], p->anisC1[1], p->anisC1[2]},
+                        {p->anisC2[0], p->anisC2[1], p->anisC2[2]}, p->Ms_mul, p->Kc1_mul, p->Kc2_mul, p->Kc3_mul,
+                        {p->anisC1_mul[0], p->anisC1_mul[1], p->anisC1_mul[2]},
+                        {p->anisC2_mul[0], p->anisC2_mul[1], p->anisC2_mul[2]}};
+    la.dbLUT = p->dbulkLUT;
+    la.thermal = (p->temp != nullptr || p->temp_mul != 0.f);
+    la.temp = p->temp;
+    la.temp_mul = p->temp_mul;
+    la.seed = p->therm_seed;
+    la.Ms = p->Ms;
+    la.Ms_mul = p->Ms_mul;
+    la.ms_uniform = p->Ms == nullptr;
+    la.alpha_uniform = p->alpha == nullptr;
+    la.anis_uniform = p->Ms == nullptr && p->Ku1 == nullptr && p->Ku2 == nullptr && p->anisU[0] == nullptr &&
+                      p->anisU[1] == nullptr && p->anisU[2] == nullptr;
+    {  // uniform factors, evaluated on the device (bit-identical to the per-cell path)
+        if (!s->kc_dev && cudaMalloc(&s->kc_dev, sizeof(LocalConsts)) != cudaSuccess)
+            return set_error(UMAG_E_NOMEM, "consts");
+        k_local_consts<<<1, 1, 0, S()>>>(la, s->kc_dev);
+        if (cudaMemcpyAsync(&la.kc, s->kc_dev, sizeof(LocalConsts), cudaMemcpyDeviceToHost, S()) != cudaSuccess ||
+            cudaStreamSynchronize(S()) != cudaSuccess)
+            return set_error(UMAG_E_CUDA, "uniform constants");
+    }
+    if (s->demag) {
+        s->pa.Ms = p->Ms;
+        s->pa.Ms_mul = p->Ms_mul;
+    }
+    return UMAG_OK;
+}
+
 int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** out) {
     UMAG_TRY(ensure_init());
     UMAG_REQUIRE(p && sp && out, "NULL argument");
     UMAG_REQUIRE(p->N[0] > 0 && p->N[1] > 0 && p->N[2] > 0, "bad mesh size");
     UMAG_REQUIRE(p->aLUT != nullptr, "aLUT (exchange LUT) is required");
-    UMAG_REQUIRE(sp->solver == 2 || sp->solver == 3 || sp->solver == 4 || sp->solver == 5,
-                 "solver must be 2 (Heun), 3 (RK23), 4 (RK4) or 5 (RK45DP)");
+    UMAG_REQUIRE(sp->solver >= 1 && sp->solver <= 5,
+                 "solver must be 1 (Euler), 2 (Heun), 3 (RK23), 4 (RK4) or 5 (RK45DP)");
     UMAG_REQUIRE(p->pbc[0] >= 0 && p->pbc[1] >= 0 && p->pbc[2] >= 0, "PBC repetitions must be non-negative");
     // engine/exchange.go:62-63
     UMAG_REQUIRE(!(p->dLUT && p->dbulkLUT), "Cannot have induced and interfacial DMI at the same time");
@@ -939,54 +1055,22 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
         s->pa.Ms_mul = p->Ms_mul;
         s->pa.ncell = s->N;
         for (int i = 0; i < 3; i++) s->pa.B[i] = s->bd + (size_t)i * s->N;
+        if (p->nodemag_lut) {  // engine/demag.go:67-98 setMaskedDemagField
+            if (cudaMalloc(&s->demag_vol, sizeof(float) * s->N) != cudaSuccess)
+                return fail(set_error(UMAG_E_NOMEM, "NoDemagSpins volume"));
+            k_nodemag_vol<<<grid_for(s->N, 256), 256, 0, S()>>>(p->vol, p->nodemag_lut, s->p.regions, s->demag_vol,
+                                                                s->N);
+            if (cudaStreamSynchronize(S()) != cudaSuccess) return fail(set_error(UMAG_E_CUDA, "NoDemagSpins volume"));
+            s->pa.vol = s->demag_vol;
+        }
     }
     LocalArgs& la = s->la;
     la.g = s->g;
     la.N = s->N;
     la.ctl = s->ctl;
     la.bd = s->bd;
-    la.aLUT = p->aLUT;
-    la.dLUT = p->dLUT;
-    la.regions = s->p.regions;
-    la.wx = (float)(2 / (p->cell[0] * p->cell[0]));
-    la.wy = (float)(2 / (p->cell[1] * p->cell[1]));
-    la.wz = (float)(2 / (p->cell[2] * p->cell[2]));
-    la.cx = (float)p->cell[0]; la.cy = (float)p->cell[1]; la.cz = (float)p->cell[2];
-    la.dmi = p->dLUT != nullptr;
-    la.openbc = p->openbc;
-    la.anis = (p->Ku1 != nullptr || p->Ku1_mul != 0.f || p->Ku2 != nullptr || p->Ku2_mul != 0.f);
-    la.up = UniaxParams{p->Ms, p->Ku1, p->Ku2, p->anisU[0], p->anisU[1], p->anisU[2],
-                        p->Ms_mul, p->Ku1_mul, p->Ku2_mul, p->anisU_mul[0], p->anisU_mul[1], p->anisU_mul[2]};
-    la.zeeman = p->bextLUT[0] != nullptr;
-    for (int i = 0; i < 3; i++) la.bext[i] = p->bextLUT[i];
-    la.alpha = p->alpha;
-    la.alpha_mul = p->alpha_mul;
-    la.precess = p->precess;
-    la.frozen = p->frozen_lut;
-    la.cubic = (p->Kc1 != nullptr || p->Kc1_mul != 0.f || p->Kc2 != nullptr || p->Kc2_mul != 0.f ||
-                p->Kc3 != nullptr || p->Kc3_mul != 0.f);
-    la.cp = CubicParams{p->Ms, p->Kc1, p->Kc2, p->Kc3, {p->anisC1[0], p->anisC1[1], p->anisC1[2]},
-                        {p->anisC2[0], p->anisC2[1], p->anisC2[2]}, p->Ms_mul, p->Kc1_mul, p->Kc2_mul, p->Kc3_mul,
-                        {p->anisC1_mul[0], p->anisC1_mul[1], p->anisC1_mul[2]},
-                        {p->anisC2_mul[0], p->anisC2_mul[1], p->anisC2_mul[2]}};
-    la.dbLUT = p->dbulkLUT;
-    la.thermal = (p->temp != nullptr || p->temp_mul != 0.f);
-    la.temp = p->temp;
-    la.temp_mul = p->temp_mul;
-    la.seed = p->therm_seed;
-    la.Ms = p->Ms;
-    la.Ms_mul = p->Ms_mul;
-    la.ms_uniform = p->Ms == nullptr;
-    la.alpha_uniform = p->alpha == nullptr;
-    la.anis_uniform = p->Ms == nullptr && p->Ku1 == nullptr && p->Ku2 == nullptr && p->anisU[0] == nullptr &&
-                      p->anisU[1] == nullptr && p->anisU[2] == nullptr;
-    {  // uniform factors, evaluated on the device (bit-identical to the per-cell path)
-        if (cudaMalloc(&s->kc_dev, sizeof(LocalConsts)) != cudaSuccess) return fail(set_error(UMAG_E_NOMEM, "consts"));
-        k_local_consts<<<1, 1, 0, S()>>>(la, s->kc_dev);
-        if (cudaMemcpyAsync(&la.kc, s->kc_dev, sizeof(LocalConsts), cudaMemcpyDeviceToHost, S()) != cudaSuccess ||
-            cudaStreamSynchronize(S()) != cudaSuccess)
-            return fail(set_error(UMAG_E_CUDA, "uniform constants"));
-    }
+    st = local_from_params(s);
+    if (st != UMAG_OK) return fail(st);
     if (la.dmi) {
         const int np = 256 * 257 / 2;
         if (cudaMalloc(&s->dmi_pairs, sizeof(float) * 7 * np) != cudaSuccess)
@@ -1025,6 +1109,7 @@ int sim_free(umag_sim* h) {
     cudaFree(s->bd);
     cudaFree(s->zero_regions);
     cudaFree(s->dmi_pairs);
+    cudaFree(s->demag_vol);
     cudaFree(s->kc_dev);
     cudaFree(s->esum);
     cudaFree(s->ctl);
@@ -1376,6 +1461,77 @@ int sim_relax(umag_sim* h, double threshold) {
     return st;
 }
 
+// Reassigning solver settings between runs: SetSolver (engine/run.go:92-125,
+// the stepper restarts), FixDt, MaxErr, RelErr, MinDt, MaxDt, Headroom,
+// MinSlope, GammaLL.  The current time and dt are kept (assigning FixDt = 0
+// resumes adaptive stepping from the last dt, as adaptDt does).
+int sim_set_solver(umag_sim* h, const umag_solver_params* sp) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && sp, "NULL argument");
+    UMAG_REQUIRE(!s->batched, "solver settings of a batched simulation");
+    UMAG_REQUIRE(sp->solver >= 1 && sp->solver <= 5,
+                 "solver must be 1 (Euler), 2 (Heun), 3 (RK23), 4 (RK4) or 5 (RK45DP)");
+    UMAG_TRY(sync_ctl_to_host(s));
+    DevCtl& c = *s->hctl;
+    c.max_err = sp->max_err; c.rel_err = sp->rel_err; c.min_dt = sp->min_dt; c.max_dt = sp->max_dt;
+    c.fix_dt = sp->fix_dt; c.headroom = sp->headroom; c.min_slope = sp->min_slope;
+    if (c.therm_gv != 0) c.therm_gv = sp->gamma_ll * (s->p.cell[0] * s->p.cell[1] * s->p.cell[2]);
+    c.gamma = sp->gamma_ll;
+    UMAG_TRY(push_ctl(s));
+    const double dt_keep = s->sp.dt;
+    const int prev = s->sp.solver;
+    s->sp = *sp;
+    s->sp.dt = dt_keep;
+    s->sp.solver = prev;
+    set_stepper(s, sp->solver, s->la.precess);  // new graphs only when the stepper changes
+    return UMAG_OK;
+}
+
+// Reassigning a material parameter between runs (engine/parameter.go
+// setRegion / SetValue): a per-cell device map (the caller keeps it alive
+// while the simulation uses it) or NULL with a uniform value.
+int sim_set_param(umag_sim* h, int which, const float* values, float mul) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s, "NULL argument");
+    UMAG_REQUIRE(!s->batched, "parameters of a batched simulation");
+    umag_sim_params& p = s->p;
+    switch (which) {
+    case UMAG_PARAM_MSAT: p.Ms = values; p.Ms_mul = mul; break;
+    case UMAG_PARAM_ALPHA: p.alpha = values; p.alpha_mul = mul; break;
+    case UMAG_PARAM_KU1: p.Ku1 = values; p.Ku1_mul = mul; break;
+    case UMAG_PARAM_KU2: p.Ku2 = values; p.Ku2_mul = mul; break;
+    case UMAG_PARAM_TEMP: p.temp = values; p.temp_mul = mul; break;
+    case UMAG_PARAM_KC1: p.Kc1 = values; p.Kc1_mul = mul; break;
+    case UMAG_PARAM_KC2: p.Kc2 = values; p.Kc2_mul = mul; break;
+    case UMAG_PARAM_KC3: p.Kc3 = values; p.Kc3_mul = mul; break;
+    default:
+        if (which >= UMAG_PARAM_ANISU_X && which <= UMAG_PARAM_ANISU_X + 2) {
+            p.anisU[which - UMAG_PARAM_ANISU_X] = values;
+            p.anisU_mul[which - UMAG_PARAM_ANISU_X] = mul;
+        } else if (which >= UMAG_PARAM_ANISC1_X && which <= UMAG_PARAM_ANISC1_X + 2) {
+            p.anisC1[which - UMAG_PARAM_ANISC1_X] = values;
+            p.anisC1_mul[which - UMAG_PARAM_ANISC1_X] = mul;
+        } else if (which >= UMAG_PARAM_ANISC2_X && which <= UMAG_PARAM_ANISC2_X + 2) {
+            p.anisC2[which - UMAG_PARAM_ANISC2_X] = values;
+            p.anisC2_mul[which - UMAG_PARAM_ANISC2_X] = mul;
+        } else {
+            return set_error(UMAG_E_ARG, "unknown parameter %d", which);
+        }
+    }
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    drop_graph(s);  // the captured launches bake the old arguments in
+    UMAG_TRY(local_from_params(s));
+    if (which == UMAG_PARAM_TEMP) {  // engine/temperature.go:111: gamma V of the noise amplitude
+        UMAG_TRY(sync_ctl_to_host(s));
+        DevCtl& c = *s->hctl;
+        c.therm_gv = s->la.thermal ? s->sp.gamma_ll * (p.cell[0] * p.cell[1] * p.cell[2]) : 0.0;
+        if (c.therm_gv != 0) c.k2 = (float)(2 * kBoltzmann / (c.therm_gv * c.dt));
+        UMAG_TRY(push_ctl(s));
+    }
+    s->need_k1 = true;  // the FSAL torque belongs to the old parameters
+    return UMAG_OK;
+}
+
 // ================================================================ ensembles
 // Many independent simulations advanced together (no reference counterpart:
 // uMagNUS runs one simulation per process).  Instances with the same mesh
@@ -1569,7 +1725,7 @@ static int ens_class_new(EnsClass& C, const umag_ens_instance* in, const std::ve
 int ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int demag, umag_ens** out) {
     UMAG_TRY(ensure_init());
     UMAG_REQUIRE(n > 0 && in && sp && out, "bad argument");
-    UMAG_REQUIRE(sp->solver == 2 || sp->solver == 3 || sp->solver == 4 || sp->solver == 5, "unknown solver");
+    UMAG_REQUIRE(sp->solver >= 1 && sp->solver <= 5, "unknown solver");
     EnsImpl* e = new EnsImpl();
     e->sp = *sp;
     e->where.resize(n);

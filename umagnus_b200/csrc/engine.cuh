@@ -20,6 +20,8 @@ int sim_torque_evals(umag_sim* s, int n);
 int sim_energies(umag_sim* s, double E[5]);
 int sim_energy_density(umag_sim* s, float* dst);
 int sim_relax(umag_sim* s, double threshold);
+int sim_set_solver(umag_sim* s, const umag_solver_params* sp);
+int sim_set_param(umag_sim* s, int which, const float* values, float mul);
 int ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int demag, umag_ens** out);
 int ens_free(umag_ens* e);
 int ens_set_m(umag_ens* e, int i, const float* host_m);

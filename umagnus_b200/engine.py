@@ -20,7 +20,7 @@ from ._lib import EnsInstance, SimParams, SolverParams, SolverState, UmagError, 
 
 NREGION = 256  # engine/regions.go:11
 GAMMA_LL = 1.7595e11  # engine/torque.go:27
-HEUN, BOGAKISHAMPINE, RUNGEKUTTA, DORMANDPRINCE = 2, 3, 4, 5  # engine/run.go:83-95
+EULER, HEUN, BOGAKISHAMPINE, RUNGEKUTTA, DORMANDPRINCE = 1, 2, 3, 4, 5  # engine/run.go:83-95
 
 
 def symmidx(i, j):
@@ -81,7 +81,9 @@ class Simulation:
     per-cell maps); Dbulk: bulk DMI (scalar or 256 per-region values; not
     together with Dind); Temp (K, scalar or per-cell map) with ThermSeed: the
     thermal field, new noise every accepted step; pbc: periodic repetitions
-    per axis (engine/mesh.go SetPBC), 0 = open.
+    per axis (engine/mesh.go SetPBC), 0 = open; NoDemagSpins: a scalar or 256
+    per-region values, cells of non-zero regions neither make nor feel demag
+    field.
     """
 
     def __init__(self, N, cell, Msat, Aex, alpha, Dind=0.0, Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
@@ -89,7 +91,7 @@ class Simulation:
                  dt=1e-15, MaxErr=1e-5, RelErr=1e-4, MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8,
                  device=0, asymptotic_radius=32, demag_kernel="newell", demag_accuracy=6.0, FrozenSpins=None,
                  Kc1=0.0, Kc2=0.0, Kc3=0.0, anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0,
-                 Temp=0.0, ThermSeed=0, pbc=(0, 0, 0)):
+                 Temp=0.0, ThermSeed=0, pbc=(0, 0, 0), NoDemagSpins=None):
         self.L = _lib.init(device)
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
@@ -163,14 +165,20 @@ class Simulation:
         # engine/temperature.go: Temp (K), scalar or per-cell; ThermSeed seeds the noise
         p.temp, p.temp_mul = param(Temp)
         p.therm_seed = int(ThermSeed) & ((1 << 64) - 1)
-        if FrozenSpins is not None:  # engine/torque.go:348-352: a scalar or 256 per-region values
-            fz = np.zeros(NREGION, np.float32)
-            v = np.asarray(FrozenSpins, np.float32).ravel()
-            fz[: v.size] = v
+        def region_lut(val):  # a scalar or up to 256 per-region values
+            lut = np.zeros(NREGION, np.float32)
+            v = np.asarray(val, np.float32).ravel()
+            lut[: v.size] = v
             if v.size == 1:
-                fz[:] = v[0]
-            self.frozen = _dev(fz)
+                lut[:] = v[0]
+            return _dev(lut)
+
+        if FrozenSpins is not None:  # engine/torque.go:348-352
+            self.frozen = region_lut(FrozenSpins)
             p.frozen_lut = keep(self.frozen)
+        if NoDemagSpins is not None:  # engine/demag.go:22, :67-98
+            self.nodemag = region_lut(NoDemagSpins)
+            p.nodemag_lut = keep(self.nodemag)
         sp = SolverParams()
         self.L.umag_solver_defaults(ctypes.byref(sp))
         sp.solver = int(solver)
@@ -251,6 +259,51 @@ class Simulation:
         self.sync()
         self.bext.copy_(torch.from_numpy(np.ascontiguousarray(lut.T)))
         torch.cuda.synchronize()
+
+    _SOLVER_KNOBS = {"FixDt": "fix_dt", "MaxErr": "max_err", "RelErr": "rel_err", "MinDt": "min_dt",
+                     "MaxDt": "max_dt", "Headroom": "headroom", "MinSlope": "min_slope", "GammaLL": "gamma_ll"}
+    _PARAMS = {"Msat": 0, "alpha": 1, "Ku1": 2, "Ku2": 3, "Temp": 4, "Kc1": 8, "Kc2": 9, "Kc3": 10}
+    _VECTORS = {"anisU": 5, "anisC1": 11, "anisC2": 14}
+
+    def set_solver(self, solver=None, **knobs):
+        """Script assignments between runs: SetSolver(solver) and FixDt, MaxErr,
+        RelErr, MinDt, MaxDt, Headroom, MinSlope, GammaLL (engine/run.go:14-43,
+        :92-125).  Time and dt are kept."""
+        sp = self.solver
+        if solver is not None:
+            sp.solver = int(solver)
+        for k, v in knobs.items():
+            if k not in self._SOLVER_KNOBS:
+                raise ValueError(f"unknown solver setting {k!r}")
+            setattr(sp, self._SOLVER_KNOBS[k], float(v))
+        torch.cuda.synchronize()
+        check(self.L.umag_sim_set_solver(self._h, ctypes.byref(sp)))
+
+    def set_param(self, name, value):
+        """Reassign a parameter between runs, as `alpha = 0.02` does in a
+        script: Msat, alpha, Ku1, Ku2, Temp, Kc1, Kc2, Kc3 (a scalar or a
+        (Nz, Ny, Nx) map) or anisU, anisC1, anisC2 (a 3-vector or (3, Nz, Ny, Nx))."""
+        if name in self._VECTORS:
+            v = value if not np.isscalar(value) else None
+            if v is None or len(v) != 3:
+                raise ValueError(f"{name} needs 3 components")
+            for c in range(3):
+                self._set_one(self._VECTORS[name] + c, v[c])
+            return
+        if name not in self._PARAMS:
+            raise ValueError(f"parameter must be one of {sorted(self._PARAMS) + sorted(self._VECTORS)}")
+        self._set_one(self._PARAMS[name], value)
+
+    def _set_one(self, which, value):
+        if np.isscalar(value):
+            t, ptr, mul = None, None, float(np.float32(value))
+        else:
+            t = _dev(np.asarray(value, np.float32).reshape(self.shape))
+            ptr, mul = t.data_ptr(), 1.0
+        torch.cuda.synchronize()
+        check(self.L.umag_sim_set_param(self._h, which, ptr, mul))
+        if t is not None:
+            self._keep.append(t)  # the device map stays alive while the simulation may use it
 
     def energies(self):
         """engine/energy.go:27 GetTotalEnergy and its terms (J) for the current m:

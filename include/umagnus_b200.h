@@ -277,6 +277,9 @@ int umag_sim_free(umag_sim* s);
 /* engine/magnetization.go:55 SetArray: copy m (device, 3 arrays) and normalise. */
 int umag_sim_set_m(umag_sim* s, const float* mx, const float* my, const float* mz);
 int umag_sim_get_m(umag_sim* s, float* mx, float* my, float* mz);   /* device destinations */
+/* Checkpoint resume: copy a state saved by umag_sim_get_m back without
+ * normalising it again (so the trajectory continues bit for bit). */
+int umag_sim_restore_m(umag_sim* s, const float* mx, const float* my, const float* mz);
 /* Device pointers of the current magnetisation (valid until the next step). */
 int umag_sim_m_ptrs(umag_sim* s, float** m3);
 /* engine/torque.go:124 SetTorque / engine/effectivefield.go:14 SetEffectiveField
@@ -342,6 +345,18 @@ int umag_sim_set_solver(umag_sim* s, const umag_solver_params* sp);
 #define UMAG_PARAM_ANISC1_X 11  /* AnisC1 components: _X + 0, 1, 2 */
 #define UMAG_PARAM_ANISC2_X 14  /* AnisC2 components: _X + 0, 1, 2 */
 int umag_sim_set_param(umag_sim* s, int which, const float* values, float mul);
+/* Launch shapes of the per-cell kernels (no reference counterpart; chosen by
+ * the autotuner, umagnus_b200/autotune.py).  Results do not depend on them:
+ * every cell's arithmetic is the same and the reductions are maxima.
+ * torque_block: CTA shape (x multiple of 32, x*y <= 256) of the field +
+ * torque kernel; stage_threads (64, 128 or 256) and stage_waves (CTAs per SM
+ * cap, 1..64) of the stage sums; err_waves of the error norms. */
+typedef struct {
+    int torque_block[2];
+    int stage_threads, stage_waves, err_waves;
+} umag_tuning;
+int umag_sim_get_tuning(umag_sim* s, umag_tuning* t);
+int umag_sim_set_tuning(umag_sim* s, const umag_tuning* t);
 
 /* ---- ensembles: many independent simulations at once --------------------
  * No counterpart in the reference, which runs one simulation per process.

@@ -346,3 +346,45 @@ def test_no_demag_spins_matches_oracle(eng, geom):
     assert np.all(t[np.broadcast_to(regions == 2, t.shape)] == 0)  # FrozenSpins region 2
     g.free()
     nd.free()
+
+
+def test_launch_shapes_do_not_change_results(eng, tmp_path):
+    """Every launch shape the autotuner may choose gives the same trajectory,
+    bit for bit (per-cell arithmetic, max reductions); the autotuner's
+    choice is one of its candidates and is cached."""
+    from umagnus_b200 import autotune
+    p = multilayer_small()
+    m = G.random_unit(p["N"], 4)
+    shapes = [autotune.DEFAULT,
+              {"torque_block": [64, 4], "stage_threads": 128, "stage_waves": 2, "err_waves": 16},
+              {"torque_block": [256, 1], "stage_threads": 64, "stage_waves": 1, "err_waves": 1}]
+    out = []
+    for t in shapes:
+        g = eng.Simulation(p["N"], p["cell"], p["Ms"], p["Aex"], p["alpha"], Dind=p["Dind"], Ku1=p["Ku1"],
+                           anisU=p["anisU"], B_ext=p["B_ext"])
+        g.set_tuning(t)
+        assert g.get_tuning() == t
+        g.set_m(m)
+        g.steps(20)
+        out.append((g.get_m().cpu(), g.state()))
+        g.free()
+    for mm, st in out[1:]:
+        assert torch.equal(mm, out[0][0])
+        assert st["nsteps"] == out[0][1]["nsteps"] and st["time"] == out[0][1]["time"]
+    g = eng.Simulation(p["N"], p["cell"], p["Ms"], p["Aex"], p["alpha"], Dind=p["Dind"], Ku1=p["Ku1"],
+                       anisU=p["anisU"], B_ext=p["B_ext"])
+    g.set_m(m)
+    m_before = g.get_m().clone()
+    cache = str(tmp_path / "tuning.json")
+    best, log = g.autotune(cache_path=cache)
+    assert log is not None and tuple(best["torque_block"]) in autotune.torque_blocks(p["N"][0])
+    assert (best["stage_threads"], best["stage_waves"]) in autotune.STAGE_SHAPES
+    assert torch.equal(g.get_m(), m_before)  # the search restored m and the time
+    assert g.state()["time"] == 0.0
+    again, log2 = g.autotune(cache_path=cache)
+    assert log2 is None and again == best
+    g.steps(20)
+    assert torch.equal(g.get_m().cpu(), out[0][0])
+    with pytest.raises(Exception):
+        g.set_tuning(dict(best, torque_block=[48, 4]))
+    g.free()

@@ -43,6 +43,10 @@ class SolverParams(ctypes.Structure):
                 ("headroom", c_double), ("gamma_ll", c_double)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("torque_block", c_int * 2), ("stage_threads", c_int), ("stage_waves", c_int), ("err_waves", c_int)]
+
+
 class SolverState(ctypes.Structure):
     _fields_ = [("time", c_double), ("dt", c_double), ("last_err", c_double), ("peak_err", c_double),
                 ("last_torque", c_double), ("nsteps", c_ll), ("nundone", c_ll), ("nevals", c_ll),
@@ -102,7 +106,7 @@ _SIGS = {
     "umag_demag_exec_noalloc": [c_int, c_int, c_int, P, P, P, P, P, P, P, P, P, c_float, P],
     "umag_solver_defaults": [ctypes.POINTER(SolverParams)],
     "umag_sim_new": [ctypes.POINTER(SimParams), ctypes.POINTER(SolverParams), ctypes.POINTER(c_void_p)],
-    "umag_sim_free": [P], "umag_sim_set_m": [P, P, P, P], "umag_sim_get_m": [P, P, P, P],
+    "umag_sim_free": [P], "umag_sim_set_m": [P, P, P, P], "umag_sim_restore_m": [P, P, P, P], "umag_sim_get_m": [P, P, P, P],
     "umag_sim_m_ptrs": [P, P], "umag_sim_torque": [P, P, P, P, P, P, P], "umag_sim_steps": [P, c_int],
     "umag_sim_run": [P, c_double, c_int, c_ll], "umag_sim_get_state": [P, ctypes.POINTER(SolverState)],
     "umag_sim_set_time": [P, c_double, c_double], "umag_sim_average_m": [P, ctypes.POINTER(c_double)],
@@ -110,6 +114,7 @@ _SIGS = {
     "umag_sim_torque_evals": [P, c_int],
     "umag_sim_energies": [P, ctypes.POINTER(c_double)], "umag_sim_energy_density": [P, P], "umag_sim_relax": [P, c_double],
     "umag_sim_set_solver": [P, ctypes.POINTER(SolverParams)], "umag_sim_set_param": [P, c_int, P, c_float],
+    "umag_sim_get_tuning": [P, ctypes.POINTER(Tuning)], "umag_sim_set_tuning": [P, ctypes.POINTER(Tuning)],
     "umag_field_read_info": [ctypes.c_char_p, P], "umag_field_read": [ctypes.c_char_p, P, c_size_t, P],
     "umag_ovf_write": [ctypes.c_char_p, P, P, ctypes.c_char_p, c_int], "umag_dump_write": [ctypes.c_char_p, P, P],
     "umag_format_float": [c_double, c_int, ctypes.c_char_p, c_int],

@@ -191,7 +191,12 @@ void umag_solver_defaults(umag_solver_params* p) {
 }
 int umag_sim_new(const umag_sim_params* p, const umag_solver_params* s, umag_sim** out) { return sim_new(p, s, out); }
 int umag_sim_free(umag_sim* s) { return sim_free(s); }
-int umag_sim_set_m(umag_sim* s, const float* mx, const float* my, const float* mz) { return sim_set_m(s, mx, my, mz); }
+int umag_sim_set_m(umag_sim* s, const float* mx, const float* my, const float* mz) {
+    return sim_set_m(s, mx, my, mz, 1);
+}
+int umag_sim_restore_m(umag_sim* s, const float* mx, const float* my, const float* mz) {
+    return sim_set_m(s, mx, my, mz, 0);
+}
 int umag_sim_get_m(umag_sim* s, float* mx, float* my, float* mz) { return sim_get_m(s, mx, my, mz); }
 int umag_sim_m_ptrs(umag_sim* s, float** m3) { return sim_m_ptrs(s, m3); }
 int umag_sim_torque(umag_sim* s, float* tx, float* ty, float* tz, float* bx, float* by, float* bz) {
@@ -214,6 +219,8 @@ int umag_sim_set_solver(umag_sim* s, const umag_solver_params* sp) { return sim_
 int umag_sim_set_param(umag_sim* s, int which, const float* values, float mul) {
     return sim_set_param(s, which, values, mul);
 }
+int umag_sim_get_tuning(umag_sim* s, umag_tuning* t) { return sim_get_tuning(s, t); }
+int umag_sim_set_tuning(umag_sim* s, const umag_tuning* t) { return sim_set_tuning(s, t); }
 int umag_ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int enable_demag, umag_ens** out) {
     return ens_new(n, in, sp, enable_demag, out);
 }

@@ -662,6 +662,7 @@ struct SimImpl {
     cudaGraphExec_t gexec1 = nullptr;  // one step
     int launches_per_step = 0;
     double* esum = nullptr;            // energy term sums (kNE doubles)
+    umag_tuning tune{{32, 8}, 256, 8, 4};  // launch shapes (umag_sim_set_tuning)
     // batched ensemble class: nb same-size instances with uniform parameters
     int nb = 1;
     bool batched = false;
@@ -688,7 +689,8 @@ static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, flo
     la.out_slot = slot;
     la.tau_direct = tau_direct;
     la.beff = beff;
-    dim3 blk(32, 8, 1), grd((s->g.Nx + 31) / 32, (s->g.Ny + 7) / 8, s->g.Nz * s->nb);
+    const int bx = s->tune.torque_block[0], by = s->tune.torque_block[1];
+    dim3 blk(bx, by, 1), grd((s->g.Nx + bx - 1) / bx, (s->g.Ny + by - 1) / by, s->g.Nz * s->nb);
     if (s->batched) k_local_torque<true, true><<<grd, blk, 0, S()>>>(la);
     else if (s->zero_regions) k_local_torque<true, false><<<grd, blk, 0, S()>>>(la);
     else k_local_torque<false, false><<<grd, blk, 0, S()>>>(la);
@@ -712,11 +714,13 @@ static int launch_stage(SimImpl* s, int src_m, std::initializer_list<int> slots,
     a.normalize = normalize;
     a.only_if_accepted = only_if_accepted;
     a.vol = s->p.vol;
-    const dim3 g(s->batched ? (unsigned)((s->N + 255) / 256) : (unsigned)grid_for(s->N, 256), s->nb);
+    const int th = s->tune.stage_threads;
+    const dim3 g(s->batched ? (unsigned)((s->N + th - 1) / th) : (unsigned)grid_for(s->N, th, s->tune.stage_waves),
+                 s->nb);
 #define STAGE(n)                                                    \
     case n:                                                         \
-        if (s->batched) k_stage<n, true><<<g, 256, 0, S()>>>(a);    \
-        else k_stage<n, false><<<g, 256, 0, S()>>>(a);              \
+        if (s->batched) k_stage<n, true><<<g, th, 0, S()>>>(a);     \
+        else k_stage<n, false><<<g, th, 0, S()>>>(a);               \
         break;
     switch (a.nterm) {
         STAGE(2) STAGE(3) STAGE(4) STAGE(5) STAGE(6)
@@ -740,7 +744,8 @@ static int launch_err(SimImpl* s, std::initializer_list<int> slots, std::initial
     for (double e : es) a.e[j++] = (float)e;
     a.dm_slot = dm_slot;
     a.heun = heun;
-    const dim3 g(s->batched ? (unsigned)((s->N + 255) / 256) : (unsigned)grid_for(s->N, 256, 4), s->nb);
+    const dim3 g(s->batched ? (unsigned)((s->N + 255) / 256) : (unsigned)grid_for(s->N, 256, s->tune.err_waves),
+                 s->nb);
 #define ERRN(n, hn)                                                       \
     do {                                                                  \
         if (s->batched) k_err_norms<n, hn, true><<<g, 256, 0, S()>>>(a);  \
@@ -1118,7 +1123,9 @@ int sim_free(umag_sim* h) {
     return UMAG_OK;
 }
 
-int sim_set_m(umag_sim* h, const float* mx, const float* my, const float* mz) {
+// normalise = 0 restores a state read by sim_get_m exactly (normalising an
+// already normalised float32 vector may change its last bit)
+int sim_set_m(umag_sim* h, const float* mx, const float* my, const float* mz, int normalise) {
     SimImpl* s = reinterpret_cast<SimImpl*>(h);
     UMAG_REQUIRE(s && mx && my && mz, "NULL argument");
     UMAG_TRY(sync_ctl_to_host(s));
@@ -1128,7 +1135,8 @@ int sim_set_m(umag_sim* h, const float* mx, const float* my, const float* mz) {
     UMAG_CUDA(cudaMemcpyAsync(m + s->N, my, b, cudaMemcpyDeviceToDevice, S()));
     UMAG_CUDA(cudaMemcpyAsync(m + 2 * s->N, mz, b, cudaMemcpyDeviceToDevice, S()));
     // engine/magnetization.go:34 normalize() (normalize2.cl)
-    UMAG_TRY(normalize(m, m + s->N, m + 2 * s->N, s->p.vol, s->N));
+    if (normalise) UMAG_TRY(normalize(m, m + s->N, m + 2 * s->N, s->p.vol, s->N));
+    else UMAG_CUDA(cudaStreamSynchronize(S()));
     s->need_k1 = true;
     return UMAG_OK;
 }
@@ -1484,6 +1492,29 @@ int sim_set_solver(umag_sim* h, const umag_solver_params* sp) {
     s->sp.dt = dt_keep;
     s->sp.solver = prev;
     set_stepper(s, sp->solver, s->la.precess);  // new graphs only when the stepper changes
+    return UMAG_OK;
+}
+
+// Launch shapes of the per-cell kernels: any valid shape gives the same
+// results (per-cell arithmetic, max reductions), only the speed differs.
+int sim_get_tuning(umag_sim* h, umag_tuning* t) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && t, "NULL argument");
+    *t = s->tune;
+    return UMAG_OK;
+}
+int sim_set_tuning(umag_sim* h, const umag_tuning* t) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s && t, "NULL argument");
+    const int bx = t->torque_block[0], by = t->torque_block[1];
+    UMAG_REQUIRE(bx >= 32 && bx % 32 == 0 && by >= 1 && bx * by <= 256, "torque block %dx%d", bx, by);
+    UMAG_REQUIRE(t->stage_threads == 64 || t->stage_threads == 128 || t->stage_threads == 256,
+                 "stage threads %d", t->stage_threads);
+    UMAG_REQUIRE(t->stage_waves >= 1 && t->stage_waves <= 64 && t->err_waves >= 1 && t->err_waves <= 64,
+                 "waves must be 1..64");
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    s->tune = *t;
+    drop_graph(s);  // the captured launches carry the old shapes
     return UMAG_OK;
 }
 

@@ -5,7 +5,7 @@
 namespace umag {
 int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** out);
 int sim_free(umag_sim* s);
-int sim_set_m(umag_sim* s, const float* mx, const float* my, const float* mz);
+int sim_set_m(umag_sim* s, const float* mx, const float* my, const float* mz, int normalise);
 int sim_get_m(umag_sim* s, float* mx, float* my, float* mz);
 int sim_m_ptrs(umag_sim* s, float** m3);
 int sim_torque(umag_sim* s, float* tx, float* ty, float* tz, float* bx, float* by, float* bz);
@@ -22,6 +22,8 @@ int sim_energy_density(umag_sim* s, float* dst);
 int sim_relax(umag_sim* s, double threshold);
 int sim_set_solver(umag_sim* s, const umag_solver_params* sp);
 int sim_set_param(umag_sim* s, int which, const float* values, float mul);
+int sim_get_tuning(umag_sim* s, umag_tuning* t);
+int sim_set_tuning(umag_sim* s, const umag_tuning* t);
 int ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int demag, umag_ens** out);
 int ens_free(umag_ens* e);
 int ens_set_m(umag_ens* e, int i, const float* host_m);

@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import EnsInstance, SimParams, SolverParams, SolverState, UmagError, check
+from ._lib import EnsInstance, SimParams, SolverParams, SolverState, Tuning, UmagError, check
 
 NREGION = 256  # engine/regions.go:11
 GAMMA_LL = 1.7595e11  # engine/torque.go:27
@@ -198,6 +198,13 @@ class Simulation:
         check(self.L.umag_sim_set_m(self._h, t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr()))
         check(self.L.umag_sync())
 
+    def restore_m(self, m):
+        """Put back a state read by get_m, without normalising it again
+        (checkpoint resume: the trajectory continues bit for bit)."""
+        t = m.contiguous()
+        torch.cuda.synchronize()
+        check(self.L.umag_sim_restore_m(self._h, t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr()))
+
     def m_ptrs(self):
         ptrs = (ctypes.c_void_p * 3)()
         check(self.L.umag_sim_m_ptrs(self._h, ptrs))
@@ -334,6 +341,28 @@ class Simulation:
     def set_stream(self, stream):
         """Queue all library work on a torch.cuda.Stream (None = library stream)."""
         check(self.L.umag_set_stream(None if stream is None else stream.cuda_stream))
+
+    def get_tuning(self):
+        """Launch shapes of the per-cell kernels (umag_tuning) as a dict."""
+        t = Tuning()
+        check(self.L.umag_sim_get_tuning(self._h, ctypes.byref(t)))
+        return {"torque_block": [t.torque_block[0], t.torque_block[1]], "stage_threads": t.stage_threads,
+                "stage_waves": t.stage_waves, "err_waves": t.err_waves}
+
+    def set_tuning(self, tuning):
+        """Apply launch shapes (a dict like get_tuning's); results are unchanged."""
+        t = Tuning()
+        t.torque_block[0], t.torque_block[1] = (int(v) for v in tuning["torque_block"])
+        t.stage_threads, t.stage_waves, t.err_waves = (int(tuning[k]) for k in ("stage_threads", "stage_waves",
+                                                                                "err_waves"))
+        torch.cuda.synchronize()
+        check(self.L.umag_sim_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self, cache_path=None, use_cache=True):
+        """Choose the fastest launch shapes for this mesh on this GPU
+        (umagnus_b200.autotune.tune); returns (tuning, timings or None)."""
+        from . import autotune
+        return autotune.tune(self, cache_path=cache_path, use_cache=use_cache)
 
     def launches_per_step(self):
         n = ctypes.c_int()

@@ -524,7 +524,8 @@ def adjoint_problem(seed=4, m0_kind="easy_axis"):
 
 def run_adjoint(args):
     """Forward and backward of the differentiation workload, timed with CUDA
-    events (each call returns after its work ends).  Options: --adj-steps
+    events (each call returns after its work ends).  Options: --adj-solver
+    (rk4, the workload's stepper, or heun), --adj-steps
     (fewer steps, the probe average over the last quarter), --adj-fd
     (central differences of the FP32 forward, relative step 1e-4: Aex, Ku1,
     B_ext and 64 random cells of Ms), --adj-fp64 (the FP64 oracle's reverse
@@ -536,7 +537,9 @@ def run_adjoint(args):
         kw["nsteps"] = args.adj_steps
         kw["avg_from"] = args.adj_steps - args.adj_steps // 4 + 1
     nsteps = kw["nsteps"]
-    sim = AdjointRK4(K=min(100, nsteps), **kw)
+    solver = 2 if args.adj_solver == "heun" else 4
+    sim = AdjointRK4(K=min(100, nsteps), solver=solver, **kw)
+    sname = "Heun" if solver == 2 else "RK4"
     fw, bw = [], []
     for it in range(max(args.warmup, 1) + args.steps):
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -553,12 +556,12 @@ def run_adjoint(args):
     N = 128 * 128
     gMs = g["Ms"].cpu().numpy()
     cells = np.random.default_rng(7).choice(N, 64, replace=False)
-    line = {"metric": f"adjoint backward/forward time, 128x128x1 film, RK4 {nsteps} steps",
+    line = {"metric": f"adjoint backward/forward time, 128x128x1 film, {sname} {nsteps} steps",
             "value": b / f, "unit": "backward/forward", "n_gpus": 1, "steps": args.steps,
             "warmup": max(args.warmup, 1), "higher_is_better": False, "dtype": "f32",
             "data": "synthetic (seeded Ms map, m0 and target)",
             "config": {"workload": "128x128x1 film, 4 nm cells, per-cell Ms U[6e5,9e5], Aex 1.3e-11, Ku1 2e5 along x, "
-                                   f"alpha 0.02, B_ext (5,5,0) mT, Newell demag, fixed-step RK4 dt 1e-13 s x {nsteps}, "
+                                   f"alpha 0.02, B_ext (5,5,0) mT, Newell demag, fixed-step {sname} dt 1e-13 s x {nsteps}, "
                                    f"checkpoints every {min(100, nsteps)} steps", "cells": N,
                        "m0": "uniform along +x" if args.adj_m0 == "easy_axis" else "random unit vectors"},
             "forward_s": f, "backward_s": b,
@@ -603,7 +606,7 @@ def run_adjoint(args):
     if args.adj_fp64:
         from oracle import adjoint_ref as R
         t0 = time.perf_counter()
-        prob = R.Problem(**kw)
+        prob = R.Problem(solver=solver, **kw)
         loss64, g64 = prob.backward(m0.astype(np.float64).reshape(3, 1, 128, 128),
                                     R.params(Ms.astype(np.float64), th["Aex"], th["Ku1"], th["B_ext"]))
         per_cell = np.abs(gMs.ravel()[cells] - g64["Ms"].ravel()[cells]) / np.abs(g64["Ms"].ravel()[cells])
@@ -858,6 +861,7 @@ def main():
     ap.add_argument("--film-time", type=float, default=1e-9, help="film: simulated time (s)")
     ap.add_argument("--prec-size", default="512x512x32", help="precision: mesh NxxNyxNz")
     ap.add_argument("--adj-m0", default="easy_axis", choices=["easy_axis", "random"], help="adjoint: initial m")
+    ap.add_argument("--adj-solver", default="rk4", choices=["rk4", "heun"], help="adjoint: fixed-step stepper")
     ap.add_argument("--ens-time", type=float, default=2e-9, help="ensemble: simulated time per instance (s)")
     ap.add_argument("--ens-plain-sample", type=int, default=2, help="ensemble: plain-form instances timed per size")
     args = ap.parse_args()

@@ -391,7 +391,7 @@ int umag_ens_count(umag_ens* e, int* n_instances, int* n_classes);
  * No counterpart in the reference (which has no gradients).  A thin film or
  * block with a per-cell Ms map, uniform exchange Aex, uniaxial Ku1 along
  * anisU, Zeeman field B_ext and damping alpha, integrated by fixed-step RK4
- * (engine/rk4.go with FixDt) for nsteps steps; m is checkpointed every K
+ * (engine/rk4.go with FixDt) or Heun (engine/heun.go) for nsteps steps; m is checkpointed every K
  * steps.  Loss = w_probe * (mean over states avg_from..nsteps of the mean
  * m_z over the probe window of layer 0) + w_target * |<m>(final) - target|^2.
  * umag_adj_backward returns dLoss/dMs (per cell), dLoss/dAex, dLoss/dKu1,
@@ -413,6 +413,7 @@ typedef struct {
     double w_probe, w_target;
     double target[3];
     int no_graph;           /* 1: plain stream launches instead of CUDA graphs */
+    int solver;             /* 4 (or 0) RK4, 2 Heun (engine/heun.go with FixDt) */
 } umag_adj_params;
 typedef struct umag_adj umag_adj;
 int umag_adj_new(const umag_adj_params* p, umag_adj** out);

@@ -1,4 +1,5 @@
-"""FP64 CPU restatement of the differentiable RK4 simulation and its adjoint.
+"""FP64 CPU restatement of the differentiable fixed-step simulation (RK4 or
+Heun) and its adjoint.
 
 TEST INFRASTRUCTURE ONLY: tests/ and bench.py import this module to check
 the GPU adjoint (umag_adj_*); the product never does.
@@ -7,7 +8,8 @@ The model is the engine's effective field and LL torque for uniform region
 0 (engine/effectivefield.go:14-24, engine/demag.go, engine/exchange.go,
 engine/anisotropy.go, engine/zeeman.go, engine/torque.go:135-144) with a
 per-cell Ms map, stepped by fixed-step RK4 (engine/rk4.go:35-61, every stage
-normalised, opencl normalize2.cl).  The reference has no gradients; this
+normalised, opencl normalize2.cl) or Heun (engine/heun.go:27-43: the
+predictor m + h k0 is not normalised, the result is).  The reference has no gradients; this
 module gives the FP64 gradient two ways: a hand-written reverse pass (the
 same vector-Jacobian products as the GPU adjoint, in FP64) and central
 finite differences of the FP64 forward, so that the two can pin each other.
@@ -26,7 +28,10 @@ class Problem:
     """Static part of the problem: mesh, demag kernel, stepper, loss."""
 
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, probe, avg_from, w_probe=1.0, w_target=1.0,
-                 target=(0.0, 0.0, 1.0), demag=True, gamma_ll=GAMMA_LL):
+                 target=(0.0, 0.0, 1.0), demag=True, gamma_ll=GAMMA_LL, solver=4):
+        if solver not in (2, 4):
+            raise ValueError("solver must be 4 (RK4) or 2 (Heun)")
+        self.solver = int(solver)
         self.N = tuple(int(n) for n in N)
         self.cell = tuple(float(c) for c in cell)
         self.alpha = float(alpha)
@@ -93,6 +98,14 @@ class Problem:
 
     def step(self, m, th, keep=False):
         h = self.h
+        if self.solver == 2:  # engine/heun.go:30-43 with FixDt
+            B0 = self.field(m, th)
+            k0 = self.torque(m, B0)
+            y1 = m + h * k0
+            B1 = self.field(y1, th)
+            k1 = self.torque(y1, B1)
+            out = self.normalize(y1 + 0.5 * h * k1 - 0.5 * h * k0)
+            return (out, [m, y1], [B0, B1], [k0, k1]) if keep else out
         ms, Bs, ks = [m], [], []
         for q in range(4):
             B = self.field(ms[q], th)
@@ -173,6 +186,19 @@ class Problem:
         wB = g * (wxm + a * np.cross(wxm, m, axis=0))
         return gm, wB
 
+    def _heun_step_vjp(self, m, ms, Bs, ks, lam, th, grads):
+        """dL/dm of one Heun step out = normalize(y1 + h/2 k1 - h/2 k0), y1 =
+        m + h k0, k_q = torque(state_q, field(state_q)), given dL/dout."""
+        h = self.h
+        y1 = ms[1]
+        gz = self._norm_vjp(y1 + 0.5 * h * ks[1] - 0.5 * h * ks[0], lam)
+        gk0 = -0.5 * h * gz
+        gm1, wB = self._torque_vjp(y1, Bs[1], 0.5 * h * gz)
+        ly1 = gz + gm1 + self._field_vjp(y1, wB, th, grads)  # dL/dy1
+        gk0 = gk0 + h * ly1
+        gm0, wB = self._torque_vjp(m, Bs[0], gk0)
+        return ly1 + gm0 + self._field_vjp(m, wB, th, grads)
+
     def backward(self, m0, th):
         """Gradient of forward(m0, th) by the reverse pass (all states kept)."""
         loss, states = self.forward(m0, th, keep=True)
@@ -184,6 +210,11 @@ class Problem:
         for n in range(self.nsteps, 0, -1):
             m = states[n - 1]
             _, ms, Bs, ks = self.step(m, th, keep=True)
+            if self.solver == 2:
+                lam = self._heun_step_vjp(m, ms, Bs, ks, lam, th, grads)
+                if n - 1 >= self.avg_from:
+                    lam = lam + self._loss_grad(states[n - 1], True, False)
+                continue
             u = m + sum(f * k for f, k in zip(fin, ks))
             gu = self._norm_vjp(u, lam)
             lam2 = gu.copy()

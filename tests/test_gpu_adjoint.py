@@ -1,4 +1,4 @@
-"""GPU adjoint (umag_adj_*): the forward pass against the engine's RK4, the
+"""GPU adjoint (umag_adj_*): the forward pass against the engine's RK4 and Heun, the
 gradients against the FP64 oracle's reverse pass (itself pinned to central
 finite differences in tests/test_oracle_adjoint.py), and the autograd
 wrapper.  The problem is the differentiation workload (per-cell Ms map in
@@ -30,20 +30,22 @@ def make_case(n, steps, seed):
     return Ms, m0, kw
 
 
-def gpu_sim(kw, K, use_graph=True):
+def gpu_sim(kw, K, use_graph=True, solver=4):
     from umagnus_b200.adjoint import AdjointRK4
-    return AdjointRK4(K=K, use_graph=use_graph, **kw)
+    return AdjointRK4(K=K, use_graph=use_graph, solver=solver, **kw)
 
 
-def test_forward_matches_engine_rk4():
-    """The adjoint's forward pass is the engine's fixed-step RK4, bit for bit."""
-    from umagnus_b200.engine import RUNGEKUTTA, Simulation
+@pytest.mark.parametrize("solver", [4, 2])
+def test_forward_matches_engine(solver):
+    """The adjoint's forward pass is the engine's fixed-step RK4 (or Heun),
+    bit for bit."""
+    from umagnus_b200.engine import Simulation
     Ms, m0, kw = make_case(32, 40, 1)
-    adj = gpu_sim(kw, K=16)
+    adj = gpu_sim(kw, K=16, solver=solver)
     adj.forward(m0, Ms, A_EX, KU1, BEXT)
     m_adj = adj.final_m().cpu().numpy()
     sim = Simulation(kw["N"], CELL, Msat=Ms, Aex=A_EX, alpha=0.02, Ku1=KU1, anisU=(1.0, 0.0, 0.0), B_ext=BEXT,
-                     solver=RUNGEKUTTA, dt=1e-13, FixDt=1e-13)
+                     solver=solver, dt=1e-13, FixDt=1e-13)
     sim.set_m(m0)
     sim.steps(40)
     m_eng = sim.get_m().cpu().numpy().reshape(m_adj.shape)
@@ -55,13 +57,13 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-@pytest.mark.parametrize("n,steps,K", [(16, 30, 7), (32, 60, 16)])
-def test_gradients_match_fp64_oracle(n, steps, K):
+@pytest.mark.parametrize("n,steps,K,solver", [(16, 30, 7, 4), (32, 60, 16, 4), (16, 30, 7, 2), (32, 60, 16, 2)])
+def test_gradients_match_fp64_oracle(n, steps, K, solver):
     Ms, m0, kw = make_case(n, steps, 2 + n)
-    adj = gpu_sim(kw, K=K)
+    adj = gpu_sim(kw, K=K, solver=solver)
     loss = adj.forward(m0, Ms, A_EX, KU1, BEXT)
     g = adj.backward()
-    prob = R.Problem(**{k: v for k, v in kw.items()})
+    prob = R.Problem(solver=solver, **{k: v for k, v in kw.items()})
     th = R.params(Ms.astype(np.float64), A_EX, KU1, BEXT)
     loss64, g64 = prob.backward(m0.astype(np.float64), th)
     assert abs(loss - loss64) <= 1e-5 * max(1.0, abs(loss64))
@@ -73,8 +75,8 @@ def test_gradients_match_fp64_oracle(n, steps, K):
         assert e < 1e-3, (k, e)
 
 
-def _run(kw, K, Ms, m0, use_graph=True):
-    adj = gpu_sim(kw, K=K, use_graph=use_graph)
+def _run(kw, K, Ms, m0, use_graph=True, solver=4):
+    adj = gpu_sim(kw, K=K, use_graph=use_graph, solver=solver)
     loss = adj.forward(m0, Ms, A_EX, KU1, BEXT)
     g = adj.backward()
     return (loss, g["Ms"].cpu().numpy(), g["m0"].cpu().numpy(), g["Aex"], g["Ku1"], tuple(g["B_ext"]))
@@ -86,13 +88,14 @@ def _same(a, b):
     assert a[3:] == b[3:]
 
 
-def test_segment_length_does_not_change_gradients():
+@pytest.mark.parametrize("solver", [4, 2])
+def test_segment_length_does_not_change_gradients(solver):
     """The checkpoint interval K only changes what is recomputed: results
     are bit-identical (per-cell FP64 accumulators, fixed-order reduction)."""
     Ms, m0, kw = make_case(16, 24, 9)
-    ref = _run(kw, 24, Ms, m0)
+    ref = _run(kw, 24, Ms, m0, solver=solver)
     for K in (1, 5, 7):
-        _same(_run(kw, K, Ms, m0), ref)
+        _same(_run(kw, K, Ms, m0, solver=solver), ref)
 
 
 def test_graphs_match_stream_launches():
@@ -145,3 +148,5 @@ def test_argument_errors():
     adj = gpu_sim(kw, K=4)
     with pytest.raises(UmagError):
         adj.backward()  # no forward yet
+    with pytest.raises(UmagError):
+        gpu_sim(kw, K=4, solver=5)  # RK4 and Heun only

@@ -1,4 +1,4 @@
-"""The FP64 oracle of the differentiable RK4 simulation: its reverse pass
+"""The FP64 oracle of the differentiable RK4 and Heun simulations: its reverse pass
 against central finite differences of its own forward (relative step 1e-4,
 randomly chosen cells), and the loss definition on hand-checkable cases.
 CPU only."""
@@ -10,21 +10,21 @@ from oracle import adjoint_ref as R
 CELL = (4e-9, 4e-9, 4e-9)
 
 
-def case(n=12, steps=24, seed=5, demag=True):
+def case(n=12, steps=24, seed=5, demag=True, solver=4):
     rng = np.random.default_rng(seed)
     Ms = rng.uniform(6e5, 9e5, (1, n, n))
     m0 = rng.normal(size=(3, 1, n, n))
     t = rng.normal(size=3)
     t /= np.linalg.norm(t)
     prob = R.Problem((n, n, 1), CELL, 0.02, (1.0, 0.0, 0.0), 1e-13, steps, (n // 4, n // 4, n // 2, n // 2),
-                     steps - steps // 4 + 1, target=t, demag=demag)
+                     steps - steps // 4 + 1, target=t, demag=demag, solver=solver)
     th = R.params(Ms, 1.3e-11, 2e5, (5e-3, 5e-3, 0.0))
     return prob, m0, th, rng
 
 
-@pytest.mark.parametrize("demag", [True, False])
-def test_reverse_pass_matches_central_fd(demag):
-    prob, m0, th, rng = case(demag=demag)
+@pytest.mark.parametrize("demag,solver", [(True, 4), (False, 4), (True, 2), (False, 2)])
+def test_reverse_pass_matches_central_fd(demag, solver):
+    prob, m0, th, rng = case(demag=demag, solver=solver)
     _, g = prob.backward(m0, th)
     checks = [("A", None), ("K1", None), ("B", 0), ("B", 1), ("B", 2)]
     n = m0.shape[-1]
@@ -36,8 +36,9 @@ def test_reverse_pass_matches_central_fd(demag):
         assert abs(fd - ad) <= 1e-4 * abs(fd) + 1e-12 * max(1.0, abs(ad)), (which, fd, ad)
 
 
-def test_m0_gradient_matches_fd():
-    prob, m0, th, rng = case(n=8, steps=12)
+@pytest.mark.parametrize("solver", [4, 2])
+def test_m0_gradient_matches_fd(solver):
+    prob, m0, th, rng = case(n=8, steps=12, solver=solver)
     _, g = prob.backward(m0, th)
     for _ in range(6):
         c, y, x = int(rng.integers(3)), int(rng.integers(8)), int(rng.integers(8))

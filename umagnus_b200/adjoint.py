@@ -1,10 +1,11 @@
-"""Differentiable fixed-step RK4 simulation on the device (umag_adj_*).
+"""Differentiable fixed-step RK4 or Heun simulation on the device (umag_adj_*).
 
 No counterpart in the reference, which has no gradients.  The forward pass
 is the engine's effective field (demag, exchange, uniaxial anisotropy,
 Zeeman; engine/effectivefield.go:14-24) and LL torque (engine/torque.go)
 for a per-cell Ms map and uniform Aex, Ku1, B_ext and alpha, stepped by
-fixed-step RK4 (engine/rk4.go with FixDt), m checkpointed every K steps.
+fixed-step RK4 (engine/rk4.go with FixDt) or Heun (engine/heun.go, solver=2),
+m checkpointed every K steps.
 The loss is
 
     w_probe * mean over states avg_from..nsteps of the mean m_z in the probe
@@ -31,7 +32,7 @@ GAMMA_LL = 1.7595e11  # engine/torque.go:27
 class AdjointRK4:
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, K, probe, avg_from, w_probe=1.0, w_target=1.0,
                  target=(0.0, 0.0, 1.0), demag=True, demag_kernel="newell", demag_accuracy=6.0, gamma_ll=GAMMA_LL,
-                 use_graph=True, device=0):
+                 use_graph=True, device=0, solver=4):
         self.L = _lib.init(device)
         p = AdjParams()
         p.N[:] = [int(n) for n in N]
@@ -48,6 +49,7 @@ class AdjointRK4:
         p.w_probe, p.w_target = float(w_probe), float(w_target)
         p.target[:] = [float(t) for t in target]
         p.no_graph = 0 if use_graph else 1
+        p.solver = int(solver)  # 4 RK4, 2 Heun
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
         h = ctypes.c_void_p()
@@ -107,6 +109,15 @@ class AdjointRK4:
             self.free()
         except Exception:
             pass
+
+
+class AdjointHeun(AdjointRK4):
+    """The same differentiable simulation stepped by fixed-step Heun
+    (engine/heun.go: predictor m + h k0 unnormalised, result normalised)."""
+
+    def __init__(self, *args, **kw):
+        kw["solver"] = 2
+        super().__init__(*args, **kw)
 
 
 class _AdjFn(torch.autograd.Function):

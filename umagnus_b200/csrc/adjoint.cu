@@ -1,11 +1,13 @@
-// adjoint.cu -- a differentiable fixed-step RK4 simulation (no counterpart in
-// the reference): forward pass with checkpoints of m every K steps, backward
-// pass by hand-written vector-Jacobian products.
+// adjoint.cu -- a differentiable fixed-step RK4 or Heun simulation (no
+// counterpart in the reference): forward pass with checkpoints of m every K
+// steps, backward pass by hand-written vector-Jacobian products.
 //
 // Model (the engine's field and stepper, engine/effectivefield.go,
 // engine/torque.go, engine/rk4.go): B = demag(Ms m) + exchange(A)/Ms +
 // uniaxial(K1, u)/Ms + B_ext, torque = LL torque with alpha, RK4 with fixed
-// dt and every stage normalised.  Parameters: a per-cell Ms map, uniform A,
+// dt and every stage normalised, or Heun (engine/heun.go:27-43: predictor
+// y1 = m + h k0 not normalised, result normalize(y1 + h/2 k1 - h/2 k0)).
+// Parameters: a per-cell Ms map, uniform A,
 // K1 and B_ext (the differentiable ones) and uniform alpha and easy axis.
 // Loss: w_probe * mean over states avg_from..nsteps of the mean m_z over a
 // probe window + w_target * |<m>_final - target|^2.
@@ -50,10 +52,14 @@ struct AdjField {
     int probe[4];      // x0, y0, width, height
 };
 
-// RK4 weights (engine/rk4.go:35-61): stage offsets 1/2, 1/2, 1 and the final
-// combination 1/6, 1/3, 1/3, 1/6, each float32(c) * h as Madd takes them
-struct Rk4Fac {
+// Stepper weights, each float32(c) * h as Madd takes them.  RK4
+// (engine/rk4.go:35-61): stage offsets 1/2, 1/2, 1 and the final combination
+// 1/6, 1/3, 1/3, 1/6.  Heun (engine/heun.go:31, :42): h for the predictor,
+// 0.5h and -0.5h for the result (Madd3 rounding, madd3.cl).
+struct StepFac {
+    int heun;
     float st[3], fin[4];
+    float h, hh, mhh;
 };
 
 __device__ __forceinline__ bool in_probe(const AdjField& a, int I) {
@@ -100,13 +106,14 @@ __device__ __forceinline__ void st3(float* p, int N, int I, f3 v) {
 __device__ __forceinline__ f3 ld3p(const float* p, int N, int I) { return f3{p[I], p[N + I], p[2 * N + I]}; }
 
 // ---------------------------------------------------------------- forward
-// Stage q of an RK4 step of state m: field and torque k_q of stage state mq
+// Stage q of a step of state m: field and torque k_q of stage state mq
 // (B_q kept if Bq), then per cell the next stage state
-//   q < 3: mnext = normalize(m + st[q] k_q)
-//   q = 3: mnext = normalize(m + fin0 k0 + fin1 k1 + fin2 k2 + fin3 k3)
-// with the Madd<n> rounding order (the engine's k_stage), and for q = 3 the
-// probe's m_z sum of mnext added to *psum when psum != NULL.
-__global__ void __launch_bounds__(256) k_adj_stage_fwd(AdjField a, Rk4Fac f, int q, const float* __restrict__ mq,
+//   RK4 q < 3: mnext = normalize(m + st[q] k_q)
+//   RK4 q = 3: mnext = normalize(m + fin0 k0 + fin1 k1 + fin2 k2 + fin3 k3)
+//   Heun q = 0: mnext = m + h k0;  q = 1: mnext = normalize(mq + hh k1 + mhh k0)
+// with the Madd<n> rounding order (the engine's k_stage), and for the last
+// stage the probe's m_z sum of mnext added to *psum when psum != NULL.
+__global__ void __launch_bounds__(256) k_adj_stage_fwd(AdjField a, StepFac f, int q, const float* __restrict__ mq,
                                                        const float* __restrict__ bd, float* Bq, float* kq,
                                                        const float* __restrict__ m, const float* k0,
                                                        const float* k1, const float* k2, float* mnext,
@@ -123,7 +130,10 @@ __global__ void __launch_bounds__(256) k_adj_stage_fwd(AdjField a, Rk4Fac f, int
         for (int c = 0; c < 3; c++) {
             const int o = c * N + I;
             float s = fm(1.0f, m[o]);
-            if (q < 3) {
+            if (f.heun) {
+                if (q == 0) s = fa(s, fm(f.h, tk[c]));                                       // y1 = m + h k0
+                else s = fa(fm(1.0f, mq[o]), fa(fm(f.hh, tk[c]), fm(f.mhh, k0[o])));         // y1 + h/2 k1 - h/2 k0
+            } else if (q < 3) {
                 s = fa(s, fm(f.st[q], tk[c]));
             } else {
                 s = fa(s, fm(f.fin[0], k0[o]));
@@ -133,7 +143,8 @@ __global__ void __launch_bounds__(256) k_adj_stage_fwd(AdjField a, Rk4Fac f, int
             }
             v[c] = s;
         }
-        const f3 r = normalize_vol(f3{v[0], v[1], v[2]}, 1.0f);
+        // Heun's predictor is not normalised (heun.go:31)
+        const f3 r = (f.heun && q == 0) ? f3{v[0], v[1], v[2]} : normalize_vol(f3{v[0], v[1], v[2]}, 1.0f);
         st3(mnext, N, I, r);
         if (psum && in_probe(a, I)) acc += (double)r.z;
     }
@@ -180,7 +191,7 @@ __device__ __forceinline__ void torque_vjp(float alpha, float gilb, f3 m, f3 B, 
 // Start of the reverse of one step, per cell: u = m + sum_j fin_j k_j,
 // g_u = VJP(normalize)(u; lam); lam2 = g_u; gk_j = fin_j g_u (j < 3); and the
 // torque VJP of stage 3 with cotangent fin_3 g_u -> gm, wB.
-__global__ void __launch_bounds__(256) k_adj_rev_start(AdjField a, Rk4Fac f, const float* __restrict__ m,
+__global__ void __launch_bounds__(256) k_adj_rev_start(AdjField a, StepFac f, const float* __restrict__ m,
                                                        const float* __restrict__ k0, const float* __restrict__ k1,
                                                        const float* __restrict__ k2, const float* __restrict__ k3,
                                                        const float* __restrict__ m3, const float* __restrict__ B3,
@@ -210,6 +221,33 @@ __global__ void __launch_bounds__(256) k_adj_rev_start(AdjField a, Rk4Fac f, con
     }
 }
 
+// Start of the reverse of one Heun step, per cell: z = y1 + hh k1 + mhh k0
+// (the forward's rounding), g_z = VJP(normalize)(z; lam); lam2 = g_z (the
+// part of dL/dy1 through z); gk0 = mhh g_z; and the torque VJP of stage 1
+// (state y1, field B1) with cotangent hh g_z -> gm, wB.
+__global__ void __launch_bounds__(256) k_adj_rev_start_heun(AdjField a, StepFac f, const float* __restrict__ y1,
+                                                            const float* __restrict__ k0,
+                                                            const float* __restrict__ k1,
+                                                            const float* __restrict__ B1,
+                                                            const float* __restrict__ lam, float* lam2, float* gk0,
+                                                            float* gm, float* wB) {
+    const int N = a.N;
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x) {
+        float z[3];
+        for (int c = 0; c < 3; c++) {
+            const int o = c * N + I;
+            z[c] = fa(fm(1.0f, y1[o]), fa(fm(f.hh, k1[o]), fm(f.mhh, k0[o])));
+        }
+        const f3 gz = norm_vjp(f3{z[0], z[1], z[2]}, ld3p(lam, N, I));
+        st3(lam2, N, I, gz);
+        st3(gk0, N, I, sc3(f.mhh, gz));
+        f3 g, w;
+        torque_vjp(a.alpha, a.gilb, ld3p(y1, N, I), ld3p(B1, N, I), sc3(f.hh, gz), g, w);
+        st3(gm, N, I, g);
+        st3(wB, N, I, w);
+    }
+}
+
 // Stage q of the reverse, per cell.  In: gm = torque-VJP part of dL/dm_q,
 // wB = dL/dB_q (all cells: the exchange transpose reads neighbours), dw =
 // mu0 K wB (demag of the cotangent) or NULL.  Field VJP:
@@ -220,9 +258,12 @@ __global__ void __launch_bounds__(256) k_adj_rev_start(AdjField a, Rk4Fac f, con
 //   q > 0: m_q = normalize(m + st[q-1] k_{q-1}): g_u = VJP; lam2 += g_u;
 //          dL/dk_{q-1} = gk_{q-1} + st[q-1] g_u, and the torque VJP of stage
 //          q-1 with it -> gm (in place), wBn
+//   Heun q = 1: y1 = m + h k0 (not normalised): l = lam2 + dL/dy1 here is the
+//          whole dL/dy1 (the part through z is in lam2), lam2 = l (m enters
+//          y1 with weight 1), dL/dk0 = gk0 + h l, and the torque VJP of stage 0
 //   q = 0: lam2 += dL/dm_0, plus the probe term wprobe (m_z in the window)
 // acc: per-cell FP64 accumulators [Ms | A | K1 | Bx | By | Bz] (N each).
-__global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, Rk4Fac f, int q, float A,
+__global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, int q, float A,
                                                        const float* __restrict__ mq, const float* __restrict__ wB,
                                                        const float* __restrict__ dw, float* gm,
                                                        const float* __restrict__ m, const float* __restrict__ kprev,
@@ -282,7 +323,14 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, Rk4Fac f, int
         acc[4 * (size_t)N + I] += w.y;
         acc[5 * (size_t)N + I] += w.z;
         f3 l = ld3p(lam2, N, I);
-        if (q > 0) {
+        if (q > 0 && f.heun) {
+            l = ad3(l, g);
+            const f3 gk = ad3(ld3p(gkprev, N, I), sc3(f.h, l));
+            f3 gn, wn;
+            torque_vjp(a.alpha, a.gilb, ld3p(mprev, N, I), ld3p(Bprev, N, I), gk, gn, wn);
+            st3(gm, N, I, gn);
+            st3(wBn, N, I, wn);
+        } else if (q > 0) {
             const float c = f.st[q - 1];
             const f3 M = ld3p(m, N, I), Kp = ld3p(kprev, N, I);
             const f3 u{fa(fm(1.0f, M.x), fm(c, Kp.x)), fa(fm(1.0f, M.y), fm(c, Kp.y)), fa(fm(1.0f, M.z), fm(c, Kp.z))};
@@ -368,6 +416,8 @@ struct AdjImpl {
     Mesh3 g{};
     umag_demag* demag = nullptr;
     float h = 0;          // float32(dt * GammaLL)
+    bool heun = false;    // Heun instead of RK4
+    int nst() const { return heun ? 2 : 4; }
     float* Ms = nullptr;  // per-cell Ms of the last forward
     float A = 0, A00 = 0, K1 = 0, B[3] = {0, 0, 0};
     std::vector<float*> ckpt;  // m at steps 0, K, 2K, ...
@@ -407,8 +457,12 @@ static AdjField adj_field(const AdjImpl* s) {
     return a;
 }
 
-static Rk4Fac rk4_fac(float h) {
-    Rk4Fac f;
+static StepFac step_fac(float h, bool heun) {
+    StepFac f{};
+    f.heun = heun ? 1 : 0;
+    f.h = (float)1. * h;       // Madd2(y, y, dy0, 1, dt)
+    f.hh = (float)0.5 * h;     // Madd3(y, y, dy, dy0, 1, 0.5*dt, -0.5*dt)
+    f.mhh = (float)-0.5 * h;
     f.st[0] = (float)(1. / 2.) * h;
     f.st[1] = (float)(1. / 2.) * h;
     f.st[2] = (float)1. * h;
@@ -432,26 +486,29 @@ static int adj_demag(AdjImpl* s, const float* v, const float* Ms, float* out) {
     return demag_launch(s->demag, a, AS());
 }
 
-// one RK4 step m -> mout (engine/rk4.go:35-61 with fixed dt).  st (or NULL)
-// receives m2..m4 (st[0..2]), B1..B4 (st[3..6]) and k1..k4 (st[7..10]);
-// psum (or NULL) accumulates the probe's m_z sum of mout.
-static int adj_step(AdjImpl* s, const AdjField& af, const Rk4Fac& f, const float* m, float* mout, float* const* st,
+// one step m -> mout (engine/rk4.go:35-61 or engine/heun.go:27-43 with fixed
+// dt).  st (or NULL) receives the stage states after m (st[0..2]: m2..m4, or
+// Heun's y1), the fields (st[3..6]) and the torques (st[7..10]); psum (or
+// NULL) accumulates the probe's m_z sum of mout.
+static int adj_step(AdjImpl* s, const AdjField& af, const StepFac& f, const float* m, float* mout, float* const* st,
                     double* psum) {
+    const int nst = s->nst();
     float* k[4];
     float* Bs[4];
     float* next[4];
     const float* ms[4];
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < nst; q++) {
         k[q] = st ? st[7 + q] : s->w(W_K + q);
         Bs[q] = st ? st[3 + q] : nullptr;
-        next[q] = q < 3 ? (st ? st[q] : s->w(W_MS + q)) : mout;
+        next[q] = q < nst - 1 ? (st ? st[q] : s->w(W_MS + q)) : mout;
         ms[q] = q == 0 ? m : next[q - 1];
     }
     const float* bd = s->demag ? s->w(W_BD) : nullptr;
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < nst; q++) {
         UMAG_TRY(adj_demag(s, ms[q], s->Ms, s->w(W_BD)));
-        k_adj_stage_fwd<<<gridN(s), 256, 0, AS()>>>(af, f, q, ms[q], bd, Bs[q], k[q], m, k[0], k[1], k[2], next[q],
-                                                     q == 3 ? psum : nullptr);
+        k_adj_stage_fwd<<<gridN(s), 256, 0, AS()>>>(af, f, q, ms[q], bd, Bs[q], k[q], m, k[0], nst > 1 ? k[1] : nullptr,
+                                                     nst > 2 ? k[2] : nullptr, next[q],
+                                                     q == nst - 1 ? psum : nullptr);
         UMAG_LAUNCH_CHECK();
     }
     return UMAG_OK;
@@ -524,10 +581,12 @@ int adj_new(const umag_adj_params* p, umag_adj** out) {
     UMAG_REQUIRE(p->probe[2] > 0 && p->probe[3] > 0 && p->probe[0] >= 0 && p->probe[1] >= 0 &&
                      p->probe[0] + p->probe[2] <= p->N[0] && p->probe[1] + p->probe[3] <= p->N[1],
                  "probe window outside the mesh");
+    UMAG_REQUIRE(p->solver == 0 || p->solver == 2 || p->solver == 4, "solver must be 4 (RK4) or 2 (Heun)");
     AdjImpl* s = new AdjImpl();
     s->p = *p;
     s->N = p->N[0] * p->N[1] * p->N[2];
     s->g = Mesh3{p->N[0], p->N[1], p->N[2], 0};
+    s->heun = p->solver == 2;
     s->h = (float)(p->dt * (p->gamma_ll > 0 ? p->gamma_ll : 1.7595e11));  // engine/torque.go:27 GammaLL
     auto fail = [&](int c) {
         adj_free(reinterpret_cast<umag_adj*>(s));
@@ -573,7 +632,7 @@ int adj_forward(umag_adj* hd, const float* m0, const float* Ms, float A, float K
     s->K1 = K1;
     for (int c = 0; c < 3; c++) s->B[c] = Bext[c];
     const AdjField af = adj_field(s);
-    const Rk4Fac f = rk4_fac(s->h);
+    const StepFac f = step_fac(s->h, s->heun);
     UMAG_CUDA(cudaMemcpyAsync(s->w(W_M0), m0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
     float* a0 = s->w(W_A);
     UMAG_CUDA(cudaMemcpyAsync(a0, m0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
@@ -634,7 +693,7 @@ int adj_final_m(umag_adj* hd, float* m) {
 // the reverse of one segment: recompute its steps from slot(0, 11) keeping
 // every stage, then the steps in reverse with lam = dL/d(state at the
 // segment's end) in W_LAM, leaving dL/d(state at its start) in W_LAM
-static int adj_rev_segment(AdjImpl* s, const AdjField& af, const Rk4Fac& f, int n_begin, int len, float wprobe) {
+static int adj_rev_segment(AdjImpl* s, const AdjField& af, const StepFac& f, int n_begin, int len, float wprobe) {
     const umag_adj_params& p = s->p;
     const unsigned G = gridN(s);
     const size_t n3 = s->n3();
@@ -655,11 +714,15 @@ static int adj_rev_segment(AdjImpl* s, const AdjField& af, const Rk4Fac& f, int 
         const float* ms[4] = {m, s->slot(j, 0), s->slot(j, 1), s->slot(j, 2)};
         const float* Bs[4] = {s->slot(j, 3), s->slot(j, 4), s->slot(j, 5), s->slot(j, 6)};
         const float* ks[4] = {s->slot(j, 7), s->slot(j, 8), s->slot(j, 9), s->slot(j, 10)};
-        // stage q's field cotangent lives in wb[q & 1]
-        k_adj_rev_start<<<G, 256, 0, AS()>>>(af, f, m, ks[0], ks[1], ks[2], ks[3], ms[3], Bs[3], lam, lam2, gk[0],
-                                              gk[1], gk[2], gm, wb[1]);
+        // stage q's field cotangent lives in wb[q & 1] (the last stage: wb[1])
+        const int nst = s->nst();
+        if (s->heun)
+            k_adj_rev_start_heun<<<G, 256, 0, AS()>>>(af, f, ms[1], ks[0], ks[1], Bs[1], lam, lam2, gk[0], gm, wb[1]);
+        else
+            k_adj_rev_start<<<G, 256, 0, AS()>>>(af, f, m, ks[0], ks[1], ks[2], ks[3], ms[3], Bs[3], lam, lam2,
+                                                  gk[0], gk[1], gk[2], gm, wb[1]);
         UMAG_LAUNCH_CHECK();
-        for (int q = 3; q >= 0; q--) {
+        for (int q = nst - 1; q >= 0; q--) {
             float* wcur = wb[q & 1];
             float* wnext = wb[(q + 1) & 1];
             UMAG_TRY(adj_demag(s, wcur, nullptr, s->w(W_BD)));
@@ -685,7 +748,7 @@ int adj_backward(umag_adj* hd, float* gMs, float* gm0, double* gA, double* gK1, 
     const int N = s->N;
     const size_t n3 = s->n3();
     const unsigned G = gridN(s);
-    const Rk4Fac f = rk4_fac(s->h);
+    const StepFac f = step_fac(s->h, s->heun);
     const AdjField af = adj_field(s);
     UMAG_CUDA(cudaMemsetAsync(s->acc, 0, sizeof(double) * 6 * (size_t)N, AS()));
     const float wprobe = (float)(p.w_probe / ((double)(p.nsteps - p.avg_from + 1) * p.probe[2] * p.probe[3]));

@@ -350,10 +350,14 @@ int umag_sim_set_param(umag_sim* s, int which, const float* values, float mul);
  * every cell's arithmetic is the same and the reductions are maxima.
  * torque_block: CTA shape (x multiple of 32, x*y <= 256) of the field +
  * torque kernel; stage_threads (64, 128 or 256) and stage_waves (CTAs per SM
- * cap, 1..64) of the stage sums; err_waves of the error norms. */
+ * cap, 1..64) of the stage sums; err_waves of the error norms; torque_tma
+ * (1 = default) feeds the torque kernel's stencils from TMA-loaded tiles with
+ * a halo where the mesh allows it (non-periodic, Nx a multiple of 4, no
+ * region map, no bulk DMI, block width <= 248), 0 = plain global loads. */
 typedef struct {
     int torque_block[2];
     int stage_threads, stage_waves, err_waves;
+    int torque_tma;
 } umag_tuning;
 int umag_sim_get_tuning(umag_sim* s, umag_tuning* t);
 int umag_sim_set_tuning(umag_sim* s, const umag_tuning* t);

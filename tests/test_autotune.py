@@ -19,16 +19,17 @@ def test_torque_blocks_fit_the_kernel():
 
 
 def test_search_finds_the_separable_minimum():
-    # a fake timer whose optimum is torque 64x2, stage 128/16, err 8
+    # a fake timer whose optimum is torque 64x2 with global loads, stage 128/16, err 8
     def measure(kind, t):
         bx, by = t["torque_block"]
-        c = abs(bx - 64) / 64 + abs(by - 2) / 2
+        c = abs(bx - 64) / 64 + abs(by - 2) / 2 + 0.1 * t["torque_tma"]
         c += abs(t["stage_threads"] - 128) / 128 + abs(t["stage_waves"] - 16) / 16 + abs(t["err_waves"] - 8) / 8
         return 1.0 + c
 
     best, log = A.search(measure, 256)
-    assert best == {"torque_block": [64, 2], "stage_threads": 128, "stage_waves": 16, "err_waves": 8}
-    assert len(log["torque"]) == len(A.torque_blocks(256))
+    assert best == {"torque_block": [64, 2], "stage_threads": 128, "stage_waves": 16, "err_waves": 8,
+                    "torque_tma": 0}
+    assert len(log["torque"]) == 2 * len(A.torque_blocks(256))
     assert len(log["stage"]) == len(A.STAGE_SHAPES) and len(log["err"]) == len(A.ERR_WAVES)
     assert A.DEFAULT["torque_block"] == [32, 8]  # the defaults are not modified
 

@@ -349,15 +349,18 @@ def test_no_demag_spins_matches_oracle(eng, geom):
 
 
 def test_launch_shapes_do_not_change_results(eng, tmp_path):
-    """Every launch shape the autotuner may choose gives the same trajectory,
-    bit for bit (per-cell arithmetic, max reductions); the autotuner's
-    choice is one of its candidates and is cached."""
+    """Every launch shape the autotuner may choose -- including the torque
+    kernel's TMA tiles against its global loads -- gives the same
+    trajectory, bit for bit (per-cell arithmetic, max reductions); the
+    autotuner's choice is one of its candidates and is cached."""
     from umagnus_b200 import autotune
     p = multilayer_small()
     m = G.random_unit(p["N"], 4)
     shapes = [autotune.DEFAULT,
-              {"torque_block": [64, 4], "stage_threads": 128, "stage_waves": 2, "err_waves": 16},
-              {"torque_block": [256, 1], "stage_threads": 64, "stage_waves": 1, "err_waves": 1}]
+              {"torque_block": [64, 4], "stage_threads": 128, "stage_waves": 2, "err_waves": 16, "torque_tma": 1},
+              {"torque_block": [32, 8], "stage_threads": 256, "stage_waves": 8, "err_waves": 4, "torque_tma": 0},
+              {"torque_block": [128, 2], "stage_threads": 64, "stage_waves": 1, "err_waves": 1, "torque_tma": 1},
+              {"torque_block": [256, 1], "stage_threads": 64, "stage_waves": 1, "err_waves": 1, "torque_tma": 0}]
     out = []
     for t in shapes:
         g = eng.Simulation(p["N"], p["cell"], p["Ms"], p["Aex"], p["alpha"], Dind=p["Dind"], Ku1=p["Ku1"],

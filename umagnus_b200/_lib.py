@@ -44,7 +44,8 @@ class SolverParams(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("torque_block", c_int * 2), ("stage_threads", c_int), ("stage_waves", c_int), ("err_waves", c_int)]
+    _fields_ = [("torque_block", c_int * 2), ("stage_threads", c_int), ("stage_waves", c_int), ("err_waves", c_int),
+                ("torque_tma", c_int)]
 
 
 class SolverState(ctypes.Structure):

@@ -1,8 +1,9 @@
 """Autotuner for the launch shapes of the per-cell kernels of a Simulation.
 
 The tunables (umag_tuning in the C header) are the CTA shape of the field +
-torque kernel, the threads and CTAs-per-SM cap of the stage sums, and the
-CTAs-per-SM cap of the error norms.  They change speed only: every cell's
+torque kernel and whether its stencils read TMA-loaded tiles (where the
+mesh allows them) or global memory, the threads and CTAs-per-SM cap of the
+stage sums, and the CTAs-per-SM cap of the error norms.  They change speed only: every cell's
 arithmetic is the same and the reductions are maxima, so a trajectory is bit
 for bit the same under every shape.  The FFT passes have no runtime shape:
 their thread layout is fixed by the register FFT's line length at compile
@@ -18,7 +19,7 @@ import json
 import os
 import tempfile
 
-DEFAULT = {"torque_block": [32, 8], "stage_threads": 256, "stage_waves": 8, "err_waves": 4}
+DEFAULT = {"torque_block": [32, 8], "stage_threads": 256, "stage_waves": 8, "err_waves": 4, "torque_tma": 1}
 STAGE_SHAPES = [(th, w) for th in (128, 256) for w in (2, 4, 8, 16)]
 ERR_WAVES = [2, 4, 8, 16]
 
@@ -72,10 +73,12 @@ def search(measure, nx):
     best = {k: (list(v) if isinstance(v, list) else v) for k, v in DEFAULT.items()}
     log = {"torque": {}, "stage": {}, "err": {}}
     for bx, by in torque_blocks(nx):
-        t = dict(best, torque_block=[bx, by])
-        log["torque"][f"{bx}x{by}"] = measure("torque", t)
-    bx, by = (int(v) for v in min(log["torque"], key=log["torque"].get).split("x"))
-    best["torque_block"] = [bx, by]
+        for tma in (1, 0):
+            t = dict(best, torque_block=[bx, by], torque_tma=tma)
+            log["torque"][f"{bx}x{by}/{tma}"] = measure("torque", t)
+    shape, tma = min(log["torque"], key=log["torque"].get).split("/")
+    bx, by = (int(v) for v in shape.split("x"))
+    best["torque_block"], best["torque_tma"] = [bx, by], int(tma)
     for th, w in STAGE_SHAPES:
         t = dict(best, stage_threads=th, stage_waves=w)
         log["stage"][f"{th}/{w}"] = measure("step", t)

@@ -20,6 +20,7 @@
 #include "demag.cuh"
 #include "engine.cuh"
 #include "ops.cuh"
+#include "tile.cuh"
 
 namespace umag {
 
@@ -102,6 +103,7 @@ struct LocalArgs {
     const float* Ms;
     float Ms_mul;
     const InstParams* ip;  // batched: per-instance parameters (uniform maps only)
+    const float* mbuf1;    // the second magnetisation buffer (selects the tile map)
 };
 
 __global__ void k_local_consts(LocalArgs a, LocalConsts* out) {
@@ -157,9 +159,13 @@ __device__ __forceinline__ f3 lltorque_g(f3 m, f3 H, float alpha, float gilb) {
 // engine/effectivefield.go:14-24 + engine/torque.go:135-144 for one cell:
 // B = demag; B += exchange(+DMI)/Ms; B += anisotropy; B += B_ext; torque.
 // UREG: every cell is in region 0 (no region map), so the region-pair
-// coefficients are scalars and no region is loaded.
-template <bool UREG, bool BAT>
-__global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
+// coefficients are scalars and no region is loaded.  TILE (with UREG, not
+// BAT, non-periodic mesh): the CTA's magnetisation tile with its halo comes
+// into shared memory by one TMA load (tile.cuh) and the stencils read it.
+template <bool UREG, bool BAT, bool TILE>
+__global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ LocalArgs a,
+                                                      const __grid_constant__ TileMaps tm) {
+    static_assert(!TILE || (UREG && !BAT), "tiles: region-free, not batched");
     // BAT: blockIdx.z = iz + Nz * instance; the instance's controller,
     // demag field and uniform parameters replace the shared ones
     static_assert(!BAT || UREG, "batched ensembles have no region maps");
@@ -183,19 +189,46 @@ __global__ void __launch_bounds__(256) k_local_torque(LocalArgs a) {
     if (!ctl->active) return;
     int ix = blockIdx.x * blockDim.x + threadIdx.x;
     int iy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ix >= a.g.Nx || iy >= a.g.Ny) return;
     const int N = a.N;
     const float* m = a.m_sel ? ctl->mw : ctl->m;
     const float *mx = m, *my = m + N, *mz = m + 2 * N;
+    TileView tv{};
+    if constexpr (TILE) {
+        extern __shared__ __align__(128) float tile[];
+        __shared__ __align__(8) uint64_t bar;
+        const bool three_d = a.g.Nz > 1;
+        const uint32_t bytes = (uint32_t)tile_bytes(blockDim.x, blockDim.y, a.g.Nz);
+        const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
+        if (leader) mbar_init(&bar, 1);
+        __syncthreads();
+        if (leader) {
+            mbar_expect_tx(&bar, bytes);
+            tma_load_4d(tile, &tm.map[m == a.mbuf1 ? 1 : 0], (int)(blockIdx.x * blockDim.x) - kTileHaloX,
+                        (int)(blockIdx.y * blockDim.y) - 1, three_d ? iz - 1 : iz, 0, &bar);
+        }
+        // bounded wait: past the limit flag the failure, wait once more for
+        // the copy in flight, and leave without writing
+        for (int it = 0; !mbar_try_wait(&bar, 0); it++) {
+            if (it == kTileWaitLimit && leader) atomicCAS(&ctl->status, 0, 7);
+            if (it >= 2 * kTileWaitLimit) return;
+        }
+        tv = TileView{tile, tile_pitch(blockDim.x), tile_rows(blockDim.y), three_d ? 3 : 1, three_d ? 1 : 0};
+    }
+    if (ix >= a.g.Nx || iy >= a.g.Ny) return;
     int I = (iz * a.g.Ny + iy) * a.g.Nx + ix;
     f3 B{0.f, 0.f, 0.f};
     if (bd) B = f3{__ldg(bd + I), __ldg(bd + N + I), __ldg(bd + 2 * N + I)};
     // engine/demag.go:95-97: NoDemagSpins cells feel no demag field
     if (!BAT && a.nodemag && __ldg(a.nodemag + (UREG ? 0 : __ldg(a.regions + I))) != 0.0f) B = f3{0.f, 0.f, 0.f};
-    f3 m0 = ld3(mx, my, mz, I);
+    f3 m0;
+    if constexpr (TILE) m0 = tv.at(threadIdx.x, threadIdx.y, 0, 0, 0);
+    else m0 = ld3(mx, my, mz, I);
     if (!is0(m0)) {
         f3 e;
-        if (!BAT && a.dbLUT) {  // engine/exchange.go:60-61 AddDMIBulk
+        if constexpr (TILE) {
+            e = dmi ? dmi_sum_tile(tv, threadIdx.x, threadIdx.y, kc.pc, a.openbc != 0, a.g.Nz > 1, m0)
+                    : exchange_sum_tile(tv, threadIdx.x, threadIdx.y, kc.pc, a.g.Nz > 1, m0);
+        } else if (!BAT && a.dbLUT) {  // engine/exchange.go:60-61 AddDMIBulk
             e = dmibulk_sum(mx, my, mz, a.aLUT, a.dbLUT, a.regions, a.cx, a.cy, a.cz, a.g, a.openbc != 0, ix, iy,
                             iz, m0, UREG ? 0 : __ldg(a.regions + I));
         } else if constexpr (UREG) {
@@ -662,7 +695,9 @@ struct SimImpl {
     cudaGraphExec_t gexec1 = nullptr;  // one step
     int launches_per_step = 0;
     double* esum = nullptr;            // energy term sums (kNE doubles)
-    umag_tuning tune{{32, 8}, 256, 8, 4};  // launch shapes (umag_sim_set_tuning)
+    umag_tuning tune{{32, 8}, 256, 8, 4, 1};  // launch shapes (umag_sim_set_tuning)
+    TileMaps tmaps{};                          // TMA maps of the two magnetisation buffers
+    bool tile_ok = false;                      // the mesh and block shape allow tiles
     // batched ensemble class: nb same-size instances with uniform parameters
     int nb = 1;
     bool batched = false;
@@ -691,9 +726,11 @@ static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, flo
     la.beff = beff;
     const int bx = s->tune.torque_block[0], by = s->tune.torque_block[1];
     dim3 blk(bx, by, 1), grd((s->g.Nx + bx - 1) / bx, (s->g.Ny + by - 1) / by, s->g.Nz * s->nb);
-    if (s->batched) k_local_torque<true, true><<<grd, blk, 0, S()>>>(la);
-    else if (s->zero_regions) k_local_torque<true, false><<<grd, blk, 0, S()>>>(la);
-    else k_local_torque<false, false><<<grd, blk, 0, S()>>>(la);
+    if (s->batched) k_local_torque<true, true, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
+    else if (s->zero_regions && s->tile_ok && s->tune.torque_tma)
+        k_local_torque<true, false, true><<<grd, blk, tile_bytes(bx, by, s->g.Nz), S()>>>(la, s->tmaps);
+    else if (s->zero_regions) k_local_torque<true, false, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
+    else k_local_torque<false, false, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
     UMAG_LAUNCH_CHECK();
     if (nl) *nl += 1;
     return UMAG_OK;
@@ -935,6 +972,52 @@ static int run_steps(SimImpl* s, long long n) {
     return UMAG_OK;
 }
 
+// cuTensorMapEncodeTiled from the driver (looked up once; no libcuda link)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// Tensor maps for the magnetisation tiles of the torque kernel (tile.cuh),
+// when the mesh allows them: region-free, non-periodic, not batched, no bulk
+// DMI, Nx a multiple of 4 (row strides and buffer offsets in 16-byte units),
+// and a box of at most 256 elements per dimension.
+static void tile_setup(SimImpl* s) {
+    s->tile_ok = false;
+    const int bx = s->tune.torque_block[0], by = s->tune.torque_block[1];
+    if (s->batched || !s->zero_regions || s->g.pbc != 0 || s->la.dbLUT || s->g.Nx % 4 != 0) return;
+    if (tile_pitch(bx) > 256 || tile_rows(by) > 256) return;
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return;
+    const cuuint64_t dims[4] = {(cuuint64_t)s->g.Nx, (cuuint64_t)s->g.Ny, (cuuint64_t)s->g.Nz, 3};
+    const cuuint64_t strides[3] = {sizeof(float) * (cuuint64_t)s->g.Nx,
+                                   sizeof(float) * (cuuint64_t)s->g.Nx * s->g.Ny, sizeof(float) * (cuuint64_t)s->N};
+    const cuuint32_t box[4] = {(cuuint32_t)tile_pitch(bx), (cuuint32_t)tile_rows(by),
+                               (cuuint32_t)(s->g.Nz > 1 ? 3 : 1), 3};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    for (int b = 0; b < 2; b++) {
+        float* base = s->bufs + (size_t)b * 3 * s->N;
+        if (reinterpret_cast<uintptr_t>(base) % 16 != 0) return;
+        if (fn(&s->tmaps.map[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return;
+    }
+    s->tile_ok = true;
+}
+
 // The local-term arguments that follow from the material parameters in s->p
 // (and the uniform factors evaluated from them); run at creation and again
 // whenever a parameter is reassigned.
@@ -1076,6 +1159,8 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
     la.bd = s->bd;
     st = local_from_params(s);
     if (st != UMAG_OK) return fail(st);
+    la.mbuf1 = s->bufs + 3 * (size_t)s->N;
+    tile_setup(s);
     if (la.dmi) {
         const int np = 256 * 257 / 2;
         if (cudaMalloc(&s->dmi_pairs, sizeof(float) * 7 * np) != cudaSuccess)
@@ -1512,8 +1597,10 @@ int sim_set_tuning(umag_sim* h, const umag_tuning* t) {
                  "stage threads %d", t->stage_threads);
     UMAG_REQUIRE(t->stage_waves >= 1 && t->stage_waves <= 64 && t->err_waves >= 1 && t->err_waves <= 64,
                  "waves must be 1..64");
+    UMAG_REQUIRE(t->torque_tma == 0 || t->torque_tma == 1, "torque_tma must be 0 or 1");
     UMAG_CUDA(cudaStreamSynchronize(S()));
     s->tune = *t;
+    if (!s->batched) tile_setup(s);  // the box follows the block shape
     drop_graph(s);  // the captured launches carry the old shapes
     return UMAG_OK;
 }

@@ -347,7 +347,7 @@ class Simulation:
         t = Tuning()
         check(self.L.umag_sim_get_tuning(self._h, ctypes.byref(t)))
         return {"torque_block": [t.torque_block[0], t.torque_block[1]], "stage_threads": t.stage_threads,
-                "stage_waves": t.stage_waves, "err_waves": t.err_waves}
+                "stage_waves": t.stage_waves, "err_waves": t.err_waves, "torque_tma": t.torque_tma}
 
     def set_tuning(self, tuning):
         """Apply launch shapes (a dict like get_tuning's); results are unchanged."""
@@ -355,6 +355,7 @@ class Simulation:
         t.torque_block[0], t.torque_block[1] = (int(v) for v in tuning["torque_block"])
         t.stage_threads, t.stage_waves, t.err_waves = (int(tuning[k]) for k in ("stage_threads", "stage_waves",
                                                                                 "err_waves"))
+        t.torque_tma = int(tuning.get("torque_tma", 1))
         torch.cuda.synchronize()
         check(self.L.umag_sim_set_tuning(self._h, ctypes.byref(t)))
 

@@ -128,10 +128,14 @@ __device__ __forceinline__ void k_fast_a_body(const PassArgs& a, const int bx, c
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) { k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) {
+    pdl_wait();
+    pdl_trigger(); k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(kNT) k_fast_a_bat(PassArgs a) {
+    pdl_wait();
+    pdl_trigger();
     const int per = 3, b = blockIdx.y / per;
     k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -214,10 +218,14 @@ __device__ __forceinline__ void k_fast_c_body(const PassArgs& a, const int bx, c
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) { k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) {
+    pdl_wait();
+    pdl_trigger(); k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(kNT) k_fast_c_bat(PassArgs a) {
+    pdl_wait();
+    pdl_trigger();
     const int per = 3, b = blockIdx.y / per;
     k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -284,10 +292,14 @@ __device__ __forceinline__ void k_fast_b_body(const PassArgs& a, const int bx, c
     }
 }
 template <int PY>
-__global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) { k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) {
+    pdl_wait();
+    pdl_trigger(); k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int PY>
 __global__ void __launch_bounds__(kNTB) k_fast_b_bat(PassArgs a) {
+    pdl_wait();
+    pdl_trigger();
     const int per = a.Pz, b = blockIdx.y / per;
     k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -432,10 +444,14 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     }
 }
 template <int PY, int WB>
-__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) { k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
+    pdl_wait();
+    pdl_trigger(); k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int PY, int WB>
 __global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b_bat(PassArgs a) {
+    pdl_wait();
+    pdl_trigger();
     const int per = a.Pz, b = blockIdx.y / per;
     k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -604,10 +620,14 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) { k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) {
+    pdl_wait();
+    pdl_trigger(); k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a_bat(PassArgs a) {
+    pdl_wait();
+    pdl_trigger();
     const int per = 3, b = blockIdx.y / per;
     k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -742,10 +762,14 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) { k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) {
+    pdl_wait();
+    pdl_trigger(); k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c_bat(PassArgs a) {
+    pdl_wait();
+    pdl_trigger();
     const int per = 3, b = blockIdx.y / per;
     k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -753,6 +777,16 @@ __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c_bat(PassArgs a) {
 template <int PY> struct RegB {
     static constexpr int T = PY / 8;
     static constexpr int WB = T >= 256 ? 1 : 256 / T > 16 ? 16 : 256 / T;
+    static constexpr int NT = T * WB;
+    static constexpr size_t smem = sizeof(float2) * ((size_t)PY + (size_t)3 * WB * rg_line<PY>()) +
+                                   sizeof(float) * (size_t)6 * (PY / 2 + 1) * WB;
+};
+
+// one warp per CTA (or one column): for small meshes, where the default
+// shape leaves most SMs idle
+template <int PY> struct RegBNarrow {
+    static constexpr int T = PY / 8;
+    static constexpr int WB = T >= 32 ? 1 : 32 / T;
     static constexpr int NT = T * WB;
     static constexpr size_t smem = sizeof(float2) * ((size_t)PY + (size_t)3 * WB * rg_line<PY>()) +
                                    sizeof(float) * (size_t)6 * (PY / 2 + 1) * WB;
@@ -785,6 +819,12 @@ template <int PY> static void fill_b(FastPasses& f) {
         f.wb = RegB<PY>::WB;
         f.nt_b = RegB<PY>::NT;
         f.b_reg = true;
+        if constexpr (RegBNarrow<PY>::WB < RegB<PY>::WB) {
+            f.b_n = k_reg_b<PY, RegBNarrow<PY>::WB>;
+            f.smem_b_n = RegBNarrow<PY>::smem;
+            f.wb_n = RegBNarrow<PY>::WB;
+            f.nt_b_n = RegBNarrow<PY>::NT;
+        }
     } else {
         f.b = k_fast_b<PY>;
         f.bb = k_fast_b_bat<PY>;
@@ -822,6 +862,12 @@ bool demag_fast_select(int M, int Py, int Pz, FastPasses& f) {
 int demag_fast_grid(FastPasses& f, int M, int Pz) {
     f.gbx = (unsigned)((M + 1 + f.wb - 1) / f.wb);
     f.gby = (unsigned)Pz;
+    // a default pass-B grid smaller than the SM count runs on a few SMs:
+    // single plans use CTAs of one warp instead (same arithmetic per column)
+    if (f.b_n) {
+        f.gbx_n = (unsigned)((M + 1 + f.wb_n - 1) / f.wb_n);
+        f.use_narrow = (long)f.gbx * f.gby < ctx().sm_count;
+    }
     return UMAG_OK;
 }
 
@@ -857,7 +903,7 @@ int demag_fast_setup() {
     // pass B instantiations
     {
         FastPasses g{};
-#define SETB(py) fill_b<py>(g); UMAG_TRY(attrs(g.b)); UMAG_TRY(attrs(g.bb));
+#define SETB(py) fill_b<py>(g); UMAG_TRY(attrs(g.b)); UMAG_TRY(attrs(g.bb)); if (g.b_n) UMAG_TRY(attrs(g.b_n));
         SETB(32) SETB(48) SETB(64) SETB(96) SETB(128) SETB(192) SETB(256) SETB(384) SETB(512) SETB(1024) SETB(2048)
 #undef SETB
     }

@@ -22,7 +22,6 @@ struct Context {
     size_t red_bytes = 0;
     double* red_host = nullptr;         // pinned, 8 doubles
     int sm_count = kNumSMs;
-    bool pdl = true;                    // programmatic dependent launch on the step path
 };
 
 Context& ctx();
@@ -49,31 +48,6 @@ int ensure_init();
     do {                                                                 \
         if (!(cond)) return ::umag::set_error(UMAG_E_ARG, __VA_ARGS__); \
     } while (0)
-
-// Programmatic dependent launch.  A kernel launched by launch_pdl may be
-// scheduled while the kernel before it on the stream drains; it starts with
-// pdl_wait() (griddepcontrol.wait, which returns once that grid has
-// completed and its writes are visible), so only the launch overlaps, never
-// the work.  pdl_trigger() lets the next kernel launch early in turn.  Both
-// are no-ops for a kernel launched the ordinary way.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
-
-template <typename... KArgs, typename... Args>
-inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                              Args&&... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = ctx().pdl ? 1 : 0;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args&&>(args)...);
-}
 
 // Grid for a grid-stride loop over n elements: enough CTAs to fill the 148
 // SMs several times over, never more than needed.

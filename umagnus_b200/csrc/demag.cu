@@ -226,8 +226,6 @@ __global__ void k_extract_spectrum(const double2* a, float* out, int Px, int Py,
 
 // ================================================================== float passes
 __global__ void __launch_bounds__(kPassThreads) k_pass_a(PassArgs a) {
-    pdl_wait();
-    pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* X1 = reinterpret_cast<float2*>(smem_raw);        // [Nz][HxP]
     float2* Z2 = X1 + a.Nz * a.HxP;                           // [Pz][W]
@@ -308,8 +306,6 @@ __global__ void __launch_bounds__(kPassThreads) k_pass_a(PassArgs a) {
 }
 
 __global__ void __launch_bounds__(kPassBThreads) k_pass_b(PassArgs a) {
-    pdl_wait();
-    pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (a.active && !*a.active) return;
     float2* S = reinterpret_cast<float2*>(smem_raw);  // [Py][3*WB]
@@ -361,8 +357,6 @@ __global__ void __launch_bounds__(kPassBThreads) k_pass_b(PassArgs a) {
 }
 
 __global__ void __launch_bounds__(kPassThreads) k_pass_c(PassArgs a) {
-    pdl_wait();
-    pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* X1 = reinterpret_cast<float2*>(smem_raw);  // [Nz][HxP]
     float2* Z2 = X1 + a.Nz * a.HxP;                    // [Pz][W]
@@ -751,16 +745,22 @@ void fill_pass_args(const umag_demag* d, PassArgs& a) {
 int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st) {
     if (d->use_fast) {
         const FastPasses& f = d->fast;
-        UMAG_CUDA(launch_pdl(f.a, dim3(d->N[1], 3), dim3(f.nt_ac), f.smem_ac, st, a));
-        if (f.use_narrow) UMAG_CUDA(launch_pdl(f.b_n, dim3(f.gbx_n, f.gby), dim3(f.nt_b_n), f.smem_b_n, st, a));
-        else UMAG_CUDA(launch_pdl(f.b, dim3(f.gbx, f.gby), dim3(f.nt_b), f.smem_b, st, a));
-        UMAG_CUDA(launch_pdl(f.c, dim3(d->N[1], 3), dim3(f.nt_ac), f.smem_ac, st, a));
+        f.a<<<dim3(d->N[1], 3), f.nt_ac, f.smem_ac, st>>>(a);
+        UMAG_LAUNCH_CHECK();
+        if (f.use_narrow) f.b_n<<<dim3(f.gbx_n, f.gby), f.nt_b_n, f.smem_b_n, st>>>(a);
+        else f.b<<<dim3(f.gbx, f.gby), f.nt_b, f.smem_b, st>>>(a);
+        UMAG_LAUNCH_CHECK();
+        f.c<<<dim3(d->N[1], 3), f.nt_ac, f.smem_ac, st>>>(a);
+        UMAG_LAUNCH_CHECK();
         return UMAG_OK;
     }
     size_t sac = pass_ac_smem(d), sb = pass_b_smem(d);
-    UMAG_CUDA(launch_pdl(k_pass_a, dim3(d->N[1], 3), dim3(kPassThreads), sac, st, a));
-    UMAG_CUDA(launch_pdl(k_pass_b, dim3((d->Hx + d->WB - 1) / d->WB, d->P[2]), dim3(kPassBThreads), sb, st, a));
-    UMAG_CUDA(launch_pdl(k_pass_c, dim3(d->N[1], 3), dim3(kPassThreads), sac, st, a));
+    k_pass_a<<<dim3(d->N[1], 3), kPassThreads, sac, st>>>(a);
+    UMAG_LAUNCH_CHECK();
+    k_pass_b<<<dim3((d->Hx + d->WB - 1) / d->WB, d->P[2]), kPassBThreads, sb, st>>>(a);
+    UMAG_LAUNCH_CHECK();
+    k_pass_c<<<dim3(d->N[1], 3), kPassThreads, sac, st>>>(a);
+    UMAG_LAUNCH_CHECK();
     return UMAG_OK;
 }
 
@@ -770,9 +770,12 @@ int demag_launch_batch(const umag_demag* d, const PassArgs& a, int nb, cudaStrea
     UMAG_REQUIRE(d->use_fast && d->fast.ab && d->fast.bb && d->fast.cb, "batched demag needs a compile-time FFT plan");
     UMAG_REQUIRE(nb >= 1 && 3L * nb <= 65535 && (long)d->fast.gby * nb <= 65535, "too many instances in one batch");
     const FastPasses& f = d->fast;
-    UMAG_CUDA(launch_pdl(f.ab, dim3(d->N[1], 3 * nb), dim3(f.nt_ac), f.smem_ac, st, a));
-    UMAG_CUDA(launch_pdl(f.bb, dim3(f.gbx, f.gby * nb), dim3(f.nt_b), f.smem_b, st, a));
-    UMAG_CUDA(launch_pdl(f.cb, dim3(d->N[1], 3 * nb), dim3(f.nt_ac), f.smem_ac, st, a));
+    f.ab<<<dim3(d->N[1], 3 * nb), f.nt_ac, f.smem_ac, st>>>(a);
+    UMAG_LAUNCH_CHECK();
+    f.bb<<<dim3(f.gbx, f.gby * nb), f.nt_b, f.smem_b, st>>>(a);
+    UMAG_LAUNCH_CHECK();
+    f.cb<<<dim3(d->N[1], 3 * nb), f.nt_ac, f.smem_ac, st>>>(a);
+    UMAG_LAUNCH_CHECK();
     return UMAG_OK;
 }
 

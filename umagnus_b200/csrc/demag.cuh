@@ -29,8 +29,8 @@ struct FastPasses {
     // pass B's column reads and writes are contiguous (set when ac_reg && b_reg)
     bool blocked = false;
     unsigned gbx = 0, gby = 0;  // pass-B grid (demag_fast_grid)
-    // narrower pass-B CTAs (fewer columns each) for meshes whose default
-    // pass-B grid has fewer CTAs than the GPU has SMs (single plans only)
+    // narrower pass-B CTAs (fewer columns each) for single meshes whose
+    // default pass-B grid has fewer CTAs than the GPU has SMs
     void (*b_n)(PassArgs) = nullptr;
     size_t smem_b_n = 0;
     int wb_n = 0, nt_b_n = 0;

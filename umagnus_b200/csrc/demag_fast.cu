@@ -128,14 +128,10 @@ __device__ __forceinline__ void k_fast_a_body(const PassArgs& a, const int bx, c
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) {
-    pdl_wait();
-    pdl_trigger(); k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(kNT) k_fast_a(PassArgs a) { k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(kNT) k_fast_a_bat(PassArgs a) {
-    pdl_wait();
-    pdl_trigger();
     const int per = 3, b = blockIdx.y / per;
     k_fast_a_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -218,14 +214,10 @@ __device__ __forceinline__ void k_fast_c_body(const PassArgs& a, const int bx, c
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) {
-    pdl_wait();
-    pdl_trigger(); k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(kNT) k_fast_c(PassArgs a) { k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(kNT) k_fast_c_bat(PassArgs a) {
-    pdl_wait();
-    pdl_trigger();
     const int per = 3, b = blockIdx.y / per;
     k_fast_c_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -292,14 +284,10 @@ __device__ __forceinline__ void k_fast_b_body(const PassArgs& a, const int bx, c
     }
 }
 template <int PY>
-__global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) {
-    pdl_wait();
-    pdl_trigger(); k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(kNTB) k_fast_b(PassArgs a) { k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int PY>
 __global__ void __launch_bounds__(kNTB) k_fast_b_bat(PassArgs a) {
-    pdl_wait();
-    pdl_trigger();
     const int per = a.Pz, b = blockIdx.y / per;
     k_fast_b_body<PY>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -426,10 +414,14 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
             Kxz = kr[4 * HY * WB] * sz;
         }
         const float2 mx = v[0][m], my = v[1][m], mz = v[2][m];
-        // conjugated products: the inverse is conj(FFT(conj(.)))
-        v[0][m] = make_float2(mx.x * Kxx + my.x * Kxy + mz.x * Kxz, -(mx.y * Kxx + my.y * Kxy + mz.y * Kxz));
-        v[1][m] = make_float2(mx.x * Kxy + my.x * Kyy + mz.x * Kyz, -(mx.y * Kxy + my.y * Kyy + mz.y * Kyz));
-        v[2][m] = make_float2(mx.x * Kxz + my.x * Kyz + mz.x * Kzz, -(mx.y * Kxz + my.y * Kyz + mz.y * Kzz));
+        // conjugated products: the inverse is conj(FFT(conj(.))); explicit
+        // multiply-adds (fft.cuh: the same bits in every instantiation)
+        auto dot = [](float a, float ka, float b, float kb, float c, float kc) {
+            return fma_rn(c, kc, fma_rn(b, kb, mul_rn(a, ka)));
+        };
+        v[0][m] = make_float2(dot(mx.x, Kxx, my.x, Kxy, mz.x, Kxz), -dot(mx.y, Kxx, my.y, Kxy, mz.y, Kxz));
+        v[1][m] = make_float2(dot(mx.x, Kxy, my.x, Kyy, mz.x, Kyz), -dot(mx.y, Kxy, my.y, Kyy, mz.y, Kyz));
+        v[2][m] = make_float2(dot(mx.x, Kxz, my.x, Kyz, mz.x, Kzz), -dot(mx.y, Kxz, my.y, Kyz, mz.y, Kzz));
     }
     rg_fft_fwd<PY, 3>(v, t, exl, exs, tw);
     if (col) {
@@ -444,14 +436,10 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     }
 }
 template <int PY, int WB>
-__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) {
-    pdl_wait();
-    pdl_trigger(); k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) { k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int PY, int WB>
 __global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b_bat(PassArgs a) {
-    pdl_wait();
-    pdl_trigger();
     const int per = a.Pz, b = blockIdx.y / per;
     k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -620,14 +608,10 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) {
-    pdl_wait();
-    pdl_trigger(); k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a(PassArgs a) { k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_a_bat(PassArgs a) {
-    pdl_wait();
-    pdl_trigger();
     const int per = 3, b = blockIdx.y / per;
     k_reg_a_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -762,14 +746,10 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
     }
 }
 template <int M, int PZ>
-__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) {
-    pdl_wait();
-    pdl_trigger(); k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c(PassArgs a) { k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y, 0); }
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int M, int PZ>
 __global__ void __launch_bounds__(RegAC<M, PZ>::NT) k_reg_c_bat(PassArgs a) {
-    pdl_wait();
-    pdl_trigger();
     const int per = 3, b = blockIdx.y / per;
     k_reg_c_body<M, PZ>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -862,8 +842,11 @@ bool demag_fast_select(int M, int Py, int Pz, FastPasses& f) {
 int demag_fast_grid(FastPasses& f, int M, int Pz) {
     f.gbx = (unsigned)((M + 1 + f.wb - 1) / f.wb);
     f.gby = (unsigned)Pz;
-    // a default pass-B grid smaller than the SM count runs on a few SMs:
-    // single plans use CTAs of one warp instead (same arithmetic per column)
+    // a default pass-B grid smaller than the SM count runs on a few SMs: such
+    // plans use CTAs of one warp instead for a single mesh (batched launches
+    // have CTAs enough and keep the default); the arithmetic per column is
+    // the same, bit for bit, because the butterflies and the kernel multiply
+    // spell out their rounding (fft.cuh)
     if (f.b_n) {
         f.gbx_n = (unsigned)((M + 1 + f.wb_n - 1) / f.wb_n);
         f.use_narrow = (long)f.gbx * f.gby < ctx().sm_count;
@@ -903,7 +886,11 @@ int demag_fast_setup() {
     // pass B instantiations
     {
         FastPasses g{};
-#define SETB(py) fill_b<py>(g); UMAG_TRY(attrs(g.b)); UMAG_TRY(attrs(g.bb)); if (g.b_n) UMAG_TRY(attrs(g.b_n));
+#define SETB(py)                                     \
+    fill_b<py>(g);                                   \
+    UMAG_TRY(attrs(g.b));                            \
+    UMAG_TRY(attrs(g.bb));                           \
+    if (g.b_n) UMAG_TRY(attrs(g.b_n));
         SETB(32) SETB(48) SETB(64) SETB(96) SETB(128) SETB(192) SETB(256) SETB(384) SETB(512) SETB(1024) SETB(2048)
 #undef SETB
     }

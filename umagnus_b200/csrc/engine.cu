@@ -165,8 +165,6 @@ __device__ __forceinline__ f3 lltorque_g(f3 m, f3 H, float alpha, float gilb) {
 template <bool UREG, bool BAT, bool TILE>
 __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ LocalArgs a,
                                                       const __grid_constant__ TileMaps tm) {
-    pdl_wait();
-    pdl_trigger();
     static_assert(!TILE || (UREG && !BAT), "tiles: region-free, not batched");
     // BAT: blockIdx.z = iz + Nz * instance; the instance's controller,
     // demag field and uniform parameters replace the shared ones
@@ -310,8 +308,6 @@ struct StageArgs {
 // (opencl/madd.go, madd<n>.cl) then normalize2.cl.  NT = number of terms.
 template <int NT, bool BAT>
 __global__ void __launch_bounds__(256) k_stage(StageArgs a) {
-    pdl_wait();
-    pdl_trigger();
     DevCtl* ctl = a.ctl + (BAT ? blockIdx.y : 0);  // BAT: one grid row per instance
     if (!ctl->active) return;
     if (a.only_if_accepted && !ctl->accepted) return;
@@ -367,8 +363,6 @@ struct ErrArgs {
 // Err itself is never written to memory.
 template <int NT, bool HEUN, bool BAT>
 __global__ void __launch_bounds__(256) k_err_norms(ErrArgs a) {
-    pdl_wait();
-    pdl_trigger();
     __shared__ float sh[32];
     DevCtl* ctl = a.ctl + (BAT ? blockIdx.y : 0);  // BAT: one grid row per instance
     if (!ctl->active) return;
@@ -445,8 +439,6 @@ __device__ void adapt_dt(DevCtl* c, double corr) {
 // engine/rk45dp.go:16-50 (start of Step): fixed dt, h, t0, clear maxima;
 // skip the step once the run's stop time is reached (engine/run.go:212-231).
 __global__ void k_step_begin(DevCtl* c0, int nb) {
-    pdl_wait();
-    pdl_trigger();
     const int b = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per instance
     if (b >= nb) return;
     DevCtl* c = c0 + b;
@@ -465,8 +457,6 @@ __global__ void k_step_begin(DevCtl* c0, int nb) {
 // kind 3: Euler (engine/euler.go:16-35), always accepted
 __global__ void k_controller(DevCtl* c0, int nb, int kind, int acc, int rej, int fsal_from, int fsal_to,
                              int nevals) {
-    pdl_wait();
-    pdl_trigger();
     const int b = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per instance
     if (b >= nb) return;
     DevCtl* c = c0 + b;
@@ -568,8 +558,6 @@ __global__ void k_controller(DevCtl* c0, int nb, int kind, int acc, int rej, int
 // accepted: the working magnetisation becomes the state (pointer swap);
 // RK4 also records max |k4| here (setMaxTorque, engine/rk4.go:64)
 __global__ void k_step_end(DevCtl* c0, int nb, int rk4) {
-    pdl_wait();
-    pdl_trigger();
     const int b = blockIdx.x * blockDim.x + threadIdx.x;  // one thread per instance
     if (b >= nb) return;
     DevCtl* c = c0 + b;
@@ -739,14 +727,13 @@ static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, flo
     const int bx = s->tune.torque_block[0], by = s->tune.torque_block[1];
     dim3 blk(bx, by, 1), grd((s->g.Nx + bx - 1) / bx, (s->g.Ny + by - 1) / by, s->g.Nz * s->nb);
     if (s->batched)
-        UMAG_CUDA(launch_pdl(k_local_torque<true, true, false>, grd, blk, 0, S(), la, s->tmaps));
+        k_local_torque<true, true, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
     else if (s->zero_regions && s->tile_ok && s->tune.torque_tma)
-        UMAG_CUDA(launch_pdl(k_local_torque<true, false, true>, grd, blk, tile_bytes(bx, by, s->g.Nz), S(), la,
-                             s->tmaps));
+        k_local_torque<true, false, true><<<grd, blk, tile_bytes(bx, by, s->g.Nz), S()>>>(la, s->tmaps);
     else if (s->zero_regions)
-        UMAG_CUDA(launch_pdl(k_local_torque<true, false, false>, grd, blk, 0, S(), la, s->tmaps));
+        k_local_torque<true, false, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
     else
-        UMAG_CUDA(launch_pdl(k_local_torque<false, false, false>, grd, blk, 0, S(), la, s->tmaps));
+        k_local_torque<false, false, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
     UMAG_LAUNCH_CHECK();
     if (nl) *nl += 1;
     return UMAG_OK;
@@ -772,8 +759,8 @@ static int launch_stage(SimImpl* s, int src_m, std::initializer_list<int> slots,
                  s->nb);
 #define STAGE(n)                                                    \
     case n:                                                         \
-        if (s->batched) UMAG_CUDA(launch_pdl(k_stage<n, true>, dim3(g), dim3(th), 0, S(), a));     \
-        else UMAG_CUDA(launch_pdl(k_stage<n, false>, dim3(g), dim3(th), 0, S(), a));               \
+        if (s->batched) k_stage<n, true><<<g, th, 0, S()>>>(a);     \
+        else k_stage<n, false><<<g, th, 0, S()>>>(a);               \
         break;
     switch (a.nterm) {
         STAGE(2) STAGE(3) STAGE(4) STAGE(5) STAGE(6)
@@ -801,8 +788,8 @@ static int launch_err(SimImpl* s, std::initializer_list<int> slots, std::initial
                  s->nb);
 #define ERRN(n, hn)                                                       \
     do {                                                                  \
-        if (s->batched) UMAG_CUDA(launch_pdl(k_err_norms<n, hn, true>, dim3(g), dim3(256), 0, S(), a));  \
-        else UMAG_CUDA(launch_pdl(k_err_norms<n, hn, false>, dim3(g), dim3(256), 0, S(), a));            \
+        if (s->batched) k_err_norms<n, hn, true><<<g, 256, 0, S()>>>(a);  \
+        else k_err_norms<n, hn, false><<<g, 256, 0, S()>>>(a);            \
     } while (0)
     if (heun) ERRN(2, true);
     else if (a.nterm == 2) ERRN(2, false);
@@ -818,7 +805,7 @@ static int launch_err(SimImpl* s, std::initializer_list<int> slots, std::initial
 // Slots: k[0] = k1 (FSAL), k[1..6] = k2..k7 buffers.
 static int launch_step(SimImpl* s, int* nl) {
     DevCtl* c = s->ctl;
-    UMAG_CUDA(launch_pdl(k_step_begin, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb));
+    k_step_begin<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb);
     UMAG_LAUNCH_CHECK();
     *nl += 1;
     switch (s->sp.solver) {
@@ -844,7 +831,7 @@ static int launch_step(SimImpl* s, int* nl) {
         UMAG_TRY(launch_err(s, {0, 2, 3, 4, 5, 6},
                             {71. / 57600., -71. / 16695., 71. / 1920., -17253. / 339200., 22. / 525., -1. / 40.}, 6,
                             false, nl));
-        UMAG_CUDA(launch_pdl(k_controller, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb, 0, 5, 6, 6, 0, 6));
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0, 5, 6, 6, 0, 6);
         break;
     }
     case 3: {  // engine/rk23.go:58-83
@@ -855,7 +842,7 @@ static int launch_step(SimImpl* s, int* nl) {
         UMAG_TRY(launch_stage(s, 0, {0, 1, 2}, {2. / 9., 1. / 3., 4. / 9.}, true, true, false, nl));
         UMAG_TRY(launch_torque(s, 1, 3, nullptr, nullptr, nl));
         UMAG_TRY(launch_err(s, {0, 1, 2, 3}, {5. / 72., -1. / 12., -1. / 9., 1. / 8.}, 3, false, nl));
-        UMAG_CUDA(launch_pdl(k_controller, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb, 0, 3, 4, 3, 0, 3));
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0, 3, 4, 3, 0, 3);
         break;
     }
     case 2: {  // engine/heun.go:15-59
@@ -863,12 +850,12 @@ static int launch_step(SimImpl* s, int* nl) {
         UMAG_TRY(launch_stage(s, 0, {0}, {1.0}, true, false, false, nl));            // y = y + dt*dy0
         UMAG_TRY(launch_torque(s, 1, 1, nullptr, nullptr, nl));                      // dy
         UMAG_TRY(launch_err(s, {0, 1}, {1.0, -1.0}, 1, true, nl));                   // |dy0 - dy|
-        UMAG_CUDA(launch_pdl(k_controller, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb, 2, 2, 3, -1, -1, 2));
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 2, 2, 3, -1, -1, 2);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         // accepted: y = y + 0.5 dt dy - 0.5 dt dy0, normalised (heun.go:45-46)
         UMAG_TRY(launch_stage(s, 1, {1, 0}, {0.5, -0.5}, true, true, true, nl));
-        UMAG_CUDA(launch_pdl(k_step_end, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb, 0));
+        k_step_end<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         return UMAG_OK;
@@ -876,12 +863,12 @@ static int launch_step(SimImpl* s, int* nl) {
     case 1: {  // engine/euler.go:11-36
         UMAG_TRY(launch_torque(s, 0, 0, nullptr, nullptr, nl));           // dy0
         UMAG_TRY(launch_err(s, {0, 0}, {1.0, -1.0}, 0, true, nl));        // max |dy0|
-        UMAG_CUDA(launch_pdl(k_controller, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb, 3, 1, 1, -1, -1, 1));
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 3, 1, 1, -1, -1, 1);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         // y = y + dt*dy0 (Madd2), normalised (euler.go:33-34)
         UMAG_TRY(launch_stage(s, 0, {0}, {1.0}, true, true, true, nl));
-        UMAG_CUDA(launch_pdl(k_step_end, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb, 0));
+        k_step_end<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         return UMAG_OK;
@@ -895,11 +882,11 @@ static int launch_step(SimImpl* s, int* nl) {
         UMAG_TRY(launch_stage(s, 0, {2}, {1.}, true, true, false, nl));
         UMAG_TRY(launch_torque(s, 1, 3, nullptr, nullptr, nl));
         UMAG_TRY(launch_err(s, {0, 3}, {1., -1.}, 3, false, nl));
-        UMAG_CUDA(launch_pdl(k_controller, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb, 1, 4, 5, -1, -1, 4));
+        k_controller<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 1, 4, 5, -1, -1, 4);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         UMAG_TRY(launch_stage(s, 0, {0, 1, 2, 3}, {1. / 6., 1. / 3., 1. / 3., 1. / 6.}, true, true, true, nl));
-        UMAG_CUDA(launch_pdl(k_step_end, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb, 1));
+        k_step_end<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 1);
         UMAG_LAUNCH_CHECK();
         *nl += 1;
         return UMAG_OK;
@@ -909,7 +896,7 @@ static int launch_step(SimImpl* s, int* nl) {
     }
     UMAG_LAUNCH_CHECK();
     *nl += 1;
-    UMAG_CUDA(launch_pdl(k_step_end, dim3(ctl_grid(s)), dim3(128), 0, S(), c, s->nb, 0));
+    k_step_end<<<ctl_grid(s), 128, 0, S()>>>(c, s->nb, 0);
     UMAG_LAUNCH_CHECK();
     *nl += 1;
     return UMAG_OK;
@@ -1176,6 +1163,10 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
     st = local_from_params(s);
     if (st != UMAG_OK) return fail(st);
     la.mbuf1 = s->bufs + 3 * (size_t)s->N;
+    // default launch shapes for small meshes: enough CTAs to reach most SMs
+    // (the autotuner may choose others; results do not depend on them)
+    if ((long)((s->g.Nx + 31) / 32) * ((s->g.Ny + 7) / 8) * s->g.Nz < ctx().sm_count) s->tune.torque_block[1] = 2;
+    if ((long)s->N < (long)ctx().sm_count * 256) s->tune.stage_threads = 64;
     tile_setup(s);
     if (la.dmi) {
         const int np = 256 * 257 / 2;

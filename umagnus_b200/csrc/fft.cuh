@@ -19,10 +19,43 @@ template <typename T> struct Cplx;
 template <> struct Cplx<float> { using t = float2; };
 template <> struct Cplx<double> { using t = double2; };
 
+// Rounding spelled out: on the device every product is either a separate
+// correctly rounded multiply or fused into an explicit FMA, so the compiler
+// cannot contract the butterflies differently in different kernel
+// instantiations -- every instantiation of a transform gives the same bits.
+__host__ __device__ __forceinline__ float mul_rn(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+__host__ __device__ __forceinline__ double mul_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+__host__ __device__ __forceinline__ float fma_rn(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+    return __fmaf_rn(a, b, c);
+#else
+    return a * b + c;
+#endif
+}
+__host__ __device__ __forceinline__ double fma_rn(double a, double b, double c) {
+#ifdef __CUDA_ARCH__
+    return __fma_rn(a, b, c);
+#else
+    return a * b + c;
+#endif
+}
+
 template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
     C r;
-    r.x = a.x * b.x - a.y * b.y;
-    r.y = a.x * b.y + a.y * b.x;
+    r.x = fma_rn(a.x, b.x, -mul_rn(a.y, b.y));
+    r.y = fma_rn(a.x, b.y, mul_rn(a.y, b.x));
     return r;
 }
 template <typename C> __host__ __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }

@@ -48,10 +48,6 @@ int init_device(int device) {
         return set_error(UMAG_E_UNSUPPORTED, "device %d (%s, sm_%d%d) is not sm_100", device, prop.name, prop.major,
                          prop.minor);
     g_ctx.sm_count = prop.multiProcessorCount;
-    {  // UMAG_PDL=0 launches the step path the ordinary way (for comparisons)
-        const char* e = getenv("UMAG_PDL");
-        g_ctx.pdl = !(e && e[0] == '0');
-    }
     UMAG_CUDA(cudaStreamCreateWithFlags(&g_ctx.own_stream, cudaStreamNonBlocking));
     g_ctx.stream = g_ctx.own_stream;
     g_ctx.red_bytes = sizeof(double) * 4 * kRedBlocks + 64;

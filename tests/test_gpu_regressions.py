@@ -291,13 +291,15 @@ def _avg_by_region(sim, m, regions):
     return {int(r): b[:, reg == r].mean(axis=1) for r in np.unique(reg)}
 
 
-def test_anisotropy_energy_conservation_without_damping():
-    """test/anisenergy.mx3: 32x10x2 cells (1, 2, 3 nm), no demag, Ku1 1e6
-    along z; the energy change over 1 ns with alpha = 0 is below 1e-6 of the
-    change with alpha = 1."""
+@pytest.mark.parametrize("which", ["Ku1", "Ku2"])  # test/anisenergy.mx3, test/anisenergy2.mx3
+def test_anisotropy_energy_conservation_without_damping(which):
+    """test/anisenergy.mx3 (Ku1 1e6) and anisenergy2.mx3 (Ku2 1e6): 32x10x2
+    cells (1, 2, 3 nm), no demag, axis z; the energy change over 1 ns with
+    alpha = 0 is below 1e-6 of the change with alpha = 1."""
     engine, config = _e()
     N, c = (32, 10, 2), 1e-9
-    sim = engine.Simulation(N, (c, 2 * c, 3 * c), 1000e3, 10e-12, 1.0, Ku1=1e6, anisU=(0, 0, 1), demag=False)
+    sim = engine.Simulation(N, (c, 2 * c, 3 * c), 1000e3, 10e-12, 1.0, anisU=(0, 0, 1), demag=False,
+                            **{which: 1e6})
     sim.set_m(config.uniform(N, 1, 0, 0.1))
     E0 = sim.energies()["total"]
     sim.run(1e-9)
@@ -311,14 +313,17 @@ def test_anisotropy_energy_conservation_without_damping():
     assert abs(d2 / d1) <= 1e-6, (d1, d2)
 
 
-def test_cubic_and_uniaxial_energy_conservation():
-    """test/anisenergyconservation.mx3: one cell, Kc1 1e3 and Ku1 1e5 along
-    (1, 1, 0), alpha 1e-6, MaxDt 1e-13; the total energy stays within 1e-5
-    (relative) over ten runs of 10 ps."""
+@pytest.mark.parametrize("extra", [{}, {"Ku2": 2e5}, {"Kc2": 1e3}, {"Kc3": 1e3}],
+                         ids=["anisenergyconservation", "2_Ku2", "3_Kc2", "4_Kc3"])
+def test_cubic_and_uniaxial_energy_conservation(extra):
+    """test/anisenergyconservation.mx3 and its variants 2-4 (adding Ku2 2e5,
+    Kc2 1e3 or Kc3 1e3): one cell, Kc1 1e3 and Ku1 1e5 along (1, 1, 0), alpha
+    1e-6, MaxDt 1e-13; the total energy stays within 1e-5 (relative) over
+    ten runs of 10 ps."""
     engine, config = _e()
     N = (1, 1, 1)
     sim = engine.Simulation(N, (1e-9, 1e-9, 1e-9), 1000e3, 0.0, 1e-6, Ku1=1e5, anisU=(1, 1, 0), Kc1=1e3,
-                            anisC1=(1, 0, 0), anisC2=(0, 1, 0), demag=False, MaxDt=1e-13)
+                            anisC1=(1, 0, 0), anisC2=(0, 1, 0), demag=False, MaxDt=1e-13, **extra)
     sim.set_m(config.uniform(N, 0.3, 0.7, 0.1))
     E0 = sim.energies()["total"]
     for _ in range(10):
@@ -437,3 +442,70 @@ def test_energy_density_integrates_to_energy():
     E = sim.energies()["total"]
     sim.free()
     assert abs(volume * avg / E - 1) <= 1e-3, (volume * avg, E)
+
+
+
+def test_dmi_bloch_to_neel_along_y():
+    """test/dmiY.mx3: test/dmi.mx3 rotated by 90 degrees (TwoDomain(...).RotZ(pi/2)),
+    MaxDt 5e-13, 5 ns: <m> = (-0.035, 0.059) within 0.01."""
+    engine, config = _e()
+    N = (128, 128, 1)
+    cell = (250e-9 / 128, 250e-9 / 128, 0.6e-9)
+    sim = engine.Simulation(N, cell, 1100e3, 16e-12, 3.0, Dind=0.1e-3, Ku1=1.27e6, anisU=(0, 0, 1), MaxDt=5e-13,
+                            demag_kernel="brute")
+    sim.set_m(config.sample(N, cell, config.rot_z(config.two_domain_fn(cell, (0, 0, -1), (1, 1, 0), (0, 0, 1)),
+                                                  np.pi / 2)))
+    sim.run(5e-9)
+    m = sim.average_m()
+    sim.free()
+    assert abs(m[0] + 0.035) <= 0.01 and abs(m[1] - 0.059) <= 0.01, m
+
+
+def test_dmi_3d_wall_cell():
+    """test/dmi3d.mx3: 64x64x2 cells (0.6, 0.6, 0.3 nm), DMI + exchange +
+    Ku1, two-domain start, 0.5 ns: m in cell (32, 32, 0) = (0.8979, 0.3989,
+    0.1859) within 1e-3 (the reference's 2D solution)."""
+    engine, config = _e()
+    N, c = (64, 64, 2), 0.6e-9
+    cell = (c, c, c / 2)
+    sim = engine.Simulation(N, cell, 1100e3, 16e-12, 3.0, Dind=0.1e-3, Ku1=1.27e6, anisU=(0, 0, 1),
+                            demag_kernel="brute")
+    sim.set_m(config.two_domain(N, cell, (0, 0, -1), (1, 1, 0), (0, 0, 1)))
+    sim.run(0.5e-9)
+    m = sim.get_m().cpu().numpy()[:, 0, 32, 32]
+    sim.free()
+    np.testing.assert_allclose(m, [0.8979, 0.3989, 0.1859], rtol=0, atol=1e-3)
+
+
+def test_cubic_anisotropy_energy_of_one_cell():
+    """test/cubic_full.mx3: E_anis / V of one cell at theta 23, phi 11 degrees
+    for Kc1, Kc2, Kc3 = +-1e6 alone (TOL 1e-2 J/m^3)."""
+    engine, config = _e()
+    N, V = (1, 1, 1), 1e-27
+    th, ph = np.deg2rad(23), np.deg2rad(11)
+    sim = engine.Simulation(N, (1e-9, 1e-9, 1e-9), 1000e3, 0.0, 0.0, Kc1=1e6, anisC1=(1, 0, 0), anisC2=(0, 1, 0),
+                            demag=False)
+    sim.set_m(config.uniform(N, np.sin(ph) * np.cos(th), np.sin(ph) * np.sin(th), np.cos(ph)))
+    for k, want in (("Kc1", 35254.007), ("Kc2", 165.23309326171875), ("Kc3", 912.3794555664062)):
+        for sign in (1, -1):
+            for kk in ("Kc1", "Kc2", "Kc3"):
+                sim.set_param(kk, sign * 1e6 if kk == k else 0.0)
+            e = sim.energies()["anisotropy"] / V
+            assert abs(e - sign * want) <= 1e-2, (k, sign, e)
+    sim.free()
+
+
+def test_uniaxial_anisotropy_energy_of_one_cell():
+    """test/uniaxial_full.mx3: E_anis / V of one cell at 17 degrees from the
+    x easy axis for Ku2 = +-1e6 and Ku1 = +-1e6 alone (TOL 1 J/m^3)."""
+    engine, config = _e()
+    N, V = (1, 1, 1), 1e-27
+    th = np.deg2rad(17)
+    sim = engine.Simulation(N, (1e-9, 1e-9, 1e-9), 1000e3, 0.0, 0.0, Ku2=1e6, anisU=(1, 0, 0), demag=False)
+    sim.set_m(config.uniform(N, np.cos(th), np.sin(th), 0))
+    for ku1, ku2, want in ((0, 1e6, -836344.9375), (0, -1e6, 836344.9375), (1e6, 0, -914519), (-1e6, 0, 914519)):
+        sim.set_param("Ku1", ku1)
+        sim.set_param("Ku2", ku2)
+        e = sim.energies()["anisotropy"] / V
+        assert abs(e - want) <= 1, (ku1, ku2, e)
+    sim.free()

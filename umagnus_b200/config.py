@@ -56,17 +56,38 @@ def ellipse(N, cell, dx, dy):
     return ellipsoid(N, cell, dx, dy)
 
 
+def two_domain_fn(cell, m1, mwall, m2):
+    """engine/config.go:144-159 TwoDomain as a function of the cell-centre
+    coordinates (X, Y, Z): m1 for x < 0, m2 for x >= 0, a Gaussian wall of
+    width 2*cellsize_x blending in mwall.  Returns (3, ...) float64."""
+    ww = 2 * cell[0]
+
+    def f(X, Y, Z):
+        gauss = np.exp(-((X / ww) ** 2))
+        return np.stack([(1 - gauss) * np.where(X < 0, m1[c], m2[c]) + gauss * mwall[c] for c in range(3)])
+    return f
+
+
+def rot_z(f, theta):
+    """engine/config.go:207-218 Config.RotZ: the configuration f rotated by
+    theta about z (coordinates rotated back, the vectors forward)."""
+    cs, sn = np.cos(theta), np.sin(theta)
+
+    def g(X, Y, Z):
+        m = f(X * cs + Y * sn, -X * sn + Y * cs, Z)
+        return np.stack([m[0] * cs - m[1] * sn, m[0] * sn + m[1] * cs, m[2]])
+    return g
+
+
+def sample(N, cell, f):
+    """A configuration function evaluated at every cell centre, as float32 (3, Nz, Ny, Nx)."""
+    return np.asarray(f(*coords(N, cell)), np.float64).astype(np.float32)
+
+
 def two_domain(N, cell, m1, mwall, m2):
     """engine/config.go TwoDomain: m1 for x < 0, m2 for x >= 0, a Gaussian
     wall of width 2*cellsize_x blending in mwall."""
-    X, _, _ = coords(N, cell)
-    ww = 2 * cell[0]
-    gauss = np.exp(-((X / ww) ** 2))
-    out = []
-    for c in range(3):
-        side = np.where(X < 0, m1[c], m2[c])
-        out.append((1 - gauss) * side + gauss * mwall[c])
-    return np.stack(out).astype(np.float32)
+    return sample(N, cell, two_domain_fn(cell, m1, mwall, m2))
 
 
 def _fmod(a, b):

@@ -509,3 +509,20 @@ def test_uniaxial_anisotropy_energy_of_one_cell():
         e = sim.energies()["anisotropy"] / V
         assert abs(e - want) <= 1, (ku1, ku2, e)
     sim.free()
+
+
+@pytest.mark.parametrize("ms", [(3.2, 4.6, 3.9, 7.8), (1.1, 1.1, 1.1, 1.1)])
+def test_exchange_inhomo_against_oommf(ms):
+    """test/exchange_inhomo.mx3: per-region Aex (harmonic mean between
+    regions) and Msat on the random 4x4x1 state of testdata/randommag4x4x1.ovf
+    (tests/golden); E_exch = OOMMF's 154.4891365 J within 1e-5, independent of
+    Msat."""
+    from tests.test_oracle_energy import _exchange_inhomo_case
+    engine, config = _e()
+    N, cell, m, regions, aex = _exchange_inhomo_case()
+    Ms = np.asarray((0.0,) + tuple(ms), np.float32)[regions]
+    sim = engine.Simulation(N, cell, Ms, aex, 0.1, regions=regions, demag=False)
+    sim.set_m(m)
+    E = sim.energies()["exchange"]
+    sim.free()
+    assert abs(E - 154.4891365) <= 1e-5, E

@@ -95,3 +95,32 @@ def test_no_demag_spins_restatement():
     r0 = np.broadcast_to(regions == 0, Ba.shape)
     assert np.array_equal(Ba[r0], Bb[r0]) and np.abs(Ba[r0]).max() > 1e-3
     assert np.all(Ba[~r0] == 0)
+
+
+def _exchange_inhomo_case():
+    """test/exchange_inhomo.mx3: 4x4x1 cells of 1 m, the random m of
+    testdata/randommag4x4x1.ovf (tests/golden/randommag4x4x1.npy), regions
+    1-4 the quadrants (rect(2,2) translated by (+-1, +-1)), Aex 1.2, 1.6, 4.3,
+    4.3 (harmonic mean between regions); E_exch from OOMMF 154.4891365 J."""
+    import os
+    from umagnus_b200 import config
+    N, cell = (4, 4, 1), (1.0, 1.0, 1.0)
+    m = np.load(os.path.join(os.path.dirname(__file__), "golden", "randommag4x4x1.npy"))
+    regions = np.zeros((1, 4, 4), np.uint8)
+    for r, (dx, dy) in zip((1, 2, 3, 4), ((1, 1), (-1, 1), (-1, -1), (1, -1))):
+        regions[config.rect(N, cell, 2, 2, transl=(dx, dy, 0)) > 0] = r
+    aex = np.ones(256)
+    aex[1:5] = (1.2, 1.6, 4.3, 4.3)
+    return N, cell, m, regions, aex
+
+
+@pytest.mark.parametrize("ms", [(3.2, 4.6, 3.9, 7.8), (1.1, 1.1, 1.1, 1.1)])
+def test_exchange_inhomo_against_oommf(ms):
+    """The oracle's exchange energy with per-region Aex and Msat equals
+    OOMMF's within the script's 1e-5 J, whatever the Msat values."""
+    N, cell, m, regions, aex = _exchange_inhomo_case()
+    assert sorted(np.unique(regions)) == [1, 2, 3, 4]
+    Ms = np.asarray((0.0,) + tuple(ms))[regions]
+    o = O.Simulation(N, cell, Ms, 1.0, 0.1, regions=regions, Aex_regions=aex, demag=False)
+    o.set_m(m)
+    assert abs(O.energies(o)["exchange"] - 154.4891365) <= 1e-5

@@ -526,3 +526,21 @@ def test_exchange_inhomo_against_oommf(ms):
     E = sim.energies()["exchange"]
     sim.free()
     assert abs(E - 154.4891365) <= 1e-5, E
+
+
+def test_antiferromagnetic_interexchange():
+    """test/interexchange.mx3: the SP4 film split at y = 0 into regions 1
+    (y >= 0) and 2 (y < 0), ext_ScaleExchange(1, 2, -1) (antiferromagnetic
+    coupling), alpha 3, 10 ns: <m> = (0, 0.114170685410499, 0) within 1e-5."""
+    engine, config = _e()
+    N = (128, 32, 1)
+    cell = (500e-9 / 128, 125e-9 / 32, 3e-9)
+    _, Y, _ = config.coords(N, cell)
+    regions = np.where(Y >= 0, 1, 2).astype(np.uint8)
+    sim = engine.Simulation(N, cell, 800e3, 13e-12, 3.0, regions=regions, exchange_scale={(1, 2): -1.0},
+                            demag_kernel="brute")
+    sim.set_m(config.uniform(N, 1, 0.1, 0))
+    sim.run(10e-9)
+    m = sim.average_m()
+    sim.free()
+    np.testing.assert_allclose(m, [0, 0.114170685410499, 0], rtol=0, atol=1e-5)

@@ -63,6 +63,22 @@ def exchange_lut(values, scale=None, inter=None):
     return lut
 
 
+def pair_tables(scale=None, inter=None):
+    """The scale and inter tables of an inter-region LUT (engine/exchange.go:
+    136-148): {(i, j): s} as ScaleExchange / ScaleDind (scale s, inter 0) and
+    {(i, j): v} as InterExchange / InterDind (scale 0, inter v); defaults 1
+    and 0.  Returns (scale, inter) arrays indexed by symmidx, or (None, None)."""
+    if not scale and not inter:
+        return None, None
+    n = NREGION * (NREGION + 1) // 2
+    sc, it = np.ones(n, np.float32), np.zeros(n, np.float32)
+    for (i, j), v in (scale or {}).items():
+        sc[symmidx(i, j)], it[symmidx(i, j)] = np.float32(v), 0
+    for (i, j), v in (inter or {}).items():
+        sc[symmidx(i, j)], it[symmidx(i, j)] = 0, np.float32(v)
+    return sc, it
+
+
 def _dev(x, dtype=torch.float32):
     return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype).cuda()
 
@@ -83,7 +99,9 @@ class Simulation:
     thermal field, new noise every accepted step; pbc: periodic repetitions
     per axis (engine/mesh.go SetPBC), 0 = open; NoDemagSpins: a scalar or 256
     per-region values, cells of non-zero regions neither make nor feel demag
-    field.
+    field; exchange_scale / exchange_inter ({(i, j): value}): ext_ScaleExchange /
+    ext_InterExchange between regions i and j, dmi_scale / dmi_inter the same
+    for Dind (engine/exchange.go:84-102).
     """
 
     def __init__(self, N, cell, Msat, Aex, alpha, Dind=0.0, Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
@@ -91,7 +109,8 @@ class Simulation:
                  dt=1e-15, MaxErr=1e-5, RelErr=1e-4, MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8,
                  device=0, asymptotic_radius=32, demag_kernel="newell", demag_accuracy=6.0, FrozenSpins=None,
                  Kc1=0.0, Kc2=0.0, Kc3=0.0, anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0,
-                 Temp=0.0, ThermSeed=0, pbc=(0, 0, 0), NoDemagSpins=None):
+                 Temp=0.0, ThermSeed=0, pbc=(0, 0, 0), NoDemagSpins=None, exchange_scale=None,
+                 exchange_inter=None, dmi_scale=None, dmi_inter=None):
         self.L = _lib.init(device)
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
@@ -138,10 +157,10 @@ class Simulation:
                     ptrs[c], muls[c] = None, float(np.float32(v[c]))
                 else:
                     ptrs[c], muls[c] = param(v[c])
-        self.aLUT = _dev(exchange_lut(Aex))
+        self.aLUT = _dev(exchange_lut(Aex, *pair_tables(exchange_scale, exchange_inter)))
         p.aLUT = keep(self.aLUT)
-        if np.any(np.asarray(Dind) != 0):
-            self.dLUT = _dev(exchange_lut(Dind))
+        if np.any(np.asarray(Dind) != 0) or dmi_inter:
+            self.dLUT = _dev(exchange_lut(Dind, *pair_tables(dmi_scale, dmi_inter)))
             p.dLUT = keep(self.dLUT)
         if np.any(np.asarray(Dbulk) != 0):  # engine/exchange.go:60-61 AddDMIBulk
             self.dbLUT = _dev(exchange_lut(Dbulk))

@@ -544,3 +544,27 @@ def test_antiferromagnetic_interexchange():
     m = sim.average_m()
     sim.free()
     np.testing.assert_allclose(m, [0, 0.114170685410499, 0], rtol=0, atol=1e-5)
+
+
+def test_demag_with_regions():
+    """test/demagRegion.mx3: 64x64x2 film (1, 1, 0.5 nm) in three regions
+    (x >= 0, x < 0, an ellipse) all with Msat = 2/mu0: the averaged B_demag of
+    uniform m along x, y, z is (0 +- 0.1, off-diagonal 1e-8, -2 +- 0.1); with
+    Msat = 1/mu0, B_demag_z of m along z is -1 +- 0.1."""
+    engine, config = _e()
+    N, cell = (64, 64, 2), (1e-9, 1e-9, 0.5e-9)
+    X, _, _ = config.coords(N, cell)
+    regions = np.where(X >= 0, 1, 2).astype(np.uint8)
+    regions[config.ellipse(N, cell, 10e-9, 20e-9) > 0] = 3
+    mu0 = 4e-7 * np.pi
+    Ms = np.full(regions.shape, 2 / mu0, np.float32)
+    sim = engine.Simulation(N, cell, Ms, 0.0, 0.0, regions=regions, demag_kernel="brute")
+    for i, want in ((0, 0.0), (1, 0.0), (2, -2.0)):
+        u = [0.0, 0.0, 0.0]
+        u[i] = 1.0
+        avg = _avg_demag(sim, config.uniform(N, *u))
+        assert abs(avg[i] - want) <= 0.1, (i, avg)
+        assert all(abs(avg[j]) <= 1e-8 for j in range(3) if j != i), (i, avg)
+    sim.set_param("Msat", 1 / mu0)
+    assert abs(_avg_demag(sim, config.uniform(N, 0, 0, 1))[2] + 1.0) <= 0.1
+    sim.free()

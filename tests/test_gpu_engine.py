@@ -391,3 +391,28 @@ def test_launch_shapes_do_not_change_results(eng, tmp_path):
     with pytest.raises(Exception):
         g.set_tuning(dict(best, torque_block=[48, 4]))
     g.free()
+
+
+@pytest.mark.parametrize("openbc", [False, True])
+def test_tma_tiles_equal_global_loads_on_awkward_meshes(eng, openbc):
+    """The torque kernel's TMA tiles against its global loads, bit for bit,
+    on a mesh whose width is not a multiple of the tile (36 cells), with
+    holes in the geometry (missing neighbours inside the mesh), interfacial
+    DMI with and without OpenBC, anisotropy, Zeeman and 3 layers."""
+    from umagnus_b200 import config
+    N, cell = (36, 20, 3), (2e-9, 2e-9, 1e-9)
+    geom = 1.0 - config.ellipse(N, cell, 14e-9, 10e-9)
+    m = G.random_unit(N, 21)
+    out = []
+    for tma in (1, 0):
+        g = eng.Simulation(N, cell, 9e5, 1.3e-11, 0.2, Dind=2e-3, Ku1=4e5, anisU=(0, 0.3, 1), B_ext=(0.01, 0, 0.02),
+                           geom=geom, open_bc=openbc)
+        t = dict(g.get_tuning(), torque_tma=tma)
+        for shape in ([32, 8], [64, 2]):
+            g.set_tuning(dict(t, torque_block=shape))
+            g.set_m(m)
+            tq, b = g.torque(beff=True)
+            out.append((tma, shape, tq.cpu(), b.cpu()))
+        g.free()
+    for tma, shape, tq, b in out[1:]:
+        assert torch.equal(tq, out[0][2]) and torch.equal(b, out[0][3]), (tma, shape)

@@ -3,6 +3,7 @@ this library implements, run on the GPU engine with the scripts' values and
 tolerances (default demag = the brute-force kernel, EnableDemag)."""
 import numpy as np
 import pytest
+import torch
 
 pytestmark = pytest.mark.gpu
 
@@ -568,3 +569,64 @@ def test_demag_with_regions():
     sim.set_param("Msat", 1 / mu0)
     assert abs(_avg_demag(sim, config.uniform(N, 0, 0, 1))[2] + 1.0) <= 0.1
     sim.free()
+
+
+def test_standard_problem_4_brute_3d():
+    """test/standardproblem4-3d.mx3: 128x32x2 cells, brute-force demag
+    (EnableDemag), relax then the 1 ns reversal with alpha 0.02 (TOL 1e-4)."""
+    engine, config = _e()
+    sim = _sp4_start(engine, config, engine.DORMANDPRINCE, N=(128, 32, 2), cz=1.5e-9)
+    sim.relax()
+    np.testing.assert_allclose(sim.average_m(), [0.9669952392578125, 0.12521563470363617, 0], rtol=0, atol=1e-4)
+    sim.set_param("alpha", 0.02)
+    sim.set_B_ext((-24.6e-3, 4.3e-3, 0.0))
+    sim.run(1e-9)
+    np.testing.assert_allclose(sim.average_m(), [-0.9846296310424805, 0.1256464719772339, 0.04335508495569229],
+                               rtol=0, atol=1e-4)
+    sim.free()
+
+
+def test_stepper_cache_is_flushed_by_a_new_m():
+    """test/steppercache.mx3: one cell, RK45DP with FixDt 1e-12 in 50 mT
+    along z; a step from m = +x and a step from m = -x rotate m by the same
+    angle (the FSAL torque of the old m must not be reused), TOL 1e-5."""
+    engine, config = _e()
+    N = (1, 1, 1)
+    sim = engine.Simulation(N, (1.0, 1.0, 1.0), 1000e3, 0.0, 0.1, B_ext=(0, 0, 0.05), demag=False,
+                            solver=engine.DORMANDPRINCE, FixDt=1e-12)
+    sim.set_m(config.uniform(N, 1, 0, 0))
+    sim.steps(1)
+    want = np.arccos(np.dot([1, 0, 0], sim.average_m()))
+    sim.set_m(config.uniform(N, -1, 0, 0))
+    sim.steps(1)
+    got = np.arccos(np.dot([-1, 0, 0], sim.average_m()))
+    sim.free()
+    assert abs(got - want) <= 1e-5 and want > 1e-3, (got, want)
+
+
+def test_run_while():
+    """test/runwhile.mx3: a 20x20 disc of 4 nm cells, alpha 1: RunWhile(MaxTorque
+    > 1e-3), then B_ext = (0, 0.01, 1) T and RunWhile(<m_y> < 0.5): <m_y> =
+    0.53 within 0.02 (the overshoot of the last step).  The condition is
+    checked before every step, as engine/run.go:200-231 runWhile does."""
+    engine, config = _e()
+    N, c = (20, 20, 1), 4e-9
+    cell = (c, c, c)
+    sim = engine.Simulation(N, cell, 800e3, 13e-12, 1.0, B_ext=(0, 0, 0), geom=config.ellipse(N, cell, 20 * c, 20 * c),
+                            demag_kernel="brute")
+    sim.set_m(config.uniform(N, 1, 0, 0))
+
+    def max_torque():  # MaxTorque: max |torque| of the current m
+        return float(torch.linalg.vector_norm(sim.torque(), dim=0).max())
+
+    n = 0
+    while max_torque() > 1e-3 and n < 200000:
+        sim.steps(1)
+        n += 1
+    sim.set_B_ext((0, 0.01, 1.0))
+    while sim.average_m()[1] < 0.5 and n < 400000:
+        sim.steps(1)
+        n += 1
+    my = sim.average_m()[1]
+    sim.free()
+    assert abs(my - 0.53) <= 0.02, (my, n)

@@ -112,6 +112,7 @@ def tune(sim, cache_path=None, evals=40, steps=16, use_cache=True):
     stream = torch.cuda.Stream()
     m0 = sim.get_m().clone()
     st0 = sim.state()
+    previous = getattr(sim, "stream", None)  # the caller's stream, put back at the end
     sim.set_stream(stream)
     try:
         def measure(kind, t):
@@ -139,7 +140,7 @@ def tune(sim, cache_path=None, evals=40, steps=16, use_cache=True):
         sim.restore_m(m0)
         sim.set_time(st0["time"], st0["dt"])
         torch.cuda.synchronize()
-        sim.set_stream(None)
+        sim.set_stream(previous)
     if use_cache:
         cache = load_cache(cache_path)
         cache[key] = sim.get_tuning()

@@ -360,6 +360,7 @@ class Simulation:
     def set_stream(self, stream):
         """Queue all library work on a torch.cuda.Stream (None = library stream)."""
         check(self.L.umag_set_stream(None if stream is None else stream.cuda_stream))
+        self.stream = stream
 
     def get_tuning(self):
         """Launch shapes of the per-cell kernels (umag_tuning) as a dict."""

@@ -27,6 +27,7 @@
 #include "demag.cuh"
 #include "fft.cuh"
 #include "newell.cuh"
+#include "tile.cuh"
 
 namespace umag {
 
@@ -436,6 +437,39 @@ static size_t pass_ac_smem(const umag_demag* d) {
 }
 static size_t pass_b_smem(const umag_demag* d) { return sizeof(float2) * (size_t)d->P[1] * 3 * d->WB; }
 
+// Tensor map for pass C's slab loads (PassArgs::slab_map): the blocked
+// spectrum as floats (8 = four complex columns, y, kx/4, kz, component), a
+// box of one (y, component) slab; only where the register passes use the
+// slab shape and the slab fits the x/z scratch it borrows.  Without it pass C
+// keeps its plain loads.
+static void slab_setup(umag_demag* d) {
+    const FastPasses& f = d->fast;
+    if (!d->use_fast || !f.blocked || !f.slab_ok || d->Lx % 4 != 0) return;
+    const int KB = d->Lx / 4, Ny = d->N[1], Pz = d->P[2];
+    const size_t bytes = sizeof(float2) * 4 * (size_t)KB * Pz;
+    if (bytes + 128 > f.ac_scratch || KB > 256 || Pz > 256) return;  // + the alignment slack
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || reinterpret_cast<uintptr_t>(d->spec) % 16 != 0) return;
+    const cuuint64_t row = sizeof(float2) * 4;  // 32 bytes: four complex columns
+    const cuuint64_t dims[5] = {8, (cuuint64_t)Ny, (cuuint64_t)KB, (cuuint64_t)Pz, 3};
+    const cuuint64_t strides[4] = {row, row * Ny, row * Ny * KB, row * Ny * KB * Pz};
+    const cuuint32_t box[5] = {8, 1, (cuuint32_t)KB, (cuuint32_t)Pz, 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUtensorMap map;
+    if (fn(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, d->spec, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+        CUDA_SUCCESS)
+        return;
+    CUtensorMap* dev = nullptr;
+    if (cudaMalloc(&dev, sizeof(CUtensorMap)) != cudaSuccess) return;
+    if (cudaMemcpyAsync(dev, &map, sizeof(map), cudaMemcpyHostToDevice, ctx().stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx().stream) != cudaSuccess) {
+        cudaFree(dev);
+        return;
+    }
+    d->slab_map = dev;
+}
+
 static int plan_common(umag_demag* d) {
     for (int i = 0; i < 3; i++) UMAG_REQUIRE(d->N[i] > 0, "mesh size must be positive");
     for (int i = 0; i < 3; i++) UMAG_REQUIRE(d->pbc[i] >= 0, "PBC repetitions must be non-negative");
@@ -500,6 +534,7 @@ static int plan_common(umag_demag* d) {
     d->use_fast = !periodic && getenv("UMAG_GENERIC_FFT") == nullptr &&
                   demag_fast_select(d->M, d->P[1], d->P[2], d->fast);
     if (d->use_fast) UMAG_TRY(demag_fast_grid(d->fast, d->M, d->P[2]));
+    slab_setup(d);
     return UMAG_OK;
 }
 
@@ -740,6 +775,7 @@ void fill_pass_args(const umag_demag* d, PassArgs& a) {
     a.Kp = d->Kp;
     a.blocked = d->use_fast && d->fast.blocked ? 1 : 0;
     a.Kblocked = a.blocked;
+    a.slab_map = d->slab_map;
 }
 
 int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st) {
@@ -770,11 +806,14 @@ int demag_launch_batch(const umag_demag* d, const PassArgs& a, int nb, cudaStrea
     UMAG_REQUIRE(d->use_fast && d->fast.ab && d->fast.bb && d->fast.cb, "batched demag needs a compile-time FFT plan");
     UMAG_REQUIRE(nb >= 1 && 3L * nb <= 65535 && (long)d->fast.gby * nb <= 65535, "too many instances in one batch");
     const FastPasses& f = d->fast;
-    f.ab<<<dim3(d->N[1], 3 * nb), f.nt_ac, f.smem_ac, st>>>(a);
+    // per-instance spectra: the slab map covers the plan's own spectrum only
+    PassArgs ab = a;
+    ab.slab_map = nullptr;
+    f.ab<<<dim3(d->N[1], 3 * nb), f.nt_ac, f.smem_ac, st>>>(ab);
     UMAG_LAUNCH_CHECK();
-    f.bb<<<dim3(f.gbx, f.gby * nb), f.nt_b, f.smem_b, st>>>(a);
+    f.bb<<<dim3(f.gbx, f.gby * nb), f.nt_b, f.smem_b, st>>>(ab);
     UMAG_LAUNCH_CHECK();
-    f.cb<<<dim3(d->N[1], 3 * nb), f.nt_ac, f.smem_ac, st>>>(a);
+    f.cb<<<dim3(d->N[1], 3 * nb), f.nt_ac, f.smem_ac, st>>>(ab);
     UMAG_LAUNCH_CHECK();
     return UMAG_OK;
 }
@@ -816,6 +855,7 @@ void demag_free(umag_demag* d) {
     for (auto p : d->tw_dev) cudaFree(p);
     cudaFree(d->twr);
     cudaFree(d->spec);
+    cudaFree(d->slab_map);
     for (int c = 0; c < 6; c++) cudaFree(d->K[c]);
     delete d;
 }

@@ -2,6 +2,8 @@
 #pragma once
 #include <vector>
 
+#include <cuda.h>
+
 #include "common.cuh"
 #include "fft.cuh"
 
@@ -36,6 +38,10 @@ struct FastPasses {
     int wb_n = 0, nt_b_n = 0;
     unsigned gbx_n = 0;
     bool use_narrow = false;
+    // bytes of pass C's x/z scratch (Xs and the exchange lines), which its
+    // z phase can borrow for a TMA-loaded spectrum slab (register passes)
+    size_t ac_scratch = 0;
+    bool slab_ok = false;  // pass C can take its z input as one slab
 };
 }  // namespace umag
 
@@ -57,6 +63,7 @@ struct umag_demag {
     float* K[6] = {};                 // xx yy zz yz xz xy (yz, xz NULL in 2D)
     size_t Kn = 0;  // floats per kernel array (Kp * (Py/2+1) * (Pz/2+1))
     int Kp = 0;     // row pitch: Px/2+1 rounded up to 4 floats (16-byte rows)
+    CUtensorMap* slab_map = nullptr;  // device copy: pass C's (y, component) slabs of spec
 };
 
 namespace umag {
@@ -90,6 +97,10 @@ struct PassArgs {
     const float* Ms;
     float Ms_mul;
     float* B[3];
+    // tensor map (device memory) of the blocked spectrum viewed as
+    // (8 floats, y, kx/4, kz, component): pass C loads the slab of one
+    // (y, component) with one bulk tensor copy; NULL: plain loads
+    const CUtensorMap* slab_map;
 };
 
 int demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy, double cz, int arad,

@@ -9,8 +9,13 @@
 #include "fft_pair.cuh"
 #include "fft_reg.cuh"
 #include "fft_static.cuh"
+#include "tile.cuh"
 
 namespace umag {
+
+// pass C slab loads that gave up waiting (bounded mbarrier poll)
+__device__ unsigned g_slab_timeouts = 0;
+
 
 static constexpr double kMu0f = 4 * 3.1415926535897932384626433 * 1e-7;  // clh/constants.clh:5
 
@@ -620,7 +625,7 @@ template <int M, int PZ>
 __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, const int by, const int ib) {
     using S = RegAC<M, PZ>;
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
-    extern __shared__ __align__(16) float2 sm[];
+    extern __shared__ __align__(128) float2 sm[];
     float2* twx = sm;
     float2* twz = twx + M;
     float2* twr = twz + PZ;
@@ -628,10 +633,33 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
     float2* ex = Xs + NZ * XP;
     if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
+    // the (y, component) slab of the spectrum by one bulk tensor copy into
+    // the x/z scratch (Xs and the exchange lines, idle until the z phase has
+    // its inputs in registers): [kz][kx/4][kx%4] complex
+    constexpr bool kSlabShape = (PZ == 16 || PZ == 32) && M / (NT / 2) == 1;
+    __shared__ __align__(8) uint64_t slab_bar;
+    // (Xs is 16-byte aligned, so the 128-byte rounding below moves it by a
+    // whole number of float2)
+    const bool slab = kSlabShape && a.slab_map != nullptr && ib == 0 && (smem_u32(Xs) & 15u) == 0;
+    if (slab && tid == 0) mbar_init(&slab_bar, 1);
     for (int i = tid; i < M; i += NT) { twx[i] = a.fx.tw[i]; twr[i] = a.twr[i]; }
     for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
     __syncthreads();
     const int y = bx, c = by, Ny = a.Ny;
+    const int KB = a.Lx >> 2;  // four-column blocks per kz row of the slab
+    // the copy's destination on a 128-byte boundary (the dynamic region
+    // need not start on one; the plan leaves 128 bytes of slack)
+    float2* const sl = Xs + ((128u - (smem_u32(Xs) & 127u)) & 127u) / sizeof(float2);
+    if (slab) {
+        if (tid == 0) {
+            mbar_expect_tx(&slab_bar, (uint32_t)(sizeof(float2) * 4 * KB * PZ));
+            tma_load_5d(sl, a.slab_map, 0, y, 0, 0, c, &slab_bar);
+        }
+        for (int it = 0; !mbar_try_wait(&slab_bar, 0); it++) {
+            if (it == kTileWaitLimit && tid == 0) atomicAdd(&g_slab_timeouts, 1u);
+            if (it >= 2 * kTileWaitLimit) return;
+        }
+    }
     const float2* in = inst_spec(a, ib) + (long)c * PZ * Ny * a.Lx + (long)y * spec_rowstride(a);
     const long kzs = (long)Ny * a.Lx;
     if constexpr (PZ == 16 || PZ == 32) {
@@ -654,13 +682,19 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
             float2 u[E2];
 #pragma unroll
             for (int j = 0; j < E2; j++) {
-                float2 q = in[(long)(2 * j + t2) * kzs + ko];
-                if (pk) {
-                    const float2 g = in[(long)(2 * j + t2) * kzs + kM];
-                    q = make_float2(q.x - g.y, q.y + g.x);
+                const int kz = 2 * j + t2;
+                float2 q, g;
+                if (slab) {
+                    q = sl[(kz * KB + (kx >> 2)) * 4 + (kx & 3)];
+                    g = sl[(kz * KB + (M >> 2)) * 4 + (M & 3)];
+                } else {
+                    q = in[(long)kz * kzs + ko];
+                    g = pk ? in[(long)kz * kzs + kM] : make_float2(0.f, 0.f);
                 }
+                if (pk) q = make_float2(q.x - g.y, q.y + g.x);
                 u[j] = make_float2(q.x, -q.y);
             }
+            if (slab) __syncthreads();  // every input is in registers before Xs is written
             reg_dft<E2>(u);
             if (t2) tw_ramp<PZ, 1, 0, E2>(u);
 #pragma unroll
@@ -780,6 +814,8 @@ template <int M, int PZ> static void fill_ac(FastPasses& f) {
         f.ab = k_reg_a_bat<M, PZ>;
         f.cb = k_reg_c_bat<M, PZ>;
         f.smem_ac = RegAC<M, PZ>::smem;
+        f.ac_scratch = sizeof(float2) * ((size_t)RegAC<M, PZ>::NZ * RegAC<M, PZ>::XP + RegAC<M, PZ>::EXN);
+        f.slab_ok = (PZ == 16 || PZ == 32) && M / (RegAC<M, PZ>::NT / 2) == 1;
         f.nt_ac = RegAC<M, PZ>::NT;
         f.ac_reg = true;
     } else {
@@ -860,7 +896,10 @@ int demag_fast_setup() {
     // opt in to the full 227 KB and ask for the largest shared-memory carveout,
     // so several CTAs of these shared-memory-heavy kernels fit on one SM
     auto attrs = [](void (*k)(PassArgs)) -> int {
-        UMAG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        cudaFuncAttributes fa;  // the opt-in covers static + dynamic shared memory
+        UMAG_CUDA(cudaFuncGetAttributes(&fa, k));
+        UMAG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       227 * 1024 - (int)fa.sharedSizeBytes));
         UMAG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                        cudaSharedmemCarveoutMaxShared));
         return UMAG_OK;

@@ -194,8 +194,11 @@ __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ Lo
     const float *mx = m, *my = m + N, *mz = m + 2 * N;
     TileView tv{};
     if constexpr (TILE) {
-        extern __shared__ __align__(128) float tile[];
+        extern __shared__ __align__(128) float tile_raw[];
         __shared__ __align__(8) uint64_t bar;
+        // the copy's destination on a 128-byte boundary whatever the offset of
+        // the dynamic region (launched with 128 bytes of slack)
+        float* const tile = tile_raw + ((128u - (smem_u32(tile_raw) & 127u)) & 127u) / sizeof(float);
         const bool three_d = a.g.Nz > 1;
         const uint32_t bytes = (uint32_t)tile_bytes(blockDim.x, blockDim.y, a.g.Nz);
         const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
@@ -729,7 +732,7 @@ static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, flo
     if (s->batched)
         k_local_torque<true, true, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
     else if (s->zero_regions && s->tile_ok && s->tune.torque_tma)
-        k_local_torque<true, false, true><<<grd, blk, tile_bytes(bx, by, s->g.Nz), S()>>>(la, s->tmaps);
+        k_local_torque<true, false, true><<<grd, blk, tile_bytes(bx, by, s->g.Nz) + 128, S()>>>(la, s->tmaps);
     else if (s->zero_regions)
         k_local_torque<true, false, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
     else
@@ -973,24 +976,6 @@ static int run_steps(SimImpl* s, long long n) {
         UMAG_TRY(launch_step(s, &nl));
     }
     return UMAG_OK;
-}
-
-// cuTensorMapEncodeTiled from the driver (looked up once; no libcuda link)
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-static EncodeTiledFn encode_tiled() {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
-    return fn;
 }
 
 // Tensor maps for the magnetisation tiles of the torque kernel (tile.cuh),

@@ -17,8 +17,13 @@ FFT), so N GPUs run N independent replicas ("replicas only").
 --impl reference times the reference's implementation of the path on the
 host cores: the reference's own OpenCL C kernels compiled for the host
 (oracle/_ref) and spread over all host threads, scipy.fft (multi-threaded)
-in place of clFFT, the RK45DP stepper and controller restated in numpy
-(oracle/ref_arm.py).  A CPU step takes seconds, so that arm times whole
+in place of the reference's vendored VkFFT (which needs an OpenCL device),
+the RK45DP stepper and controller restated in numpy (oracle/ref_arm.py).
+
+Accuracy: outside every timed region, B_eff and the torque of the seeded
+m0 from the engine are compared with the FP64 oracle (oracle/gpu64.py, the
+checker; its Newell tensor comes from the CPU oracle) and the line carries
+the error (`error_vs_fp64`).  A CPU step takes seconds, so that arm times whole
 steps until --steps or --ref-budget seconds, whichever comes first.
 """
 import argparse
@@ -41,6 +46,7 @@ UNIT = "cell-updates/s"
 # this workload (79,291,392 + 5,342,208 B), from one ncu --set full capture of
 # that launch (cold cache: ncu flushes the caches between its passes)
 TRAFFIC_B = 84633600
+TRAFFIC_B_SOURCE = "ncu capture of k_reg_b<512,4> (profiles/k_reg_b_multilayer_256x256x16.md)"
 
 
 def alg_bytes_per_eval(N):
@@ -232,7 +238,40 @@ def cpu_baseline(config, budget_s=12.0):
     return {"value": acc * ncell / t, "unit": UNIT, "cores": r.threads, "kind": "reference",
             "sample": (f"{n} RK45DP steps ({acc} accepted) of the full 256x256x16 workload in {t:.1f} s after one "
                        f"warm-up step: reference OpenCL C kernels compiled for the host on {r.threads} threads, "
-                       "scipy.fft for clFFT; Newell kernel setup excluded")}
+                       "scipy.fft for the reference's VkFFT; Newell kernel setup excluded")}
+
+
+# ------------------------------------------------------------------ accuracy
+def error_vs_fp64(sim, m0, cfg):
+    """B_eff and the torque of m0 from the engine (the kernels the benchmark
+    times) against the FP64 oracle (oracle/gpu64.py with the CPU oracle's
+    Newell tensor): max and RMS of |dB| / max|B|, |dtau| / max|tau|.  The
+    oracle is the checker here; this runs after every timed region."""
+    import torch
+    from oracle import gpu64
+    from oracle import oracle as O
+    N = cfg["N"]
+    sim.set_m(m0)
+    tau, B = sim.torque(beff=True)
+    m = sim.get_m().reshape((3,) + sim.shape).double()
+    sys64 = gpu64.System64(N, cfg["cell"], cfg["Ms"], O.exch_lut(np.full(256, cfg["Aex"]), dtype=np.float64),
+                           np.zeros(N[::-1], np.uint8), cfg["alpha"], kernel=O.newell_kernel(N, cfg["cell"]),
+                           Ku1=cfg["Ku1"], anisU=cfg["anisU"], B_ext=cfg["B_ext"],
+                           dLUT=O.exch_lut(np.full(256, cfg["Dind"]), dtype=np.float64))
+    B64 = sys64.beff(m)
+    t64 = sys64.torque(m, B64)
+    del sys64
+
+    def rel(a, b):
+        d = torch.sqrt(((a.reshape(b.shape).double() - b) ** 2).sum(0))
+        n = torch.sqrt((b ** 2).sum(0))
+        return {"max_rel_to_max": float(d.max() / n.max()),
+                "rms_rel_to_rms": float(torch.sqrt((d ** 2).mean() / (n ** 2).mean()))}
+
+    out = {"B_eff": rel(B, B64), "torque": rel(tau, t64), "tolerance": 1e-5,
+           "what": "one field + torque evaluation of the seeded m0 against the FP64 oracle"}
+    out["within_tolerance"] = out["B_eff"]["max_rel_to_max"] <= 1e-5 and out["torque"]["max_rel_to_max"] <= 1e-5
+    return out
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -312,18 +351,25 @@ def run_ours(args, rank, world, local_rank):
     t_e0 = time.perf_counter()
     dev_m.copy_(host_m, non_blocking=True)
     sim.set_m(dev_m)
-    chunks = max(1, args.steps // graph_steps)
+    # the same step count as the device-timed region: chunks of graph_steps
+    # and the remainder, with a solver-state read-back after each chunk
+    steps_e2e = args.steps
     s_before = sim.state()
-    for _ in range(chunks):
-        sim.steps(graph_steps)
+    chunks, left = 0, steps_e2e
+    while left > 0:
+        n = min(graph_steps, left)
+        sim.steps(n)
         s_now = sim.state()  # D2H of the solver state after every chunk
+        left -= n
+        chunks += 1
     out = sim.get_m()
     host_out.copy_(out)
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t_e0
     acc_e2e = s_now["nsteps"] - s_before["nsteps"]
-    steps_e2e = chunks * graph_steps
     bytes_state = 88
+    # accuracy of the timed path (checker, outside every timed region)
+    err64 = error_vs_fp64(sim, m0, cfg) if rank == 0 else None
     (ms_max, ms_eval_max, t_e2e_max), (acc_tot, acc_e2e_tot) = combine_ranks(
         torch.tensor([ms, ms_eval, t_e2e], dtype=torch.float64, device="cuda"),
         torch.tensor([acc, acc_e2e], dtype=torch.float64, device="cuda"), dist)
@@ -347,7 +393,8 @@ def run_ours(args, rank, world, local_rank):
             "roofline": {"bound": "hbm", "kernel": f"k_reg_b (demag pass B: y FFT, kernel multiply, inverse y)",
                          "achieved": bp["B"] / (ms_pass["B"] * 1e-3) / 1e9, "peak": peak, "peak_source": peak_kind,
                          "unit": "GB/s", "frac": bp["B"] / (ms_pass["B"] * 1e-3) / 1e9 / peak,
-                         "traffic": TRAFFIC_B, "alg_bytes_per_launch": bp["B"], "ms_per_launch": ms_pass["B"],
+                         "traffic": TRAFFIC_B, "traffic_source": TRAFFIC_B_SOURCE,
+                         "alg_bytes_per_launch": bp["B"], "ms_per_launch": ms_pass["B"],
                          "passes": {k: {"ms": ms_pass[k], "alg_bytes": bp[k],
                                         "gbs": bp[k] / (ms_pass[k] * 1e-3) / 1e9} for k in "ABC"},
                          "field_eval": {"ms": ms_eval_max, "alg_bytes": b_eval, "gbs": achieved,
@@ -356,10 +403,13 @@ def run_ours(args, rank, world, local_rank):
             "e2e": {"value": acc_e2e_tot * ncell / t_e2e_max, "unit": UNIT,
                     "h2d_bytes_per_step": (12 * ncell) / steps_e2e,
                     "d2h_bytes_per_step": (12 * ncell + bytes_state * chunks) / steps_e2e,
-                    "how": "pinned host m -> device, set_m, steps in graph chunks of 16 with a solver-state "
-                           "read-back per chunk, final m -> pinned host; wall clock"},
+                    "steps": steps_e2e,
+                    "how": "pinned host m -> device, set_m, the same step count as the timed region in graph "
+                           "chunks of 16 (and the remainder) with a solver-state read-back per chunk, final m -> "
+                           "pinned host; wall clock"},
             "gpu_launches": sim.launches_per_step() * args.steps,
             "clocks": clk.summary(),
+            "error_vs_fp64": err64,
         }
     sim.free()
     return result
@@ -887,7 +937,7 @@ def main():
         value = acc * ncell / t
         sample = (f"{n} of the {args.steps} requested RK45DP steps ({acc} accepted, {t:.1f} s budget-bounded) of "
                   f"the full workload: reference OpenCL C kernels compiled for the host on {r.threads} threads, "
-                  "scipy.fft (multi-threaded) standing in for clFFT")
+                  "scipy.fft (multi-threaded) standing in for the reference's VkFFT")
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": n,
                 "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": t / n * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

@@ -41,6 +41,7 @@ extern "C" {
 #define UMAG_E_NOMEM 4
 #define UMAG_E_NOT_INIT 5
 #define UMAG_E_SOLVER 6      /* time step underflow / NaN in the solver */
+#define UMAG_E_TIMEOUT 7     /* a kernel gave up waiting for a bulk copy (bounded wait) */
 
 /* ---- device bring-up (opencl/init.go) ------------------------------------ */
 /* opencl/init.go:48 Init(gpu): select the device, create the stream. */
@@ -174,7 +175,11 @@ int umag_demag_new_brute(int Nx, int Ny, int Nz, const int pbc[3], double cx, do
 int umag_demag_new_from_kernel(int Nx, int Ny, int Nz, const double* const kern[6],
                                umag_demag** out);
 /* opencl/conv_demag.go:43 (*DemagConvolution).Exec: B = demag field of
- * MU0*Ms*vol*m (B is overwritten).  vol and Ms may be NULL. */
+ * MU0*Ms*vol*m (B is overwritten).  vol and Ms may be NULL.  Returns after
+ * the field is complete (the reference's Exec waits for its kernels too);
+ * UMAG_E_TIMEOUT if a pass gave up waiting for one of its bulk copies (the
+ * count stays set, like a sticky CUDA error, until umag_debug_plant_fault
+ * clears it). */
 int umag_demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float* mx,
                     const float* my, const float* mz, const float* vol, const float* Ms,
                     float Ms_mul);
@@ -200,16 +205,28 @@ int umag_demag_free(umag_demag* d);
  * arrays (the layout umag_demag_get_spectrum returns, yz/xz may be NULL for
  * Nz == 1) on the device, and all working memory lives in one 16 MiB
  * __device__ array that every GPU loading this library keeps until the
- * process exits.  Meshes whose spectrum and twiddles exceed 16 MiB, or
- * without a compile-time FFT plan, return UMAG_E_UNSUPPORTED.  The first
- * call on a device looks up the array's device address (make that call
- * before any stream capture).  Work is queued on `stream` (a cudaStream_t,
- * NULL = legacy default stream); every call shares the array, so calls that
+ * process exits.  The driver reserves that array when the library's module
+ * is loaded on a device: umag_init does this for its device, otherwise the
+ * first call of this function does (and looks up the array's address) --
+ * make one of the two on each device before an external pool claims the
+ * device's memory and before any stream capture.  Meshes whose spectrum
+ * and twiddles exceed 16 MiB, or without a compile-time FFT plan, return
+ * UMAG_E_UNSUPPORTED.  Work is queued on `stream` (a cudaStream_t, NULL =
+ * legacy default stream); every call shares the array, so calls that
  * overlap on the GPU (other streams, other host threads) race.  Calls no
  * cudaMalloc, cudaFree or other allocating routine. */
 int umag_demag_exec_noalloc(int Nx, int Ny, int Nz, const float* const K[6], float* Bx, float* By, float* Bz,
                             const float* mx, const float* my, const float* mz, const float* vol, const float* Ms,
                             float Ms_mul, void* stream);
+
+/* Test hook for the error paths of bounded device waits (no counterpart in
+ * the reference): with sim == NULL, sets the device counter of timed-out
+ * demag bulk copies that umag_demag_exec reports (0 clears it); with a
+ * simulation, writes `code` into its device-side solver status, as a
+ * device kernel does when a wait gives up (status 7).  Nothing on the GPU
+ * faults or waits: the planted value is what the host-side checks read. */
+typedef struct umag_sim umag_sim;
+int umag_debug_plant_fault(umag_sim* sim, unsigned code);
 
 /* ---- engine: a whole simulation on the device ---------------------------- */
 /* Material and mesh description.  Uniform parameters use the *_mul value
@@ -270,7 +287,6 @@ typedef struct {
     int status;      /* 0 ok; nonzero: UMAG_E_SOLVER cause code */
 } umag_solver_state;
 
-typedef struct umag_sim umag_sim;
 void umag_solver_defaults(umag_solver_params* p);
 int umag_sim_new(const umag_sim_params* p, const umag_solver_params* s, umag_sim** out);
 int umag_sim_free(umag_sim* s);

@@ -17,8 +17,28 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF = os.environ.get("UMAG_REFERENCE", "/root/reference")
-KS = os.path.join(REF, "kernels_src")
+# Where the reference checkout lives: $UMAG_REFERENCE, else the build
+# machine's read-only checkout.  This recipe is the one place that names the
+# default; tests and fixture scripts ask reference_root().
+DEFAULT_REFERENCE = "/root/reference"
+
+
+def reference_root():
+    """The reference checkout ($UMAG_REFERENCE, else the default location), or
+    None when neither exists (the GPU box has no reference tree)."""
+    env = os.environ.get("UMAG_REFERENCE")
+    if env:
+        if not os.path.isdir(env):
+            raise FileNotFoundError(f"UMAG_REFERENCE={env} is not a directory")
+        return env
+    return DEFAULT_REFERENCE if os.path.isdir(DEFAULT_REFERENCE) else None
+
+
+def _kernels_src():
+    ref = reference_root()
+    if ref is None:
+        raise FileNotFoundError("reference checkout not found: set UMAG_REFERENCE to its root")
+    return os.path.join(ref, "kernels_src")
 
 HEADERS = ["typedefs.clh", "constants.clh", "stencil.clh", "float3.clh", "exchange.clh", "amul.clh"]
 KERNELS = ["copypadmul2", "copyunpad", "kernmulrsymm3d", "kernmulrsymm2dxy", "kernmulrsymm2dz",
@@ -80,6 +100,7 @@ MADD = {n: ", ".join(["R* dst"] + [f"R* s{i}, R f{i}" for i in range(1, n + 1)] 
 
 
 def gen_tu(real, sfx):
+    KS = _kernels_src()
     lines = ["// generated by oracle/build_ref.py -- do not edit", '#include "../clshim.hpp"']
     if real == "double":
         lines += ["#define __REAL_IS_DOUBLE__ 1", "#define cl_khr_fp64 1"]
@@ -118,6 +139,7 @@ def gen_tu(real, sfx):
 
 
 def build(verbose=False):
+    KS = _kernels_src()
     if not os.path.isdir(KS):
         raise FileNotFoundError(f"reference kernels not found at {KS}")
     os.makedirs(OUT, exist_ok=True)

@@ -32,10 +32,14 @@ class System64:
     kernel: real-space demag kernel (6, Pz, Py, Px) float64 (xx yy zz yz xz
     xy) or None for no demag; Ms, Ku1: (Nz, Ny, Nx) arrays or scalars; aLUT:
     32896 float64 exchange LUT with `regions` (uint8 map); anisU: 3-vector or
-    (3, Nz, Ny, Nx); B_ext: 3-vector or None; alpha scalar."""
+    (3, Nz, Ny, Nx); B_ext: 3-vector or None; alpha scalar; dLUT: 32896
+    float64 interfacial-DMI LUT (None: exchange only), which switches the
+    exchange term to dmi.cl's exchange + DMI as engine/exchange.go:49-66
+    does; openbc: dmi.cl's OpenBC (no boundary extrapolation).  Open
+    boundaries only (no PBC)."""
 
     def __init__(self, N, cell, Ms, aLUT, regions, alpha, kernel=None, Ku1=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
-                 device="cuda"):
+                 device="cuda", dLUT=None, openbc=False):
         self.dev = torch.device(device)
         self.N = tuple(int(n) for n in N)
         Nx, Ny, Nz = self.N
@@ -61,6 +65,10 @@ class System64:
         reg = torch.as_tensor(np.asarray(regions, np.uint8).reshape(self.shape), device=self.dev).long()
         lut = torch.as_tensor(np.asarray(aLUT, np.float64), device=self.dev)
         w = [2.0 / (c * c) for c in cell]
+        self.cell = tuple(float(c) for c in cell)
+        self.reg, self.aLUT = reg, lut
+        self.dLUT = None if dLUT is None else torch.as_tensor(np.asarray(dLUT, np.float64), device=self.dev)
+        self.openbc = bool(openbc)
         self.dirs = []  # (axis, side, coefficient tensor)
         for axis, wd in ((2, w[0]), (1, w[1]), (0, w[2])):
             if axis == 0 and Nz == 1:
@@ -124,10 +132,63 @@ class System64:
         e = e * self.inv_ms[None]
         return torch.where(m0zero[None], torch.zeros_like(e), e)
 
+    def dmi_field(self, m):
+        """dmi.cl:8-148 (exchange + interfacial DMI) in FP64.  In-plane
+        neighbours outside the mesh or empty (m = 0) take the Neumann
+        extrapolation of dmi.cl:46-50, 67-71, 89-93, 110-114 (nothing with
+        OpenBC); the pair coefficients A, D come from the LUTs at (r0, rn) with
+        rn = r0 for a missing neighbour; z neighbours carry exchange only
+        (clamped, an empty one counts as m0); the sum is times 1/Ms and zero
+        where m0 is zero."""
+        m0zero = (m * m).sum(0) == 0
+        h = torch.zeros_like(m)
+        reg = self.reg
+        for axis, c in ((2, self.cell[0]), (1, self.cell[1])):  # x, y: tensor axes of (Nz, Ny, Nx)
+            n = m.shape[axis + 1]
+            for side in (-1, 1):
+                idx = torch.arange(n, device=m.device) + side
+                inside = (idx >= 0) & (idx < n)
+                mn = torch.index_select(m, axis + 1, idx.clamp(0, n - 1))
+                shape = [1, 1, 1]
+                shape[axis] = n
+                mn = mn * inside.to(m.dtype).reshape([1] + shape)
+                nz = (mn * mn).sum(0) == 0
+                rn = torch.where(nz, reg, self._shift(reg, axis, side))
+                k = symidx(reg, rn)
+                A = self.aLUT[k]
+                D = self.dLUT[k]
+                sc = -c if side < 0 else c
+                q = sc * (0.5 * D / A)
+                mx, my, mz = m[0], m[1], m[2]
+                if axis == 2:
+                    ext = torch.stack([mx - q * mz, my, mz + q * mx])
+                else:
+                    ext = torch.stack([mx, my - q * mz, mz + q * my])
+                mn = torch.where(nz[None], ext, mn)
+                act = (~nz) if self.openbc else torch.ones_like(nz)
+                act = act.to(m.dtype)
+                s = 2.0 * A / (c * c)
+                h += (act * s)[None] * (mn - m)
+                Dc = act * D / c
+                tz = -mn[2] if side < 0 else mn[2]
+                tp = -mn[0 if axis == 2 else 1] if side < 0 else mn[0 if axis == 2 else 1]
+                h[0 if axis == 2 else 1] += Dc * tz
+                h[2] -= Dc * tp
+        if self.shape[0] != 1:
+            cz = self.cell[2]
+            for side in (-1, 1):
+                mn = self._shift(m, 1, side)
+                nz = (mn * mn).sum(0) == 0
+                mn = torch.where(nz[None], m, mn)
+                A = self.aLUT[symidx(reg, self._shift(reg, 0, side))]
+                h += (2.0 * A / (cz * cz))[None] * (mn - m)
+        h = h * self.inv_ms[None]
+        return torch.where(m0zero[None], torch.zeros_like(h), h)
+
     def field_terms(self, m):
-        """(demag, exchange, anisotropy, zeeman) fields of m."""
+        """(demag, exchange or exchange + DMI, anisotropy, zeeman) fields of m."""
         Bd = self.demag_field(m) if self.demag else torch.zeros_like(m)
-        Be = self.exchange_field(m)
+        Be = self.exchange_field(m) if self.dLUT is None else self.dmi_field(m)
         if self.anis:
             mu = (m * self.u).sum(0)
             Ba = (2.0 * self.K1 * self.inv_ms * mu)[None] * self.u

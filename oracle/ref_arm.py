@@ -6,7 +6,8 @@ the host (oracle/_ref/libclref.so, spread over host threads):
 copypadmul2 -> FFT -> kernmulRSymm3D -> inverse FFT -> copyunpad
 (mag/demag convolution, opencl/conv_*.go), adddmi, adduniaxialanisotropy2,
 regionaddv, lltorque2, madd2..madd7 and normalize2.  The reference runs its
-FFTs with clFFT on the OpenCL device; here scipy.fft's multi-threaded
+FFTs with the vendored VkFFT library on the OpenCL device
+(cl/fft_interface.h, opencl/fft3dr2c.go); here scipy.fft's multi-threaded
 pocketfft stands in for it.  The stepper restates engine/rk45dp.go:12-98 and
 the integral controller of engine/stepcontroller.go:35-97 (the same
 restatement as oracle/orc_sim.inc, in numpy).

@@ -14,13 +14,15 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
+from oracle import build_ref  # noqa: E402
 from umagnus_b200 import fileio  # noqa: E402
-
-REF = os.environ.get("UMAG_REFERENCE", "/root/reference")
 
 
 def main():
-    arr, _ = fileio.read(os.path.join(REF, "test", "testdata", "randommag4x4x1.ovf"))
+    ref = build_ref.reference_root()
+    if ref is None:
+        raise SystemExit("reference checkout not found: set UMAG_REFERENCE to its root")
+    arr, _ = fileio.read(os.path.join(ref, "test", "testdata", "randommag4x4x1.ovf"))
     np.save(os.path.join(HERE, "randommag4x4x1.npy"), np.asarray(arr, np.float32))
 
 

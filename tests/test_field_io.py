@@ -8,11 +8,12 @@ import os
 import numpy as np
 import pytest
 
+from oracle import build_ref
 from umagnus_b200 import fileio
 
-REF = os.environ.get("UMAG_REFERENCE", "/root/reference")
-DATA = os.path.join(REF, "test", "testdata")
-needs_ref = pytest.mark.skipif(not os.path.isdir(DATA), reason="reference test data not present")
+REF = build_ref.reference_root()
+DATA = os.path.join(REF, "test", "testdata") if REF else ""
+needs_ref = pytest.mark.skipif(not (REF and os.path.isdir(DATA)), reason="reference test data not present")
 
 
 @needs_ref

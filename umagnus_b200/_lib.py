@@ -105,6 +105,7 @@ _SIGS = {
     "umag_demag_get_spectrum": [P, P], "umag_demag_get_kernel": [P, P],
     "umag_demag_padded_size": [P, ctypes.POINTER(c_int)], "umag_demag_free": [P],
     "umag_demag_exec_noalloc": [c_int, c_int, c_int, P, P, P, P, P, P, P, P, P, c_float, P],
+    "umag_debug_plant_fault": [P, ctypes.c_uint],
     "umag_solver_defaults": [ctypes.POINTER(SolverParams)],
     "umag_sim_new": [ctypes.POINTER(SimParams), ctypes.POINTER(SolverParams), ctypes.POINTER(c_void_p)],
     "umag_sim_free": [P], "umag_sim_set_m": [P, P, P, P], "umag_sim_restore_m": [P, P, P, P], "umag_sim_get_m": [P, P, P, P],

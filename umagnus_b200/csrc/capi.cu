@@ -15,6 +15,12 @@ int umag_release(void) { return release_device(); }
 const char* umag_last_error(void) { return last_error(); }
 const char* umag_version(void) { return "umagnus_b200 1.0 (sm_100a)"; }
 
+int umag_debug_plant_fault(umag_sim* sim, unsigned code) {
+    UMAG_TRY(ensure_init());
+    if (sim == nullptr) return demag_set_slab_timeouts(code);
+    return sim_plant_status(sim, (int)code);
+}
+
 int umag_set_stream(void* s) {
     UMAG_TRY(ensure_init());
     ctx().stream = s ? (cudaStream_t)s : ctx().own_stream;

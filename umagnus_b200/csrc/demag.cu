@@ -847,7 +847,18 @@ int demag_exec(umag_demag* d, float* Bx, float* By, float* Bz, const float* mx, 
     a.B[0] = Bx; a.B[1] = By; a.B[2] = Bz;
     a.vol = vol; a.Ms = Ms; a.Ms_mul = Ms_mul;
     if (pass >= 0) return demag_launch_pass(d, a, ctx().stream, pass);
-    return demag_launch(d, a, ctx().stream);
+    UMAG_TRY(demag_launch(d, a, ctx().stream));
+    // Exec completes before it returns, as the reference's does; a bulk copy
+    // that timed out (a field left unwritten) is an error here, not a silent
+    // wrong result.  Skipped while the stream is being captured.
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    UMAG_CUDA(cudaStreamIsCapturing(ctx().stream, &cs));
+    if (cs == cudaStreamCaptureStatusNone) {
+        unsigned n = 0;
+        UMAG_TRY(demag_slab_timeouts(&n, ctx().stream));
+        if (n != 0) return set_error(UMAG_E_TIMEOUT, "demag pass C: %u spectrum-slab copies timed out", n);
+    }
+    return UMAG_OK;
 }
 
 void demag_free(umag_demag* d) {

@@ -101,6 +101,11 @@ struct PassArgs {
     // (8 floats, y, kx/4, kz, component): pass C loads the slab of one
     // (y, component) with one bulk tensor copy; NULL: plain loads
     const CUtensorMap* slab_map;
+    // engine use: the controller's status word (instance ib at fault +
+    // ib * ctl_stride bytes), set to 7 when a pass gives up waiting for a
+    // bulk copy; NULL for the plain device-op API, which counts such
+    // timeouts in g_slab_timeouts instead
+    int* fault;
 };
 
 int demag_new_newell(int Nx, int Ny, int Nz, const int pbc[3], double cx, double cy, double cz, int arad,
@@ -119,8 +124,17 @@ void fill_pass_args(const umag_demag* d, PassArgs& a);
 int demag_launch(const umag_demag* d, const PassArgs& a, cudaStream_t st);
 int demag_launch_batch(const umag_demag* d, const PassArgs& a, int nb, cudaStream_t st);
 bool demag_fast_select(int M, int Py, int Pz, FastPasses& f);
-// pass-B launch grid for a selected plan (after demag_fast_setup; current device)
-int demag_fast_grid(FastPasses& f, int M, int Pz);
+// pass-B launch grid for a selected plan (after demag_fast_setup; current
+// device); sm_count <= 0: the library context's SM count
+int demag_fast_grid(FastPasses& f, int M, int Pz, int sm_count = 0);
+// opt-in shared memory of the compile-time-planned passes, once per device
+// (the attributes are per device context); thread-safe
 int demag_fast_setup();
+// no-alloc entry point: load its module on the current device (umag_init)
+int noalloc_preload();
+// bulk-copy waits that gave up in pass C since the counter was last cleared
+// (demag_fast.cu); demag_exec reports them as an error
+int demag_slab_timeouts(unsigned* out, cudaStream_t st);
+int demag_set_slab_timeouts(unsigned v);
 
 }  // namespace umag

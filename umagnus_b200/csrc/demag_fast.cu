@@ -5,6 +5,8 @@
 // every FFT index computation is a constant, register arrays are unrolled,
 // twiddles are staged in shared memory.  demag_fast_select() returns the
 // instantiation for a plan, or nothing (the generic kernels then run).
+#include <mutex>
+
 #include "demag.cuh"
 #include "fft_pair.cuh"
 #include "fft_reg.cuh"
@@ -13,8 +15,29 @@
 
 namespace umag {
 
-// pass C slab loads that gave up waiting (bounded mbarrier poll)
+// pass C slab loads that gave up waiting (bounded mbarrier poll); the plain
+// device-op API reads it after each demag_exec (engine launches report the
+// timeout through the controller status instead, PassArgs::fault)
 __device__ unsigned g_slab_timeouts = 0;
+
+int demag_slab_timeouts(unsigned* out, cudaStream_t st) {
+    UMAG_CUDA(cudaMemcpyFromSymbolAsync(out, g_slab_timeouts, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, st));
+    UMAG_CUDA(cudaStreamSynchronize(st));
+    return UMAG_OK;
+}
+int demag_set_slab_timeouts(unsigned v) {
+    UMAG_CUDA(cudaMemcpyToSymbol(g_slab_timeouts, &v, sizeof(unsigned)));
+    UMAG_CUDA(cudaDeviceSynchronize());
+    return UMAG_OK;
+}
+
+// record a pass that gave up waiting for a bulk copy: the counter, and the
+// instance's controller status (7, as the torque kernel's tile wait) when
+// the launch belongs to a simulation
+__device__ __forceinline__ void pass_timeout(const PassArgs& a, int ib) {
+    atomicAdd(&g_slab_timeouts, 1u);
+    if (a.fault) atomicCAS(reinterpret_cast<int*>(reinterpret_cast<char*>(a.fault) + (long)ib * a.ctl_stride), 0, 7);
+}
 
 
 static constexpr double kMu0f = 4 * 3.1415926535897932384626433 * 1e-7;  // clh/constants.clh:5
@@ -656,7 +679,7 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
             tma_load_5d(sl, a.slab_map, 0, y, 0, 0, c, &slab_bar);
         }
         for (int it = 0; !mbar_try_wait(&slab_bar, 0); it++) {
-            if (it == kTileWaitLimit && tid == 0) atomicAdd(&g_slab_timeouts, 1u);
+            if (it == kTileWaitLimit && tid == 0) pass_timeout(a, ib);
             if (it >= 2 * kTileWaitLimit) return;
         }
     }
@@ -875,7 +898,8 @@ bool demag_fast_select(int M, int Py, int Pz, FastPasses& f) {
     return ac && b;
 }
 
-int demag_fast_grid(FastPasses& f, int M, int Pz) {
+int demag_fast_grid(FastPasses& f, int M, int Pz, int sm_count) {
+    if (sm_count <= 0) sm_count = ctx().sm_count;
     f.gbx = (unsigned)((M + 1 + f.wb - 1) / f.wb);
     f.gby = (unsigned)Pz;
     // a default pass-B grid smaller than the SM count runs on a few SMs: such
@@ -885,14 +909,29 @@ int demag_fast_grid(FastPasses& f, int M, int Pz) {
     // spell out their rounding (fft.cuh)
     if (f.b_n) {
         f.gbx_n = (unsigned)((M + 1 + f.wb_n - 1) / f.wb_n);
-        f.use_narrow = (long)f.gbx * f.gby < ctx().sm_count;
+        f.use_narrow = (long)f.gbx * f.gby < sm_count;
     }
     return UMAG_OK;
 }
 
+static int demag_fast_setup_device();
+
 int demag_fast_setup() {
-    static bool done = false;
-    if (done) return UMAG_OK;
+    // cudaFuncSetAttribute applies to the current device's context, so the
+    // opt-in is made once per device, under a lock (host threads may race)
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    UMAG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(UMAG_E_ARG, "device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return UMAG_OK;
+    UMAG_TRY(demag_fast_setup_device());
+    done[dev] = true;
+    return UMAG_OK;
+}
+
+static int demag_fast_setup_device() {
     // opt in to the full 227 KB and ask for the largest shared-memory carveout,
     // so several CTAs of these shared-memory-heavy kernels fit on one SM
     auto attrs = [](void (*k)(PassArgs)) -> int {
@@ -933,7 +972,6 @@ int demag_fast_setup() {
         SETB(32) SETB(48) SETB(64) SETB(96) SETB(128) SETB(192) SETB(256) SETB(384) SETB(512) SETB(1024) SETB(2048)
 #undef SETB
     }
-    done = true;
     return UMAG_OK;
 }
 

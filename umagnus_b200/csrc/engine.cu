@@ -1126,6 +1126,7 @@ int sim_new(const umag_sim_params* p, const umag_solver_params* sp, umag_sim** o
         s->pa.m_ind = &s->ctl->m;
         s->pa.m_ind_w = &s->ctl->mw;
         s->pa.active = &s->ctl->active;
+        s->pa.fault = &s->ctl->status;
         s->pa.vol = p->vol;
         s->pa.Ms = p->Ms;
         s->pa.Ms_mul = p->Ms_mul;
@@ -1281,6 +1282,18 @@ int sim_run(umag_sim* h, double seconds, int chunk, long long max_steps) {
                                                    s->hctl->t);
         if (!(s->hctl->t < stop)) break;
     }
+    return UMAG_OK;
+}
+
+// test hook: the device-side status word set as a kernel whose bounded wait
+// gave up would set it (the host-side checks then see it)
+int sim_plant_status(umag_sim* h, int code) {
+    SimImpl* s = reinterpret_cast<SimImpl*>(h);
+    UMAG_REQUIRE(s, "NULL simulation");
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    UMAG_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(s->ctl) + offsetof(DevCtl, status), &code, sizeof(int),
+                              cudaMemcpyHostToDevice, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
     return UMAG_OK;
 }
 
@@ -1820,6 +1833,7 @@ static int ens_class_new(EnsClass& C, const umag_ens_instance* in, const std::ve
         s->pa.m_ind = &s->ctl[0].m;
         s->pa.m_ind_w = &s->ctl[0].mw;
         s->pa.active = &s->ctl[0].active;
+        s->pa.fault = &s->ctl[0].status;
         s->pa.ctl_stride = sizeof(DevCtl);
         s->pa.vol = nullptr;
         s->pa.Ms = nullptr;

@@ -12,6 +12,7 @@ int sim_torque(umag_sim* s, float* tx, float* ty, float* tz, float* bx, float* b
 int sim_steps(umag_sim* s, int n);
 int sim_run(umag_sim* s, double seconds, int chunk, long long max_steps);
 int sim_get_state(umag_sim* s, umag_solver_state* st);
+int sim_plant_status(umag_sim* s, int code);
 int sim_set_time(umag_sim* s, double t, double dt);
 int sim_average_m(umag_sim* s, double avg[3]);
 int sim_use_graph(umag_sim* s, int enable, int steps);

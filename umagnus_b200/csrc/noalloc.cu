@@ -10,6 +10,14 @@
 // exits.  The caller passes the kernel spectrum, m, the output B and a
 // stream; nothing is allocated or freed, neither by this file nor by any
 // library routine it calls.
+//
+// With lazy module loading (the CUDA default since 12.2) the driver reserves
+// the array when this file's module is first loaded on a device, i.e. on the
+// first look-up of its address.  umag_init does that look-up for its device
+// (noalloc_preload), so a caller that initialises the library before an
+// external pool claims the device's memory never sees that reservation fail
+// later; a caller that skips umag_init gets it on its first no-alloc call.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -26,22 +34,30 @@ constexpr size_t kNoallocScratchBytes = (size_t)16 << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
 // Device address of g_noalloc_scratch, looked up once per device (the host
-// symbol is only a stand-in and must never be handed to a kernel).
-static void* g_noalloc_ptr[64] = {};
+// symbol is only a stand-in and must never be handed to a kernel).  Atomic:
+// two host threads may look it up at once (both store the same address).
+static std::atomic<void*> g_noalloc_ptr[64];
 
 static int noalloc_scratch(void** out) {
     int dev = 0;
     UMAG_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return set_error(UMAG_E_ARG, "device %d out of range", dev);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
+    void* p = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+    if (!p) {
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess)
             return set_error(UMAG_E_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
-        g_noalloc_ptr[dev] = p;
+        g_noalloc_ptr[dev].store(p, std::memory_order_release);
     }
-    *out = g_noalloc_ptr[dev];
+    *out = p;
     return UMAG_OK;
+}
+
+// Loads this module on the current device (reserving the scratch array) and
+// caches the array's address; called by umag_init.
+int noalloc_preload() {
+    void* p = nullptr;
+    return noalloc_scratch(&p);
 }
 
 // twiddles exp(-2 pi i j / L) of the four tables, evaluated in FP64 on the device
@@ -87,7 +103,10 @@ extern "C" __attribute__((visibility("default"))) int umag_demag_exec_noalloc(
     UMAG_TRY(demag_fast_setup());
     if (!demag_fast_select(d.M, d.P[1], d.P[2], d.fast))
         return set_error(UMAG_E_UNSUPPORTED, "mesh %dx%dx%d has no compile-time FFT plan (no-alloc path)", Nx, Ny, Nz);
-    UMAG_TRY(demag_fast_grid(d.fast, d.M, d.P[2]));
+    int dev = 0, sms = 0;
+    UMAG_CUDA(cudaGetDevice(&dev));
+    UMAG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    UMAG_TRY(demag_fast_grid(d.fast, d.M, d.P[2], sms));
     d.use_fast = true;
     d.WB = d.fast.wb;
     // scratch layout: spectrum | tw(M) | tw(Py) | tw(Pz) | exp(-2 pi i k/Px), k < M

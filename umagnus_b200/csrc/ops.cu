@@ -53,6 +53,9 @@ int init_device(int device) {
     g_ctx.red_bytes = sizeof(double) * 4 * kRedBlocks + 64;
     UMAG_CUDA(cudaMalloc(&g_ctx.red_dev, g_ctx.red_bytes));
     UMAG_CUDA(cudaMallocHost(&g_ctx.red_host, sizeof(double) * 8));
+    // load the no-alloc entry point's module now, so that its fixed scratch
+    // array is reserved before a caller's pool claims the device
+    UMAG_TRY(noalloc_preload());
     g_ctx.device = device;
     g_ctx.initialised = true;
     return UMAG_OK;

@@ -348,20 +348,47 @@ __device__ __forceinline__ long kern_idx(const PassArgs& a, int kz, int ky, int 
                       : ((long)kz * hy + ky) * a.Kp + kx;
 }
 
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Shared memory of a pass-B CTA (k_reg_b): twiddles, two exchange buffers of
+// WB padded lines, the kernel block [6][WB/KW][HY][KW] (KW = 4 columns per
+// 16-byte piece, or WB when narrower).
+template <int PY, int WB> struct RegBShape {
+    static constexpr int KW = WB >= 4 ? 4 : WB;
+    static constexpr size_t smem = sizeof(float2) * ((size_t)PY + (size_t)2 * WB * rg_line<PY>()) +
+                                   sizeof(float) * (size_t)6 * (PY / 2 + 1) * WB;
+    // three CTAs per SM (80 registers) up to Py = 512; longer lines hold more
+    // live state per thread and keep two
+    static constexpr int minb = PY <= 512 && 3 * (smem + 1024) <= 227 * 1024 ? 3 : 2;
+};
+
 // Pass B with the register-blocked FFT (power-of-two Py): thread (t, w) holds
 // rows t + T*m (m < 8) of column kx0 + w for all three components.  Rows
 // y >= Ny are zero padding (m >= 4): the loads are skipped and the first
-// butterflies fold; only rows y < Ny are computed by the inverse and stored.
-// With the blocked layouts a warp's loads and stores of one component are one
-// contiguous run (WB = 4: 8 rows x 4 columns = 256 bytes).
+// radix-8 butterfly folds them (dft8_zhalf); only rows y < Ny are computed by
+// the inverse and stored.  With the blocked layouts a warp's loads and stores
+// of one component are one contiguous run (WB = 4: 8 rows x 4 columns = 256
+// bytes).  The components exchange one at a time through two buffers
+// (rg_fft_fwd_seq), which with the kernel block fits three CTAs per SM; the
+// kernel block arrives by bulk copies (6 contiguous runs per 4 columns,
+// issued by one thread, completing on an mbarrier while the forward
+// transform runs), or by 16-byte cp.async pieces where the block is not
+// whole 4-column runs (narrow CTAs, the packed Nyquist column).
 template <int PY, int WB>
 __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, const int by, const int ib) {
     constexpr int T = PY / 8, NT = T * WB, NY = PY / 2, HY = PY / 2 + 1;
     constexpr int LP = rg_line<PY>();
+    constexpr int KW = RegBShape<PY, WB>::KW;
     extern __shared__ __align__(16) float2 sm[];
     float2* tw = sm;                  // PY twiddles
-    float2* ex = tw + PY;             // [3][WB][LP] exchange lines
-    float* Ks = reinterpret_cast<float*>(ex + 3 * WB * LP);  // [6][HY][WB] kernel block
+    float2* ex = tw + PY;             // [2][WB][LP] exchange lines
+    float* Ks = reinterpret_cast<float*>(ex + 2 * WB * LP);  // [6][WB/KW][HY][KW] kernel block
+    __shared__ __align__(8) uint64_t kbar;
     if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
     const int w = tid % WB, t = tid / WB;
@@ -375,40 +402,52 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     for (int i = tid; i < PY; i += NT) tw[i] = a.fy.tw[i];
     const int kx0 = bx * WB;
     const int kx = nyq ? hx - 1 : kx0 + w, kz = nyq ? by * WB + w : by;
-    // the kernel block this CTA multiplies with: asynchronous copies that
-    // complete while the forward transform runs
     auto kz_mirror = [&](int z) { return z > Pz / 2 ? Pz - z : z; };
     const int kzm = kz_mirror(kz);
     const float sz = kz > Pz / 2 ? -1.f : 1.f;
     const bool k3d = a.K[3] != nullptr;
-    {
-        const int ncomp = k3d ? 6 : 4;
+    const int ncomp = k3d ? 6 : 4;
+    auto kcomp = [&](int cc) { return k3d ? cc : (cc == 3 ? 5 : cc); };  // 2D stores xx yy zz xy
+    // the kernel block: whole 4-column runs of the blocked kernel layout by
+    // bulk copies, else 16- or 4-byte asynchronous copies
+    bool bulk = false;
+    if constexpr (WB % 4 == 0) bulk = !nyq && a.Kblocked && kx0 + WB <= a.Kp;
+    if (bulk) {
+        if (tid == 0) {
+            mbar_init(&kbar, 1);
+            mbar_expect_tx(&kbar, (uint32_t)(sizeof(float) * ncomp * HY * WB));
+            for (int cc = 0; cc < ncomp; cc++)
+                for (int b4 = 0; b4 < WB / 4; b4++)
+                    bulk_g2s(Ks + kcomp(cc) * HY * WB + b4 * HY * 4, a.K[kcomp(cc)] + kern_idx(a, kzm, 0, kx0 + 4 * b4, HY),
+                             (uint32_t)(sizeof(float) * HY * 4), &kbar);
+        }
+    } else {
         bool wide = false;
         if constexpr (WB % 4 == 0) {
-            // 16-byte pieces of 4 columns: plan layouts (pitch padded to 4
-            // floats, pad columns zero); blocked pieces are consecutive in ky
+            // 16-byte pieces of 4 columns (plan layouts: pitch padded to 4
+            // floats, pad columns zero)
             wide = !nyq && a.Kp % 4 == 0 && kx0 + WB <= a.Kp;
             if (wide) {
                 constexpr int CH = WB / 4;
                 for (int e = tid; e < ncomp * HY * CH; e += NT) {
                     const int cc = e / (HY * CH), r = e % (HY * CH), ky = r / CH, ch = r % CH;
-                    const int comp = k3d ? cc : (cc == 3 ? 5 : cc);  // 2D stores xx yy zz xy
-                    cpa16(Ks + comp * HY * WB + ky * WB + 4 * ch, a.K[comp] + kern_idx(a, kzm, ky, kx0 + 4 * ch, HY));
+                    cpa16(Ks + kcomp(cc) * HY * WB + ch * HY * 4 + ky * 4, a.K[kcomp(cc)] + kern_idx(a, kzm, ky, kx0 + 4 * ch, HY));
                 }
             }
         }
         if (!wide) {
             for (int e = tid; e < ncomp * HY * WB; e += NT) {
                 const int cc = e / (HY * WB), r = e % (HY * WB), ky = r / WB, ww = r % WB;
-                const int comp = k3d ? cc : (cc == 3 ? 5 : cc);
-                float* dst = Ks + comp * HY * WB + ky * WB + ww;
+                float* dst = Ks + kcomp(cc) * HY * WB + (ww / KW) * HY * KW + ky * KW + ww % KW;
                 const int kxw = nyq ? hx - 1 : kx0 + ww, kzw = nyq ? kz_mirror(by * WB + ww) : kzm;
-                if (kxw < hx) cpa4(dst, a.K[comp] + kern_idx(a, kzw, ky, kxw, HY));
+                if (kxw < hx) cpa4(dst, a.K[kcomp(cc)] + kern_idx(a, kzw, ky, kxw, HY));
                 else *dst = 0.f;
             }
         }
         cpa_commit();
     }
+    if (!k3d)  // 2D: no yz / xz components; zeros keep the multiply branch-free
+        for (int e = tid; e < 2 * HY * WB; e += NT) Ks[3 * HY * WB + e] = 0.f;
     const bool col = kx < hx;
     const long cs = (long)Pz * NY * a.Lx, rs = spec_rowstride(a);
     const float2* in = inst_spec(a, ib) + (long)kz * NY * a.Lx + spec_col(a, kx);
@@ -420,27 +459,32 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
             const int y = t + T * m;
             v[c][m] = (m < 4 && col) ? in[c * cs + y * rs] : make_float2(0.f, 0.f);
         }
-    __syncthreads();  // twiddles
+    __syncthreads();  // twiddles, barrier initialised
     float2* exl = ex + w * LP;
     const int exs = WB * LP;
-    rg_fft_fwd<PY, 3>(v, t, exl, exs, tw);
-    cpa_wait_all();
+    rg_fft_fwd_seq<PY, 3, true>(v, t, exl, exs, tw);
+    if (bulk) {
+        for (int it = 0; !mbar_try_wait(&kbar, 0); it++) {
+            if (it == kTileWaitLimit && tid == 0) pass_timeout(a, ib);
+            if (it >= 2 * kTileWaitLimit) return;
+        }
+    } else {
+        cpa_wait_all();
+    }
     __syncthreads();
     // kernel multiply (kernmulrsymm3d.cl:41-90), mirrored into the stored block
+    const float* kcol = Ks + (w / KW) * HY * KW + w % KW;
 #pragma unroll
     for (int m = 0; m < 8; m++) {
         const int ky = t + T * m;
         int kym = ky;
         float sy = 1.f;
         if (ky > NY) { kym = PY - ky; sy = -1.f; }
-        const float* kr = Ks + kym * WB + w;
+        const float* kr = kcol + kym * KW;
         const float Kxx = kr[0], Kyy = kr[HY * WB], Kzz = kr[2 * HY * WB];
         const float Kxy = kr[5 * HY * WB] * sy;
-        float Kyz = 0.f, Kxz = 0.f;
-        if (k3d) {
-            Kyz = kr[3 * HY * WB] * (sy * sz);
-            Kxz = kr[4 * HY * WB] * sz;
-        }
+        const float Kyz = kr[3 * HY * WB] * (sy * sz);
+        const float Kxz = kr[4 * HY * WB] * sz;
         const float2 mx = v[0][m], my = v[1][m], mz = v[2][m];
         // conjugated products: the inverse is conj(FFT(conj(.))); explicit
         // multiply-adds (fft.cuh: the same bits in every instantiation)
@@ -451,7 +495,9 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
         v[1][m] = make_float2(dot(mx.x, Kxy, my.x, Kyy, mz.x, Kyz), -dot(mx.y, Kxy, my.y, Kyy, mz.y, Kyz));
         v[2][m] = make_float2(dot(mx.x, Kxz, my.x, Kyz, mz.x, Kzz), -dot(mx.y, Kxz, my.y, Kyz, mz.y, Kzz));
     }
-    rg_fft_fwd<PY, 3>(v, t, exl, exs, tw);
+    // (the barrier before the multiply separates the forward transform's last
+    // reads of the exchange buffers from the inverse's first writes)
+    rg_fft_fwd_seq<PY, 3, false>(v, t, exl, exs, tw);
     if (col) {
         float2* out = inst_spec(a, ib) + (long)kz * NY * a.Lx + spec_col(a, kx);
 #pragma unroll
@@ -464,10 +510,12 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     }
 }
 template <int PY, int WB>
-__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b(PassArgs a) { k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y, 0); }
+__global__ void __launch_bounds__((PY / 8) * WB, RegBShape<PY, WB>::minb) k_reg_b(PassArgs a) {
+    k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y, 0);
+}
 // batched: blockIdx.y = index + per * instance (the inst_* views above)
 template <int PY, int WB>
-__global__ void __launch_bounds__((PY / 8) * WB, 2) k_reg_b_bat(PassArgs a) {
+__global__ void __launch_bounds__((PY / 8) * WB, RegBShape<PY, WB>::minb) k_reg_b_bat(PassArgs a) {
     const int per = a.Pz, b = blockIdx.y / per;
     k_reg_b_body<PY, WB>(a, blockIdx.x, blockIdx.y - b * per, b);
 }
@@ -815,8 +863,7 @@ template <int PY> struct RegB {
     static constexpr int T = PY / 8;
     static constexpr int WB = T >= 256 ? 1 : 256 / T > 16 ? 16 : 256 / T;
     static constexpr int NT = T * WB;
-    static constexpr size_t smem = sizeof(float2) * ((size_t)PY + (size_t)3 * WB * rg_line<PY>()) +
-                                   sizeof(float) * (size_t)6 * (PY / 2 + 1) * WB;
+    static constexpr size_t smem = RegBShape<PY, WB>::smem;
 };
 
 // one warp per CTA (or one column): for small meshes, where the default
@@ -825,8 +872,7 @@ template <int PY> struct RegBNarrow {
     static constexpr int T = PY / 8;
     static constexpr int WB = T >= 32 ? 1 : 32 / T;
     static constexpr int NT = T * WB;
-    static constexpr size_t smem = sizeof(float2) * ((size_t)PY + (size_t)3 * WB * rg_line<PY>()) +
-                                   sizeof(float) * (size_t)6 * (PY / 2 + 1) * WB;
+    static constexpr size_t smem = RegBShape<PY, WB>::smem;
 };
 
 // ------------------------------------------------------------------ dispatch

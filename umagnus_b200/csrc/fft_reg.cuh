@@ -117,6 +117,95 @@ __device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, 
     }
 }
 
+// dft8 (forward) of (u0, u1, u2, u3, 0, 0, 0, 0), natural order out: the
+// even outputs are the DFT4 of u, the odd ones the DFT4 of u_n W8^n -- 40
+// instructions instead of the 56 of dft8 (x + 0 is not folded by the
+// compiler: it is not an identity for x = -0).
+__device__ __forceinline__ void dft8_zhalf(float2* v) {
+    const float s = 0.70710678118654752440084436210485f;
+    const float2 a = v[0], b = v[1], c = v[2], d = v[3];
+    const float2 t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = mul_mi(csub(b, d), -1);
+    float2 w1, w3;
+    w1.x = s; w1.y = -s;   // W8
+    w3.x = -s; w3.y = -s;  // W8^3
+    const float2 b1 = cmul(b, w1), c1 = mul_mi(c, -1), d1 = cmul(d, w3);
+    const float2 s0 = cadd(a, c1), s1 = csub(a, c1), s2 = cadd(b1, d1), s3 = mul_mi(csub(b1, d1), -1);
+    v[0] = cadd(t0, t2); v[2] = cadd(t1, t3); v[4] = csub(t0, t2); v[6] = csub(t1, t3);
+    v[1] = cadd(s0, s2); v[3] = cadd(s1, s3); v[5] = csub(s0, s2); v[7] = csub(s1, s3);
+}
+
+// Like rg_stage, for NC lines that exchange one at a time through two
+// alternating buffers (ex and ex + exs; P = the buffer of the first line):
+// a line is written, the CTA synchronises once and reads it back, so a
+// buffer is rewritten only after a barrier that follows every read of it.
+// Two buffers instead of NC, and one barrier per line and stage.  ZH: the
+// upper half of the input is zero (the first radix-8 butterfly folds it).
+template <int L, int NC, int ST, int NS, int P, bool ZH>
+__device__ __forceinline__ void rg_stage_seq(float2 (&v)[NC][8], int t, float2* ex, int exs,
+                                             const float2* __restrict__ tw) {
+    constexpr int PS = 3;
+    if constexpr (ST < rg_nst(L)) {
+        constexpr int R = rg_radix(L, ST);
+        constexpr int NB = 8 / R;
+        constexpr int T = L / 8;
+        constexpr int TWS = L / (NS * R);
+        constexpr bool last = (ST + 1 == rg_nst(L));
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            const int k = (t + T * i) % NS;
+            float2 w[R];
+            if constexpr (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) w[r] = rg_tw<-1>(tw, r * k * TWS);
+            }
+#pragma unroll
+            for (int c = 0; c < NC; c++) {
+                float2 u[R];
+#pragma unroll
+                for (int r = 0; r < R; r++) u[r] = v[c][i + r * NB];
+                if constexpr (NS > 1) {
+#pragma unroll
+                    for (int r = 1; r < R; r++) u[r] = cmul(u[r], w[r]);
+                }
+                if constexpr (R == 8 && ZH && ST == 0) dft8_zhalf(u);
+                else if constexpr (R == 2) dft2(u);
+                else if constexpr (R == 4) dft4(u, -1);
+                else dft8<float>(u, -1);
+#pragma unroll
+                for (int q = 0; q < R; q++) v[c][i + q * NB] = u[q];
+            }
+        }
+        if constexpr (!last) {
+#pragma unroll
+            for (int c = 0; c < NC; c++) {
+                float2* b = ex + ((P + c) & 1) * exs;
+#pragma unroll
+                for (int i = 0; i < NB; i++) {
+                    const int j = t + T * i;
+                    const int o = (j / NS) * NS * R + j % NS;
+#pragma unroll
+                    for (int q = 0; q < R; q++) b[rg_pad<PS>(o + q * NS)] = v[c][i + q * NB];
+                }
+                __syncthreads();
+#pragma unroll
+                for (int m = 0; m < 8; m++) v[c][m] = b[rg_pad<PS>(t + T * m)];
+            }
+            rg_stage_seq<L, NC, ST + 1, NS * R, (P + NC) & 1, ZH>(v, t, ex, exs, tw);
+        }
+    }
+}
+
+// Forward FFT of NC lines held by the whole CTA, exchanged one line at a
+// time through two buffers (rg_stage_seq); ZH: zero upper half of the input.
+// The caller must separate it by a barrier from any earlier use of the
+// buffers.
+template <int L, int NC, bool ZH>
+__device__ __forceinline__ void rg_fft_fwd_seq(float2 (&v)[NC][8], int t, float2* ex, int exs,
+                                               const float2* __restrict__ tw) {
+    static_assert(rg_ok(L), "register FFT needs a power-of-two length >= 8");
+    rg_stage_seq<L, NC, 0, 1, 0, ZH>(v, t, ex, exs, tw);
+}
+
 // Unnormalised forward FFT (DIR = -1) of NC lines.  All threads that share
 // the exchange lines must call it: the whole CTA, or (WARP = true) one warp.
 template <int L, int NC, bool WARP = false, int PS = 3>

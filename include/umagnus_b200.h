@@ -434,6 +434,8 @@ typedef struct {
     double target[3];
     int no_graph;           /* 1: plain stream launches instead of CUDA graphs */
     int solver;             /* 4 (or 0) RK4, 2 Heun (engine/heun.go with FixDt) */
+    float Dind;             /* uniform interfacial DMI (J/m^2; 0 = exchange only): dmi.cl's
+                               exchange + DMI stencil, a fixed (not differentiated) parameter */
 } umag_adj_params;
 typedef struct umag_adj umag_adj;
 int umag_adj_new(const umag_adj_params* p, umag_adj** out);

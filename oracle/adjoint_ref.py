@@ -7,7 +7,9 @@ the GPU adjoint (umag_adj_*); the product never does.
 The model is the engine's effective field and LL torque for uniform region
 0 (engine/effectivefield.go:14-24, engine/demag.go, engine/exchange.go,
 engine/anisotropy.go, engine/zeeman.go, engine/torque.go:135-144) with a
-per-cell Ms map, stepped by fixed-step RK4 (engine/rk4.go:35-61, every stage
+per-cell Ms map, exchange or (Dind != 0) exchange + interfacial DMI
+(kernels_src/cl/dmi.cl:8-148 with its Neumann extrapolation of missing
+in-plane neighbours, uniform A and D), stepped by fixed-step RK4 (engine/rk4.go:35-61, every stage
 normalised, opencl normalize2.cl) or Heun (engine/heun.go:27-43: the
 predictor m + h k0 is not normalised, the result is).  The reference has no gradients; this
 module gives the FP64 gradient two ways: a hand-written reverse pass (the
@@ -24,77 +26,255 @@ MU0 = 4 * np.pi * 1e-7  # kernels_src/clh/constants.clh:5
 GAMMA_LL = 1.7595e11    # engine/torque.go:27
 
 
+class _Numpy:
+    """Array operations of the restatement in numpy (FP64, host)."""
+
+    def asarray(self, x):
+        return np.asarray(x, np.float64)
+
+    def zeros(self, shape):
+        return np.zeros(shape)
+
+    def zeros_like(self, x):
+        return np.zeros_like(x)
+
+    def cross(self, a, b):
+        return np.cross(a, b, axis=0)
+
+    def rfftn(self, x):
+        return np.fft.rfftn(x, axes=(1, 2, 3))
+
+    def irfftn(self, x, s):
+        return np.fft.irfftn(x, s=s, axes=(1, 2, 3))
+
+    def stack(self, xs):
+        return np.stack(xs)
+
+    def take(self, v, idx, axis):
+        return np.take(v, idx, axis=axis)
+
+    def index(self, idx):
+        return idx
+
+    def col(self, u):  # a 3-vector as a (3, 1, 1, 1) field
+        return np.asarray(u, np.float64)[:, None, None, None]
+
+    def scalar(self, x):
+        return float(x)
+
+    def host(self, x):
+        return x
+
+    def sqrt(self, x):
+        return np.sqrt(x)
+
+    def numel(self, x):
+        return x.size
+
+
+class _Torch:
+    """The same operations in torch float64 on a device (CUDA for the
+    benchmark's FP64 gradient check: thousands of steps in seconds)."""
+
+    def __init__(self, device):
+        import torch
+        self.t = torch
+        self.dev = torch.device(device)
+
+    def asarray(self, x):
+        return self.t.as_tensor(np.asarray(x, np.float64) if not isinstance(x, self.t.Tensor) else x,
+                                dtype=self.t.float64, device=self.dev)
+
+    def zeros(self, shape):
+        return self.t.zeros(shape, dtype=self.t.float64, device=self.dev)
+
+    def zeros_like(self, x):
+        return self.t.zeros_like(x)
+
+    def cross(self, a, b):
+        return self.t.linalg.cross(a, b, dim=0)
+
+    def rfftn(self, x):
+        return self.t.fft.rfftn(x, dim=(1, 2, 3))
+
+    def irfftn(self, x, s):
+        return self.t.fft.irfftn(x, s=tuple(s), dim=(1, 2, 3))
+
+    def stack(self, xs):
+        return self.t.stack(xs)
+
+    def take(self, v, idx, axis):
+        return self.t.index_select(v, axis, idx)
+
+    def index(self, idx):
+        return self.t.as_tensor(idx, device=self.dev)
+
+    def col(self, u):
+        return self.asarray(u).reshape(3, 1, 1, 1)
+
+    def scalar(self, x):
+        return float(x)
+
+    def host(self, x):
+        return x.cpu().numpy() if isinstance(x, self.t.Tensor) else x
+
+    def sqrt(self, x):
+        return self.t.sqrt(x)
+
+    def numel(self, x):
+        return x.numel()
+
+
 class Problem:
     """Static part of the problem: mesh, demag kernel, stepper, loss."""
 
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, probe, avg_from, w_probe=1.0, w_target=1.0,
-                 target=(0.0, 0.0, 1.0), demag=True, gamma_ll=GAMMA_LL, solver=4):
+                 target=(0.0, 0.0, 1.0), demag=True, gamma_ll=GAMMA_LL, solver=4, backend="numpy", device="cuda",
+                 Dind=0.0):
+        """backend: "numpy" (host) or "torch" (float64 on `device`), the same
+        operations in the same order.  Dind: uniform interfacial DMI (J/m^2),
+        a fixed (not differentiated) parameter."""
         if solver not in (2, 4):
             raise ValueError("solver must be 4 (RK4) or 2 (Heun)")
+        self.xp = _Numpy() if backend == "numpy" else _Torch(device)
         self.solver = int(solver)
         self.N = tuple(int(n) for n in N)
         self.cell = tuple(float(c) for c in cell)
         self.alpha = float(alpha)
         u = np.asarray(anisU, np.float64)
-        self.u = u / np.linalg.norm(u) if np.linalg.norm(u) > 0 else u
+        u = u / np.linalg.norm(u) if np.linalg.norm(u) > 0 else u
+        self.u = u
+        self.ucol = self.xp.col(u)
         self.h = dt * gamma_ll
         self.nsteps = int(nsteps)
         self.probe = tuple(int(p) for p in probe)
         self.avg_from = int(avg_from)
         self.w_probe, self.w_target = float(w_probe), float(w_target)
-        self.target = np.asarray(target, np.float64)
+        self.target = self.xp.asarray(target)
         self.gilb = -1.0 / (1.0 + self.alpha ** 2)
         self.w = [2.0 / (c * c) for c in self.cell]
+        self.D = float(Dind)
+        if self.D != 0:
+            # in-plane neighbour masks (1 inside the mesh) along x and y
+            Nx, Ny, Nz = self.N
+            self.ins = {}
+            for ax, n in ((3, Nx), (2, Ny)):
+                for sd in (-1, 1):
+                    idx = np.arange(n) + sd
+                    shape = [1, 1, 1, 1]
+                    shape[ax] = n
+                    self.ins[(ax, sd)] = self.xp.asarray(((idx >= 0) & (idx < n)).astype(np.float64).reshape(shape))
         self.demag = demag
         if demag:
             K = oracle.newell_kernel(self.N, self.cell)  # (6, Pz, Py, Px): xx yy zz yz xz xy
             self.P = K.shape[1:]
-            self.Kf = np.fft.rfftn(K, axes=(1, 2, 3))
+            self.Kf = self.xp.rfftn(self.xp.asarray(K))
 
     # ------------------------------------------------------------ field
     def demag_field(self, v):
         """mu0 * K * v (v already scaled by Ms), zero-padded convolution."""
         Nx, Ny, Nz = self.N
         Pz, Py, Px = self.P
-        V = np.zeros((3, Pz, Py, Px))
+        xp = self.xp
+        V = xp.zeros((3, Pz, Py, Px))
         V[:, :Nz, :Ny, :Nx] = v
-        F = np.fft.rfftn(V, axes=(1, 2, 3))
+        F = xp.rfftn(V)
         xx, yy, zz, yz, xz, xy = self.Kf
-        Bf = np.stack([xx * F[0] + xy * F[1] + xz * F[2],
+        Bf = xp.stack([xx * F[0] + xy * F[1] + xz * F[2],
                        xy * F[0] + yy * F[1] + yz * F[2],
                        xz * F[0] + yz * F[1] + zz * F[2]])
-        B = np.fft.irfftn(Bf, s=(Pz, Py, Px), axes=(1, 2, 3))
+        B = xp.irfftn(Bf, (Pz, Py, Px))
         return MU0 * B[:, :Nz, :Ny, :Nx]
 
     def stencil(self, v):
         """sum_d w_d (v_neighbour - v) with clamped neighbours (exchange.cl)."""
-        out = np.zeros_like(v)
+        xp = self.xp
+        out = xp.zeros_like(v)
         Nz = v.shape[1]
         axes = [(3, self.w[0]), (2, self.w[1])] + ([(1, self.w[2])] if Nz > 1 else [])
         for ax, w in axes:
             n = v.shape[ax]
             idx = np.arange(n)
-            lo = np.take(v, np.maximum(idx - 1, 0), axis=ax)
-            hi = np.take(v, np.minimum(idx + 1, n - 1), axis=ax)
+            lo = xp.take(v, xp.index(np.maximum(idx - 1, 0)), ax)
+            hi = xp.take(v, xp.index(np.minimum(idx + 1, n - 1)), ax)
             out += w * ((lo - v) + (hi - v))
         return out
 
+    def _zstencil(self, v):
+        """sum over z neighbours of (v_nb - v), clamped (exchange.cl z terms)."""
+        xp = self.xp
+        out = xp.zeros_like(v)
+        n = v.shape[1]
+        if n > 1:
+            idx = np.arange(n)
+            lo = xp.take(v, xp.index(np.maximum(idx - 1, 0)), 1)
+            hi = xp.take(v, xp.index(np.minimum(idx + 1, n - 1)), 1)
+            out += (lo - v) + (hi - v)
+        return out
+
+    def dmi(self, m, A):
+        """dmi.cl:8-148 (exchange + interfacial DMI, uniform A and D, no
+        holes, not OpenBC) in FP64, the reference's operations: for each
+        in-plane side a neighbour outside the mesh is extrapolated from m0
+        (dmi.cl:46-50, 67-71, 89-93, 110-114), then 2A/c^2 (mn - m0) and the
+        D/c terms; z neighbours add exchange only.  Linear in m, and (with a
+        geometry-based rather than value-based test for missing neighbours)
+        its own transpose, which the reverse pass uses."""
+        xp = self.xp
+        D = self.D
+        h = xp.zeros_like(m)
+        for ax, c, d in ((3, self.cell[0], 0), (2, self.cell[1], 1)):
+            n = m.shape[ax]
+            for sd in (-1, 1):
+                idx = np.arange(n) + sd
+                mn = xp.take(m, xp.index(np.clip(idx, 0, n - 1)), ax)
+                ins = self.ins[(ax, sd)]
+                q = sd * c * (0.5 * D / A)
+                if d == 0:
+                    ext = xp.stack([m[0] - q * m[2], m[1], m[2] + q * m[0]])
+                else:
+                    ext = xp.stack([m[0], m[1] - q * m[2], m[2] + q * m[1]])
+                mn = ins * mn + (1.0 - ins) * ext
+                h += (2.0 * A / (c * c)) * (mn - m)
+                Dc = D / c
+                h[d] += Dc * sd * mn[2]
+                h[2] -= Dc * sd * mn[d]
+        return h + (2.0 * A / (self.cell[2] ** 2)) * self._zstencil(m)
+
+    def dmi_dA(self, m, A):
+        """d dmi(m, A) / dA: the exchange terms over A, and -D^2/(2A^2) times
+        the boundary cells' (m0x, 0, m0z) (x sides) / (0, m0y, m0z) (y sides),
+        which is what the extrapolated neighbour contributes (D^2/(2A) m0)."""
+        xp = self.xp
+        D = self.D
+        g = xp.zeros_like(m)
+        for ax, c, d in ((3, self.cell[0], 0), (2, self.cell[1], 1)):
+            n = m.shape[ax]
+            for sd in (-1, 1):
+                idx = np.arange(n) + sd
+                mn = xp.take(m, xp.index(np.clip(idx, 0, n - 1)), ax)
+                ins = self.ins[(ax, sd)]
+                g += (2.0 / (c * c)) * ins * (mn - m)
+                bd = (1.0 - ins) * (-(D * D) / (2.0 * A * A))
+                g[d] += bd[0] * m[d]
+                g[2] += bd[0] * m[2]
+        return g + (2.0 / (self.cell[2] ** 2)) * self._zstencil(m)
+
     def field(self, m, th):
         Ms, A, K1, Bext = th["Ms"], th["A"], th["K1"], th["B"]
-        B = self.demag_field(Ms * m) if self.demag else np.zeros_like(m)
-        B = B + A * self.stencil(m) / Ms
+        B = self.demag_field(Ms * m) if self.demag else self.xp.zeros_like(m)
+        B = B + (self.dmi(m, A) if self.D != 0 else A * self.stencil(m)) / Ms
         if K1 != 0:
-            mu = np.einsum("c...,c->...", m, self.u)
-            B = B + (2 * K1 / Ms * mu)[None] * self.u[:, None, None, None]
-        return B + np.asarray(Bext, np.float64)[:, None, None, None]
+            mu = (m * self.ucol).sum(0)
+            B = B + (2 * K1 / Ms * mu)[None] * self.ucol
+        return B + self.xp.col(Bext)
 
     def torque(self, m, B):
-        mxB = np.cross(m, B, axis=0)
-        return self.gilb * (mxB + self.alpha * np.cross(m, mxB, axis=0))
+        mxB = self.xp.cross(m, B)
+        return self.gilb * (mxB + self.alpha * self.xp.cross(m, mxB))
 
-    @staticmethod
-    def normalize(v):
-        return v / np.sqrt((v * v).sum(0))[None]
+    def normalize(self, v):
+        return v / self.xp.sqrt((v * v).sum(0))[None]
 
     def step(self, m, th, keep=False):
         h = self.h
@@ -124,7 +304,8 @@ class Problem:
         return m[2, 0, y0:y0 + h, x0:x0 + w].mean()
 
     def forward(self, m0, th, keep=False):
-        m = self.normalize(np.asarray(m0, np.float64))
+        th = self._params(th)
+        m = self.normalize(self.xp.asarray(m0))
         states = [m]
         acc = 0.0
         for n in range(1, self.nsteps + 1):
@@ -135,43 +316,53 @@ class Problem:
                 acc += self.probe_mean(m)
         navg = self.nsteps - self.avg_from + 1
         avg = m.reshape(3, -1).mean(1)
-        loss = self.w_probe * acc / navg + self.w_target * ((avg - self.target) ** 2).sum()
+        loss = self.xp.scalar(self.w_probe * acc / navg + self.w_target * ((avg - self.target) ** 2).sum())
         return (loss, states) if keep else loss
+
+    def _params(self, th):
+        """th on this backend (Ms a field, B a 3-vector, A and K1 floats)."""
+        xp = self.xp
+        return {"Ms": xp.asarray(th["Ms"]), "A": float(th["A"]), "K1": float(th["K1"]), "B": xp.asarray(th["B"])}
 
     # ------------------------------------------------------------ adjoint
     def _loss_grad(self, m, with_probe, with_avg):
-        g = np.zeros_like(m)
+        g = self.xp.zeros_like(m)
         x0, y0, w, h = self.probe
         navg = self.nsteps - self.avg_from + 1
         if with_probe:
             g[2, 0, y0:y0 + h, x0:x0 + w] += self.w_probe / (navg * w * h)
         if with_avg:
             avg = m.reshape(3, -1).mean(1)
-            g += (2 * self.w_target * (avg - self.target) / m[0].size)[:, None, None, None]
+            g += (2 * self.w_target * (avg - self.target) / self.xp.numel(m[0]))[:, None, None, None]
         return g
 
-    @staticmethod
-    def _norm_vjp(u, w):
-        ln = np.sqrt((u * u).sum(0))[None]
+    def _norm_vjp(self, u, w):
+        ln = self.xp.sqrt((u * u).sum(0))[None]
         n = u / ln
         return (w - n * (n * w).sum(0)[None]) / ln
 
     def _field_vjp(self, m, wB, th, grads):
         Ms, A, K1 = th["Ms"], th["A"], th["K1"]
-        gm = np.zeros_like(m)
+        gm = self.xp.zeros_like(m)
         if self.demag:
             dw = self.demag_field(wB)
             gm += Ms * dw
             grads["Ms"] += (m * dw).sum(0)
-        e = self.stencil(m)
-        gm += A * self.stencil(wB / Ms)
-        we = (wB * e).sum(0)
-        grads["Ms"] -= A * we / Ms ** 2
-        grads["A"] += (we / Ms).sum()
+        if self.D != 0:
+            h = self.dmi(m, A)
+            gm += self.dmi(wB / Ms, A)  # the operator is symmetric
+            grads["Ms"] -= (wB * h).sum(0) / Ms ** 2
+            grads["A"] += ((wB * self.dmi_dA(m, A)).sum(0) / Ms).sum()
+        else:
+            e = self.stencil(m)
+            gm += A * self.stencil(wB / Ms)
+            we = (wB * e).sum(0)
+            grads["Ms"] -= A * we / Ms ** 2
+            grads["A"] += (we / Ms).sum()
         if K1 != 0:
-            mu = np.einsum("c...,c->...", m, self.u)
-            wu = np.einsum("c...,c->...", wB, self.u)
-            gm += (2 * K1 / Ms * wu)[None] * self.u[:, None, None, None]
+            mu = (m * self.ucol).sum(0)
+            wu = (wB * self.ucol).sum(0)
+            gm += (2 * K1 / Ms * wu)[None] * self.ucol
             grads["Ms"] -= 2 * K1 * mu * wu / Ms ** 2
             grads["K1"] += (2 * mu * wu / Ms).sum()
         grads["B"] += wB.reshape(3, -1).sum(1)
@@ -180,10 +371,11 @@ class Problem:
     def _torque_vjp(self, m, B, w):
         g = self.gilb
         a = self.alpha
-        mxB = np.cross(m, B, axis=0)
-        wxm = np.cross(w, m, axis=0)
-        gm = g * (np.cross(B, w, axis=0) + a * (np.cross(mxB, w, axis=0) + np.cross(B, wxm, axis=0)))
-        wB = g * (wxm + a * np.cross(wxm, m, axis=0))
+        cross = self.xp.cross
+        mxB = cross(m, B)
+        wxm = cross(w, m)
+        gm = g * (cross(B, w) + a * (cross(mxB, w) + cross(B, wxm)))
+        wB = g * (wxm + a * cross(wxm, m))
         return gm, wB
 
     def _heun_step_vjp(self, m, ms, Bs, ks, lam, th, grads):
@@ -201,8 +393,10 @@ class Problem:
 
     def backward(self, m0, th):
         """Gradient of forward(m0, th) by the reverse pass (all states kept)."""
+        th = self._params(th)
         loss, states = self.forward(m0, th, keep=True)
-        grads = {"Ms": np.zeros_like(th["Ms"], dtype=np.float64), "A": 0.0, "K1": 0.0, "B": np.zeros(3)}
+        xp = self.xp
+        grads = {"Ms": xp.zeros_like(th["Ms"]), "A": 0.0, "K1": 0.0, "B": xp.zeros((3,))}
         h = self.h
         lam = self._loss_grad(states[-1], self.nsteps >= self.avg_from, True)
         fin = (h / 6, h / 3, h / 3, h / 6)
@@ -217,7 +411,7 @@ class Problem:
                 continue
             u = m + sum(f * k for f, k in zip(fin, ks))
             gu = self._norm_vjp(u, lam)
-            lam2 = gu.copy()
+            lam2 = gu + 0.0
             gk = [f * gu for f in fin]
             for q in range(3, -1, -1):
                 gmq, wB = self._torque_vjp(ms[q], Bs[q], gk[q])
@@ -231,7 +425,8 @@ class Problem:
             lam = lam2
             if n - 1 >= self.avg_from:
                 lam = lam + self._loss_grad(states[n - 1], True, False)
-        grads["m0"] = self._norm_vjp(np.asarray(m0, np.float64), lam)
+        grads["m0"] = self._norm_vjp(xp.asarray(m0), lam)
+        grads = {k: (float(v) if k in ("A", "K1") else xp.host(v)) for k, v in grads.items()}
         return loss, grads
 
 

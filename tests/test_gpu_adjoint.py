@@ -150,3 +150,62 @@ def test_argument_errors():
         adj.backward()  # no forward yet
     with pytest.raises(UmagError):
         gpu_sim(kw, K=4, solver=5)  # RK4 and Heun only
+
+
+# ---------------------------------------------------------------- interfacial DMI
+MULTI = dict(cell=(2e-9, 2e-9, 1e-9), alpha=0.3, anisU=(0.0, 0.0, 1.0), dt=5e-14)
+M_AEX, M_KU1, M_BEXT, M_D = 1.6e-11, 5e5, (0.0, 0.0, 0.05), 3e-3
+
+
+def multilayer_case(N, steps, seed):
+    """The multilayer's material (Aex 1.6e-11, D 3e-3, Ku1 5e5 along z,
+    alpha 0.3, B_ext (0, 0, 50 mT), 2x2x1 nm cells) on a small mesh with a
+    per-cell Ms map around 1.1e6 A/m."""
+    rng = np.random.default_rng(seed)
+    shape = (N[2], N[1], N[0])
+    Ms = rng.uniform(1.0e6, 1.2e6, shape).astype(np.float32)
+    m0 = rng.normal(size=(3,) + shape)
+    m0 = (m0 / np.linalg.norm(m0, axis=0)).astype(np.float32)
+    t = rng.normal(size=3)
+    t /= np.linalg.norm(t)
+    kw = dict(N=N, nsteps=steps, probe=(2, 2, N[0] // 2, N[1] // 2), avg_from=steps - steps // 4 + 1,
+              target=tuple(t), **MULTI)
+    return Ms, m0, kw
+
+
+@pytest.mark.parametrize("solver", [4, 2])
+def test_dmi_forward_matches_engine(solver):
+    """With interfacial DMI on a 3D mesh the adjoint's forward is still the
+    engine's fixed-step stepper bit for bit (dmi.cl arithmetic)."""
+    from umagnus_b200.engine import Simulation
+    Ms, m0, kw = multilayer_case((16, 12, 3), 24, 5)
+    adj = gpu_sim(dict(kw, Dind=M_D), K=8, solver=solver)
+    adj.forward(m0, Ms, M_AEX, M_KU1, M_BEXT)
+    m_adj = adj.final_m().cpu().numpy()
+    sim = Simulation(kw["N"], kw["cell"], Msat=Ms, Aex=M_AEX, alpha=kw["alpha"], Dind=M_D, Ku1=M_KU1,
+                     anisU=kw["anisU"], B_ext=M_BEXT, solver=solver, dt=kw["dt"], FixDt=kw["dt"])
+    sim.set_m(m0)
+    sim.steps(24)
+    m_eng = sim.get_m().cpu().numpy().reshape(m_adj.shape)
+    assert np.array_equal(m_adj, m_eng), np.abs(m_adj - m_eng).max()
+
+
+@pytest.mark.parametrize("N,solver", [((24, 16, 1), 4), ((16, 12, 4), 4), ((16, 12, 4), 2)])
+def test_dmi_gradients_match_fp64_oracle(N, solver):
+    """Gradients through the transposed DMI stencil (including the
+    extrapolated boundary neighbours) against the FP64 reverse pass, which
+    tests/test_oracle_adjoint.py pins to central differences."""
+    Ms, m0, kw = multilayer_case(N, 30, 7 + N[2])
+    adj = gpu_sim(dict(kw, Dind=M_D), K=8, solver=solver)
+    loss = adj.forward(m0, Ms, M_AEX, M_KU1, M_BEXT)
+    g = adj.backward()
+    prob = R.Problem(solver=solver, Dind=M_D, **kw)
+    th = R.params(Ms.astype(np.float64), M_AEX, M_KU1, M_BEXT)
+    loss64, g64 = prob.backward(m0.astype(np.float64), th)
+    assert abs(loss - loss64) <= 1e-5 * max(1.0, abs(loss64))
+    errs = {"Ms": _rel(g["Ms"].cpu().numpy(), g64["Ms"]), "m0": _rel(g["m0"].cpu().numpy(), g64["m0"]),
+            "Aex": _rel(g["Aex"], g64["A"]), "Ku1": _rel(g["Ku1"], g64["K1"]),
+            "B_ext": _rel(g["B_ext"], g64["B"])}
+    print("relative gradient error vs FP64 (DMI):", errs)
+    for k, e in errs.items():
+        assert e < 1e-3, (k, e)

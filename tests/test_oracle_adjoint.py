@@ -60,3 +60,69 @@ def test_loss_of_a_static_state():
     m0[2] = 1.0
     th = R.params(np.full((1, n, n), 8e5), 1.3e-11, 0.0, (0.0, 0.0, 0.1))
     assert prob.forward(m0, th) == pytest.approx(2.0 * 1.0 + 3.0 * 2.0, abs=1e-12)
+
+
+@pytest.mark.parametrize("solver", [4, 2])
+def test_torch_backend_matches_numpy(solver):
+    """The torch float64 backend (the benchmark's FP64 gradient check on the
+    GPU) is the numpy restatement operation for operation: loss and every
+    gradient agree to 1e-12 (FFT libraries differ in the last bits)."""
+    torch = pytest.importorskip("torch")  # noqa: F841
+    prob, m0, th, _ = case(n=10, steps=16, solver=solver)
+    loss, g = prob.backward(m0, th)
+    p2 = R.Problem((10, 10, 1), CELL, 0.02, (1.0, 0.0, 0.0), 1e-13, 16, prob.probe, prob.avg_from,
+                   target=prob.target, solver=solver, backend="torch", device="cpu")
+    loss2, g2 = p2.backward(m0, th)
+    assert loss2 == pytest.approx(loss, rel=1e-12)
+    for k in ("A", "K1"):
+        assert g2[k] == pytest.approx(g[k], rel=1e-10)
+    for k in ("Ms", "B", "m0"):
+        a, b = np.asarray(g2[k]), np.asarray(g[k])
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max(), k
+
+
+def dmi_case(N=(10, 8, 1), steps=20, seed=6, solver=4, D=3e-3, Ku_axis=(0.0, 0.0, 1.0)):
+    """Exchange + interfacial DMI (the multilayer's material: D 3e-3 J/m^2,
+    Ku1 along z), 2D or 3D."""
+    rng = np.random.default_rng(seed)
+    shape = (N[2], N[1], N[0])
+    Ms = rng.uniform(9e5, 1.2e6, shape)
+    m0 = rng.normal(size=(3,) + shape)
+    t = rng.normal(size=3)
+    t /= np.linalg.norm(t)
+    prob = R.Problem(N, (2e-9, 2e-9, 1e-9), 0.3, Ku_axis, 5e-14, steps, (1, 1, N[0] // 2, N[1] // 2),
+                     steps - steps // 4 + 1, target=t, solver=solver, Dind=D)
+    th = R.params(Ms, 1.6e-11, 5e5, (0.0, 0.0, 0.05))
+    return prob, m0, th, rng
+
+
+def test_dmi_field_is_the_reference_restatement():
+    """The FP64 dmi() equals the CPU oracle's dmi.cl restatement (orc_add_dmi,
+    FP64) on a 3D mesh, and is its own transpose."""
+    from oracle import oracle as O
+    prob, m0, th, rng = dmi_case(N=(9, 7, 3))
+    m = m0 / np.sqrt((m0 * m0).sum(0))
+    B = np.zeros_like(m)
+    A, D = th["A"], prob.D
+    O.add_dmi(B, m, O.exch_lut(np.full(256, A), dtype=np.float64), O.exch_lut(np.full(256, D), dtype=np.float64),
+              np.zeros(m.shape[1:], np.uint8), prob.cell, 1.0)
+    h = prob.dmi(m, A)
+    assert np.abs(h - B).max() <= 1e-13 * np.abs(B).max()
+    x, y = rng.normal(size=m.shape), rng.normal(size=m.shape)
+    lhs, rhs = (x * prob.dmi(y, A)).sum(), (prob.dmi(x, A) * y).sum()
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+@pytest.mark.parametrize("N,solver", [((10, 8, 1), 4), ((8, 6, 3), 4), ((10, 8, 1), 2)])
+def test_dmi_reverse_pass_matches_central_fd(N, solver):
+    prob, m0, th, rng = dmi_case(N=N, solver=solver)
+    _, g = prob.backward(m0, th)
+    checks = [("A", None), ("K1", None), ("B", 0), ("B", 1), ("B", 2)]
+    cells = rng.choice(N[0] * N[1] * N[2], size=24, replace=False)
+    for c in cells:
+        z, r = divmod(int(c), N[0] * N[1])
+        checks.append(("Ms", (z, r // N[0], r % N[0])))
+    for which in checks:
+        fd = R.fd_gradient(prob, m0, th, which, rel=1e-4)
+        ad = g[which[0]] if which[1] is None else g[which[0]][which[1]]
+        assert abs(fd - ad) <= 1e-4 * abs(fd) + 1e-12 * max(1.0, abs(ad)), (which, fd, ad)

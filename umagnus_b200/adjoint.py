@@ -32,7 +32,7 @@ GAMMA_LL = 1.7595e11  # engine/torque.go:27
 class AdjointRK4:
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, K, probe, avg_from, w_probe=1.0, w_target=1.0,
                  target=(0.0, 0.0, 1.0), demag=True, demag_kernel="newell", demag_accuracy=6.0, gamma_ll=GAMMA_LL,
-                 use_graph=True, device=0, solver=4):
+                 use_graph=True, device=0, solver=4, Dind=0.0):
         self.L = _lib.init(device)
         p = AdjParams()
         p.N[:] = [int(n) for n in N]
@@ -50,6 +50,7 @@ class AdjointRK4:
         p.target[:] = [float(t) for t in target]
         p.no_graph = 0 if use_graph else 1
         p.solver = int(solver)  # 4 RK4, 2 Heun
+        p.Dind = float(Dind)    # interfacial DMI (fixed parameter)
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
         h = ctypes.c_void_p()

@@ -44,7 +44,9 @@ struct AdjField {
     Mesh3 g;
     int N;
     const float* Ms;   // per-cell map
-    PairCoef pc;       // exchange pair coefficients w_d * A (region (0,0))
+    PairCoef pc;       // exchange pair coefficients w_d * A (region (0,0)); with DMI also 2A/c^2, D/c, c D/(2A)
+    int dmi;           // exchange + interfacial DMI (dmi.cl) instead of exchange (exchange.cl)
+    float dq[2];       // DMI: (D/c)(c D/(2A)) = D^2/(2A) per in-plane axis, the missing neighbour's net weight
     float K1, alpha, gilb;
     float u[3];        // easy axis as given (normalised per cell like uniaxialanisotropy2.cl)
     float bext[3];
@@ -79,7 +81,8 @@ __device__ __forceinline__ void adj_field_cell(const AdjField& a, const float* _
     b = f3{0.f, 0.f, 0.f};
     if (bd) b = f3{bd[I], bd[N + I], bd[2 * N + I]};
     if (!is0(m0)) {
-        const f3 e = exchange_sum_u(mx, my, mz, a.pc, a.g, ix, iy, iz, m0);
+        const f3 e = a.dmi ? dmi_sum_u(mx, my, mz, a.pc, a.g, false, ix, iy, iz, m0)
+                           : exchange_sum_u(mx, my, mz, a.pc, a.g, ix, iy, iz, m0);
         const float inv = inv_msat(a.Ms, 1.0f, I);
         b.x = fa(b.x, fm(e.x, inv));
         b.y = fa(b.y, fm(e.y, inv));
@@ -285,7 +288,56 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, in
             g = ad3(g, sc3(ms, d));
             gms += (double)m0.x * d.x + (double)m0.y * d.y + (double)m0.z * d.z;
         }
-        {
+        if (a.dmi) {
+            // h = A E(m) + D R(m) + (D^2/2A) P(m) (dmi.cl with the missing in-plane
+            // neighbours extrapolated): linear in m and symmetric, so the
+            // cotangent x = wB/Ms goes through the same stencil, with the
+            // missing neighbours decided by the geometry, not by zero values.
+            // dh/dA = E(m) - (D^2/2A^2) P(m).
+            const f3 x0 = sc3(inv, w);
+            f3 lx{0.f, 0.f, 0.f}, eA{0.f, 0.f, 0.f}, pb{0.f, 0.f, 0.f};
+#pragma unroll
+            for (int d = 0; d < 2; d++) {
+#pragma unroll
+                for (int sd = -1; sd <= 1; sd += 2) {
+                    const bool in = d == 0 ? (sd < 0 ? ix > 0 : ix + 1 < a.g.Nx) : (sd < 0 ? iy > 0 : iy + 1 < a.g.Ny);
+                    const float S = d == 0 ? a.pc.sx : a.pc.sy, Dc = (d == 0 ? a.pc.dcx : a.pc.dcy) * sd;
+                    if (in) {
+                        const int j = d == 0 ? I + sd : I + sd * a.g.Nx;
+                        const float msj = a.Ms[j];
+                        const float ij = msj == 0.f ? 0.f : 1.0f / msj;
+                        const f3 xn{wB[j] * ij, wB[N + j] * ij, wB[2 * N + j] * ij};
+                        const f3 mn{mq[j], mq[N + j], mq[2 * N + j]};
+                        lx = ad3(lx, sc3(S, f3{xn.x - x0.x, xn.y - x0.y, xn.z - x0.z}));
+                        eA = ad3(eA, sc3(S, f3{mn.x - m0.x, mn.y - m0.y, mn.z - m0.z}));
+                        if (d == 0) { lx.x += Dc * xn.z; lx.z -= Dc * xn.x; }
+                        else { lx.y += Dc * xn.z; lx.z -= Dc * xn.y; }
+                    } else {
+                        const float q = a.dq[d];
+                        if (d == 0) { lx.x += q * x0.x; lx.z += q * x0.z; pb.x += q * m0.x; pb.z += q * m0.z; }
+                        else { lx.y += q * x0.y; lx.z += q * x0.z; pb.y += q * m0.y; pb.z += q * m0.z; }
+                    }
+                }
+            }
+            if (a.g.Nz != 1) {
+#pragma unroll
+                for (int sd = -1; sd <= 1; sd += 2) {
+                    const int j = ((sd < 0 ? lclamp(iz - 1, a.g.Nz, false) : hclamp(iz + 1, a.g.Nz, false)) * a.g.Ny +
+                                   iy) * a.g.Nx + ix;
+                    const float msj = a.Ms[j];
+                    const float ij = msj == 0.f ? 0.f : 1.0f / msj;
+                    lx = ad3(lx, sc3(a.pc.sz, f3{wB[j] * ij - x0.x, wB[N + j] * ij - x0.y, wB[2 * N + j] * ij - x0.z}));
+                    eA = ad3(eA, sc3(a.pc.sz, f3{mq[j] - m0.x, mq[N + j] - m0.y, mq[2 * N + j] - m0.z}));
+                }
+            }
+            g = ad3(g, lx);
+            // the field itself, as the forward computes it (for the Ms gradient)
+            const f3 h = dmi_sum_u(mq, mq + N, mq + 2 * (size_t)N, a.pc, a.g, false, ix, iy, iz, m0);
+            const double wh = (double)w.x * h.x + (double)w.y * h.y + (double)w.z * h.z;
+            gms -= wh * (double)inv * (double)inv;
+            const double wA = (double)w.x * (eA.x - pb.x) + (double)w.y * (eA.y - pb.y) + (double)w.z * (eA.z - pb.z);
+            acc[(size_t)N + I] += wA * (double)inv / (double)A;
+        } else {
             int nb[6];
             nb[0] = (iz * a.g.Ny + iy) * a.g.Nx + lclamp(ix - 1, a.g.Nx, false);
             nb[1] = (iz * a.g.Ny + iy) * a.g.Nx + hclamp(ix + 1, a.g.Nx, false);
@@ -419,7 +471,7 @@ struct AdjImpl {
     bool heun = false;    // Heun instead of RK4
     int nst() const { return heun ? 2 : 4; }
     float* Ms = nullptr;  // per-cell Ms of the last forward
-    float A = 0, A00 = 0, K1 = 0, B[3] = {0, 0, 0};
+    float A = 0, A00 = 0, D00 = 0, K1 = 0, B[3] = {0, 0, 0};
     std::vector<float*> ckpt;  // m at steps 0, K, 2K, ...
     float* seg = nullptr;      // one segment: K steps x 12 x 3N (m2..m4, B1..B4, k1..k4, start state)
     float* work = nullptr;     // W_COUNT x 3N
@@ -446,6 +498,24 @@ static AdjField adj_field(const AdjImpl* s) {
     a.pc.wax = wx * s->A00;
     a.pc.way = wy * s->A00;
     a.pc.waz = wz * s->A00;
+    // DMI pair coefficients of region (0, 0), float32 operations as the
+    // engine's k_local_consts (dmi.cl: 2A/c^2, D/c and the extrapolation
+    // factor c (D/2)/A), cell sizes as float32 (opencl/dmi.go:61)
+    a.dmi = s->D00 != 0.f;
+    if (a.dmi) {
+        const float cx = (float)s->p.cell[0], cy = (float)s->p.cell[1], cz = (float)s->p.cell[2];
+        const float A = s->A00, D = s->D00;
+        a.pc.sx = (2.0f * A) / (cx * cx);
+        a.pc.sy = (2.0f * A) / (cy * cy);
+        a.pc.sz = (2.0f * A) / (cz * cz);
+        a.pc.dcx = D / cx;
+        a.pc.dcy = D / cy;
+        const float t = (0.5f * D) / A;
+        a.pc.qx = cx * t;
+        a.pc.qy = cy * t;
+        a.dq[0] = a.pc.dcx * a.pc.qx;
+        a.dq[1] = a.pc.dcy * a.pc.qy;
+    }
     a.K1 = s->K1;
     a.alpha = s->p.alpha;
     const float aa = s->p.alpha * s->p.alpha;
@@ -629,6 +699,8 @@ int adj_forward(umag_adj* hd, const float* m0, const float* Ms, float A, float K
     UMAG_CUDA(cudaMemcpyAsync(s->Ms, Ms, sizeof(float) * s->N, cudaMemcpyDeviceToDevice, AS()));
     s->A = A;
     s->A00 = 2.0f / (1.0f / A + 1.0f / A);  // engine/exchange.go:153-167, region 0 with itself
+    const float D = s->p.Dind;
+    s->D00 = D == 0.f ? 0.f : 2.0f / (1.0f / D + 1.0f / D);  // the same average for the DMI LUT
     s->K1 = K1;
     for (int c = 0; c < 3; c++) s->B[c] = Bext[c];
     const AdjField af = adj_field(s);

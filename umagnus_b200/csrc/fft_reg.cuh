@@ -183,12 +183,24 @@ __device__ __forceinline__ void rg_stage_seq(float2 (&v)[NC][8], int t, float2* 
                 for (int i = 0; i < NB; i++) {
                     const int j = t + T * i;
                     const int o = (j / NS) * NS * R + j % NS;
+                    if constexpr (NS % (1 << PS) == 0) {  // pad(o + q*NS) = pad(o) + q*pad(NS)
+                        float2* base = b + rg_pad<PS>(o);
 #pragma unroll
-                    for (int q = 0; q < R; q++) b[rg_pad<PS>(o + q * NS)] = v[c][i + q * NB];
+                        for (int q = 0; q < R; q++) base[q * (NS + (NS >> PS))] = v[c][i + q * NB];
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < R; q++) b[rg_pad<PS>(o + q * NS)] = v[c][i + q * NB];
+                    }
                 }
                 __syncthreads();
+                if constexpr (T % (1 << PS) == 0) {  // pad(t + T*m) = pad(t) + m*pad(T)
+                    const float2* base = b + rg_pad<PS>(t);
 #pragma unroll
-                for (int m = 0; m < 8; m++) v[c][m] = b[rg_pad<PS>(t + T * m)];
+                    for (int m = 0; m < 8; m++) v[c][m] = base[m * (T + (T >> PS))];
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 8; m++) v[c][m] = b[rg_pad<PS>(t + T * m)];
+                }
             }
             rg_stage_seq<L, NC, ST + 1, NS * R, (P + NC) & 1, ZH>(v, t, ex, exs, tw);
         }

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "cellmath.cuh"
@@ -1663,24 +1664,40 @@ int sim_set_param(umag_sim* h, int which, const float* values, float mul) {
 // the instance index) and one controller thread per instance keeps its own
 // time, dt and accept/reject decisions.  One CUDA graph steps every class,
 // the classes on parallel branches.
+//
+// Scheduling: each class has its own stream and its own graph of
+// graph_steps steps; the host keeps every unfinished class's stream fed with
+// chunks of replays and polls each class on its own (an event after the
+// chunk and its state copy), so a cheap class never waits for an expensive
+// one.  When a chunk leaves at most 3/4 of a class's batch still running,
+// the running instances are compacted to the front of the batch (their
+// controller records, parameters and per-instance indices permuted; the
+// state buffers stay where they are, the records point at them) and the
+// class's graph is recaptured for the smaller batch, so finished instances
+// stop costing launches.  Every instance's arithmetic is unchanged.
 struct EnsClass {
     SimImpl* s = nullptr;
-    std::vector<int> members;  // ensemble index of each instance
+    std::vector<int> members;  // ensemble index of each batch slot
     float2* spec = nullptr;    // nb spectrum scratch copies
-    float* params = nullptr;   // device: Ms[nb], A00[nb], D00[nb]
+    float* params = nullptr;   // device: Ms[n_all], A00[n_all], D00[n_all]
+    std::vector<float> hparams;  // host copy of params (permuted with the slots)
+    int n_all = 0;             // instances of the class; the first s->nb slots are in the batch
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
+    cudaGraphExec_t gexec = nullptr;  // graph_steps steps of the current batch
+    bool busy = false, finished = false;
+    long long replays = 0;
 };
 struct EnsImpl {
     std::vector<EnsClass> cls;
-    std::vector<std::pair<int, int>> where;  // instance -> (class, index in class)
+    std::vector<std::pair<int, int>> where;  // instance -> (class, slot in class)
     umag_solver_params sp;
     int graph_steps = 16;
-    cudaGraphExec_t gexec = nullptr;
-    cudaEvent_t fork = nullptr;
 };
 
 static void ens_class_free(EnsClass& c) {
+    if (c.gexec) cudaGraphExecDestroy(c.gexec);
+    c.gexec = nullptr;
     if (c.s) {
         SimImpl* s = c.s;
         drop_graph(s);
@@ -1709,8 +1726,6 @@ int ens_free(umag_ens* h) {
     EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
     if (!e) return UMAG_OK;
     cudaDeviceSynchronize();
-    if (e->gexec) cudaGraphExecDestroy(e->gexec);
-    if (e->fork) cudaEventDestroy(e->fork);
     for (auto& c : e->cls) ens_class_free(c);
     delete e;
     return UMAG_OK;
@@ -1724,6 +1739,7 @@ static int ens_class_new(EnsClass& C, const umag_ens_instance* in, const std::ve
     SimImpl* s = new SimImpl();
     C.s = s;
     C.members = members;
+    C.n_all = nb;
     s->nb = nb;
     s->batched = true;
     s->sp = *sp;
@@ -1780,6 +1796,7 @@ static int ens_class_new(EnsClass& C, const umag_ens_instance* in, const std::ve
     }
     UMAG_CUDA(cudaMalloc(&C.params, sizeof(float) * 3 * nb));
     UMAG_CUDA(cudaMemcpyAsync(C.params, hp.data(), sizeof(float) * 3 * nb, cudaMemcpyHostToDevice, S()));
+    C.hparams = hp;
     UMAG_CUDA(cudaStreamSynchronize(S()));
     UMAG_CUDA(cudaMalloc(&s->ip_dev, sizeof(InstParams) * nb));
     LocalArgs& la = s->la;
@@ -1876,9 +1893,22 @@ int ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, in
         int st = ens_class_new(e->cls[k], in, groups[k], sp, demag);
         if (st != UMAG_OK) return fail(st);
     }
-    if (cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess)
-        return fail(set_error(UMAG_E_CUDA, "event"));
     *out = reinterpret_cast<umag_ens*>(e);
+    return UMAG_OK;
+}
+
+// every slot's controller record to the host (the batch may be smaller
+// than the class after compaction; records past it do not change)
+static int ens_sync_all(EnsClass& C) {
+    SimImpl* s = C.s;
+    UMAG_CUDA(cudaMemcpyAsync(s->hctl, s->ctl, sizeof(DevCtl) * C.n_all, cudaMemcpyDeviceToHost, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    return UMAG_OK;
+}
+static int ens_push_all(EnsClass& C) {
+    SimImpl* s = C.s;
+    UMAG_CUDA(cudaMemcpyAsync(s->ctl, s->hctl, sizeof(DevCtl) * C.n_all, cudaMemcpyHostToDevice, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
     return UMAG_OK;
 }
 
@@ -1893,7 +1923,7 @@ int ens_set_m(umag_ens* h, int i, const float* host_m) {
     UMAG_REQUIRE(e && host_m && i >= 0 && i < (int)e->where.size(), "bad argument");
     int b;
     SimImpl* s = ens_sim(e, i, &b);
-    UMAG_TRY(sync_ctl_to_host(s));
+    UMAG_TRY(ens_sync_all(e->cls[e->where[i].first]));
     float* m = s->hctl[b].m;
     // on the library stream, so that the normalisation below sees the copy
     UMAG_CUDA(cudaMemcpyAsync(m, host_m, sizeof(float) * 3 * s->N, cudaMemcpyHostToDevice, S()));
@@ -1908,7 +1938,7 @@ int ens_get_m(umag_ens* h, int i, float* host_m) {
     UMAG_REQUIRE(e && host_m && i >= 0 && i < (int)e->where.size(), "bad argument");
     int b;
     SimImpl* s = ens_sim(e, i, &b);
-    UMAG_TRY(sync_ctl_to_host(s));
+    UMAG_TRY(ens_sync_all(e->cls[e->where[i].first]));
     UMAG_CUDA(cudaMemcpyAsync(host_m, s->hctl[b].m, sizeof(float) * 3 * s->N, cudaMemcpyDeviceToHost, S()));
     UMAG_CUDA(cudaStreamSynchronize(S()));
     return UMAG_OK;
@@ -1919,7 +1949,7 @@ int ens_get_state(umag_ens* h, int i, umag_solver_state* st) {
     UMAG_REQUIRE(e && st && i >= 0 && i < (int)e->where.size(), "bad argument");
     int b;
     SimImpl* s = ens_sim(e, i, &b);
-    UMAG_TRY(sync_ctl_to_host(s));
+    UMAG_TRY(ens_sync_all(e->cls[e->where[i].first]));
     const DevCtl& c = s->hctl[b];
     st->time = c.t; st->dt = c.dt; st->last_err = c.last_err; st->peak_err = c.peak_err;
     st->last_torque = c.last_torque; st->nsteps = c.nsteps; st->nundone = c.nundone; st->nevals = c.nevals;
@@ -1927,70 +1957,123 @@ int ens_get_state(umag_ens* h, int i, umag_solver_state* st) {
     return UMAG_OK;
 }
 
-// one graph: graph_steps steps of every class, classes on parallel branches
-static int ens_build_graph(EnsImpl* e) {
-    if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
-    cudaStream_t main = ctx().stream;
-    cudaGraph_t graph;
-    UMAG_CUDA(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
-    int st = UMAG_OK;
-    if (cudaEventRecord(e->fork, main) != cudaSuccess) st = set_error(UMAG_E_CUDA, "fork");
-    for (auto& c : e->cls) {
-        if (st != UMAG_OK) break;
-        if (cudaStreamWaitEvent(c.st, e->fork, 0) != cudaSuccess) { st = set_error(UMAG_E_CUDA, "fork wait"); break; }
-        g_launch_stream = c.st;
-        int nl = 0;
-        for (int k = 0; k < e->graph_steps && st == UMAG_OK; k++) st = launch_step(c.s, &nl);
-        g_launch_stream = nullptr;
-        if (st == UMAG_OK && cudaEventRecord(c.done, c.st) != cudaSuccess) st = set_error(UMAG_E_CUDA, "join");
-        if (st == UMAG_OK && cudaStreamWaitEvent(main, c.done, 0) != cudaSuccess) st = set_error(UMAG_E_CUDA, "join");
-    }
+// graph_steps steps of class C's current batch, captured on its stream
+static int ens_capture(EnsImpl* e, EnsClass& C) {
+    if (C.gexec) { cudaGraphExecDestroy(C.gexec); C.gexec = nullptr; }
+    g_launch_stream = C.st;
+    const int st = capture_steps(C.s, e->graph_steps, &C.gexec);
     g_launch_stream = nullptr;
-    cudaError_t ce = cudaStreamEndCapture(main, &graph);
-    if (st != UMAG_OK) return st;
-    if (ce != cudaSuccess) return set_error(UMAG_E_CUDA, "ensemble graph capture: %s", cudaGetErrorString(ce));
-    ce = cudaGraphInstantiate(&e->gexec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ce != cudaSuccess) return set_error(UMAG_E_CUDA, "ensemble graph instantiate: %s", cudaGetErrorString(ce));
-    return UMAG_OK;
+    return st;
+}
+
+// Compact the running instances of class C to the front of its batch (the
+// host records are fresh: its stream is idle).  Slot k takes the instance of
+// old slot order[k]: its controller record (which points at its own state
+// buffers; the demag-field scratch pointer is the slot's), its parameters
+// and its uniform constants.
+static int ens_compact(EnsImpl* e, int ci) {
+    EnsClass& C = e->cls[ci];
+    SimImpl* s = C.s;
+    const int nb = s->nb;
+    std::vector<int> order;
+    for (int b = 0; b < nb; b++)
+        if (s->hctl[b].t < s->hctl[b].stop && s->hctl[b].status == 0) order.push_back(b);
+    const int na = (int)order.size();
+    if (na == 0 || 4 * na > 3 * nb) return UMAG_OK;
+    for (int b = 0; b < nb; b++)
+        if (!(s->hctl[b].t < s->hctl[b].stop && s->hctl[b].status == 0)) order.push_back(b);
+    std::vector<DevCtl> ctl(nb);
+    std::vector<int> mem(nb);
+    std::vector<float> hp = C.hparams;
+    const size_t n3 = 3 * (size_t)s->N;
+    InstParams* tmp = nullptr;
+    UMAG_CUDA(cudaMalloc(&tmp, sizeof(InstParams) * nb));
+    for (int k = 0; k < nb; k++) {
+        const int o = order[k];
+        ctl[k] = s->hctl[o];
+        if (s->bd) ctl[k].bd = s->bd + (size_t)k * n3;
+        mem[k] = C.members[o];
+        for (int q = 0; q < 3; q++) hp[q * C.n_all + k] = C.hparams[q * C.n_all + o];
+        UMAG_CUDA(cudaMemcpyAsync(tmp + k, s->ip_dev + o, sizeof(InstParams), cudaMemcpyDeviceToDevice, S()));
+    }
+    UMAG_CUDA(cudaMemcpyAsync(s->ip_dev, tmp, sizeof(InstParams) * nb, cudaMemcpyDeviceToDevice, S()));
+    UMAG_CUDA(cudaStreamSynchronize(S()));
+    cudaFree(tmp);
+    for (int k = 0; k < nb; k++) {
+        s->hctl[k] = ctl[k];
+        C.members[k] = mem[k];
+        e->where[mem[k]] = {ci, k};
+    }
+    C.hparams = hp;
+    UMAG_CUDA(cudaMemcpyAsync(C.params, hp.data(), sizeof(float) * hp.size(), cudaMemcpyHostToDevice, S()));
+    UMAG_TRY(ens_push_all(C));
+    s->nb = na;
+    return ens_capture(e, C);
 }
 
 // engine/run.go:190 Run(seconds) for every instance: each runs until its own
-// time reaches start + seconds (its dt honours that alarm); the host checks
-// the instances every `chunk` graph replays
+// time reaches start + seconds (its dt honours that alarm).  Classes advance
+// independently, `chunk` graph replays at a time (at most max_replays each).
 int ens_run(umag_ens* h, double seconds, int chunk, long long max_replays) {
     EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
     UMAG_REQUIRE(e && seconds >= 0, "bad argument");
     if (chunk <= 0) chunk = 8;
-    for (auto& c : e->cls) {
-        SimImpl* s = c.s;
-        UMAG_TRY(sync_ctl_to_host(s));
+    for (auto& C : e->cls) {
+        SimImpl* s = C.s;
+        UMAG_TRY(ens_sync_all(C));
+        s->nb = C.n_all;  // every instance takes part again
         for (int b = 0; b < s->nb; b++) {
             s->hctl[b].stop = s->hctl[b].t + seconds;
             s->hctl[b].alarm = s->hctl[b].stop;
         }
-        UMAG_TRY(push_ctl(s));
+        UMAG_TRY(ens_push_all(C));
         s->need_k1 = true;  // RunWhile frees the stepper (engine/run.go:207)
         UMAG_TRY(ensure_k1(s));
+        UMAG_TRY(ens_capture(e, C));
+        C.busy = false;
+        C.finished = false;
+        C.replays = 0;
     }
-    if (!e->gexec) UMAG_TRY(ens_build_graph(e));
-    long long done = 0;
-    while (done < max_replays) {
-        for (int k = 0; k < chunk && done < max_replays; k++, done++)
-            UMAG_CUDA(cudaGraphLaunch(e->gexec, ctx().stream));
-        bool running = false;
-        for (auto& c : e->cls) {
-            UMAG_TRY(sync_ctl_to_host(c.s));
-            for (int b = 0; b < c.s->nb; b++) {
-                const DevCtl& d = c.s->hctl[b];
-                if (d.status != 0)
-                    return set_error(UMAG_E_SOLVER, "instance %d: solver failure code %d at t=%g", c.members[b],
-                                     d.status, d.t);
-                running |= d.t < d.stop;
+    UMAG_CUDA(cudaDeviceSynchronize());
+    for (;;) {
+        bool all_done = true, progressed = false;
+        for (size_t ci = 0; ci < e->cls.size(); ci++) {
+            EnsClass& C = e->cls[ci];
+            SimImpl* s = C.s;
+            if (C.finished) continue;
+            all_done = false;
+            if (C.busy) {
+                const cudaError_t q = cudaEventQuery(C.done);
+                if (q == cudaErrorNotReady) continue;
+                if (q != cudaSuccess) return set_error(UMAG_E_CUDA, "ensemble class %zu: %s", ci, cudaGetErrorString(q));
+                C.busy = false;
+                progressed = true;
+                int running = 0;
+                for (int b = 0; b < s->nb; b++) {
+                    const DevCtl& d = s->hctl[b];
+                    if (d.status != 0)
+                        return set_error(UMAG_E_SOLVER, "instance %d: solver failure code %d at t=%g", C.members[b],
+                                         d.status, d.t);
+                    running += d.t < d.stop;
+                }
+                if (running == 0 || C.replays >= max_replays) {
+                    C.finished = true;
+                    continue;
+                }
+                UMAG_TRY(ens_compact(e, (int)ci));
             }
+            // the next chunk, then the batch's records back to the host
+            for (int k = 0; k < chunk && C.replays < max_replays; k++, C.replays++)
+                UMAG_CUDA(cudaGraphLaunch(C.gexec, C.st));
+            UMAG_CUDA(cudaMemcpyAsync(s->hctl, s->ctl, sizeof(DevCtl) * s->nb, cudaMemcpyDeviceToHost, C.st));
+            UMAG_CUDA(cudaEventRecord(C.done, C.st));
+            C.busy = true;
+            progressed = true;
         }
-        if (!running) break;
+        if (all_done) break;
+        if (!progressed) std::this_thread::yield();
     }
+    UMAG_CUDA(cudaDeviceSynchronize());
     return UMAG_OK;
 }
 

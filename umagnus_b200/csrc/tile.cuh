@@ -44,16 +44,20 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
 }
+// One bounded wait step: the thread may be suspended until the phase
+// completes or about kMbarSuspendNs nanoseconds pass (PTX suspendTimeHint),
+// so waiting warps sleep instead of spinning through issue slots.
+constexpr uint32_t kMbarSuspendNs = 1000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     uint32_t ok;
     asm volatile(
         "{\n"
         ".reg .pred p;\n"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
         "selp.u32 %0, 1, 0, p;\n"
         "}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(phase)
+        : "r"(smem_u32(bar)), "r"(phase), "r"(kMbarSuspendNs)
         : "memory");
     return ok != 0;
 }

@@ -520,8 +520,14 @@ def ensemble_measure(args, rank=0, world=1, dist=None, local_rank=0, plain=True,
     insts_all = ensemble_instances()
     T = args.ens_time
 
+    tunings = {}
+
     def make(ins):
-        return engine.Ensemble([{k: v for k, v in d.items() if k != "m_seed"} for d in ins], device=local_rank)
+        e = engine.Ensemble([{k: v for k, v in d.items() if k != "m_seed"} for d in ins], device=local_rank)
+        # launch shapes of each class's batched kernels (speed only), before timing
+        chosen, _ = e.autotune(ins)
+        tunings.update({"x".join(str(v) for v in e.class_info(c)[0]): t for c, t in chosen.items()})
+        return e
 
     t_batch, cells_steps, n_done, alg_tot, insts, states = ensemble_shard(insts_all, T, rank, world, dist, make)
     ncell = [d["N"][0] * d["N"][1] for d in insts]
@@ -535,7 +541,8 @@ def ensemble_measure(args, rank=0, world=1, dist=None, local_rank=0, plain=True,
                        "hbm": {"alg_bytes": alg_tot, "gbs": alg_tot / t_batch / 1e9, "peak": peak,
                                "peak_source": peak_kind, "frac": alg_tot / t_batch / 1e9 / peak,
                                "what": "sum over instances of accepted steps x (6 B_eval + 480 N) / wall time"},
-                       "accepted_steps_rank0": {"total": int(acc.sum()), "min": int(acc.min()), "max": int(acc.max())}}}
+                       "accepted_steps_rank0": {"total": int(acc.sum()), "min": int(acc.min()), "max": int(acc.max())},
+                       "launch_shapes_rank0": tunings}}
     if not plain or world != 1:
         return out
     per_size = {}

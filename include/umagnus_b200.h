@@ -401,11 +401,23 @@ int umag_ens_set_m(umag_ens* e, int i, const float* host_m);
 int umag_ens_get_m(umag_ens* e, int i, float* host_m);
 int umag_ens_get_state(umag_ens* e, int i, umag_solver_state* st);
 /* engine/run.go:190 Run(seconds) for every instance from its own current
- * time; steps are replayed from one CUDA graph (16 steps of every class per
- * replay, finished instances idle), checked on the host every `chunk`
- * replays, at most max_replays replays. */
+ * time.  Each class (instances of one mesh) replays its own CUDA graph of 16
+ * steps on its own stream, fed and checked by the host every `chunk`
+ * replays independently of the other classes (at most max_replays replays
+ * per class); finished instances leave their class's batch (compaction) and
+ * return at the next run.  No counterpart in the reference. */
 int umag_ens_run(umag_ens* e, double seconds, int chunk, long long max_replays);
 int umag_ens_count(umag_ens* e, int* n_instances, int* n_classes);
+/* Classes (instances of one mesh and cell size, numbered in the order their
+ * first instance appears): the mesh and the number of instances of class
+ * `cls`.  No counterpart in the reference. */
+int umag_ens_class_info(umag_ens* e, int cls, int N[3], int* n_instances);
+/* Launch shapes of class `cls`'s batched per-cell kernels (the fields of
+ * umag_tuning; the torque kernel of a batch reads global memory, so
+ * torque_tma is ignored).  Speed only: every instance's arithmetic is the
+ * same under every shape.  No counterpart in the reference. */
+int umag_ens_get_tuning(umag_ens* e, int cls, umag_tuning* t);
+int umag_ens_set_tuning(umag_ens* e, int cls, const umag_tuning* t);
 
 /* ---- differentiable simulation: forward RK4 and its adjoint --------------
  * No counterpart in the reference (which has no gradients).  A thin film or

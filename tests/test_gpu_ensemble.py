@@ -129,3 +129,44 @@ def test_ensemble_compaction_and_second_run():
         np.testing.assert_array_equal(sim.get_m().cpu().numpy(), ens.get_m(i))
         sim.free()
     ens.free()
+
+
+def test_class_launch_shapes_change_nothing_but_speed():
+    """Launch shapes set per class (as the ensemble autotuner does) leave
+    every instance's trajectory bit for bit the same."""
+    import bench
+    from umagnus_b200 import engine
+    insts = bench.ensemble_instances(count=12, seed=31)
+    runs = []
+    for shapes in (None, {"torque_block": [64, 2], "stage_threads": 128, "stage_waves": 2, "err_waves": 16}):
+        ens = engine.Ensemble([{k: v for k, v in d.items() if k != "m_seed"} for d in insts])
+        if shapes:
+            for c in range(ens.classes()):
+                ens.set_tuning(c, shapes)
+                assert ens.get_tuning(c)["stage_threads"] == 128
+        for i, d in enumerate(insts):
+            ens.set_m(i, bench.random_m(d["N"], d["m_seed"]))
+        ens.run(3e-12, chunk=2)
+        runs.append(([ens.state(i) for i in range(len(insts))], [ens.get_m(i) for i in range(len(insts))]))
+        ens.free()
+    for i in range(len(insts)):
+        assert runs[0][0][i] == runs[1][0][i], i
+        np.testing.assert_array_equal(runs[0][1][i], runs[1][1][i])
+
+
+def test_ensemble_autotune_chooses_and_caches(tmp_path):
+    """The ensemble tuner gives every class valid shapes, stores them and
+    applies the cached ones without timing the second time."""
+    import bench
+    from umagnus_b200 import engine
+    insts = [d for d in bench.ensemble_instances(count=20, seed=3) if d["N"][0] in (32, 48)]
+    clean = [{k: v for k, v in d.items() if k != "m_seed"} for d in insts]
+    ens = engine.Ensemble(clean)
+    cache = str(tmp_path / "tune.json")
+    chosen, logs = ens.autotune(clean, cache_path=cache)
+    assert set(chosen) == set(range(ens.classes())) and all(v is not None for v in logs.values())
+    ens2 = engine.Ensemble(clean)
+    chosen2, logs2 = ens2.autotune(clean, cache_path=cache)
+    assert chosen2 == chosen and all(v is None for v in logs2.values())
+    ens.free()
+    ens2.free()

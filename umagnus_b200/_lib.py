@@ -123,6 +123,8 @@ _SIGS = {
     "umag_ens_new": [c_int, P, P, c_int, ctypes.POINTER(c_void_p)], "umag_ens_free": [P],
     "umag_ens_set_m": [P, c_int, P], "umag_ens_get_m": [P, c_int, P], "umag_ens_get_state": [P, c_int, P],
     "umag_ens_run": [P, c_double, c_int, c_ll], "umag_ens_count": [P, ctypes.POINTER(c_int), ctypes.POINTER(c_int)],
+    "umag_ens_class_info": [P, c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int)],
+    "umag_ens_get_tuning": [P, c_int, ctypes.POINTER(Tuning)], "umag_ens_set_tuning": [P, c_int, ctypes.POINTER(Tuning)],
     "umag_adj_new": [ctypes.POINTER(AdjParams), ctypes.POINTER(c_void_p)], "umag_adj_free": [P],
     "umag_adj_forward": [P, P, P, c_float, c_float, ctypes.POINTER(c_float), ctypes.POINTER(c_double)],
     "umag_adj_final_m": [P, P],

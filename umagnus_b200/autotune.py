@@ -1,4 +1,5 @@
-"""Autotuner for the launch shapes of the per-cell kernels of a Simulation.
+"""Autotuner for the launch shapes of the per-cell kernels of a Simulation
+and of the batched classes of an Ensemble.
 
 The tunables (umag_tuning in the C header) are the CTA shape of the field +
 torque kernel and whether its stencils read TMA-loaded tiles (where the
@@ -67,13 +68,13 @@ def save_cache(path, data):
     os.replace(tmp, path)
 
 
-def search(measure, nx):
+def search(measure, nx, tma_choices=(1, 0)):
     """Coordinate descent over the three tunables.  measure(kind, tuning) ->
     seconds, kind "torque" or "step"; returns (best tuning, {kind: timings})."""
     best = {k: (list(v) if isinstance(v, list) else v) for k, v in DEFAULT.items()}
     log = {"torque": {}, "stage": {}, "err": {}}
     for bx, by in torque_blocks(nx):
-        for tma in (1, 0):
+        for tma in tma_choices:
             t = dict(best, torque_block=[bx, by], torque_tma=tma)
             log["torque"][f"{bx}x{by}/{tma}"] = measure("torque", t)
     shape, tma = min(log["torque"], key=log["torque"].get).split("/")
@@ -146,3 +147,66 @@ def tune(sim, cache_path=None, evals=40, steps=16, use_cache=True):
         cache[key] = sim.get_tuning()
         save_cache(cache_path, cache)
     return sim.get_tuning(), log
+
+
+def tune_ensemble(ens, instances, cache_path=None, use_cache=True, probe_size=8, replays=3):
+    """Choose and apply the launch shapes of every class of `ens` (an
+    engine.Ensemble made from `instances`).  Each class is timed on a probe
+    ensemble of up to probe_size of its instances (fresh random states, a
+    stop time no instance reaches, `replays` graph replays per candidate,
+    wall clock around whole runs), so the real ensemble's state is never
+    touched; the same coordinate descent as tune(), every kind timed on
+    steps, no TMA tiles (a batch's torque kernel reads global memory).  With
+    use_cache a cached choice is applied without timing.  Returns
+    ({class: tuning}, {class: timings or None})."""
+    import time
+
+    import numpy as np
+    import torch
+
+    from .engine import Ensemble
+    cache_path = cache_path or default_cache_path()
+    cache = load_cache(cache_path) if use_cache else {}
+    name = torch.cuda.get_device_name()
+    chosen, logs = {}, {}
+    strip = ("m_seed",)
+    for cls in range(ens.classes()):
+        N, _ = ens.class_info(cls)
+        members = [d for d in instances if tuple(int(v) for v in d["N"]) == tuple(N)]
+        feats = "ens|dmi={}|anis={}".format(int(any(d.get("Dind", 0) for d in members)),
+                                            int(any(d.get("Ku1", 0) or d.get("Ku2", 0) for d in members)))
+        key = cache_key(name, N, feats)
+        if key in cache:
+            ens.set_tuning(cls, cache[key])
+            chosen[cls], logs[cls] = ens.get_tuning(cls), None
+            continue
+        probe_insts = [{k: v for k, v in d.items() if k not in strip} for d in members[:probe_size]]
+        probe = Ensemble(probe_insts)
+        rng = np.random.default_rng(7)
+        for i, d in enumerate(probe_insts):
+            m = rng.standard_normal((3, d["N"][2], d["N"][1], d["N"][0]))
+            probe.set_m(i, m / np.sqrt((m * m).sum(0)))
+        try:
+            def measure(kind, t):
+                probe.set_tuning(0, t)
+                best = float("inf")
+                for rep in range(3):  # the first includes the graph capture
+                    torch.cuda.synchronize()
+                    a = time.perf_counter()
+                    probe.run(1.0, chunk=replays, max_replays=replays)
+                    torch.cuda.synchronize()
+                    if rep:
+                        best = min(best, time.perf_counter() - a)
+                return best
+
+            best, log = search(measure, N[0], tma_choices=(0,))
+        finally:
+            probe.free()
+        best["torque_tma"] = 0
+        ens.set_tuning(cls, best)
+        chosen[cls], logs[cls] = ens.get_tuning(cls), log
+        if use_cache:
+            c = load_cache(cache_path)
+            c[key] = chosen[cls]
+            save_cache(cache_path, c)
+    return chosen, logs

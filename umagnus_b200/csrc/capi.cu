@@ -238,6 +238,11 @@ int umag_ens_run(umag_ens* e, double seconds, int chunk, long long max_replays) 
     return ens_run(e, seconds, chunk, max_replays);
 }
 int umag_ens_count(umag_ens* e, int* n_instances, int* n_classes) { return ens_count(e, n_instances, n_classes); }
+int umag_ens_class_info(umag_ens* e, int cls, int N[3], int* n_instances) {
+    return ens_class_info(e, cls, N, n_instances);
+}
+int umag_ens_get_tuning(umag_ens* e, int cls, umag_tuning* t) { return ens_get_tuning(e, cls, t); }
+int umag_ens_set_tuning(umag_ens* e, int cls, const umag_tuning* t) { return ens_set_tuning(e, cls, t); }
 int umag_adj_new(const umag_adj_params* p, umag_adj** out) { return adj_new(p, out); }
 int umag_adj_free(umag_adj* a) { return adj_free(a); }
 int umag_adj_forward(umag_adj* a, const float* m0, const float* Ms, float Aex, float Ku1, const float B_ext[3],

@@ -1685,6 +1685,7 @@ struct EnsClass {
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     cudaGraphExec_t gexec = nullptr;  // graph_steps steps of the current batch
+    int gexec_nb = 0;                 // the batch size gexec was captured for
     bool busy = false, finished = false;
     long long replays = 0;
 };
@@ -1959,10 +1960,12 @@ int ens_get_state(umag_ens* h, int i, umag_solver_state* st) {
 
 // graph_steps steps of class C's current batch, captured on its stream
 static int ens_capture(EnsImpl* e, EnsClass& C) {
+    if (C.gexec && C.gexec_nb == C.s->nb) return UMAG_OK;  // still valid (shapes unchanged)
     if (C.gexec) { cudaGraphExecDestroy(C.gexec); C.gexec = nullptr; }
     g_launch_stream = C.st;
     const int st = capture_steps(C.s, e->graph_steps, &C.gexec);
     g_launch_stream = nullptr;
+    C.gexec_nb = st == UMAG_OK ? C.s->nb : 0;
     return st;
 }
 
@@ -2082,6 +2085,35 @@ int ens_count(umag_ens* h, int* n_instances, int* n_classes) {
     UMAG_REQUIRE(e, "NULL argument");
     if (n_instances) *n_instances = (int)e->where.size();
     if (n_classes) *n_classes = (int)e->cls.size();
+    return UMAG_OK;
+}
+
+int ens_class_info(umag_ens* h, int cls, int N[3], int* n_instances) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    UMAG_REQUIRE(e && N && n_instances, "NULL argument");
+    UMAG_REQUIRE(cls >= 0 && cls < (int)e->cls.size(), "class %d out of range", cls);
+    const SimImpl* s = e->cls[cls].s;
+    for (int i = 0; i < 3; i++) N[i] = s->p.N[i];
+    *n_instances = e->cls[cls].n_all;
+    return UMAG_OK;
+}
+
+int ens_get_tuning(umag_ens* h, int cls, umag_tuning* t) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    UMAG_REQUIRE(e && t, "NULL argument");
+    UMAG_REQUIRE(cls >= 0 && cls < (int)e->cls.size(), "class %d out of range", cls);
+    *t = e->cls[cls].s->tune;
+    return UMAG_OK;
+}
+
+// the class's launches take the new shapes at its next capture
+int ens_set_tuning(umag_ens* h, int cls, const umag_tuning* t) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    UMAG_REQUIRE(e && t, "NULL argument");
+    UMAG_REQUIRE(cls >= 0 && cls < (int)e->cls.size(), "class %d out of range", cls);
+    EnsClass& C = e->cls[cls];
+    UMAG_TRY(sim_set_tuning(reinterpret_cast<umag_sim*>(C.s), t));
+    if (C.gexec) { cudaGraphExecDestroy(C.gexec); C.gexec = nullptr; }
     return UMAG_OK;
 }
 

@@ -32,6 +32,9 @@ int ens_get_m(umag_ens* e, int i, float* host_m);
 int ens_get_state(umag_ens* e, int i, umag_solver_state* st);
 int ens_run(umag_ens* e, double seconds, int chunk, long long max_replays);
 int ens_count(umag_ens* e, int* n_instances, int* n_classes);
+int ens_class_info(umag_ens* e, int cls, int N[3], int* n_instances);
+int ens_get_tuning(umag_ens* e, int cls, umag_tuning* t);
+int ens_set_tuning(umag_ens* e, int cls, const umag_tuning* t);
 int adj_new(const umag_adj_params* p, umag_adj** out);
 int adj_free(umag_adj* a);
 int adj_forward(umag_adj* a, const float* m0, const float* Ms, float A, float K1, const float Bext[3], double* loss);

@@ -445,6 +445,37 @@ class Ensemble:
         check(self.L.umag_ens_count(self._h, ctypes.byref(n), ctypes.byref(c)))
         return c.value
 
+    def class_info(self, cls):
+        """(mesh N, number of instances) of class `cls` (classes numbered in
+        the order their first instance appears)."""
+        N = (ctypes.c_int * 3)()
+        n = ctypes.c_int()
+        check(self.L.umag_ens_class_info(self._h, int(cls), N, ctypes.byref(n)))
+        return tuple(N), n.value
+
+    def get_tuning(self, cls):
+        """Launch shapes of class `cls`'s batched per-cell kernels (a dict)."""
+        t = Tuning()
+        check(self.L.umag_ens_get_tuning(self._h, int(cls), ctypes.byref(t)))
+        return {"torque_block": [t.torque_block[0], t.torque_block[1]], "stage_threads": t.stage_threads,
+                "stage_waves": t.stage_waves, "err_waves": t.err_waves, "torque_tma": t.torque_tma}
+
+    def set_tuning(self, cls, tuning):
+        """Apply launch shapes to class `cls` (speed only; results unchanged)."""
+        t = Tuning()
+        t.torque_block[0], t.torque_block[1] = (int(v) for v in tuning["torque_block"])
+        t.stage_threads, t.stage_waves, t.err_waves = (int(tuning[k]) for k in ("stage_threads", "stage_waves",
+                                                                                "err_waves"))
+        t.torque_tma = int(tuning.get("torque_tma", 0))
+        torch.cuda.synchronize()
+        check(self.L.umag_ens_set_tuning(self._h, int(cls), ctypes.byref(t)))
+
+    def autotune(self, instances, cache_path=None, use_cache=True):
+        """Launch shapes of every class from umagnus_b200.autotune.tune_ensemble
+        (`instances`: the list this ensemble was made from)."""
+        from . import autotune
+        return autotune.tune_ensemble(self, instances, cache_path=cache_path, use_cache=use_cache)
+
     def set_m(self, i, m):
         a = np.ascontiguousarray(np.asarray(m, np.float32).reshape(self.shapes[i]))
         check(self.L.umag_ens_set_m(self._h, int(i), a.ctypes.data))

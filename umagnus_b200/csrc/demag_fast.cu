@@ -578,7 +578,7 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
         }
     }
     __syncthreads();
-    rg_fft_fwd<M, 1, true, 4>(v, t, ex + z * S::LX, 0, twx);
+    rg_fft_fwd<M, 1, true, 4, rg_radix(M, 0) == 8>(v, t, ex + z * S::LX, 0, twx);  // n >= M/2 is zero padding
     // R2C unpack: partner element Z[M-k] lives in lane (TX - t) % TX, element 7-j
     // (or (8-j) & 7 for t = 0); exchanged with warp shuffles.
     const int lane = threadIdx.x & 31;

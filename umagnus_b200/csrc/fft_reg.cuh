@@ -14,6 +14,7 @@
 // ignores elements.  Radices 8, then 4 or 2 for the remaining power of two.
 #pragma once
 #include "fft.cuh"
+#include "fft_packed.cuh"
 
 namespace umag {
 
@@ -50,9 +51,10 @@ template <bool WARP> __device__ __forceinline__ void rg_sync() {
 
 // One stage for NC lines held by this thread (v[c][m] = element t + T*m of
 // line c).  ex + c*exs is the padded exchange line of component c.
-template <int L, int NC, int DIR, int ST, int NS, bool WARP = false, int PS = 3>
+template <int L, int NC, int DIR, int ST, int NS, bool WARP = false, int PS = 3, bool ZH = false>
 __device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, int exs,
                                          const float2* __restrict__ tw) {
+    static_assert(DIR == -1, "forward transforms only (the inverse is the forward of the conjugate)");
     if constexpr (ST < rg_nst(L)) {
         constexpr int R = rg_radix(L, ST);
         constexpr int NB = 8 / R;          // butterflies per thread
@@ -63,36 +65,42 @@ __device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, 
         for (int i = 0; i < NB; i++) {
             const int j = t + T * i;
             const int k = j % NS;
-            // twiddles are shared by the NC lines: read them once
-            float2 w[R];
+            // twiddles are shared by the NC lines: read them once, as the
+            // pairs (w.re, w.re) and (-w.im, w.im) of the packed product
+            P2 wrr[R], wii[R];
             if constexpr (NS > 1) {
 #pragma unroll
-                for (int r = 1; r < R; r++) w[r] = rg_tw<DIR>(tw, r * k * TWS);
+                for (int r = 1; r < R; r++) {
+                    const float2 w = rg_tw<DIR>(tw, r * k * TWS);
+                    wrr[r] = p2(w.x, w.x);
+                    wii[r] = p2(-w.y, w.y);
+                }
             }
 #pragma unroll
             for (int c = 0; c < NC; c++) {
-                float2 u[R];
+                P2 u[R];
 #pragma unroll
-                for (int r = 0; r < R; r++) u[r] = v[c][i + r * NB];
+                for (int r = 0; r < R; r++) u[r] = p2(v[c][i + r * NB]);
                 if constexpr (NS > 1) {
 #pragma unroll
-                    for (int r = 1; r < R; r++) u[r] = cmul(u[r], w[r]);
+                    for (int r = 1; r < R; r++) u[r] = pcmul(u[r], wrr[r], wii[r]);
                 }
-                if constexpr (R == 2) dft2(u);
-                else if constexpr (R == 4) dft4(u, DIR);
-                else dft8<float>(u, DIR);
+                if constexpr (R == 8 && ZH && ST == 0) pdft8_zhalf(u);
+                else if constexpr (R == 2) pdft2(u);
+                else if constexpr (R == 4) pdft4(u);
+                else pdft8(u);
                 if constexpr (last) {
 #pragma unroll
-                    for (int q = 0; q < R; q++) v[c][i + q * NB] = u[q];
+                    for (int q = 0; q < R; q++) v[c][i + q * NB] = f2(u[q]);
                 } else {
                     const int o = (j / NS) * NS * R + k;
                     if constexpr (NS % (1 << PS) == 0) {  // pad(o + q*NS) = pad(o) + q*pad(NS)
                         float2* base = ex + c * exs + rg_pad<PS>(o);
 #pragma unroll
-                        for (int q = 0; q < R; q++) base[q * (NS + (NS >> PS))] = u[q];
+                        for (int q = 0; q < R; q++) base[q * (NS + (NS >> PS))] = f2(u[q]);
                     } else {
 #pragma unroll
-                        for (int q = 0; q < R; q++) ex[c * exs + rg_pad<PS>(o + q * NS)] = u[q];
+                        for (int q = 0; q < R; q++) ex[c * exs + rg_pad<PS>(o + q * NS)] = f2(u[q]);
                     }
                 }
             }
@@ -112,7 +120,7 @@ __device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, 
                     for (int m = 0; m < 8; m++) v[c][m] = ex[c * exs + rg_pad<PS>(t + T * m)];
             }
             rg_sync<WARP>();
-            rg_stage<L, NC, DIR, ST + 1, NS * R, WARP, PS>(v, t, ex, exs, tw);
+            rg_stage<L, NC, DIR, ST + 1, NS * R, WARP, PS, ZH>(v, t, ex, exs, tw);
         }
     }
 }
@@ -140,6 +148,7 @@ __device__ __forceinline__ void dft8_zhalf(float2* v) {
 // buffer is rewritten only after a barrier that follows every read of it.
 // Two buffers instead of NC, and one barrier per line and stage.  ZH: the
 // upper half of the input is zero (the first radix-8 butterfly folds it).
+// The butterflies and twiddle products run in packed FP32 (fft_packed.cuh).
 template <int L, int NC, int ST, int NS, int P, bool ZH>
 __device__ __forceinline__ void rg_stage_seq(float2 (&v)[NC][8], int t, float2* ex, int exs,
                                              const float2* __restrict__ tw) {
@@ -153,26 +162,30 @@ __device__ __forceinline__ void rg_stage_seq(float2 (&v)[NC][8], int t, float2* 
 #pragma unroll
         for (int i = 0; i < NB; i++) {
             const int k = (t + T * i) % NS;
-            float2 w[R];
+            P2 wrr[R], wii[R];  // twiddle w as (w.re, w.re) and (-w.im, w.im)
             if constexpr (NS > 1) {
 #pragma unroll
-                for (int r = 1; r < R; r++) w[r] = rg_tw<-1>(tw, r * k * TWS);
+                for (int r = 1; r < R; r++) {
+                    const float2 w = rg_tw<-1>(tw, r * k * TWS);
+                    wrr[r] = p2(w.x, w.x);
+                    wii[r] = p2(-w.y, w.y);
+                }
             }
 #pragma unroll
             for (int c = 0; c < NC; c++) {
-                float2 u[R];
+                P2 u[R];
 #pragma unroll
-                for (int r = 0; r < R; r++) u[r] = v[c][i + r * NB];
+                for (int r = 0; r < R; r++) u[r] = p2(v[c][i + r * NB]);
                 if constexpr (NS > 1) {
 #pragma unroll
-                    for (int r = 1; r < R; r++) u[r] = cmul(u[r], w[r]);
+                    for (int r = 1; r < R; r++) u[r] = pcmul(u[r], wrr[r], wii[r]);
                 }
-                if constexpr (R == 8 && ZH && ST == 0) dft8_zhalf(u);
-                else if constexpr (R == 2) dft2(u);
-                else if constexpr (R == 4) dft4(u, -1);
-                else dft8<float>(u, -1);
+                if constexpr (R == 8 && ZH && ST == 0) pdft8_zhalf(u);
+                else if constexpr (R == 2) pdft2(u);
+                else if constexpr (R == 4) pdft4(u);
+                else pdft8(u);
 #pragma unroll
-                for (int q = 0; q < R; q++) v[c][i + q * NB] = u[q];
+                for (int q = 0; q < R; q++) v[c][i + q * NB] = f2(u[q]);
             }
         }
         if constexpr (!last) {
@@ -220,11 +233,15 @@ __device__ __forceinline__ void rg_fft_fwd_seq(float2 (&v)[NC][8], int t, float2
 
 // Unnormalised forward FFT (DIR = -1) of NC lines.  All threads that share
 // the exchange lines must call it: the whole CTA, or (WARP = true) one warp.
-template <int L, int NC, bool WARP = false, int PS = 3>
+// ZH: the upper half of every line is zero (elements m >= 4 of each thread;
+// the first radix-8 butterfly folds them).  Packed FP32 butterflies
+// (fft_packed.cuh).
+template <int L, int NC, bool WARP = false, int PS = 3, bool ZH = false>
 __device__ __forceinline__ void rg_fft_fwd(float2 (&v)[NC][8], int t, float2* ex, int exs,
                                            const float2* __restrict__ tw) {
     static_assert(rg_ok(L), "register FFT needs a power-of-two length >= 8");
-    rg_stage<L, NC, -1, 0, 1, WARP, PS>(v, t, ex, exs, tw);
+    static_assert(!ZH || rg_radix(L, 0) == 8, "the folded first stage is radix 8");
+    rg_stage<L, NC, -1, 0, 1, WARP, PS, ZH>(v, t, ex, exs, tw);
 }
 
 }  // namespace umag

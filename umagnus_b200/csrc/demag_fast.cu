@@ -355,12 +355,14 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                  : "memory");
 }
 
-// Shared memory of a pass-B CTA (k_reg_b): twiddles, two exchange buffers of
-// WB padded lines, the kernel block [6][WB/KW][HY][KW] (KW = 4 columns per
-// 16-byte piece, or WB when narrower).
+// Shared memory of a pass-B CTA (k_reg_b): the staged twiddle tables (TWN
+// slots, an even count so what follows stays 16-byte aligned), two exchange
+// buffers of WB padded lines, the kernel block [6][WB/KW][HY][KW] (KW = 4
+// columns per 16-byte piece, or WB when narrower).
 template <int PY, int WB> struct RegBShape {
     static constexpr int KW = WB >= 4 ? 4 : WB;
-    static constexpr size_t smem = sizeof(float2) * ((size_t)PY + (size_t)2 * WB * rg_line<PY>()) +
+    static constexpr int TWN = (RgTw<PY>::size + 1) & ~1;
+    static constexpr size_t smem = sizeof(float2) * ((size_t)TWN + (size_t)2 * WB * rg_line<PY>()) +
                                    sizeof(float) * (size_t)6 * (PY / 2 + 1) * WB;
     // three CTAs per SM (80 registers) up to Py = 512; longer lines hold more
     // live state per thread and keep two
@@ -385,8 +387,8 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     constexpr int LP = rg_line<PY>();
     constexpr int KW = RegBShape<PY, WB>::KW;
     extern __shared__ __align__(16) float2 sm[];
-    float2* tw = sm;                  // PY twiddles
-    float2* ex = tw + PY;             // [2][WB][LP] exchange lines
+    float2* tw = sm;                                 // staged twiddles (RgTw<PY>)
+    float2* ex = tw + RegBShape<PY, WB>::TWN;        // [2][WB][LP] exchange lines
     float* Ks = reinterpret_cast<float*>(ex + 2 * WB * LP);  // [6][WB/KW][HY][KW] kernel block
     __shared__ __align__(8) uint64_t kbar;
     if (inst_inactive(a, ib)) return;
@@ -399,7 +401,7 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     // carries Pz/WB such CTAs instead of Pz mostly idle ones.
     const bool nyq = bx * WB == hx - 1 && WB > 1 && Pz % WB == 0 && Pz >= WB;
     if (nyq && by * WB >= Pz) return;
-    for (int i = tid; i < PY; i += NT) tw[i] = a.fy.tw[i];
+    rg_tw_fill<PY>(tw, a.fy.tw, tid, NT);
     const int kx0 = bx * WB;
     const int kx = nyq ? hx - 1 : kx0 + w, kz = nyq ? by * WB + w : by;
     auto kz_mirror = [&](int z) { return z > Pz / 2 ? Pz - z : z; };
@@ -523,12 +525,17 @@ __global__ void __launch_bounds__((PY / 8) * WB, RegBShape<PY, WB>::minb) k_reg_
 // ---- passes A and C with the register-blocked FFT (3D, power-of-two sizes)
 // x transform: TX = M/8 threads per row (one row per warp or less), rows z
 // of one (y, component) slab; z transform: TZ = PZ/8 threads per column.
+// Shared memory: staged x and z twiddle tables (RgTw; even slot counts keep
+// the later regions 16-byte aligned), the R2C twiddles twr (M), the rows Xs
+// [NZ][XP] and the exchange lines (x: one line of LX slots per row, padded
+// rg_pad<4> after the first stage and rg_pad<4, 2> after the later ones).
 template <int M, int PZ> struct RegAC {
     static constexpr int NZ = nz_of_pz(PZ), TX = M / 8, TZ = PZ / 8, NT = NZ * TX, CPR = NT / TZ;
     static constexpr int XP = ((M + 1 + 11) / 16) * 16 + 4;  // Xs row pitch, = 4 (mod 16) against bank conflicts
-    static constexpr int LX = rg_line<M, 4>(), LZ = rg_line<PZ, 3>();
+    static constexpr int LX = rg_line<M, 4, 2>(), LZ = rg_line<PZ, 3>();
+    static constexpr int TWX = (RgTw<M>::size + 1) & ~1, TWZ = (RgTw<PZ>::size + 1) & ~1;
     static constexpr int EXN = NZ * LX > CPR * LZ ? NZ * LX : CPR * LZ;
-    static constexpr size_t smem = sizeof(float2) * ((size_t)2 * M + PZ + (size_t)NZ * XP + EXN);
+    static constexpr size_t smem = sizeof(float2) * ((size_t)TWX + TWZ + M + (size_t)NZ * XP + EXN);
     static constexpr bool ok = rg_ok(M) && rg_ok(PZ) && TX <= 32 && PZ % 2 == 0 && NT % TZ == 0 && NT <= 1024;
 };
 
@@ -537,15 +544,16 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
     using S = RegAC<M, PZ>;
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
     extern __shared__ __align__(16) float2 sm[];
-    float2* twx = sm;          // M
-    float2* twz = twx + M;     // PZ
-    float2* twr = twz + PZ;    // M: exp(-2 pi i k / Px)
-    float2* Xs = twr + M;      // [NZ][XP]
+    float2* twx = sm;             // staged x twiddles (RgTw<M>)
+    float2* twz = twx + S::TWX;   // staged z twiddles (RgTw<PZ>)
+    float2* twr = twz + S::TWZ;   // M: exp(-2 pi i k / Px)
+    float2* Xs = twr + M;         // [NZ][XP]
     float2* ex = Xs + NZ * XP; // exchange lines
     if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
-    for (int i = tid; i < M; i += NT) { twx[i] = a.fx.tw[i]; twr[i] = a.twr[i]; }
-    for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
+    for (int i = tid; i < M; i += NT) twr[i] = a.twr[i];
+    rg_tw_fill<M>(twx, a.fx.tw, tid, NT);
+    if constexpr (PZ != 16 && PZ != 32) rg_tw_fill<PZ>(twz, a.fz.tw, tid, NT);  // (the pair z phase has none)
     const int y = bx, c = by, Ny = a.Ny;
     const float* __restrict__ mp = inst_m(a, ib, c);
     const float msm = inst_msmul(a, ib);
@@ -578,7 +586,7 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
         }
     }
     __syncthreads();
-    rg_fft_fwd<M, 1, true, 4, rg_radix(M, 0) == 8>(v, t, ex + z * S::LX, 0, twx);  // n >= M/2 is zero padding
+    rg_fft_fwd<M, 1, true, 4, rg_radix(M, 0) == 8, 2>(v, t, ex + z * S::LX, 0, twx);  // n >= M/2 is zero padding
     // R2C unpack: partner element Z[M-k] lives in lane (TX - t) % TX, element 7-j
     // (or (8-j) & 7 for t = 0); exchanged with warp shuffles.
     const int lane = threadIdx.x & 31;
@@ -713,8 +721,8 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
     extern __shared__ __align__(128) float2 sm[];
     float2* twx = sm;
-    float2* twz = twx + M;
-    float2* twr = twz + PZ;
+    float2* twz = twx + S::TWX;
+    float2* twr = twz + S::TWZ;
     float2* Xs = twr + M;
     float2* ex = Xs + NZ * XP;
     if (inst_inactive(a, ib)) return;
@@ -728,8 +736,9 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
     // whole number of float2)
     const bool slab = kSlabShape && a.slab_map != nullptr && ib == 0 && (smem_u32(Xs) & 15u) == 0;
     if (slab && tid == 0) mbar_init(&slab_bar, 1);
-    for (int i = tid; i < M; i += NT) { twx[i] = a.fx.tw[i]; twr[i] = a.twr[i]; }
-    for (int i = tid; i < PZ; i += NT) twz[i] = a.fz.tw[i];
+    for (int i = tid; i < M; i += NT) twr[i] = a.twr[i];
+    rg_tw_fill<M>(twx, a.fx.tw, tid, NT);
+    if constexpr (PZ != 16 && PZ != 32) rg_tw_fill<PZ>(twz, a.fz.tw, tid, NT);  // (the pair z phase has none)
     __syncthreads();
     const int y = bx, c = by, Ny = a.Ny;
     const int KB = a.Lx >> 2;  // four-column blocks per kz row of the slab
@@ -750,15 +759,18 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
     const long kzs = (long)Ny * a.Lx;
     if constexpr (PZ == 16 || PZ == 32) {
         // z phase on lane pairs, inverse by the conjugate trick, decimation in
-        // time: lane t transforms the samples kz = 2j + t (u = conj G), lane 1
-        // scales by W_PZ^k, and the kept outputs z < PZ/2 are
-        // X[z] = A[z] + W^z B[z]; lane 0 forms z < PZ/4 and lane 1 the rest,
+        // time: partner t transforms the samples kz = 2j + t (u = conj G),
+        // partner 1 scales by W_PZ^k, and the kept outputs z < PZ/2 are
+        // X[z] = A[z] + W^z B[z]; partner 0 forms z < PZ/4 and 1 the rest,
         // exchanging one value per output by shuffle.  The DC and Nyquist
         // columns invert to real sequences and share one transform of
         // G0 + i GM (real part -> column 0, imaginary -> column M).
         constexpr int E2 = PZ / 2, H2 = E2 / 2, CP2 = NT / 2;
         static_assert(E2 == NZ && M % CP2 == 0, "pair z phase");
-        const int t2 = tid & 1, cl2 = tid >> 1;
+        // pair partners are lanes l and l ^ 16: a half-warp reads and writes 16
+        // consecutive columns of one row (conflict-free in shared memory)
+        static_assert(NT % 32 == 0, "whole warps of lane pairs");
+        const int t2 = (tid >> 4) & 1, cl2 = ((tid >> 5) << 4) | (tid & 15);
         const long kM = spec_col(a, M);
 #pragma unroll
         for (int r0 = 0; r0 < M / CP2; r0++) {
@@ -787,8 +799,8 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
             for (int i = 0; i < H2; i++) {
                 const float2 snd = t2 ? u[i] : u[H2 + i];
                 float2 rcv;
-                rcv.x = __shfl_xor_sync(0xffffffffu, snd.x, 1);
-                rcv.y = __shfl_xor_sync(0xffffffffu, snd.y, 1);
+                rcv.x = __shfl_xor_sync(0xffffffffu, snd.x, 16);
+                rcv.y = __shfl_xor_sync(0xffffffffu, snd.y, 16);
                 const float2 own = t2 ? u[H2 + i] : u[i];
                 const float2 X = make_float2(own.x + rcv.x, own.y + rcv.y);
                 const int z = i + H2 * t2;
@@ -856,7 +868,7 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
         const float2 T1 = make_float2(W.x * D1.x + W.y * D1.y, W.x * D1.y - W.y * D1.x);
         v[0][j] = make_float2(S1.x - T1.y, -(S1.y + T1.x));  // conj(Z[k])
     }
-    rg_fft_fwd<M, 1, true, 4>(v, t, ex + z * S::LX, 0, twx);
+    rg_fft_fwd<M, 1, true, 4, false, 2>(v, t, ex + z * S::LX, 0, twx);
     float* __restrict__ B = inst_B(a, ib, c);
     const int rowo = (z * Ny + y) * M;
 #pragma unroll

@@ -25,21 +25,51 @@ constexpr int rg_radix(int L, int s) {
     return (s < rg_log2(L) / 3) ? 8 : (rg_log2(L) % 3 == 1 ? 2 : 4);
 }
 constexpr bool rg_ok(int L) { return L >= 8 && (L & (L - 1)) == 0; }
-// padded shared-memory index: one slot of padding after every 2^PS elements
-// (PS = 3 when threads of several lines share a warp, 4 for one line per
-// warp: the choices with the fewest 8-byte bank conflicts for these access
-// patterns)
-template <int PS> __host__ __device__ constexpr int rg_pad(int i) { return i + (i >> PS); }
+// padded shared-memory index: MU slots of padding after every 2^PS elements.
+// An 8-byte access of a warp is served as two half-warps of 16 lanes, each
+// one wavefront when its lanes fall in 16 different 8-byte bank pairs.  PS =
+// 3 when threads of several lines share a warp; 4 for one line per warp,
+// where the exchanges after the first stage (outputs spaced NS = 8, 64 ...
+// apart) take MU = 2 -- the choices that make these access patterns
+// conflict-free.
+template <int PS, int MU = 1> __host__ __device__ constexpr int rg_pad(int i) { return i + (i >> PS) * MU; }
 // exchange-line stride: padded length rounded up to 4 (mod 16) 8-byte slots,
 // so lines accessed by neighbouring threads start in different banks
-template <int L, int PS = 3> __host__ __device__ constexpr int rg_line() {
-    return ((rg_pad<PS>(L - 1) + 1 + 11) / 16) * 16 + 4;
+template <int L, int PS = 3, int MU = 1> __host__ __device__ constexpr int rg_line() {
+    return ((rg_pad<PS, MU>(L - 1) + 1 + 11) / 16) * 16 + 4;
 }
 
-template <int DIR> __device__ __forceinline__ float2 rg_tw(const float2* __restrict__ tw, int e) {
-    float2 w = tw[e];
-    if (DIR > 0) w.y = -w.y;
-    return w;
+// Staged twiddle tables.  Stage s >= 1 multiplies element r of butterfly k
+// (k < NS, the product of the earlier radices; radix R) by W_L^(r k L/(NS R)).
+// Read from one length-L table, lanes with different k would share banks
+// (index strides r*L/(NS R)); the staged tables hold the twiddles of stage s
+// as rows k of R + 1 slots (entries r = 1..R-1 used), an odd pitch, so the
+// lanes of a stage read different banks.
+template <int L> struct RgTw {
+    static constexpr int nst = (rg_log2(L) + 2) / 3;
+    static constexpr int radix(int s) { return s < rg_log2(L) / 3 ? 8 : (rg_log2(L) % 3 == 1 ? 2 : 4); }
+    static constexpr int ns(int s) { return s == 0 ? 1 : ns(s - 1) * radix(s - 1); }
+    static constexpr int pitch(int s) { return radix(s) + 1; }
+    static constexpr int offset(int s) { return s <= 1 ? 0 : offset(s - 1) + ns(s - 1) * pitch(s - 1); }
+    static constexpr int size = nst <= 1 ? 1 : offset(nst);
+};
+
+// Fill the staged tables of RgTw<L> from tw (tw[j] = exp(-2 pi i j / L),
+// j < L; any memory space) by threads tid = 0..nth-1, stage by stage with
+// compile-time shapes; the caller synchronises before the transform reads
+// them.
+template <int L, int S = 1>
+__device__ __forceinline__ void rg_tw_fill(float2* tws, const float2* __restrict__ tw, int tid, int nth) {
+    using G = RgTw<L>;
+    if constexpr (S < G::nst) {
+        constexpr int R = G::radix(S), P = G::pitch(S), N = G::ns(S) * P, STEP = L / (G::ns(S) * R);
+        constexpr int OFF = G::offset(S);
+        for (int e = tid; e < N; e += nth) {
+            const int k = e / P, r = e - k * P;
+            tws[OFF + e] = r < R ? tw[r * k * STEP] : make_float2(0.f, 0.f);
+        }
+        rg_tw_fill<L, S + 1>(tws, tw, tid, nth);
+    }
 }
 
 // Barrier between exchange phases: the whole CTA, or only the warp when all
@@ -50,8 +80,10 @@ template <bool WARP> __device__ __forceinline__ void rg_sync() {
 }
 
 // One stage for NC lines held by this thread (v[c][m] = element t + T*m of
-// line c).  ex + c*exs is the padded exchange line of component c.
-template <int L, int NC, int DIR, int ST, int NS, bool WARP = false, int PS = 3, bool ZH = false>
+// line c).  ex + c*exs is the padded exchange line of component c; the
+// exchange after stage 0 pads by rg_pad<PS>, the later ones by rg_pad<PS, MU>.
+// tw: the staged twiddle tables of RgTw<L>.
+template <int L, int NC, int DIR, int ST, int NS, bool WARP = false, int PS = 3, bool ZH = false, int MU = 1>
 __device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, int exs,
                                          const float2* __restrict__ tw) {
     static_assert(DIR == -1, "forward transforms only (the inverse is the forward of the conjugate)");
@@ -59,7 +91,7 @@ __device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, 
         constexpr int R = rg_radix(L, ST);
         constexpr int NB = 8 / R;          // butterflies per thread
         constexpr int T = L / 8;
-        constexpr int TWS = L / (NS * R);
+        constexpr int U = ST == 0 ? 1 : MU;  // padding slots of this stage's exchange
         constexpr bool last = (ST + 1 == rg_nst(L));
 #pragma unroll
         for (int i = 0; i < NB; i++) {
@@ -69,9 +101,12 @@ __device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, 
             // pairs (w.re, w.re) and (-w.im, w.im) of the packed product
             P2 wrr[R], wii[R];
             if constexpr (NS > 1) {
+                using G = RgTw<L>;
+                static_assert(G::radix(ST) == R && G::ns(ST) == NS, "staged twiddle layout");
+                const float2* wk = tw + G::offset(ST) + k * G::pitch(ST);
 #pragma unroll
                 for (int r = 1; r < R; r++) {
-                    const float2 w = rg_tw<DIR>(tw, r * k * TWS);
+                    const float2 w = wk[r];
                     wrr[r] = p2(w.x, w.x);
                     wii[r] = p2(-w.y, w.y);
                 }
@@ -95,12 +130,12 @@ __device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, 
                 } else {
                     const int o = (j / NS) * NS * R + k;
                     if constexpr (NS % (1 << PS) == 0) {  // pad(o + q*NS) = pad(o) + q*pad(NS)
-                        float2* base = ex + c * exs + rg_pad<PS>(o);
+                        float2* base = ex + c * exs + rg_pad<PS, U>(o);
 #pragma unroll
-                        for (int q = 0; q < R; q++) base[q * (NS + (NS >> PS))] = f2(u[q]);
+                        for (int q = 0; q < R; q++) base[q * rg_pad<PS, U>(NS)] = f2(u[q]);
                     } else {
 #pragma unroll
-                        for (int q = 0; q < R; q++) ex[c * exs + rg_pad<PS>(o + q * NS)] = f2(u[q]);
+                        for (int q = 0; q < R; q++) ex[c * exs + rg_pad<PS, U>(o + q * NS)] = f2(u[q]);
                     }
                 }
             }
@@ -108,19 +143,19 @@ __device__ __forceinline__ void rg_stage(float2 (&v)[NC][8], int t, float2* ex, 
         if constexpr (!last) {
             rg_sync<WARP>();
             if constexpr (T % (1 << PS) == 0) {  // pad(t + T*m) = pad(t) + m*pad(T)
-                const float2* base = ex + rg_pad<PS>(t);
+                const float2* base = ex + rg_pad<PS, U>(t);
 #pragma unroll
                 for (int c = 0; c < NC; c++)
 #pragma unroll
-                    for (int m = 0; m < 8; m++) v[c][m] = base[c * exs + m * (T + (T >> PS))];
+                    for (int m = 0; m < 8; m++) v[c][m] = base[c * exs + m * rg_pad<PS, U>(T)];
             } else {
 #pragma unroll
                 for (int c = 0; c < NC; c++)
 #pragma unroll
-                    for (int m = 0; m < 8; m++) v[c][m] = ex[c * exs + rg_pad<PS>(t + T * m)];
+                    for (int m = 0; m < 8; m++) v[c][m] = ex[c * exs + rg_pad<PS, U>(t + T * m)];
             }
             rg_sync<WARP>();
-            rg_stage<L, NC, DIR, ST + 1, NS * R, WARP, PS, ZH>(v, t, ex, exs, tw);
+            rg_stage<L, NC, DIR, ST + 1, NS * R, WARP, PS, ZH, MU>(v, t, ex, exs, tw);
         }
     }
 }
@@ -157,16 +192,18 @@ __device__ __forceinline__ void rg_stage_seq(float2 (&v)[NC][8], int t, float2* 
         constexpr int R = rg_radix(L, ST);
         constexpr int NB = 8 / R;
         constexpr int T = L / 8;
-        constexpr int TWS = L / (NS * R);
         constexpr bool last = (ST + 1 == rg_nst(L));
 #pragma unroll
         for (int i = 0; i < NB; i++) {
             const int k = (t + T * i) % NS;
             P2 wrr[R], wii[R];  // twiddle w as (w.re, w.re) and (-w.im, w.im)
             if constexpr (NS > 1) {
+                using G = RgTw<L>;
+                static_assert(G::radix(ST) == R && G::ns(ST) == NS, "staged twiddle layout");
+                const float2* wk = tw + G::offset(ST) + k * G::pitch(ST);
 #pragma unroll
                 for (int r = 1; r < R; r++) {
-                    const float2 w = rg_tw<-1>(tw, r * k * TWS);
+                    const float2 w = wk[r];
                     wrr[r] = p2(w.x, w.x);
                     wii[r] = p2(-w.y, w.y);
                 }
@@ -221,7 +258,8 @@ __device__ __forceinline__ void rg_stage_seq(float2 (&v)[NC][8], int t, float2* 
 }
 
 // Forward FFT of NC lines held by the whole CTA, exchanged one line at a
-// time through two buffers (rg_stage_seq); ZH: zero upper half of the input.
+// time through two buffers (rg_stage_seq); ZH: zero upper half of the input;
+// tw: the staged twiddle tables of RgTw<L> (rg_tw_fill).
 // The caller must separate it by a barrier from any earlier use of the
 // buffers.
 template <int L, int NC, bool ZH>
@@ -234,14 +272,15 @@ __device__ __forceinline__ void rg_fft_fwd_seq(float2 (&v)[NC][8], int t, float2
 // Unnormalised forward FFT (DIR = -1) of NC lines.  All threads that share
 // the exchange lines must call it: the whole CTA, or (WARP = true) one warp.
 // ZH: the upper half of every line is zero (elements m >= 4 of each thread;
-// the first radix-8 butterfly folds them).  Packed FP32 butterflies
-// (fft_packed.cuh).
-template <int L, int NC, bool WARP = false, int PS = 3, bool ZH = false>
+// the first radix-8 butterfly folds them).  PS, MU: exchange padding
+// (rg_pad; lines of rg_line<L, PS, MU> slots).  tw: the staged twiddle
+// tables of RgTw<L> (rg_tw_fill).  Packed FP32 butterflies (fft_packed.cuh).
+template <int L, int NC, bool WARP = false, int PS = 3, bool ZH = false, int MU = 1>
 __device__ __forceinline__ void rg_fft_fwd(float2 (&v)[NC][8], int t, float2* ex, int exs,
                                            const float2* __restrict__ tw) {
     static_assert(rg_ok(L), "register FFT needs a power-of-two length >= 8");
     static_assert(!ZH || rg_radix(L, 0) == 8, "the folded first stage is radix 8");
-    rg_stage<L, NC, -1, 0, 1, WARP, PS, ZH>(v, t, ex, exs, tw);
+    rg_stage<L, NC, -1, 0, 1, WARP, PS, ZH, MU>(v, t, ex, exs, tw);
 }
 
 }  // namespace umag

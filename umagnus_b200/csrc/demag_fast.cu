@@ -626,8 +626,20 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
         // conj P[-k]) / 2i); P[-k] has the parity of k, so it is in the lane.
         constexpr int E2 = PZ / 2, CP2 = NT / 2;
         static_assert(E2 == NZ && M % CP2 == 0, "pair z phase");
-        const int t2 = tid & 1, cl2 = tid >> 1;
+        static_assert(NT % 32 == 0, "whole warps of lane pairs");
+        // pair partners are lanes l and l ^ 16: a half-warp reads and writes 16
+        // consecutive columns of one row
+        const int t2 = (tid >> 4) & 1, cl2 = ((tid >> 5) << 4) | (tid & 15);
         const long kM = spec_col(a, M);
+        // With one column per pair, the (y, component) slab of the blocked
+        // spectrum is assembled in the x/z scratch ([kz][kx/4][kx%4], 128-byte
+        // aligned; Xs is read into registers first) and written by one bulk
+        // tensor store (the slab map pass C loads with), not by 8-byte
+        // stores from every thread.
+        constexpr bool kSlabShape = M / CP2 == 1;
+        const bool slab = kSlabShape && a.slab_map != nullptr && ib == 0 && (smem_u32(Xs) & 15u) == 0;
+        const int KB = a.Lx >> 2;
+        float2* const sl = Xs + ((128u - (smem_u32(Xs) & 127u)) & 127u) / sizeof(float2);
 #pragma unroll
         for (int r0 = 0; r0 < M / CP2; r0++) {
             const int kx = r0 * CP2 + cl2;
@@ -639,20 +651,46 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
                 if (pk) q.y = Xs[n * XP + M].x;
                 u[n] = q;
             }
+            if (slab) __syncthreads();  // every Xs read is done before the slab overwrites it
             if (t2) tw_ramp<PZ, 1, 0, E2>(u);
             reg_dft<E2>(u);  // u[r] = X[2r + t2]
             if (pk) {
 #pragma unroll
                 for (int r = 0; r < E2; r++) {
                     const float2 P = u[r], Q = t2 ? u[E2 - 1 - r] : u[(E2 - r) & (E2 - 1)];
-                    const long o = (long)(2 * r + t2) * kzs;
-                    out[o] = make_float2(0.5f * (P.x + Q.x), 0.5f * (P.y - Q.y));
-                    out[o + kM] = make_float2(0.5f * (P.y + Q.y), -0.5f * (P.x - Q.x));
+                    const int kz = 2 * r + t2;
+                    const float2 X0 = make_float2(0.5f * (P.x + Q.x), 0.5f * (P.y - Q.y));
+                    const float2 XM = make_float2(0.5f * (P.y + Q.y), -0.5f * (P.x - Q.x));
+                    if (slab) {
+                        sl[kz * KB * 4] = X0;
+                        sl[(kz * KB + (M >> 2)) * 4 + (M & 3)] = XM;
+                    } else {
+                        out[(long)kz * kzs] = X0;
+                        out[(long)kz * kzs + kM] = XM;
+                    }
                 }
+            } else if (slab) {
+#pragma unroll
+                for (int r = 0; r < E2; r++) sl[((2 * r + t2) * KB + (kx >> 2)) * 4 + (kx & 3)] = u[r];
             } else {
                 const long ko = spec_col(a, kx);
 #pragma unroll
                 for (int r = 0; r < E2; r++) out[(long)(2 * r + t2) * kzs + ko] = u[r];
+            }
+        }
+        if (slab) {
+            // the block's padding columns M+1 .. 4 KB - 1 (read by no pass) as zeros
+            const int padc = 4 * KB - (M + 1);
+            for (int e = tid; e < PZ * padc; e += NT) {
+                const int kz = e / padc, kx = M + 1 + e % padc;
+                sl[(kz * KB + (kx >> 2)) * 4 + (kx & 3)] = make_float2(0.f, 0.f);
+            }
+            fence_proxy_async();
+            __syncthreads();
+            if (tid == 0) {
+                tma_store_5d(a.slab_map, sl, 0, y, 0, 0, c);
+                bulk_commit();
+                bulk_wait_read0();
             }
         }
     } else {

@@ -163,10 +163,16 @@ __device__ __forceinline__ f3 lltorque_g(f3 m, f3 H, float alpha, float gilb) {
 // coefficients are scalars and no region is loaded.  TILE (with UREG, not
 // BAT, non-periodic mesh): the CTA's magnetisation tile with its halo comes
 // into shared memory by one TMA load (tile.cuh) and the stencils read it.
-template <bool UREG, bool BAT, bool TILE>
+// UNI (with UREG, not BAT): a uniform material with only the common terms --
+// uniform Ms, alpha and anisotropy, precession on, and no NoDemagSpins,
+// bulk DMI, cubic anisotropy, thermal field, FreezeSpins or B_eff output --
+// so that those tests and branches leave the instruction stream; the
+// arithmetic is the same operations in the same order.
+template <bool UREG, bool BAT, bool TILE, bool UNI = false>
 __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ LocalArgs a,
                                                       const __grid_constant__ TileMaps tm) {
     static_assert(!TILE || (UREG && !BAT), "tiles: region-free, not batched");
+    static_assert(!UNI || (UREG && !BAT), "uniform material: region-free, not batched");
     // BAT: blockIdx.z = iz + Nz * instance; the instance's controller,
     // demag field and uniform parameters replace the shared ones
     static_assert(!BAT || UREG, "batched ensembles have no region maps");
@@ -223,7 +229,7 @@ __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ Lo
     f3 B{0.f, 0.f, 0.f};
     if (bd) B = f3{__ldg(bd + I), __ldg(bd + N + I), __ldg(bd + 2 * N + I)};
     // engine/demag.go:95-97: NoDemagSpins cells feel no demag field
-    if (!BAT && a.nodemag && __ldg(a.nodemag + (UREG ? 0 : __ldg(a.regions + I))) != 0.0f) B = f3{0.f, 0.f, 0.f};
+    if (!BAT && !UNI && a.nodemag && __ldg(a.nodemag + (UREG ? 0 : __ldg(a.regions + I))) != 0.0f) B = f3{0.f, 0.f, 0.f};
     f3 m0;
     if constexpr (TILE) m0 = tv.at(threadIdx.x, threadIdx.y, 0, 0, 0);
     else m0 = ld3(mx, my, mz, I);
@@ -232,7 +238,7 @@ __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ Lo
         if constexpr (TILE) {
             e = dmi ? dmi_sum_tile(tv, threadIdx.x, threadIdx.y, kc.pc, a.openbc != 0, a.g.Nz > 1, m0)
                     : exchange_sum_tile(tv, threadIdx.x, threadIdx.y, kc.pc, a.g.Nz > 1, m0);
-        } else if (!BAT && a.dbLUT) {  // engine/exchange.go:60-61 AddDMIBulk
+        } else if (!BAT && !UNI && a.dbLUT) {  // engine/exchange.go:60-61 AddDMIBulk
             e = dmibulk_sum(mx, my, mz, a.aLUT, a.dbLUT, a.regions, a.cx, a.cy, a.cz, a.g, a.openbc != 0, ix, iy,
                             iz, m0, UREG ? 0 : __ldg(a.regions + I));
         } else if constexpr (UREG) {
@@ -243,13 +249,13 @@ __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ Lo
             e = a.dmi ? dmi_sum_lut(mx, my, mz, a.dl, a.regions, a.g, a.openbc != 0, ix, iy, iz, m0, r0)
                       : exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0);
         }
-        float inv = (BAT || a.ms_uniform) ? kc.inv_ms : inv_msat(a.Ms, a.Ms_mul, I);
+        float inv = (BAT || UNI || a.ms_uniform) ? kc.inv_ms : inv_msat(a.Ms, a.Ms_mul, I);
         B.x = fa(B.x, fm(e.x, inv));
         B.y = fa(B.y, fm(e.y, inv));
         B.z = fa(B.z, fm(e.z, inv));
     }
     if (a.anis) {
-        if (BAT || a.anis_uniform) {  // uniaxialanisotropy2.cl:27-34 with the uniform factors hoisted
+        if (BAT || UNI || a.anis_uniform) {  // uniaxialanisotropy2.cl:27-34 with the uniform factors hoisted
             f3 u{kc.u[0], kc.u[1], kc.u[2]};
             float mu = dot3(m0, u);
             float f1 = fm(kc.f1k, mu);
@@ -261,7 +267,7 @@ __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ Lo
             add_uniaxial(B, a.up, m0, I);
         }
     }
-    if (!BAT && a.cubic) add_cubic(B, a.cp, m0, I);  // engine/anisotropy.go:158
+    if (!BAT && !UNI && a.cubic) add_cubic(B, a.cp, m0, I);  // engine/anisotropy.go:158
     if (a.zeeman) {
         if constexpr (BAT) {
             B.x = fa(B.x, ip->bext[0]);
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ Lo
             B.z = fa(B.z, __ldg(a.bext[2] + r));
         }
     }
-    if (!BAT && a.thermal) {  // engine/effectivefield.go:20-22 B_therm (temperature2.cl)
+    if (!BAT && !UNI && a.thermal) {  // engine/effectivefield.go:20-22 B_therm (temperature2.cl)
         const float sc = therm_scale(ctl->k2, amul(a.alpha, a.alpha_mul, I), amul(a.temp, a.temp_mul, I),
                                      inv_msat(a.Ms, a.Ms_mul, I));
         const f3 n = therm_normals(a.seed, ctl->nsteps, I);
@@ -282,13 +288,13 @@ __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ Lo
         B.y = fa(B.y, fm(n.y, sc));
         B.z = fa(B.z, fm(n.z, sc));
     }
-    if (a.beff) { a.beff[I] = B.x; a.beff[N + I] = B.y; a.beff[2 * N + I] = B.z; }
+    if (!UNI && a.beff) { a.beff[I] = B.x; a.beff[N + I] = B.y; a.beff[2 * N + I] = B.z; }
     f3 t;
-    if (!a.precess) t = llnoprecess(m0, B);
-    else if (BAT || a.alpha_uniform) t = lltorque_g(m0, B, alpha_mul, kc.gilb);
+    if (!UNI && !a.precess) t = llnoprecess(m0, B);
+    else if (BAT || UNI || a.alpha_uniform) t = lltorque_g(m0, B, alpha_mul, kc.gilb);
     else t = lltorque(m0, B, amul(a.alpha, a.alpha_mul, I));
     // engine/torque.go:348-352 FreezeSpins (zeromask.cl)
-    if (!BAT && a.frozen && __ldg(a.frozen + (UREG ? 0 : __ldg(a.regions + I))) != 0.0f) t = f3{0.f, 0.f, 0.f};
+    if (!BAT && !UNI && a.frozen && __ldg(a.frozen + (UREG ? 0 : __ldg(a.regions + I))) != 0.0f) t = f3{0.f, 0.f, 0.f};
     float* out = a.tau_direct ? a.tau_direct : ctl->k[a.out_slot];
     out[I] = t.x; out[N + I] = t.y; out[2 * N + I] = t.z;
 }
@@ -730,8 +736,13 @@ static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, flo
     la.beff = beff;
     const int bx = s->tune.torque_block[0], by = s->tune.torque_block[1];
     dim3 blk(bx, by, 1), grd((s->g.Nx + bx - 1) / bx, (s->g.Ny + by - 1) / by, s->g.Nz * s->nb);
+    // the uniform-material instantiation where every term it leaves out is off
+    const bool uni = s->zero_regions && !la.nodemag && !la.dbLUT && !la.cubic && !la.thermal && !beff &&
+                     !la.frozen && la.precess && la.alpha_uniform && la.ms_uniform && (!la.anis || la.anis_uniform);
     if (s->batched)
         k_local_torque<true, true, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
+    else if (s->zero_regions && s->tile_ok && s->tune.torque_tma && uni)
+        k_local_torque<true, false, true, true><<<grd, blk, tile_bytes(bx, by, s->g.Nz) + 128, S()>>>(la, s->tmaps);
     else if (s->zero_regions && s->tile_ok && s->tune.torque_tma)
         k_local_torque<true, false, true><<<grd, blk, tile_bytes(bx, by, s->g.Nz) + 128, S()>>>(la, s->tmaps);
     else if (s->zero_regions)

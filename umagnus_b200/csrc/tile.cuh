@@ -81,6 +81,23 @@ __device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// Bulk tensor store of a shared-memory box (the async proxy reads it): the
+// writers' stores are made visible to that proxy by fence_proxy_async before
+// the barrier that precedes the store; the issuing thread then commits the
+// group and waits until the box has been read before the memory is reused or
+// the CTA exits.  The global writes complete with the grid.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, const void* src, int c0, int c1, int c2, int c3,
+                                             int c4) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];\n" ::"l"(
+            reinterpret_cast<uint64_t>(map)),
+        "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(src))
+        : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+
 // cuTensorMapEncodeTiled from the driver (looked up once; no libcuda link)
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,

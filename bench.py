@@ -43,11 +43,11 @@ CONFIG = dict(N=(256, 256, 16), cell=(2e-9, 2e-9, 1e-9), Ms=1.1e6, Aex=1.6e-11, 
 METRIC = "RK45DP cell-updates/s (256x256x16 multilayer, FP32, Newell demag)"
 UNIT = "cell-updates/s"
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_reg_b<512,4> launch on
-# this workload (80,050,176 + 5,405,184 B), from one ncu --set full capture of
-# that launch with the two-buffer exchange and bulk-copied kernel block (cold
+# this workload (79,423,232 + 6,178,304 B), from one ncu --set full capture of
+# that launch with packed FP32 butterflies and staged twiddle tables (cold
 # cache: ncu flushes the caches between its passes)
-TRAFFIC_B = 85455360
-TRAFFIC_B_SOURCE = ("ncu capture of k_reg_b<512,4>, two-buffer exchange + bulk kernel block "
+TRAFFIC_B = 85601536
+TRAFFIC_B_SOURCE = ("ncu capture of k_reg_b<512,4>, packed FP32 butterflies + staged twiddle tables "
                     "(profiles/k_reg_b_multilayer_256x256x16.md)")
 
 
@@ -811,6 +811,35 @@ def run_adjoint(args):
 
 
 # ------------------------------------------------------------------ thin-film comparison workload
+def run_fieldevals(args):
+    """A short run of the multilayer's field + torque evaluations and of the
+    three demag passes one by one (--steps evaluations after --warmup): the
+    target for kernel profilers, whose launch list holds only these kernels.
+    Prints the evaluation and pass times (CUDA events)."""
+    import torch
+    from umagnus_b200 import engine
+    torch.cuda.set_device(0)
+    cfg = CONFIG
+    N = cfg["N"]
+    sim = engine.Simulation(N, cfg["cell"], cfg["Ms"], cfg["Aex"], cfg["alpha"], Dind=cfg["Dind"], Ku1=cfg["Ku1"],
+                            anisU=cfg["anisU"], B_ext=cfg["B_ext"], device=0)
+    sim.set_m(random_m(N, cfg["seed"]))
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream)
+    sim.torque_evals(max(args.warmup, 1))
+    stream.synchronize()
+    E = max(args.steps, 1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.torque_evals(E)
+    e1.record(stream)
+    e1.synchronize()
+    ms_pass = time_passes(N, cfg["cell"], cfg["Ms"], stream, reps=E)
+    print(json.dumps({"workload": "fieldevals", "N": list(N), "evals": E, "us_per_eval": e0.elapsed_time(e1) / E * 1e3,
+                      "us_per_pass": {k: v * 1e3 for k, v in ms_pass.items()}}))
+    return 0
+
+
 def run_film(args):
     """The plain thin film (64x64x1 cells of 4x4x3 nm, Ms 8e5 A/m, Aex
     1.3e-11 J/m, alpha 0.1, B_ext (0, 0, 10 mT), no anisotropy, m0 random
@@ -1062,7 +1091,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="multilayer: default launch shapes, no search")
     ap.add_argument("--ref-budget", type=float, default=90.0, help="seconds of timed CPU steps (reference arm)")
-    ap.add_argument("--workload", default="multilayer", choices=["multilayer", "ensemble", "adjoint", "precision", "film"])
+    ap.add_argument("--workload", default="multilayer",
+                    choices=["multilayer", "ensemble", "adjoint", "precision", "film", "fieldevals"])
     ap.add_argument("--adj-fp64", action="store_true", help="adjoint: compare with the FP64 oracle (minutes of CPU)")
     ap.add_argument("--adj-fd", action="store_true", help="adjoint: central differences of the FP32 forward")
     ap.add_argument("--adj-steps", type=int, default=0, help="adjoint: steps instead of 4000")
@@ -1089,6 +1119,8 @@ def main():
         return run_precision(args)
     if args.workload == "film":
         return run_film(args)
+    if args.workload == "fieldevals":
+        return run_fieldevals(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

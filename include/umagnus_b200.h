@@ -383,8 +383,8 @@ int umag_sim_set_tuning(umag_sim* s, const umag_tuning* t);
  * Each instance has its own mesh (instances with the same mesh and cell
  * size are batched into one set of launches), its own uniform material and
  * applied field, its own time, dt and step controller (the solver knobs of
- * `sp` are shared); Newell demag when enable_demag.  Regions, per-cell maps,
- * geometry masks and PBC are not supported here. */
+ * `sp` are shared); Newell demag when enable_demag.  Region maps, per-cell
+ * maps, geometry masks and PBC: general instances (umag_ens_new_general). */
 typedef struct {
     int N[3];
     double cell[3];
@@ -395,8 +395,21 @@ typedef struct {
 typedef struct umag_ens umag_ens;
 int umag_ens_new(int n, const umag_ens_instance* instances, const umag_solver_params* sp, int enable_demag,
                  umag_ens** out);
+/* As umag_ens_new, with general instances: where general[i] is not NULL,
+ * instance i is the simulation umag_sim_new would make from *general[i]
+ * (region maps and LUTs, per-cell parameters, geometry, PBC, thermal field,
+ * every term; enable_demag taken from it) and `instances[i]` is not read
+ * (`instances` may be NULL when every instance is general).  A general
+ * instance is a class of its own, stepped by the single-simulation kernels
+ * in its own CUDA graph on its own stream, concurrently with the other
+ * classes; its trajectory equals the lone simulation's bit for bit.  The
+ * device arrays *general[i] points to must stay valid until umag_ens_free.
+ * No counterpart in the reference (one simulation per process there). */
+int umag_ens_new_general(int n, const umag_ens_instance* instances, const umag_sim_params* const* general,
+                         const umag_solver_params* sp, int enable_demag, umag_ens** out);
 int umag_ens_free(umag_ens* e);
-/* host arrays of 3*N floats (SoA); set_m normalises (engine/magnetization.go:34) */
+/* host arrays of 3*N floats (SoA); set_m normalises (engine/magnetization.go:34;
+ * a general instance within its geometry) */
 int umag_ens_set_m(umag_ens* e, int i, const float* host_m);
 int umag_ens_get_m(umag_ens* e, int i, float* host_m);
 int umag_ens_get_state(umag_ens* e, int i, umag_solver_state* st);
@@ -412,6 +425,8 @@ int umag_ens_count(umag_ens* e, int* n_instances, int* n_classes);
  * first instance appears): the mesh and the number of instances of class
  * `cls`.  No counterpart in the reference. */
 int umag_ens_class_info(umag_ens* e, int cls, int N[3], int* n_instances);
+/* 1 when class `cls` is a general instance (umag_ens_new_general), else 0. */
+int umag_ens_class_general(umag_ens* e, int cls, int* general);
 /* Launch shapes of class `cls`'s batched per-cell kernels (the fields of
  * umag_tuning; the torque kernel of a batch reads global memory, so
  * torque_tma is ignored).  Speed only: every instance's arithmetic is the

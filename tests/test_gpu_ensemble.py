@@ -170,3 +170,74 @@ def test_ensemble_autotune_chooses_and_caches(tmp_path):
     assert chosen2 == chosen and all(v is None for v in logs2.values())
     ens.free()
     ens2.free()
+
+
+def _general_instances():
+    """Instances the batched kernels do not serve: a region map with
+    per-region exchange, Ms map and per-region applied field; a geometry
+    mask (disc); periodic boundaries with interfacial DMI; a thermal field."""
+    n = 32
+    shape = (1, n, n)
+    yy, xx = np.mgrid[0:n, 0:n]
+    regions = ((xx >= n // 2).astype(np.uint8) + 2 * (yy >= n // 2).astype(np.uint8)).reshape(shape)
+    ms_map = np.where(regions == 0, 8e5, 6e5).astype(np.float32)
+    bext = np.zeros((256, 3), np.float32)
+    bext[1] = (0.01, 0.0, 0.0)
+    bext[3] = (0.0, 0.02, 0.0)
+    disc = (((xx - n / 2 + 0.5) ** 2 + (yy - n / 2 + 0.5) ** 2) <= (n / 2 - 1) ** 2).astype(np.float32).reshape(shape)
+    base = dict(N=(n, n, 1), cell=(4e-9, 4e-9, 3e-9), alpha=0.1)
+    return [
+        dict(base, Msat=ms_map, Aex=[1.3e-11, 1.0e-11, 1.5e-11, 1.2e-11], regions=regions, B_ext=bext),
+        dict(base, Msat=8e5, Aex=1.3e-11, geom=disc, B_ext=(0.0, 0.0, 0.01)),
+        dict(base, Msat=9e5, Aex=1.2e-11, Dind=1e-3, pbc=(2, 0, 0), B_ext=(0.01, 0.01, 0.0)),
+        dict(base, Msat=8e5, Aex=1.3e-11, Temp=50.0, ThermSeed=5, B_ext=(0.0, 0.0, 0.02)),
+    ]
+
+
+def test_ensemble_general_instances_match_single_runs():
+    """General instances (region maps, geometry, PBC, thermal field) run in
+    an ensemble beside batched uniform ones; each ends bit for bit where the
+    same Simulation run alone ends, and the batched instances still match
+    theirs."""
+    from umagnus_b200 import engine
+    gen = _general_instances()
+    uni = [_inst(32, 8e5, 1.3e-11, 0.1, (0.0, 0.0, 0.01)), _inst(32, 1.1e6, 1.9e-11, 0.02, (0.0, 0.05, 0.05))]
+    insts = [uni[0], gen[0], gen[1], uni[1], gen[2], gen[3]]
+    assert [engine.Ensemble.is_general(d) for d in insts] == [False, True, True, False, True, True]
+    ens = engine.Ensemble(insts)
+    assert ens.classes() == 5  # the two uniform films share one batch
+    assert [ens.class_general(c) for c in range(5)] == [False, True, True, True, True]
+    ms = [G.random_unit(d["N"], 70 + k) for k, d in enumerate(insts)]
+    for k, m in enumerate(ms):
+        ens.set_m(k, m)
+    T = 2e-11
+    ens.run(T, chunk=2)
+    ens.run(T / 2, chunk=3)  # a second run continues every instance from its own time
+    for k, d in enumerate(insts):
+        sim = engine.Simulation(**d)
+        sim.set_m(ms[k])
+        sim.run(T)
+        sim.run(T / 2)
+        a, b = ens.state(k), sim.state()
+        assert (a["nsteps"], a["nundone"]) == (b["nsteps"], b["nundone"]), (k, a, b)
+        assert a["time"] == b["time"] and a["dt"] == b["dt"], (k, a, b)
+        np.testing.assert_array_equal(ens.get_m(k), sim.get_m().cpu().numpy())
+        sim.free()
+    ens.free()
+
+
+def test_ensemble_all_general_and_set_m_in_geometry():
+    """An ensemble of general instances only; set_m keeps a geometry's empty
+    cells at zero, as Simulation.set_m does."""
+    from umagnus_b200 import engine
+    gen = _general_instances()
+    ens = engine.Ensemble([gen[1], gen[1]])
+    assert ens.classes() == 2  # general instances never share a batch
+    m = G.random_unit(gen[1]["N"], 3)
+    ens.set_m(0, m)
+    sim = engine.Simulation(**gen[1])
+    sim.set_m(m)
+    np.testing.assert_array_equal(ens.get_m(0), sim.get_m().cpu().numpy())
+    assert np.all(ens.get_m(0)[:, gen[1]["geom"] == 0] == 0)
+    sim.free()
+    ens.free()

@@ -121,6 +121,8 @@ _SIGS = {
     "umag_ovf_write": [ctypes.c_char_p, P, P, ctypes.c_char_p, c_int], "umag_dump_write": [ctypes.c_char_p, P, P],
     "umag_format_float": [c_double, c_int, ctypes.c_char_p, c_int],
     "umag_ens_new": [c_int, P, P, c_int, ctypes.POINTER(c_void_p)], "umag_ens_free": [P],
+    "umag_ens_new_general": [c_int, P, P, P, c_int, ctypes.POINTER(c_void_p)],
+    "umag_ens_class_general": [P, c_int, ctypes.POINTER(c_int)],
     "umag_ens_set_m": [P, c_int, P], "umag_ens_get_m": [P, c_int, P], "umag_ens_get_state": [P, c_int, P],
     "umag_ens_run": [P, c_double, c_int, c_ll], "umag_ens_count": [P, ctypes.POINTER(c_int), ctypes.POINTER(c_int)],
     "umag_ens_class_info": [P, c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int)],

@@ -230,6 +230,10 @@ int umag_sim_set_tuning(umag_sim* s, const umag_tuning* t) { return sim_set_tuni
 int umag_ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int enable_demag, umag_ens** out) {
     return ens_new(n, in, sp, enable_demag, out);
 }
+int umag_ens_new_general(int n, const umag_ens_instance* in, const umag_sim_params* const* general,
+                         const umag_solver_params* sp, int enable_demag, umag_ens** out) {
+    return ens_new_general(n, in, general, sp, enable_demag, out);
+}
 int umag_ens_free(umag_ens* e) { return ens_free(e); }
 int umag_ens_set_m(umag_ens* e, int i, const float* host_m) { return ens_set_m(e, i, host_m); }
 int umag_ens_get_m(umag_ens* e, int i, float* host_m) { return ens_get_m(e, i, host_m); }
@@ -241,6 +245,7 @@ int umag_ens_count(umag_ens* e, int* n_instances, int* n_classes) { return ens_c
 int umag_ens_class_info(umag_ens* e, int cls, int N[3], int* n_instances) {
     return ens_class_info(e, cls, N, n_instances);
 }
+int umag_ens_class_general(umag_ens* e, int cls, int* general) { return ens_class_general(e, cls, general); }
 int umag_ens_get_tuning(umag_ens* e, int cls, umag_tuning* t) { return ens_get_tuning(e, cls, t); }
 int umag_ens_set_tuning(umag_ens* e, int cls, const umag_tuning* t) { return ens_set_tuning(e, cls, t); }
 int umag_adj_new(const umag_adj_params* p, umag_adj** out) { return adj_new(p, out); }

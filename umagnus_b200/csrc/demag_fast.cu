@@ -757,7 +757,7 @@ template <int M, int PZ>
 __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, const int by, const int ib) {
     using S = RegAC<M, PZ>;
     constexpr int NZ = S::NZ, TX = S::TX, TZ = S::TZ, NT = S::NT, CPR = S::CPR, XP = S::XP;
-    extern __shared__ __align__(128) float2 sm[];
+    extern __shared__ __align__(16) float2 sm[];
     float2* twx = sm;
     float2* twz = twx + S::TWX;
     float2* twr = twz + S::TWZ;

@@ -1688,6 +1688,10 @@ int sim_set_param(umag_sim* h, int which, const float* values, float mul) {
 // stop costing launches.  Every instance's arithmetic is unchanged.
 struct EnsClass {
     SimImpl* s = nullptr;
+    // a general instance: one simulation made by sim_new from a full
+    // umag_sim_params (region maps, per-cell maps, geometry, PBC, every
+    // term), stepped by the single-simulation kernels on the class's stream
+    bool general = false;
     std::vector<int> members;  // ensemble index of each batch slot
     float2* spec = nullptr;    // nb spectrum scratch copies
     float* params = nullptr;   // device: Ms[n_all], A00[n_all], D00[n_all]
@@ -1710,6 +1714,10 @@ struct EnsImpl {
 static void ens_class_free(EnsClass& c) {
     if (c.gexec) cudaGraphExecDestroy(c.gexec);
     c.gexec = nullptr;
+    if (c.s && c.general) {
+        sim_free(reinterpret_cast<umag_sim*>(c.s));
+        c.s = nullptr;
+    }
     if (c.s) {
         SimImpl* s = c.s;
         drop_graph(s);
@@ -1875,34 +1883,64 @@ static int ens_class_new(EnsClass& C, const umag_ens_instance* in, const std::ve
     return UMAG_OK;
 }
 
+// a class of one general instance: the simulation sim_new makes from the
+// full parameter record, with its own stream and completion event
+static int ens_class_new_general(EnsClass& C, int member, const umag_sim_params* p, const umag_solver_params* sp) {
+    C.general = true;
+    C.members = {member};
+    C.n_all = 1;
+    umag_sim* h = nullptr;
+    UMAG_TRY(sim_new(p, sp, &h));
+    C.s = reinterpret_cast<SimImpl*>(h);
+    UMAG_CUDA(cudaStreamCreateWithFlags(&C.st, cudaStreamNonBlocking));
+    UMAG_CUDA(cudaEventCreateWithFlags(&C.done, cudaEventDisableTiming));
+    return UMAG_OK;
+}
+
 int ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int demag, umag_ens** out) {
+    return ens_new_general(n, in, nullptr, sp, demag, out);
+}
+
+int ens_new_general(int n, const umag_ens_instance* in, const umag_sim_params* const* general,
+                    const umag_solver_params* sp, int demag, umag_ens** out) {
     UMAG_TRY(ensure_init());
-    UMAG_REQUIRE(n > 0 && in && sp && out, "bad argument");
+    UMAG_REQUIRE(n > 0 && sp && out, "bad argument");
     UMAG_REQUIRE(sp->solver >= 1 && sp->solver <= 5, "unknown solver");
+    for (int i = 0; i < n; i++)
+        UMAG_REQUIRE(in || (general && general[i]), "instance %d: no uniform record and no general parameters", i);
     EnsImpl* e = new EnsImpl();
     e->sp = *sp;
     e->where.resize(n);
     auto fail = [&](int code) { ens_free(reinterpret_cast<umag_ens*>(e)); return code; };
-    // classes: same mesh and cell size
+    // classes: same mesh and cell size; each general instance is a class of its own
     std::vector<std::vector<int>> groups;
+    std::vector<int> gen_of;  // class -> general instance, or -1
     for (int i = 0; i < n; i++) {
+        if (general && general[i]) {
+            e->where[i] = {(int)groups.size(), 0};
+            groups.push_back({i});
+            gen_of.push_back(i);
+            continue;
+        }
         const umag_ens_instance& r = in[i];
         if (r.N[0] <= 0 || r.N[1] <= 0 || r.N[2] <= 0) return fail(set_error(UMAG_E_ARG, "instance %d: bad mesh", i));
         if (!(r.Ms > 0) || !(r.Aex > 0)) return fail(set_error(UMAG_E_ARG, "instance %d: Ms and Aex must be > 0", i));
         int g = -1;
         for (size_t k = 0; k < groups.size(); k++) {
+            if (gen_of[k] >= 0) continue;
             const umag_ens_instance& q = in[groups[k][0]];
             if (q.N[0] == r.N[0] && q.N[1] == r.N[1] && q.N[2] == r.N[2] && q.cell[0] == r.cell[0] &&
                 q.cell[1] == r.cell[1] && q.cell[2] == r.cell[2])
                 g = (int)k;
         }
-        if (g < 0) { groups.push_back({}); g = (int)groups.size() - 1; }
+        if (g < 0) { groups.push_back({}); gen_of.push_back(-1); g = (int)groups.size() - 1; }
         e->where[i] = {g, (int)groups[g].size()};
         groups[g].push_back(i);
     }
     e->cls.resize(groups.size());
     for (size_t k = 0; k < groups.size(); k++) {
-        int st = ens_class_new(e->cls[k], in, groups[k], sp, demag);
+        const int st = gen_of[k] >= 0 ? ens_class_new_general(e->cls[k], gen_of[k], general[gen_of[k]], sp)
+                                      : ens_class_new(e->cls[k], in, groups[k], sp, demag);
         if (st != UMAG_OK) return fail(st);
     }
     *out = reinterpret_cast<umag_ens*>(e);
@@ -1939,7 +1977,8 @@ int ens_set_m(umag_ens* h, int i, const float* host_m) {
     float* m = s->hctl[b].m;
     // on the library stream, so that the normalisation below sees the copy
     UMAG_CUDA(cudaMemcpyAsync(m, host_m, sizeof(float) * 3 * s->N, cudaMemcpyHostToDevice, S()));
-    UMAG_TRY(normalize(m, m + s->N, m + 2 * (size_t)s->N, nullptr, s->N));  // engine/magnetization.go:34
+    // engine/magnetization.go:34 (the geometry mask of a general instance; none in a batch)
+    UMAG_TRY(normalize(m, m + s->N, m + 2 * (size_t)s->N, s->p.vol, s->N));
     UMAG_CUDA(cudaDeviceSynchronize());
     s->need_k1 = true;
     return UMAG_OK;
@@ -1987,6 +2026,7 @@ static int ens_capture(EnsImpl* e, EnsClass& C) {
 // and its uniform constants.
 static int ens_compact(EnsImpl* e, int ci) {
     EnsClass& C = e->cls[ci];
+    if (C.general) return UMAG_OK;  // one instance: nothing to compact
     SimImpl* s = C.s;
     const int nb = s->nb;
     std::vector<int> order;
@@ -2106,6 +2146,14 @@ int ens_class_info(umag_ens* h, int cls, int N[3], int* n_instances) {
     const SimImpl* s = e->cls[cls].s;
     for (int i = 0; i < 3; i++) N[i] = s->p.N[i];
     *n_instances = e->cls[cls].n_all;
+    return UMAG_OK;
+}
+
+int ens_class_general(umag_ens* h, int cls, int* general) {
+    EnsImpl* e = reinterpret_cast<EnsImpl*>(h);
+    UMAG_REQUIRE(e && general, "NULL argument");
+    UMAG_REQUIRE(cls >= 0 && cls < (int)e->cls.size(), "class %d out of range", cls);
+    *general = e->cls[cls].general ? 1 : 0;
     return UMAG_OK;
 }
 

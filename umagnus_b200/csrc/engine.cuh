@@ -26,6 +26,8 @@ int sim_set_param(umag_sim* s, int which, const float* values, float mul);
 int sim_get_tuning(umag_sim* s, umag_tuning* t);
 int sim_set_tuning(umag_sim* s, const umag_tuning* t);
 int ens_new(int n, const umag_ens_instance* in, const umag_solver_params* sp, int demag, umag_ens** out);
+int ens_new_general(int n, const umag_ens_instance* in, const umag_sim_params* const* general,
+                    const umag_solver_params* sp, int demag, umag_ens** out);
 int ens_free(umag_ens* e);
 int ens_set_m(umag_ens* e, int i, const float* host_m);
 int ens_get_m(umag_ens* e, int i, float* host_m);
@@ -33,6 +35,7 @@ int ens_get_state(umag_ens* e, int i, umag_solver_state* st);
 int ens_run(umag_ens* e, double seconds, int chunk, long long max_replays);
 int ens_count(umag_ens* e, int* n_instances, int* n_classes);
 int ens_class_info(umag_ens* e, int cls, int N[3], int* n_instances);
+int ens_class_general(umag_ens* e, int cls, int* general);
 int ens_get_tuning(umag_ens* e, int cls, umag_tuning* t);
 int ens_set_tuning(umag_ens* e, int cls, const umag_tuning* t);
 int adj_new(const umag_adj_params* p, umag_adj** out);

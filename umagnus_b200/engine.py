@@ -83,6 +83,105 @@ def _dev(x, dtype=torch.float32):
     return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype).cuda()
 
 
+def sim_params(keepalive, N, cell, Msat, Aex, alpha, Dind=0.0, Ku1=0.0, Ku2=0.0, anisU=(0.0, 0.0, 1.0), B_ext=None,
+               regions=None, geom=None, demag=True, open_bc=False, precess=True, asymptotic_radius=32,
+               demag_kernel="newell", demag_accuracy=6.0, FrozenSpins=None, Kc1=0.0, Kc2=0.0, Kc3=0.0,
+               anisC1=(1.0, 0.0, 0.0), anisC2=(0.0, 1.0, 0.0), Dbulk=0.0, Temp=0.0, ThermSeed=0, pbc=(0, 0, 0),
+               NoDemagSpins=None, exchange_scale=None, exchange_inter=None, dmi_scale=None, dmi_inter=None):
+    """The umag_sim_params record of a simulation (the arguments of
+    Simulation, which documents them), with its device maps and LUTs
+    appended to `keepalive` (they must outlive the simulation).  Returns
+    (params, luts): luts names the device LUTs built here (aLUT, dLUT,
+    dbLUT, bext, frozen, nodemag) that exist."""
+    N = tuple(int(n) for n in N)
+    shape = (N[2], N[1], N[0])
+    luts = {}
+    p = SimParams()
+    p.N[:] = N
+    p.cell[:] = [float(c) for c in cell]
+    p.pbc[:] = tuple(int(x) for x in pbc)  # data/mesh.go PBC repetitions (SetPBC)
+
+    def keep(t):
+        keepalive.append(t)
+        return t.data_ptr()
+
+    if regions is not None:
+        p.regions = keep(_dev(np.asarray(regions, np.uint8).reshape(shape), torch.uint8))
+    if geom is not None:
+        p.vol = keep(_dev(np.asarray(geom, np.float32).reshape(shape)))
+
+    def param(v):
+        if np.isscalar(v):
+            return None, float(np.float32(v))
+        return keep(_dev(np.asarray(v, np.float32).reshape(shape))), 1.0
+
+    p.Ms, p.Ms_mul = param(Msat)
+    p.alpha, p.alpha_mul = param(alpha)
+    p.Ku1, p.Ku1_mul = param(Ku1)
+    p.Ku2, p.Ku2_mul = param(Ku2)
+    u = np.asarray(anisU, np.float64)
+    for c in range(3):
+        if u.ndim == 1:
+            p.anisU[c], p.anisU_mul[c] = None, float(np.float32(u[c]))
+        else:
+            p.anisU[c], p.anisU_mul[c] = param(u[c])
+    # cubic anisotropy (engine/anisotropy.go:14-19)
+    p.Kc1, p.Kc1_mul = param(Kc1)
+    p.Kc2, p.Kc2_mul = param(Kc2)
+    p.Kc3, p.Kc3_mul = param(Kc3)
+    for name, val in (("anisC1", anisC1), ("anisC2", anisC2)):
+        v = np.asarray(val, np.float64)
+        ptrs, muls = getattr(p, name), getattr(p, name + "_mul")
+        for c in range(3):
+            if v.ndim == 1:
+                ptrs[c], muls[c] = None, float(np.float32(v[c]))
+            else:
+                ptrs[c], muls[c] = param(v[c])
+    luts["aLUT"] = _dev(exchange_lut(Aex, *pair_tables(exchange_scale, exchange_inter)))
+    p.aLUT = keep(luts["aLUT"])
+    if np.any(np.asarray(Dind) != 0) or dmi_inter:
+        luts["dLUT"] = _dev(exchange_lut(Dind, *pair_tables(dmi_scale, dmi_inter)))
+        p.dLUT = keep(luts["dLUT"])
+    if np.any(np.asarray(Dbulk) != 0):  # engine/exchange.go:60-61 AddDMIBulk
+        luts["dbLUT"] = _dev(exchange_lut(Dbulk))
+        p.dbulkLUT = keep(luts["dbLUT"])
+    if B_ext is not None:
+        b = np.asarray(B_ext, np.float32)
+        lut = np.tile(b, (NREGION, 1)) if b.ndim == 1 else b
+        luts["bext"] = _dev(np.ascontiguousarray(lut.T))
+        keep(luts["bext"])
+        for c in range(3):
+            p.bextLUT[c] = luts["bext"][c].data_ptr()
+    p.enable_demag = int(bool(demag))
+    p.openbc = int(bool(open_bc))
+    p.precess = int(bool(precess))
+    p.asymptotic_radius = int(asymptotic_radius)
+    # engine/demag.go:21-27: EnableDemag (brute force, the reference default) or EnableNewellDemag
+    if demag_kernel not in ("newell", "brute"):
+        raise ValueError("demag_kernel must be 'newell' or 'brute'")
+    p.demag_kernel = 1 if demag_kernel == "brute" else 0
+    p.demag_accuracy = float(demag_accuracy)
+    # engine/temperature.go: Temp (K), scalar or per-cell; ThermSeed seeds the noise
+    p.temp, p.temp_mul = param(Temp)
+    p.therm_seed = int(ThermSeed) & ((1 << 64) - 1)
+
+    def region_lut(val):  # a scalar or up to 256 per-region values
+        lut = np.zeros(NREGION, np.float32)
+        v = np.asarray(val, np.float32).ravel()
+        lut[: v.size] = v
+        if v.size == 1:
+            lut[:] = v[0]
+        return _dev(lut)
+
+    if FrozenSpins is not None:  # engine/torque.go:348-352
+        luts["frozen"] = region_lut(FrozenSpins)
+        p.frozen_lut = keep(luts["frozen"])
+    if NoDemagSpins is not None:  # engine/demag.go:22, :67-98
+        luts["nodemag"] = region_lut(NoDemagSpins)
+        p.nodemag_lut = keep(luts["nodemag"])
+    return p, luts
+
+
 class Simulation:
     """A micromagnetic simulation on one GPU.
 
@@ -116,88 +215,15 @@ class Simulation:
         self.ncell = self.N[0] * self.N[1] * self.N[2]
         self.shape = (self.N[2], self.N[1], self.N[0])
         self._keep = []
-        p = SimParams()
-        p.N[:] = self.N
-        p.cell[:] = [float(c) for c in cell]
-        p.pbc[:] = tuple(int(x) for x in pbc)  # data/mesh.go PBC repetitions (SetPBC)
-
-        def keep(t):
-            self._keep.append(t)
-            return t.data_ptr()
-
-        if regions is not None:
-            p.regions = keep(_dev(np.asarray(regions, np.uint8).reshape(self.shape), torch.uint8))
-        if geom is not None:
-            p.vol = keep(_dev(np.asarray(geom, np.float32).reshape(self.shape)))
-
-        def param(v):
-            if np.isscalar(v):
-                return None, float(np.float32(v))
-            return keep(_dev(np.asarray(v, np.float32).reshape(self.shape))), 1.0
-
-        p.Ms, p.Ms_mul = param(Msat)
-        p.alpha, p.alpha_mul = param(alpha)
-        p.Ku1, p.Ku1_mul = param(Ku1)
-        p.Ku2, p.Ku2_mul = param(Ku2)
-        u = np.asarray(anisU, np.float64)
-        for c in range(3):
-            if u.ndim == 1:
-                p.anisU[c], p.anisU_mul[c] = None, float(np.float32(u[c]))
-            else:
-                p.anisU[c], p.anisU_mul[c] = param(u[c])
-        # cubic anisotropy (engine/anisotropy.go:14-19)
-        p.Kc1, p.Kc1_mul = param(Kc1)
-        p.Kc2, p.Kc2_mul = param(Kc2)
-        p.Kc3, p.Kc3_mul = param(Kc3)
-        for name, val in (("anisC1", anisC1), ("anisC2", anisC2)):
-            v = np.asarray(val, np.float64)
-            ptrs, muls = getattr(p, name), getattr(p, name + "_mul")
-            for c in range(3):
-                if v.ndim == 1:
-                    ptrs[c], muls[c] = None, float(np.float32(v[c]))
-                else:
-                    ptrs[c], muls[c] = param(v[c])
-        self.aLUT = _dev(exchange_lut(Aex, *pair_tables(exchange_scale, exchange_inter)))
-        p.aLUT = keep(self.aLUT)
-        if np.any(np.asarray(Dind) != 0) or dmi_inter:
-            self.dLUT = _dev(exchange_lut(Dind, *pair_tables(dmi_scale, dmi_inter)))
-            p.dLUT = keep(self.dLUT)
-        if np.any(np.asarray(Dbulk) != 0):  # engine/exchange.go:60-61 AddDMIBulk
-            self.dbLUT = _dev(exchange_lut(Dbulk))
-            p.dbulkLUT = keep(self.dbLUT)
-        if B_ext is not None:
-            b = np.asarray(B_ext, np.float32)
-            lut = np.tile(b, (NREGION, 1)) if b.ndim == 1 else b
-            self.bext = _dev(np.ascontiguousarray(lut.T))
-            keep(self.bext)
-            for c in range(3):
-                p.bextLUT[c] = self.bext[c].data_ptr()
-        p.enable_demag = int(bool(demag))
-        p.openbc = int(bool(open_bc))
-        p.precess = int(bool(precess))
-        p.asymptotic_radius = int(asymptotic_radius)
-        # engine/demag.go:21-27: EnableDemag (brute force, the reference default) or EnableNewellDemag
-        if demag_kernel not in ("newell", "brute"):
-            raise ValueError("demag_kernel must be 'newell' or 'brute'")
-        p.demag_kernel = 1 if demag_kernel == "brute" else 0
-        p.demag_accuracy = float(demag_accuracy)
-        # engine/temperature.go: Temp (K), scalar or per-cell; ThermSeed seeds the noise
-        p.temp, p.temp_mul = param(Temp)
-        p.therm_seed = int(ThermSeed) & ((1 << 64) - 1)
-        def region_lut(val):  # a scalar or up to 256 per-region values
-            lut = np.zeros(NREGION, np.float32)
-            v = np.asarray(val, np.float32).ravel()
-            lut[: v.size] = v
-            if v.size == 1:
-                lut[:] = v[0]
-            return _dev(lut)
-
-        if FrozenSpins is not None:  # engine/torque.go:348-352
-            self.frozen = region_lut(FrozenSpins)
-            p.frozen_lut = keep(self.frozen)
-        if NoDemagSpins is not None:  # engine/demag.go:22, :67-98
-            self.nodemag = region_lut(NoDemagSpins)
-            p.nodemag_lut = keep(self.nodemag)
+        p, luts = sim_params(self._keep, N, cell, Msat, Aex, alpha, Dind=Dind, Ku1=Ku1, Ku2=Ku2, anisU=anisU,
+                             B_ext=B_ext, regions=regions, geom=geom, demag=demag, open_bc=open_bc, precess=precess,
+                             asymptotic_radius=asymptotic_radius, demag_kernel=demag_kernel,
+                             demag_accuracy=demag_accuracy, FrozenSpins=FrozenSpins, Kc1=Kc1, Kc2=Kc2, Kc3=Kc3,
+                             anisC1=anisC1, anisC2=anisC2, Dbulk=Dbulk, Temp=Temp, ThermSeed=ThermSeed, pbc=pbc,
+                             NoDemagSpins=NoDemagSpins, exchange_scale=exchange_scale,
+                             exchange_inter=exchange_inter, dmi_scale=dmi_scale, dmi_inter=dmi_inter)
+        for k, v in luts.items():
+            setattr(self, k, v)
         sp = SolverParams()
         self.L.umag_solver_defaults(ctypes.byref(sp))
         sp.solver = int(solver)
@@ -407,18 +433,47 @@ class Ensemble:
     counterpart in the reference, which runs one simulation per process).
 
     instances: list of dicts with N, cell, Msat, Aex, alpha and optional
-    Dind, Ku1, Ku2, anisU, B_ext (uniform values only).  Each instance keeps
-    its own time, dt and step controller; the solver knobs are shared.
-    Instances with the same mesh run as one batch of launches, and one CUDA
-    graph steps all of them.
+    Dind, Ku1, Ku2, anisU, B_ext.  Each instance keeps its own time, dt and
+    step controller; the solver knobs are shared.  Instances with uniform
+    values of those parameters and the same mesh run as one batch of
+    launches, and one CUDA graph steps all of them.  An instance whose dict
+    holds anything else -- region maps, per-cell or per-region parameter
+    arrays, geom, pbc, Temp, FrozenSpins, any other Simulation argument -- or
+    "general": True is a general instance: the simulation Simulation(**dict)
+    would be, stepped by the single-simulation kernels in a graph of its own,
+    concurrently with the batches, with the same trajectory bit for bit
+    (umag_ens_new_general).
     """
+
+    UNIFORM_KEYS = {"N", "cell", "Msat", "Aex", "alpha", "Dind", "Ku1", "Ku2", "anisU", "B_ext"}
+
+    @classmethod
+    def is_general(cls, d):
+        if d.get("general", False) or set(d) - cls.UNIFORM_KEYS - {"general"}:
+            return True
+        scal = ("Msat", "Aex", "alpha", "Dind", "Ku1", "Ku2")
+        if any(np.ndim(d[k]) != 0 for k in scal if k in d):
+            return True
+        return any(np.ndim(d[k]) > 1 for k in ("anisU", "B_ext") if k in d)
 
     def __init__(self, instances, demag=True, solver=DORMANDPRINCE, dt=1e-15, MaxErr=1e-5, RelErr=1e-4,
                  MinDt=0.0, MaxDt=0.0, FixDt=0.0, Headroom=0.8, device=0):
         self.L = _lib.init(device)
         arr = (EnsInstance * len(instances))()
+        gen = (ctypes.c_void_p * len(instances))()
+        self._keep = []
+        self._gen_params = []
         self.shapes = []
         for k, d in enumerate(instances):
+            if self.is_general(d):
+                kw = {key: v for key, v in d.items() if key != "general"}
+                kw.setdefault("demag", demag)
+                p, _ = sim_params(self._keep, **kw)
+                self._gen_params.append(p)
+                gen[k] = ctypes.addressof(p)
+                N = tuple(int(n) for n in d["N"])
+                self.shapes.append((3, N[2], N[1], N[0]))
+                continue
             r = arr[k]
             N = tuple(int(n) for n in d["N"])
             r.N[:] = N
@@ -434,7 +489,9 @@ class Ensemble:
         sp.dt, sp.max_err, sp.rel_err, sp.min_dt, sp.max_dt = dt, MaxErr, RelErr, MinDt, MaxDt
         sp.fix_dt, sp.headroom, sp.gamma_ll = FixDt, Headroom, GAMMA_LL
         h = ctypes.c_void_p()
-        check(self.L.umag_ens_new(len(instances), arr, ctypes.byref(sp), int(bool(demag)), ctypes.byref(h)))
+        torch.cuda.synchronize()  # the general instances' device maps are in place
+        check(self.L.umag_ens_new_general(len(instances), arr, gen, ctypes.byref(sp), int(bool(demag)),
+                                          ctypes.byref(h)))
         self._h = h.value
 
     def __len__(self):
@@ -452,6 +509,13 @@ class Ensemble:
         n = ctypes.c_int()
         check(self.L.umag_ens_class_info(self._h, int(cls), N, ctypes.byref(n)))
         return tuple(N), n.value
+
+    def class_general(self, cls):
+        """True when class `cls` is a general instance (one simulation with
+        the single-simulation kernels)."""
+        g = ctypes.c_int()
+        check(self.L.umag_ens_class_general(self._h, int(cls), ctypes.byref(g)))
+        return bool(g.value)
 
     def get_tuning(self, cls):
         """Launch shapes of class `cls`'s batched per-cell kernels (a dict)."""

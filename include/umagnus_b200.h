@@ -463,6 +463,8 @@ typedef struct {
     int solver;             /* 4 (or 0) RK4, 2 Heun (engine/heun.go with FixDt) */
     float Dind;             /* uniform interfacial DMI (J/m^2; 0 = exchange only): dmi.cl's
                                exchange + DMI stencil, a fixed (not differentiated) parameter */
+    int pbc[3];             /* periodic repetitions per axis (engine/mesh.go SetPBC; 0 = open):
+                               the demag kernel's images and wrapped stencils, as umag_sim_params */
 } umag_adj_params;
 typedef struct umag_adj umag_adj;
 int umag_adj_new(const umag_adj_params* p, umag_adj** out);

@@ -130,10 +130,12 @@ class Problem:
 
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, probe, avg_from, w_probe=1.0, w_target=1.0,
                  target=(0.0, 0.0, 1.0), demag=True, gamma_ll=GAMMA_LL, solver=4, backend="numpy", device="cuda",
-                 Dind=0.0):
+                 Dind=0.0, pbc=(0, 0, 0)):
         """backend: "numpy" (host) or "torch" (float64 on `device`), the same
         operations in the same order.  Dind: uniform interfacial DMI (J/m^2),
-        a fixed (not differentiated) parameter."""
+        a fixed (not differentiated) parameter.  pbc: periodic repetitions
+        per axis (data/mesh.go): the demag kernel sums the images
+        (mag/demagkernel.go) and the stencils wrap (stencil.clh:13-29)."""
         if solver not in (2, 4):
             raise ValueError("solver must be 4 (RK4) or 2 (Heun)")
         self.xp = _Numpy() if backend == "numpy" else _Torch(device)
@@ -154,8 +156,11 @@ class Problem:
         self.gilb = -1.0 / (1.0 + self.alpha ** 2)
         self.w = [2.0 / (c * c) for c in self.cell]
         self.D = float(Dind)
+        self.pbc = tuple(int(p) for p in pbc)
+        # periodic flag per array axis of (3, Nz, Ny, Nx) fields
+        self.per = {3: self.pbc[0] > 0, 2: self.pbc[1] > 0, 1: self.pbc[2] > 0}
         if self.D != 0:
-            # in-plane neighbour masks (1 inside the mesh) along x and y
+            # in-plane neighbour masks (1 where the neighbour exists) along x and y
             Nx, Ny, Nz = self.N
             self.ins = {}
             for ax, n in ((3, Nx), (2, Ny)):
@@ -163,10 +168,11 @@ class Problem:
                     idx = np.arange(n) + sd
                     shape = [1, 1, 1, 1]
                     shape[ax] = n
-                    self.ins[(ax, sd)] = self.xp.asarray(((idx >= 0) & (idx < n)).astype(np.float64).reshape(shape))
+                    has = np.ones(n, bool) if self.per[ax] else (idx >= 0) & (idx < n)
+                    self.ins[(ax, sd)] = self.xp.asarray(has.astype(np.float64).reshape(shape))
         self.demag = demag
         if demag:
-            K = oracle.newell_kernel(self.N, self.cell)  # (6, Pz, Py, Px): xx yy zz yz xz xy
+            K = oracle.newell_kernel(self.N, self.cell, pbc=self.pbc)  # (6, Pz, Py, Px): xx yy zz yz xz xy
             self.P = K.shape[1:]
             self.Kf = self.xp.rfftn(self.xp.asarray(K))
 
@@ -186,29 +192,33 @@ class Problem:
         B = xp.irfftn(Bf, (Pz, Py, Px))
         return MU0 * B[:, :Nz, :Ny, :Nx]
 
+    def _nb(self, ax, n, sd):
+        """neighbour index along array axis ax: clamped (stencil.clh hclamp /
+        lclamp) or wrapped on a periodic axis"""
+        idx = np.arange(n) + sd
+        return idx % n if self.per[ax] else np.clip(idx, 0, n - 1)
+
     def stencil(self, v):
-        """sum_d w_d (v_neighbour - v) with clamped neighbours (exchange.cl)."""
+        """sum_d w_d (v_neighbour - v) with clamped or wrapped neighbours (exchange.cl)."""
         xp = self.xp
         out = xp.zeros_like(v)
         Nz = v.shape[1]
         axes = [(3, self.w[0]), (2, self.w[1])] + ([(1, self.w[2])] if Nz > 1 else [])
         for ax, w in axes:
             n = v.shape[ax]
-            idx = np.arange(n)
-            lo = xp.take(v, xp.index(np.maximum(idx - 1, 0)), ax)
-            hi = xp.take(v, xp.index(np.minimum(idx + 1, n - 1)), ax)
+            lo = xp.take(v, xp.index(self._nb(ax, n, -1)), ax)
+            hi = xp.take(v, xp.index(self._nb(ax, n, 1)), ax)
             out += w * ((lo - v) + (hi - v))
         return out
 
     def _zstencil(self, v):
-        """sum over z neighbours of (v_nb - v), clamped (exchange.cl z terms)."""
+        """sum over z neighbours of (v_nb - v), clamped or wrapped (exchange.cl z terms)."""
         xp = self.xp
         out = xp.zeros_like(v)
         n = v.shape[1]
         if n > 1:
-            idx = np.arange(n)
-            lo = xp.take(v, xp.index(np.maximum(idx - 1, 0)), 1)
-            hi = xp.take(v, xp.index(np.minimum(idx + 1, n - 1)), 1)
+            lo = xp.take(v, xp.index(self._nb(1, n, -1)), 1)
+            hi = xp.take(v, xp.index(self._nb(1, n, 1)), 1)
             out += (lo - v) + (hi - v)
         return out
 
@@ -226,8 +236,7 @@ class Problem:
         for ax, c, d in ((3, self.cell[0], 0), (2, self.cell[1], 1)):
             n = m.shape[ax]
             for sd in (-1, 1):
-                idx = np.arange(n) + sd
-                mn = xp.take(m, xp.index(np.clip(idx, 0, n - 1)), ax)
+                mn = xp.take(m, xp.index(self._nb(ax, n, sd)), ax)
                 ins = self.ins[(ax, sd)]
                 q = sd * c * (0.5 * D / A)
                 if d == 0:
@@ -251,8 +260,7 @@ class Problem:
         for ax, c, d in ((3, self.cell[0], 0), (2, self.cell[1], 1)):
             n = m.shape[ax]
             for sd in (-1, 1):
-                idx = np.arange(n) + sd
-                mn = xp.take(m, xp.index(np.clip(idx, 0, n - 1)), ax)
+                mn = xp.take(m, xp.index(self._nb(ax, n, sd)), ax)
                 ins = self.ins[(ax, sd)]
                 g += (2.0 / (c * c)) * ins * (mn - m)
                 bd = (1.0 - ins) * (-(D * D) / (2.0 * A * A))

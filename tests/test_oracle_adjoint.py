@@ -81,9 +81,9 @@ def test_torch_backend_matches_numpy(solver):
         assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max(), k
 
 
-def dmi_case(N=(10, 8, 1), steps=20, seed=6, solver=4, D=3e-3, Ku_axis=(0.0, 0.0, 1.0)):
+def dmi_case(N=(10, 8, 1), steps=20, seed=6, solver=4, D=3e-3, Ku_axis=(0.0, 0.0, 1.0), pbc=(0, 0, 0)):
     """Exchange + interfacial DMI (the multilayer's material: D 3e-3 J/m^2,
-    Ku1 along z), 2D or 3D."""
+    Ku1 along z), 2D or 3D, open or periodic."""
     rng = np.random.default_rng(seed)
     shape = (N[2], N[1], N[0])
     Ms = rng.uniform(9e5, 1.2e6, shape)
@@ -91,7 +91,7 @@ def dmi_case(N=(10, 8, 1), steps=20, seed=6, solver=4, D=3e-3, Ku_axis=(0.0, 0.0
     t = rng.normal(size=3)
     t /= np.linalg.norm(t)
     prob = R.Problem(N, (2e-9, 2e-9, 1e-9), 0.3, Ku_axis, 5e-14, steps, (1, 1, N[0] // 2, N[1] // 2),
-                     steps - steps // 4 + 1, target=t, solver=solver, Dind=D)
+                     steps - steps // 4 + 1, target=t, solver=solver, Dind=D, pbc=pbc)
     th = R.params(Ms, 1.6e-11, 5e5, (0.0, 0.0, 0.05))
     return prob, m0, th, rng
 
@@ -119,6 +119,44 @@ def test_dmi_reverse_pass_matches_central_fd(N, solver):
     _, g = prob.backward(m0, th)
     checks = [("A", None), ("K1", None), ("B", 0), ("B", 1), ("B", 2)]
     cells = rng.choice(N[0] * N[1] * N[2], size=24, replace=False)
+    for c in cells:
+        z, r = divmod(int(c), N[0] * N[1])
+        checks.append(("Ms", (z, r // N[0], r % N[0])))
+    for which in checks:
+        fd = R.fd_gradient(prob, m0, th, which, rel=1e-4)
+        ad = g[which[0]] if which[1] is None else g[which[0]][which[1]]
+        assert abs(fd - ad) <= 1e-4 * abs(fd) + 1e-12 * max(1.0, abs(ad)), (which, fd, ad)
+
+
+def test_periodic_dmi_field_is_the_reference_restatement():
+    """With periodic x and y the FP64 dmi() equals the CPU oracle's dmi.cl
+    restatement with wrapped neighbours (PBC code 3), and stays its own
+    transpose; so does the periodic exchange stencil."""
+    from oracle import oracle as O
+    prob, m0, th, rng = dmi_case(N=(9, 7, 3), pbc=(2, 3, 0))
+    m = m0 / np.sqrt((m0 * m0).sum(0))
+    B = np.zeros_like(m)
+    A, D = th["A"], prob.D
+    O.add_dmi(B, m, O.exch_lut(np.full(256, A), dtype=np.float64), O.exch_lut(np.full(256, D), dtype=np.float64),
+              np.zeros(m.shape[1:], np.uint8), prob.cell, 1.0, pbc=3)
+    h = prob.dmi(m, A)
+    assert np.abs(h - B).max() <= 1e-13 * np.abs(B).max()
+    x, y = rng.normal(size=m.shape), rng.normal(size=m.shape)
+    lhs, rhs = (x * prob.dmi(y, A)).sum(), (prob.dmi(x, A) * y).sum()
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+    lhs, rhs = (x * prob.stencil(y)).sum(), (prob.stencil(x) * y).sum()
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+@pytest.mark.parametrize("N,pbc,D", [((10, 8, 1), (2, 0, 0), 3e-3), ((8, 6, 3), (1, 1, 1), 3e-3),
+                                     ((10, 8, 1), (0, 2, 0), 0.0)])
+def test_periodic_reverse_pass_matches_central_fd(N, pbc, D):
+    """Periodic meshes (the demag kernel's images, wrapped stencils): the
+    reverse pass against central differences."""
+    prob, m0, th, rng = dmi_case(N=N, pbc=pbc, D=D)
+    _, g = prob.backward(m0, th)
+    checks = [("A", None), ("K1", None), ("B", 0), ("B", 1), ("B", 2)]
+    cells = rng.choice(N[0] * N[1] * N[2], size=16, replace=False)
     for c in cells:
         z, r = divmod(int(c), N[0] * N[1])
         checks.append(("Ms", (z, r // N[0], r % N[0])))

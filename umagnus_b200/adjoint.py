@@ -3,9 +3,10 @@
 No counterpart in the reference, which has no gradients.  The forward pass
 is the engine's effective field (demag, exchange, uniaxial anisotropy,
 Zeeman; engine/effectivefield.go:14-24) and LL torque (engine/torque.go)
-for a per-cell Ms map and uniform Aex, Ku1, B_ext and alpha, stepped by
-fixed-step RK4 (engine/rk4.go with FixDt) or Heun (engine/heun.go, solver=2),
-m checkpointed every K steps.
+for a per-cell Ms map and uniform Aex, Ku1, B_ext and alpha (and a fixed
+uniform interfacial DMI, Dind), on an open or periodic mesh (pbc), stepped
+by fixed-step RK4 (engine/rk4.go with FixDt) or Heun (engine/heun.go,
+solver=2), m checkpointed every K steps.
 The loss is
 
     w_probe * mean over states avg_from..nsteps of the mean m_z in the probe
@@ -32,7 +33,7 @@ GAMMA_LL = 1.7595e11  # engine/torque.go:27
 class AdjointRK4:
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, K, probe, avg_from, w_probe=1.0, w_target=1.0,
                  target=(0.0, 0.0, 1.0), demag=True, demag_kernel="newell", demag_accuracy=6.0, gamma_ll=GAMMA_LL,
-                 use_graph=True, device=0, solver=4, Dind=0.0):
+                 use_graph=True, device=0, solver=4, Dind=0.0, pbc=(0, 0, 0)):
         self.L = _lib.init(device)
         p = AdjParams()
         p.N[:] = [int(n) for n in N]
@@ -51,6 +52,7 @@ class AdjointRK4:
         p.no_graph = 0 if use_graph else 1
         p.solver = int(solver)  # 4 RK4, 2 Heun
         p.Dind = float(Dind)    # interfacial DMI (fixed parameter)
+        p.pbc[:] = [int(v) for v in pbc]  # periodic repetitions per axis (engine/mesh.go SetPBC)
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
         h = ctypes.c_void_p()

@@ -16,8 +16,9 @@
 // segment's checkpoint and kept): the normalisation's VJP (w - n (n.w))/|u|,
 // the LL torque's VJP (cross products), and the effective field's VJP: the
 // demag convolution with a real, even kernel is self-adjoint (the same plan
-// applied to the cotangent), the exchange stencil with its clamped boundary
-// is symmetric, anisotropy and Zeeman are local.
+// applied to the cotangent; with periodic axes the same holds for the
+// periodic kernel), the exchange stencil with its clamped boundary, or
+// wrapped on a periodic axis, is symmetric, anisotropy and Zeeman are local.
 //
 // Launch structure.  Forward, per stage: the three demag passes, then one
 // kernel that evaluates the field and torque of the stage state and, per
@@ -257,7 +258,8 @@ __global__ void __launch_bounds__(256) k_adj_rev_start_heun(AdjField a, StepFac 
 //   dL/dm_q = gm + Ms dw + S(wB / Ms) + 2 (K1/Ms) (wB.u) u
 //   acc[Ms] += m.dw - wB.e/Ms^2 - 2 K1 (m.u)(wB.u)/Ms^2,  e = S m_q
 //   acc[A] += wB.e/(Ms A);  acc[K1] += 2 (m.u)(wB.u)/Ms;  acc[B] += wB
-// (S: the exchange stencil with the clamped boundary, symmetric).  Then
+// (S: the exchange stencil with the clamped or periodic boundary,
+// symmetric).  Then
 //   q > 0: m_q = normalize(m + st[q-1] k_{q-1}): g_u = VJP; lam2 += g_u;
 //          dL/dk_{q-1} = gk_{q-1} + st[q-1] g_u, and the torque VJP of stage
 //          q-1 with it -> gm (in place), wBn
@@ -300,10 +302,16 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, in
             for (int d = 0; d < 2; d++) {
 #pragma unroll
                 for (int sd = -1; sd <= 1; sd += 2) {
-                    const bool in = d == 0 ? (sd < 0 ? ix > 0 : ix + 1 < a.g.Nx) : (sd < 0 ? iy > 0 : iy + 1 < a.g.Ny);
+                    // a periodic axis has every neighbour (wrapped)
+                    const bool per = (a.g.pbc & (d == 0 ? 1 : 2)) != 0;
+                    const bool in = per || (d == 0 ? (sd < 0 ? ix > 0 : ix + 1 < a.g.Nx)
+                                                   : (sd < 0 ? iy > 0 : iy + 1 < a.g.Ny));
                     const float S = d == 0 ? a.pc.sx : a.pc.sy, Dc = (d == 0 ? a.pc.dcx : a.pc.dcy) * sd;
                     if (in) {
-                        const int j = d == 0 ? I + sd : I + sd * a.g.Nx;
+                        const int j = d == 0 ? (iz * a.g.Ny + iy) * a.g.Nx + (sd < 0 ? lclamp(ix - 1, a.g.Nx, per)
+                                                                                      : hclamp(ix + 1, a.g.Nx, per))
+                                             : (iz * a.g.Ny + (sd < 0 ? lclamp(iy - 1, a.g.Ny, per)
+                                                                      : hclamp(iy + 1, a.g.Ny, per))) * a.g.Nx + ix;
                         const float msj = a.Ms[j];
                         const float ij = msj == 0.f ? 0.f : 1.0f / msj;
                         const f3 xn{wB[j] * ij, wB[N + j] * ij, wB[2 * N + j] * ij};
@@ -322,7 +330,8 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, in
             if (a.g.Nz != 1) {
 #pragma unroll
                 for (int sd = -1; sd <= 1; sd += 2) {
-                    const int j = ((sd < 0 ? lclamp(iz - 1, a.g.Nz, false) : hclamp(iz + 1, a.g.Nz, false)) * a.g.Ny +
+                    const bool pz = (a.g.pbc & 4) != 0;
+                    const int j = ((sd < 0 ? lclamp(iz - 1, a.g.Nz, pz) : hclamp(iz + 1, a.g.Nz, pz)) * a.g.Ny +
                                    iy) * a.g.Nx + ix;
                     const float msj = a.Ms[j];
                     const float ij = msj == 0.f ? 0.f : 1.0f / msj;
@@ -339,12 +348,14 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, in
             acc[(size_t)N + I] += wA * (double)inv / (double)A;
         } else {
             int nb[6];
-            nb[0] = (iz * a.g.Ny + iy) * a.g.Nx + lclamp(ix - 1, a.g.Nx, false);
-            nb[1] = (iz * a.g.Ny + iy) * a.g.Nx + hclamp(ix + 1, a.g.Nx, false);
-            nb[2] = (iz * a.g.Ny + lclamp(iy - 1, a.g.Ny, false)) * a.g.Nx + ix;
-            nb[3] = (iz * a.g.Ny + hclamp(iy + 1, a.g.Ny, false)) * a.g.Nx + ix;
-            nb[4] = (lclamp(iz - 1, a.g.Nz, false) * a.g.Ny + iy) * a.g.Nx + ix;
-            nb[5] = (hclamp(iz + 1, a.g.Nz, false) * a.g.Ny + iy) * a.g.Nx + ix;
+            // exchange.cl's neighbours: clamped, or wrapped on a periodic axis
+            const bool px = a.g.pbc & 1, py = a.g.pbc & 2, pz = a.g.pbc & 4;
+            nb[0] = (iz * a.g.Ny + iy) * a.g.Nx + lclamp(ix - 1, a.g.Nx, px);
+            nb[1] = (iz * a.g.Ny + iy) * a.g.Nx + hclamp(ix + 1, a.g.Nx, px);
+            nb[2] = (iz * a.g.Ny + lclamp(iy - 1, a.g.Ny, py)) * a.g.Nx + ix;
+            nb[3] = (iz * a.g.Ny + hclamp(iy + 1, a.g.Ny, py)) * a.g.Nx + ix;
+            nb[4] = (lclamp(iz - 1, a.g.Nz, pz) * a.g.Ny + iy) * a.g.Nx + ix;
+            nb[5] = (hclamp(iz + 1, a.g.Nz, pz) * a.g.Ny + iy) * a.g.Nx + ix;
             const int nn = a.g.Nz != 1 ? 6 : 4;
             f3 sx{0.f, 0.f, 0.f}, e{0.f, 0.f, 0.f};
             const f3 x0 = sc3(inv, w);
@@ -652,10 +663,12 @@ int adj_new(const umag_adj_params* p, umag_adj** out) {
                      p->probe[0] + p->probe[2] <= p->N[0] && p->probe[1] + p->probe[3] <= p->N[1],
                  "probe window outside the mesh");
     UMAG_REQUIRE(p->solver == 0 || p->solver == 2 || p->solver == 4, "solver must be 4 (RK4) or 2 (Heun)");
+    UMAG_REQUIRE(p->pbc[0] >= 0 && p->pbc[1] >= 0 && p->pbc[2] >= 0, "PBC repetitions must be non-negative");
     AdjImpl* s = new AdjImpl();
     s->p = *p;
     s->N = p->N[0] * p->N[1] * p->N[2];
-    s->g = Mesh3{p->N[0], p->N[1], p->N[2], 0};
+    // periodic axes wrap the stencils (data/mesh.go PBC_code: 1 x, 2 y, 4 z)
+    s->g = Mesh3{p->N[0], p->N[1], p->N[2], (p->pbc[0] ? 1 : 0) | (p->pbc[1] ? 2 : 0) | (p->pbc[2] ? 4 : 0)};
     s->heun = p->solver == 2;
     s->h = (float)(p->dt * (p->gamma_ll > 0 ? p->gamma_ll : 1.7595e11));  // engine/torque.go:27 GammaLL
     auto fail = [&](int c) {
@@ -677,7 +690,7 @@ int adj_new(const umag_adj_params* p, umag_adj** out) {
         s->ckpt.push_back(c);
     }
     if (p->enable_demag) {
-        const int pbc[3] = {0, 0, 0};
+        const int* pbc = p->pbc;
         const int st = p->demag_kernel == 1
                            ? demag_new_brute(p->N[0], p->N[1], p->N[2], pbc, p->cell[0], p->cell[1], p->cell[2],
                                              p->demag_accuracy > 0 ? p->demag_accuracy : 6.0, &s->demag)

@@ -164,8 +164,9 @@ __device__ __forceinline__ f3 lltorque_g(f3 m, f3 H, float alpha, float gilb) {
 // BAT, non-periodic mesh): the CTA's magnetisation tile with its halo comes
 // into shared memory by one TMA load (tile.cuh) and the stencils read it.
 // UNI (with UREG, not BAT): a uniform material with only the common terms --
-// uniform Ms, alpha and anisotropy, precession on, and no NoDemagSpins,
-// bulk DMI, cubic anisotropy, thermal field, FreezeSpins or B_eff output --
+// uniform Ms, alpha and anisotropy, precession on, no OpenBC, and no
+// NoDemagSpins, bulk DMI, cubic anisotropy, thermal field, FreezeSpins or
+// B_eff output --
 // so that those tests and branches leave the instruction stream; the
 // arithmetic is the same operations in the same order.
 template <bool UREG, bool BAT, bool TILE, bool UNI = false>
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(256) k_local_torque(const __grid_constant__ Lo
     if (!is0(m0)) {
         f3 e;
         if constexpr (TILE) {
-            e = dmi ? dmi_sum_tile(tv, threadIdx.x, threadIdx.y, kc.pc, a.openbc != 0, a.g.Nz > 1, m0)
+            e = dmi ? dmi_sum_tile<UNI>(tv, threadIdx.x, threadIdx.y, kc.pc, a.openbc != 0, a.g.Nz > 1, m0)
                     : exchange_sum_tile(tv, threadIdx.x, threadIdx.y, kc.pc, a.g.Nz > 1, m0);
         } else if (!BAT && !UNI && a.dbLUT) {  // engine/exchange.go:60-61 AddDMIBulk
             e = dmibulk_sum(mx, my, mz, a.aLUT, a.dbLUT, a.regions, a.cx, a.cy, a.cz, a.g, a.openbc != 0, ix, iy,
@@ -738,7 +739,8 @@ static int launch_torque(SimImpl* s, int m_sel, int slot, float* tau_direct, flo
     dim3 blk(bx, by, 1), grd((s->g.Nx + bx - 1) / bx, (s->g.Ny + by - 1) / by, s->g.Nz * s->nb);
     // the uniform-material instantiation where every term it leaves out is off
     const bool uni = s->zero_regions && !la.nodemag && !la.dbLUT && !la.cubic && !la.thermal && !beff &&
-                     !la.frozen && la.precess && la.alpha_uniform && la.ms_uniform && (!la.anis || la.anis_uniform);
+                     !la.frozen && la.precess && la.alpha_uniform && la.ms_uniform && (!la.anis || la.anis_uniform) &&
+                     !la.openbc;
     if (s->batched)
         k_local_torque<true, true, false><<<grd, blk, 0, S()>>>(la, s->tmaps);
     else if (s->zero_regions && s->tile_ok && s->tune.torque_tma && uni)

@@ -147,7 +147,11 @@ __device__ __forceinline__ f3 exchange_sum_tile(const TileView& v, int tx, int t
     return b;
 }
 
-// dmi_sum_u with the neighbours from a tile (same operations, same order)
+// dmi_sum_u with the neighbours from a tile (same operations, same order).
+// CLOSED: the mesh is known not to use OpenBC, so every neighbour counts
+// and a missing one is always extrapolated (computed and selected without
+// a branch: the same values).
+template <bool CLOSED = false>
 __device__ __forceinline__ f3 dmi_sum_tile(const TileView& v, int tx, int ty, const PairCoef& P, bool openbc,
                                            bool three_d, f3 m0) {
     f3 h{0.f, 0.f, 0.f};
@@ -157,8 +161,14 @@ __device__ __forceinline__ f3 dmi_sum_tile(const TileView& v, int tx, int ty, co
         for (int side = -1; side <= 1; side += 2) {
             f3 mn = d == 0 ? v.at(tx, ty, side, 0, 0) : v.at(tx, ty, 0, side, 0);
             const bool missing = is0(mn);
-            if (!missing || !openbc) {
-                if (missing) {
+            if (CLOSED || !missing || !openbc) {
+                if (CLOSED) {
+                    float q = d == 0 ? P.qx : P.qy;
+                    if (side < 0) q = -q;
+                    const f3 ext = d == 0 ? f3{fs(m0.x, fm(q, m0.z)), m0.y, fa(m0.z, fm(q, m0.x))}
+                                          : f3{m0.x, fs(m0.y, fm(q, m0.z)), fa(m0.z, fm(q, m0.y))};
+                    mn = missing ? ext : mn;
+                } else if (missing) {
                     float q = d == 0 ? P.qx : P.qy;
                     if (side < 0) q = -q;
                     if (d == 0) {

@@ -241,3 +241,22 @@ def test_ensemble_all_general_and_set_m_in_geometry():
     assert np.all(ens.get_m(0)[:, gen[1]["geom"] == 0] == 0)
     sim.free()
     ens.free()
+
+
+def test_ensemble_autotune_with_bench_records_and_general_instances(tmp_path):
+    """The tuner takes the instance records as bench.py passes them (with
+    their m_seed key) and skips general instances, which keep the
+    single-simulation shapes."""
+    import bench
+    from umagnus_b200 import engine
+    insts = [d for d in bench.ensemble_instances(count=12, seed=5) if d["N"][0] == 32][:3]
+    assert insts
+    gen = _general_instances()[1]
+    clean = [{k: v for k, v in d.items() if k != "m_seed"} for d in insts] + [gen]
+    ens = engine.Ensemble(clean)
+    assert [ens.class_general(c) for c in range(ens.classes())] == [False, True]
+    before = ens.get_tuning(1)
+    chosen, logs = ens.autotune(insts + [gen], cache_path=str(tmp_path / "tune.json"))
+    assert set(chosen) == {0} and logs[0] is not None
+    assert ens.get_tuning(1) == before
+    ens.free()

@@ -174,8 +174,8 @@ def tune_ensemble(ens, instances, cache_path=None, use_cache=True, probe_size=8,
         if ens.class_general(cls):  # a general instance keeps the single-simulation shapes
             continue
         N, _ = ens.class_info(cls)
-        members = [d for d in instances
-                   if tuple(int(v) for v in d["N"]) == tuple(N) and not Ensemble.is_general(d)]
+        members = [d for d in instances if tuple(int(v) for v in d["N"]) == tuple(N)
+                   and not Ensemble.is_general({k: v for k, v in d.items() if k not in strip})]
         feats = "ens|dmi={}|anis={}".format(int(any(d.get("Dind", 0) for d in members)),
                                             int(any(d.get("Ku1", 0) or d.get("Ku2", 0) for d in members)))
         key = cache_key(name, N, feats)

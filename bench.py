@@ -43,10 +43,10 @@ CONFIG = dict(N=(256, 256, 16), cell=(2e-9, 2e-9, 1e-9), Ms=1.1e6, Aex=1.6e-11, 
 METRIC = "RK45DP cell-updates/s (256x256x16 multilayer, FP32, Newell demag)"
 UNIT = "cell-updates/s"
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_reg_b<512,4> launch on
-# this workload (79,423,232 + 6,178,304 B), from one ncu --set full capture of
+# this workload (79,939,328 + 4,860,160 B), from one ncu --set full capture of
 # that launch with packed FP32 butterflies and staged twiddle tables (cold
 # cache: ncu flushes the caches between its passes)
-TRAFFIC_B = 85601536
+TRAFFIC_B = 84799488
 TRAFFIC_B_SOURCE = ("ncu capture of k_reg_b<512,4>, packed FP32 butterflies + staged twiddle tables "
                     "(profiles/k_reg_b_multilayer_256x256x16.md)")
 

@@ -465,6 +465,9 @@ typedef struct {
                                exchange + DMI stencil, a fixed (not differentiated) parameter */
     int pbc[3];             /* periodic repetitions per axis (engine/mesh.go SetPBC; 0 = open):
                                the demag kernel's images and wrapped stencils, as umag_sim_params */
+    const float* vol;       /* device geometry (cell volume fractions, N floats) or NULL, as
+                               umag_sim_params.vol: m = 0 where it is 0, demag source Ms*vol*m;
+                               it must stay valid while the handle is used */
 } umag_adj_params;
 typedef struct umag_adj umag_adj;
 int umag_adj_new(const umag_adj_params* p, umag_adj** out);

@@ -130,12 +130,17 @@ class Problem:
 
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, probe, avg_from, w_probe=1.0, w_target=1.0,
                  target=(0.0, 0.0, 1.0), demag=True, gamma_ll=GAMMA_LL, solver=4, backend="numpy", device="cuda",
-                 Dind=0.0, pbc=(0, 0, 0)):
+                 Dind=0.0, pbc=(0, 0, 0), geom=None):
         """backend: "numpy" (host) or "torch" (float64 on `device`), the same
         operations in the same order.  Dind: uniform interfacial DMI (J/m^2),
         a fixed (not differentiated) parameter.  pbc: periodic repetitions
         per axis (data/mesh.go): the demag kernel sums the images
-        (mag/demagkernel.go) and the stencils wrap (stencil.clh:13-29)."""
+        (mag/demagkernel.go) and the stencils wrap (stencil.clh:13-29).
+        geom: cell volume fractions (Nz, Ny, Nx) or None (engine/geom.go):
+        m is zero where geom is 0 (normalize2.cl), the demag source is
+        Ms * geom * m (copypadmul2.cl), and a neighbour outside the geometry
+        is a missing neighbour of the stencils (exchange.cl, dmi.cl: a zero
+        m)."""
         if solver not in (2, 4):
             raise ValueError("solver must be 4 (RK4) or 2 (Heun)")
         self.xp = _Numpy() if backend == "numpy" else _Torch(device)
@@ -157,6 +162,13 @@ class Problem:
         self.w = [2.0 / (c * c) for c in self.cell]
         self.D = float(Dind)
         self.pbc = tuple(int(p) for p in pbc)
+        shape = (self.N[2], self.N[1], self.N[0])
+        if geom is None:
+            self.vol, self.inside = None, None
+        else:
+            g = np.asarray(geom, np.float64).reshape(shape)
+            self.vol = self.xp.asarray(g)
+            self.inside = self.xp.asarray((g != 0).astype(np.float64))  # cells of the geometry
         # periodic flag per array axis of (3, Nz, Ny, Nx) fields
         self.per = {3: self.pbc[0] > 0, 2: self.pbc[1] > 0, 1: self.pbc[2] > 0}
         if self.D != 0:
@@ -170,6 +182,9 @@ class Problem:
                     shape[ax] = n
                     has = np.ones(n, bool) if self.per[ax] else (idx >= 0) & (idx < n)
                     self.ins[(ax, sd)] = self.xp.asarray(has.astype(np.float64).reshape(shape))
+                    if self.inside is not None:  # and the neighbour is in the geometry
+                        nbin = self.xp.take(self.inside[None], self.xp.index(self._nb(ax, n, sd)), ax)
+                        self.ins[(ax, sd)] = self.ins[(ax, sd)] * nbin
         self.demag = demag
         if demag:
             K = oracle.newell_kernel(self.N, self.cell, pbc=self.pbc)  # (6, Pz, Py, Px): xx yy zz yz xz xy
@@ -178,7 +193,8 @@ class Problem:
 
     # ------------------------------------------------------------ field
     def demag_field(self, v):
-        """mu0 * K * v (v already scaled by Ms), zero-padded convolution."""
+        """mu0 * K * v (v already scaled by Ms and the geometry), zero-padded
+        convolution."""
         Nx, Ny, Nz = self.N
         Pz, Py, Px = self.P
         xp = self.xp
@@ -198,28 +214,41 @@ class Problem:
         idx = np.arange(n) + sd
         return idx % n if self.per[ax] else np.clip(idx, 0, n - 1)
 
+    def _present(self, ax, n, sd):
+        """1 where the neighbour along array axis ax is in the geometry (a
+        neighbour outside it has m = 0, which the stencils treat as missing:
+        its term vanishes), or None without a geometry"""
+        if self.inside is None:
+            return None
+        return self.xp.take(self.inside[None], self.xp.index(self._nb(ax, n, sd)), ax)
+
     def stencil(self, v):
-        """sum_d w_d (v_neighbour - v) with clamped or wrapped neighbours (exchange.cl)."""
+        """sum_d w_d (v_neighbour - v) with clamped or wrapped neighbours
+        (exchange.cl), over the neighbours in the geometry and zero at cells
+        outside it; symmetric."""
         xp = self.xp
         out = xp.zeros_like(v)
         Nz = v.shape[1]
         axes = [(3, self.w[0]), (2, self.w[1])] + ([(1, self.w[2])] if Nz > 1 else [])
         for ax, w in axes:
             n = v.shape[ax]
-            lo = xp.take(v, xp.index(self._nb(ax, n, -1)), ax)
-            hi = xp.take(v, xp.index(self._nb(ax, n, 1)), ax)
-            out += w * ((lo - v) + (hi - v))
-        return out
+            for sd in (-1, 1):
+                nb = xp.take(v, xp.index(self._nb(ax, n, sd)), ax)
+                pr = self._present(ax, n, sd)
+                out += w * (nb - v) if pr is None else w * pr * (nb - v)
+        return out if self.inside is None else self.inside[None] * out
 
     def _zstencil(self, v):
-        """sum over z neighbours of (v_nb - v), clamped or wrapped (exchange.cl z terms)."""
+        """sum over z neighbours of (v_nb - v), clamped or wrapped, over the
+        neighbours in the geometry (exchange.cl z terms)."""
         xp = self.xp
         out = xp.zeros_like(v)
         n = v.shape[1]
         if n > 1:
-            lo = xp.take(v, xp.index(self._nb(1, n, -1)), 1)
-            hi = xp.take(v, xp.index(self._nb(1, n, 1)), 1)
-            out += (lo - v) + (hi - v)
+            for sd in (-1, 1):
+                nb = xp.take(v, xp.index(self._nb(1, n, sd)), 1)
+                pr = self._present(1, n, sd)
+                out += (nb - v) if pr is None else pr * (nb - v)
         return out
 
     def dmi(self, m, A):
@@ -248,7 +277,8 @@ class Problem:
                 Dc = D / c
                 h[d] += Dc * sd * mn[2]
                 h[2] -= Dc * sd * mn[d]
-        return h + (2.0 * A / (self.cell[2] ** 2)) * self._zstencil(m)
+        h = h + (2.0 * A / (self.cell[2] ** 2)) * self._zstencil(m)
+        return h if self.inside is None else self.inside[None] * h
 
     def dmi_dA(self, m, A):
         """d dmi(m, A) / dA: the exchange terms over A, and -D^2/(2A^2) times
@@ -266,11 +296,13 @@ class Problem:
                 bd = (1.0 - ins) * (-(D * D) / (2.0 * A * A))
                 g[d] += bd[0] * m[d]
                 g[2] += bd[0] * m[2]
-        return g + (2.0 / (self.cell[2] ** 2)) * self._zstencil(m)
+        g = g + (2.0 / (self.cell[2] ** 2)) * self._zstencil(m)
+        return g if self.inside is None else self.inside[None] * g
 
     def field(self, m, th):
         Ms, A, K1, Bext = th["Ms"], th["A"], th["K1"], th["B"]
-        B = self.demag_field(Ms * m) if self.demag else self.xp.zeros_like(m)
+        src = Ms * m if self.vol is None else Ms * self.vol * m
+        B = self.demag_field(src) if self.demag else self.xp.zeros_like(m)
         B = B + (self.dmi(m, A) if self.D != 0 else A * self.stencil(m)) / Ms
         if K1 != 0:
             mu = (m * self.ucol).sum(0)
@@ -282,7 +314,11 @@ class Problem:
         return self.gilb * (mxB + self.alpha * self.xp.cross(m, mxB))
 
     def normalize(self, v):
-        return v / self.xp.sqrt((v * v).sum(0))[None]
+        if self.inside is None:
+            return v / self.xp.sqrt((v * v).sum(0))[None]
+        ln = self.xp.sqrt((v * v).sum(0))
+        ln = ln + (1.0 - self.inside)  # no division by zero outside the geometry
+        return self.inside[None] * v / ln[None]
 
     def step(self, m, th, keep=False):
         h = self.h
@@ -346,14 +382,19 @@ class Problem:
 
     def _norm_vjp(self, u, w):
         ln = self.xp.sqrt((u * u).sum(0))[None]
+        if self.inside is not None:
+            ln = ln + (1.0 - self.inside[None])
         n = u / ln
-        return (w - n * (n * w).sum(0)[None]) / ln
+        g = (w - n * (n * w).sum(0)[None]) / ln
+        return g if self.inside is None else self.inside[None] * g
 
     def _field_vjp(self, m, wB, th, grads):
         Ms, A, K1 = th["Ms"], th["A"], th["K1"]
         gm = self.xp.zeros_like(m)
         if self.demag:
             dw = self.demag_field(wB)
+            if self.vol is not None:
+                dw = self.vol[None] * dw
             gm += Ms * dw
             grads["Ms"] += (m * dw).sum(0)
         if self.D != 0:

@@ -252,3 +252,67 @@ def test_periodic_gradients_match_fp64_oracle(N, pbc, dmi):
     print("relative gradient error vs FP64 (periodic):", errs)
     for k, e in errs.items():
         assert e < 1e-3, (k, e)
+
+
+# ---------------------------------------------------------------- geometry
+def _geometry(N, seed=3):
+    """A disc per layer with three empty cells inside and one cell of
+    volume fraction 0.6."""
+    rng = np.random.default_rng(seed)
+    Nx, Ny, Nz = N
+    yy, xx = np.mgrid[0:Ny, 0:Nx]
+    disc = (((xx - Nx / 2 + 0.5) / (Nx / 2)) ** 2 + ((yy - Ny / 2 + 0.5) / (Ny / 2)) ** 2 <= 1.0).astype(np.float32)
+    g = np.repeat(disc[None], Nz, axis=0)
+    inner = np.argwhere(g > 0)
+    pick = inner[rng.choice(len(inner), size=4, replace=False)]
+    for z, y, x in pick[:3]:
+        g[z, y, x] = 0.0
+    z, y, x = pick[3]
+    g[z, y, x] = 0.6
+    return g
+
+
+@pytest.mark.parametrize("N,dmi,solver", [((16, 12, 1), True, 4), ((16, 12, 3), False, 4), ((16, 12, 1), True, 2)])
+def test_geometry_forward_matches_engine(N, dmi, solver):
+    """With a geometry (holes, a partial cell) the adjoint's forward is the
+    engine's fixed-step run with the same geometry, bit for bit."""
+    from umagnus_b200.engine import Simulation
+    Ms, m0, kw = multilayer_case(N, 24, 21 + N[2])
+    g = _geometry(N)
+    D = M_D if dmi else 0.0
+    adj = gpu_sim(dict(kw, Dind=D, geom=g), K=8, solver=solver)
+    adj.forward(m0, Ms, M_AEX, M_KU1, M_BEXT)
+    m_adj = adj.final_m().cpu().numpy()
+    sim = Simulation(kw["N"], kw["cell"], Msat=Ms, Aex=M_AEX, alpha=kw["alpha"], Dind=D, Ku1=M_KU1,
+                     anisU=kw["anisU"], B_ext=M_BEXT, solver=solver, dt=kw["dt"], FixDt=kw["dt"], geom=g)
+    sim.set_m(m0)
+    sim.steps(24)
+    m_eng = sim.get_m().cpu().numpy().reshape(m_adj.shape)
+    assert np.array_equal(m_adj, m_eng), np.abs(m_adj - m_eng).max()
+    assert np.all(m_adj.reshape(3, -1)[:, g.ravel() == 0] == 0)
+
+
+@pytest.mark.parametrize("N,dmi,solver", [((16, 12, 1), True, 4), ((16, 12, 3), False, 4), ((16, 12, 2), True, 2)])
+def test_geometry_gradients_match_fp64_oracle(N, dmi, solver):
+    """Gradients with a geometry against the FP64 reverse pass with the same
+    geometry (pinned to central differences in tests/test_oracle_adjoint.py);
+    cells outside the geometry get zero Ms and m0 gradients."""
+    Ms, m0, kw = multilayer_case(N, 30, 13 + N[2])
+    g = _geometry(N)
+    D = M_D if dmi else 0.0
+    adj = gpu_sim(dict(kw, Dind=D, geom=g), K=8, solver=solver)
+    loss = adj.forward(m0, Ms, M_AEX, M_KU1, M_BEXT)
+    gr = adj.backward()
+    prob = R.Problem(solver=solver, Dind=D, geom=g, **kw)
+    th = R.params(Ms.astype(np.float64), M_AEX, M_KU1, M_BEXT)
+    loss64, g64 = prob.backward(m0.astype(np.float64), th)
+    assert abs(loss - loss64) <= 1e-5 * max(1.0, abs(loss64))
+    gms = gr["Ms"].cpu().numpy().reshape(g.shape)
+    assert np.all(gms[g == 0] == 0)
+    assert np.all(gr["m0"].cpu().numpy().reshape((3,) + g.shape)[:, g == 0] == 0)
+    errs = {"Ms": _rel(gms, g64["Ms"]), "m0": _rel(gr["m0"].cpu().numpy(), g64["m0"]),
+            "Aex": _rel(gr["Aex"], g64["A"]), "Ku1": _rel(gr["Ku1"], g64["K1"]),
+            "B_ext": _rel(gr["B_ext"], g64["B"])}
+    print("relative gradient error vs FP64 (geometry):", errs)
+    for k, e in errs.items():
+        assert e < 1e-3, (k, e)

@@ -164,3 +164,67 @@ def test_periodic_reverse_pass_matches_central_fd(N, pbc, D):
         fd = R.fd_gradient(prob, m0, th, which, rel=1e-4)
         ad = g[which[0]] if which[1] is None else g[which[0]][which[1]]
         assert abs(fd - ad) <= 1e-4 * abs(fd) + 1e-12 * max(1.0, abs(ad)), (which, fd, ad)
+
+
+def _holes(N, seed=9):
+    """A geometry with holes: a disc-like region plus a few empty cells
+    inside it, and one partial-volume cell."""
+    rng = np.random.default_rng(seed)
+    Nx, Ny, Nz = N
+    yy, xx = np.mgrid[0:Ny, 0:Nx]
+    disc = (((xx - Nx / 2 + 0.5) / (Nx / 2)) ** 2 + ((yy - Ny / 2 + 0.5) / (Ny / 2)) ** 2 <= 1.0).astype(np.float64)
+    g = np.repeat(disc[None], Nz, axis=0)
+    inner = np.argwhere(g > 0)
+    for z, y, x in inner[rng.choice(len(inner), size=3, replace=False)]:
+        g[z, y, x] = 0.0
+    z, y, x = inner[rng.choice(len(inner))]
+    if g[z, y, x] > 0:
+        g[z, y, x] = 0.6
+    return g
+
+
+@pytest.mark.parametrize("D", [3e-3, 0.0])
+def test_geometry_operators_are_symmetric_and_restate_the_reference(D):
+    """With a geometry the masked exchange stencil and the DMI field stay
+    their own transposes, and the DMI field equals the CPU oracle's dmi.cl
+    restatement on the masked state (a zero m is a missing neighbour)."""
+    from oracle import oracle as O
+    N = (9, 8, 3)
+    g = _holes(N)
+    prob, m0, th, rng = dmi_case(N=N, D=D if D else 3e-3)
+    prob = R.Problem(N, prob.cell, 0.3, (0.0, 0.0, 1.0), 5e-14, 4, (1, 1, 2, 2), 3, Dind=D, geom=g)
+    m = prob.normalize(m0)
+    assert np.all(m[:, g == 0] == 0)
+    x, y = rng.normal(size=m.shape) * (g > 0), rng.normal(size=m.shape) * (g > 0)
+    A = th["A"]
+    for op in ((lambda v: prob.dmi(v, A)) if D else None, prob.stencil):
+        if op is None:
+            continue
+        lhs, rhs = (x * op(y)).sum(), (op(x) * y).sum()
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+    if D:
+        B = np.zeros_like(m)
+        O.add_dmi(B, m, O.exch_lut(np.full(256, A), dtype=np.float64), O.exch_lut(np.full(256, D), dtype=np.float64),
+                  np.zeros(m.shape[1:], np.uint8), prob.cell, 1.0)
+        h = prob.dmi(m, A)
+        assert np.abs(h - B * (g > 0)).max() <= 1e-13 * np.abs(B).max()
+
+
+@pytest.mark.parametrize("N,D,solver", [((10, 8, 1), 3e-3, 4), ((8, 8, 2), 0.0, 4), ((10, 8, 1), 3e-3, 2)])
+def test_geometry_reverse_pass_matches_central_fd(N, D, solver):
+    """With a geometry (holes and a partial cell): the reverse pass against
+    central differences."""
+    g = _holes(N)
+    prob0, m0, th, rng = dmi_case(N=N, solver=solver)
+    prob = R.Problem(N, prob0.cell, 0.3, (0.0, 0.0, 1.0), 5e-14, 20, (1, 1, N[0] // 2, N[1] // 2), 16,
+                     target=np.array([0.0, 0.6, 0.8]), solver=solver, Dind=D, geom=g)
+    _, gr = prob.backward(m0, th)
+    assert np.all(gr["Ms"][g == 0] == 0) and np.all(gr["m0"][:, g == 0] == 0)
+    checks = [("A", None), ("K1", None), ("B", 0), ("B", 1), ("B", 2)]
+    cells = np.argwhere(g > 0)
+    for z, y, x in cells[rng.choice(len(cells), size=12, replace=False)]:
+        checks.append(("Ms", (int(z), int(y), int(x))))
+    for which in checks:
+        fd = R.fd_gradient(prob, m0, th, which, rel=1e-4)
+        ad = gr[which[0]] if which[1] is None else gr[which[0]][which[1]]
+        assert abs(fd - ad) <= 1e-4 * abs(fd) + 1e-12 * max(1.0, abs(ad)), (which, fd, ad)

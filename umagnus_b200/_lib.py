@@ -64,7 +64,8 @@ class AdjParams(ctypes.Structure):
                 ("enable_demag", c_int), ("demag_kernel", c_int), ("demag_accuracy", c_double),
                 ("dt", c_double), ("gamma_ll", c_double), ("nsteps", c_int), ("K", c_int), ("probe", c_int * 4),
                 ("avg_from", c_int), ("w_probe", c_double), ("w_target", c_double), ("target", c_double * 3),
-                ("no_graph", c_int), ("solver", c_int), ("Dind", c_float), ("pbc", c_int * 3)]
+                ("no_graph", c_int), ("solver", c_int), ("Dind", c_float), ("pbc", c_int * 3),
+                ("vol", c_void_p)]
 
 
 # name -> argtypes (restype int unless listed in _RESTYPE)

@@ -4,7 +4,8 @@ No counterpart in the reference, which has no gradients.  The forward pass
 is the engine's effective field (demag, exchange, uniaxial anisotropy,
 Zeeman; engine/effectivefield.go:14-24) and LL torque (engine/torque.go)
 for a per-cell Ms map and uniform Aex, Ku1, B_ext and alpha (and a fixed
-uniform interfacial DMI, Dind), on an open or periodic mesh (pbc), stepped
+uniform interfacial DMI, Dind), on an open or periodic mesh (pbc) with an
+optional geometry (geom: cell volume fractions), stepped
 by fixed-step RK4 (engine/rk4.go with FixDt) or Heun (engine/heun.go,
 solver=2), m checkpointed every K steps.
 The loss is
@@ -33,7 +34,7 @@ GAMMA_LL = 1.7595e11  # engine/torque.go:27
 class AdjointRK4:
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, K, probe, avg_from, w_probe=1.0, w_target=1.0,
                  target=(0.0, 0.0, 1.0), demag=True, demag_kernel="newell", demag_accuracy=6.0, gamma_ll=GAMMA_LL,
-                 use_graph=True, device=0, solver=4, Dind=0.0, pbc=(0, 0, 0)):
+                 use_graph=True, device=0, solver=4, Dind=0.0, pbc=(0, 0, 0), geom=None):
         self.L = _lib.init(device)
         p = AdjParams()
         p.N[:] = [int(n) for n in N]
@@ -53,6 +54,12 @@ class AdjointRK4:
         p.solver = int(solver)  # 4 RK4, 2 Heun
         p.Dind = float(Dind)    # interfacial DMI (fixed parameter)
         p.pbc[:] = [int(v) for v in pbc]  # periodic repetitions per axis (engine/mesh.go SetPBC)
+        self._vol = None
+        if geom is not None:  # cell volume fractions (engine/geom.go), kept on the device
+            g = torch.as_tensor(np.asarray(geom, np.float32)).reshape(-1)
+            self._vol = g.to(torch.device("cuda", device)).contiguous()
+            torch.cuda.synchronize()
+            p.vol = self._vol.data_ptr()
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
         h = ctypes.c_void_p()

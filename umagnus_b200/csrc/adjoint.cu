@@ -45,6 +45,7 @@ struct AdjField {
     Mesh3 g;
     int N;
     const float* Ms;   // per-cell map
+    const float* vol;  // geometry (cell volume fractions) or NULL: m is zero where it is 0
     PairCoef pc;       // exchange pair coefficients w_d * A (region (0,0)); with DMI also 2A/c^2, D/c, c D/(2A)
     int dmi;           // exchange + interfacial DMI (dmi.cl) instead of exchange (exchange.cl)
     float dq[2];       // DMI: (D/c)(c D/(2A)) = D^2/(2A) per in-plane axis, the missing neighbour's net weight
@@ -148,7 +149,8 @@ __global__ void __launch_bounds__(256) k_adj_stage_fwd(AdjField a, StepFac f, in
             v[c] = s;
         }
         // Heun's predictor is not normalised (heun.go:31)
-        const f3 r = (f.heun && q == 0) ? f3{v[0], v[1], v[2]} : normalize_vol(f3{v[0], v[1], v[2]}, 1.0f);
+        const f3 r = (f.heun && q == 0) ? f3{v[0], v[1], v[2]}
+                                        : normalize_vol(f3{v[0], v[1], v[2]}, a.vol ? a.vol[I] : 1.0f);
         st3(mnext, N, I, r);
         if (psum && in_probe(a, I)) acc += (double)r.z;
     }
@@ -285,12 +287,20 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, in
         const f3 m0 = ld3p(mq, N, I);
         f3 g = ld3p(gm, N, I);
         double gms = 0;
+        // geometry: a cell outside it has m = 0, no exchange/DMI field, and
+        // is a missing neighbour of the stencils (a zero m in exchange.cl and
+        // dmi.cl); the demag source carries the volume fraction
+        const float vI = a.vol ? a.vol[I] : 1.0f;
+        auto hole = [&](int j) { return a.vol != nullptr && a.vol[j] == 0.f; };
         if (dw) {
-            const f3 d = ld3p(dw, N, I);
+            const f3 d = sc3(vI, ld3p(dw, N, I));
             g = ad3(g, sc3(ms, d));
             gms += (double)m0.x * d.x + (double)m0.y * d.y + (double)m0.z * d.z;
         }
-        if (a.dmi) {
+        if (vI == 0.f) {
+            // outside the geometry: no local field terms (the normalisation's
+            // VJP zeroes this cell's cotangent)
+        } else if (a.dmi) {
             // h = A E(m) + D R(m) + (D^2/2A) P(m) (dmi.cl with the missing in-plane
             // neighbours extrapolated): linear in m and symmetric, so the
             // cotangent x = wB/Ms goes through the same stencil, with the
@@ -304,14 +314,14 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, in
                 for (int sd = -1; sd <= 1; sd += 2) {
                     // a periodic axis has every neighbour (wrapped)
                     const bool per = (a.g.pbc & (d == 0 ? 1 : 2)) != 0;
-                    const bool in = per || (d == 0 ? (sd < 0 ? ix > 0 : ix + 1 < a.g.Nx)
-                                                   : (sd < 0 ? iy > 0 : iy + 1 < a.g.Ny));
+                    const int j = d == 0 ? (iz * a.g.Ny + iy) * a.g.Nx + (sd < 0 ? lclamp(ix - 1, a.g.Nx, per)
+                                                                                  : hclamp(ix + 1, a.g.Nx, per))
+                                         : (iz * a.g.Ny + (sd < 0 ? lclamp(iy - 1, a.g.Ny, per)
+                                                                  : hclamp(iy + 1, a.g.Ny, per))) * a.g.Nx + ix;
+                    const bool in = (per || (d == 0 ? (sd < 0 ? ix > 0 : ix + 1 < a.g.Nx)
+                                                    : (sd < 0 ? iy > 0 : iy + 1 < a.g.Ny))) && !hole(j);
                     const float S = d == 0 ? a.pc.sx : a.pc.sy, Dc = (d == 0 ? a.pc.dcx : a.pc.dcy) * sd;
                     if (in) {
-                        const int j = d == 0 ? (iz * a.g.Ny + iy) * a.g.Nx + (sd < 0 ? lclamp(ix - 1, a.g.Nx, per)
-                                                                                      : hclamp(ix + 1, a.g.Nx, per))
-                                             : (iz * a.g.Ny + (sd < 0 ? lclamp(iy - 1, a.g.Ny, per)
-                                                                      : hclamp(iy + 1, a.g.Ny, per))) * a.g.Nx + ix;
                         const float msj = a.Ms[j];
                         const float ij = msj == 0.f ? 0.f : 1.0f / msj;
                         const f3 xn{wB[j] * ij, wB[N + j] * ij, wB[2 * N + j] * ij};
@@ -333,6 +343,7 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, in
                     const bool pz = (a.g.pbc & 4) != 0;
                     const int j = ((sd < 0 ? lclamp(iz - 1, a.g.Nz, pz) : hclamp(iz + 1, a.g.Nz, pz)) * a.g.Ny +
                                    iy) * a.g.Nx + ix;
+                    if (hole(j)) continue;  // a zero neighbour: the term vanishes
                     const float msj = a.Ms[j];
                     const float ij = msj == 0.f ? 0.f : 1.0f / msj;
                     lx = ad3(lx, sc3(a.pc.sz, f3{wB[j] * ij - x0.x, wB[N + j] * ij - x0.y, wB[2 * N + j] * ij - x0.z}));
@@ -362,6 +373,7 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, in
             for (int k = 0; k < nn; k++) {
                 const float s = k < 2 ? a.pc.wax : (k < 4 ? a.pc.way : a.pc.waz);
                 const int j = nb[k];
+                if (hole(j)) continue;  // a zero neighbour: the term vanishes
                 const float msj = a.Ms[j];
                 const float ij = msj == 0.f ? 0.f : 1.0f / msj;
                 sx = ad3(sx, sc3(s, f3{wB[j] * ij - x0.x, wB[N + j] * ij - x0.y, wB[2 * N + j] * ij - x0.z}));
@@ -424,9 +436,11 @@ __global__ void k_adj_loss_final(AdjField a, float* lam, float wprobe, float gx,
 }
 
 // dL/dm0 through the initial normalisation
-__global__ void k_adj_m0(int N, const float* __restrict__ m0, const float* __restrict__ lam, float* gm0) {
+// (zero outside the geometry, where the normalisation gives m = 0)
+__global__ void k_adj_m0(int N, const float* __restrict__ m0, const float* __restrict__ lam, float* gm0,
+                         const float* __restrict__ vol) {
     for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < N; I += gridDim.x * blockDim.x)
-        st3(gm0, N, I, norm_vjp(ld3p(m0, N, I), ld3p(lam, N, I)));
+        st3(gm0, N, I, (vol && vol[I] == 0.f) ? f3{0.f, 0.f, 0.f} : norm_vjp(ld3p(m0, N, I), ld3p(lam, N, I)));
 }
 
 // per-cell accumulators -> gMs (float) and the five scalar sums, in a fixed
@@ -503,6 +517,7 @@ static AdjField adj_field(const AdjImpl* s) {
     a.g = s->g;
     a.N = s->N;
     a.Ms = s->Ms;
+    a.vol = s->p.vol;
     // engine/exchange.go: w_d = 2/c_d^2 (float32), coefficient w_d * A(0,0)
     const float wx = (float)(2 / (s->p.cell[0] * s->p.cell[0])), wy = (float)(2 / (s->p.cell[1] * s->p.cell[1])),
                 wz = (float)(2 / (s->p.cell[2] * s->p.cell[2]));
@@ -556,7 +571,8 @@ static StepFac step_fac(float h, bool heun) {
 
 static unsigned gridN(const AdjImpl* s) { return (unsigned)grid_for(s->N, 256); }
 
-// demag of v (3N) into out: Ms map (forward) or Ms = 1 (cotangent)
+// demag of v (3N) into out: Ms map and geometry (forward), or Ms = 1 and no
+// geometry (cotangent: the reverse kernel applies Ms and vol per cell)
 static int adj_demag(AdjImpl* s, const float* v, const float* Ms, float* out) {
     if (!s->demag) return UMAG_OK;
     PassArgs a{};
@@ -564,6 +580,7 @@ static int adj_demag(AdjImpl* s, const float* v, const float* Ms, float* out) {
     for (int c = 0; c < 3; c++) { a.m[c] = v + (size_t)c * s->N; a.B[c] = out + (size_t)c * s->N; }
     a.Ms = Ms;
     a.Ms_mul = 1.0f;
+    a.vol = Ms ? s->p.vol : nullptr;
     return demag_launch(s->demag, a, AS());
 }
 
@@ -721,7 +738,7 @@ int adj_forward(umag_adj* hd, const float* m0, const float* Ms, float A, float K
     UMAG_CUDA(cudaMemcpyAsync(s->w(W_M0), m0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
     float* a0 = s->w(W_A);
     UMAG_CUDA(cudaMemcpyAsync(a0, m0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
-    UMAG_TRY(normalize(a0, a0 + s->N, a0 + 2 * (size_t)s->N, nullptr, s->N));  // engine/magnetization.go:34
+    UMAG_TRY(normalize(a0, a0 + s->N, a0 + 2 * (size_t)s->N, s->p.vol, s->N));  // engine/magnetization.go:34
     UMAG_CUDA(cudaMemsetAsync(s->dsum, 0, sizeof(double) * 8, AS()));
     const int nseg = (p.nsteps + p.K - 1) / p.K;
     const std::string pk = param_key(s);
@@ -852,7 +869,7 @@ int adj_backward(umag_adj* hd, float* gMs, float* gm0, double* gA, double* gK1, 
         UMAG_TRY(adj_run(s, key, [&]() { return adj_rev_segment(s, af, f, n_begin, len, wprobe); }));
     }
     if (gm0) {
-        k_adj_m0<<<G, 256, 0, AS()>>>(N, s->w(W_M0), s->w(W_LAM), gm0);
+        k_adj_m0<<<G, 256, 0, AS()>>>(N, s->w(W_M0), s->w(W_LAM), gm0, s->p.vol);
         UMAG_LAUNCH_CHECK();
     }
     k_adj_reduce<<<1, 1024, 0, AS()>>>(N, s->acc, gMs, s->dsum);

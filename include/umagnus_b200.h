@@ -436,8 +436,9 @@ int umag_ens_set_tuning(umag_ens* e, int cls, const umag_tuning* t);
 
 /* ---- differentiable simulation: forward RK4 and its adjoint --------------
  * No counterpart in the reference (which has no gradients).  A thin film or
- * block with a per-cell Ms map, uniform exchange Aex, uniaxial Ku1 along
- * anisU, Zeeman field B_ext and damping alpha, integrated by fixed-step RK4
+ * block (open or periodic, optionally with a geometry) with a per-cell Ms
+ * map, uniform exchange Aex, uniaxial Ku1 along anisU, Zeeman field B_ext,
+ * an optional fixed interfacial DMI and damping alpha, integrated by fixed-step RK4
  * (engine/rk4.go with FixDt) or Heun (engine/heun.go) for nsteps steps; m is checkpointed every K
  * steps.  Loss = w_probe * (mean over states avg_from..nsteps of the mean
  * m_z over the probe window of layer 0) + w_target * |<m>(final) - target|^2.

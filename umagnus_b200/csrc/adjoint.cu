@@ -8,7 +8,8 @@
 // dt and every stage normalised, or Heun (engine/heun.go:27-43: predictor
 // y1 = m + h k0 not normalised, result normalize(y1 + h/2 k1 - h/2 k0)).
 // Parameters: a per-cell Ms map, uniform A,
-// K1 and B_ext (the differentiable ones) and uniform alpha and easy axis.
+// K1 and B_ext (the differentiable ones) and uniform alpha and easy axis, on
+// an open or periodic mesh, with an optional geometry (volume fractions).
 // Loss: w_probe * mean over states avg_from..nsteps of the mean m_z over a
 // probe window + w_target * |<m>_final - target|^2.
 //

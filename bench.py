@@ -1157,8 +1157,9 @@ def main():
     if world > 1:
         import torch.distributed as dist_mod
     # the ensemble (sharded over the ranks, no collective during the run) and,
-    # at N = 1, the differentiation workload: the north star's other two
-    # targets, measured in the same run (outside the multilayer's timed region)
+    # at N = 1, the differentiation workload: the batched-against-plain and
+    # backward-over-forward figures, measured in the same run (outside the
+    # multilayer's timed region)
     if not args.no_ensemble:
         ens = ensemble_measure(args, rank, world, dist_mod, local_rank, plain=(world == 1),
                                fp64_check=not args.no_fp64_check)

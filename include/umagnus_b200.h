@@ -469,6 +469,11 @@ typedef struct {
     const float* vol;       /* device geometry (cell volume fractions, N floats) or NULL, as
                                umag_sim_params.vol: m = 0 where it is 0, demag source Ms*vol*m;
                                it must stay valid while the handle is used */
+    const uint8_t* regions; /* device region map (N bytes, values < nregions) or NULL; with it
+                               Aex, Ku1 and B_ext are per region (the _regions entry points), the
+                               exchange of a cell pair the engine's harmonic-mean LUT
+                               (engine/exchange.go:153-167); not with Dind */
+    int nregions;           /* 1..256 with a region map */
 } umag_adj_params;
 typedef struct umag_adj umag_adj;
 int umag_adj_new(const umag_adj_params* p, umag_adj** out);
@@ -481,6 +486,13 @@ int umag_adj_final_m(umag_adj* a, float* m);
 /* gradients of the last forward's loss: gMs device N floats, gm0 device 3N
  * floats or NULL; the scalars on the host */
 int umag_adj_backward(umag_adj* a, float* gMs, float* gm0, double* gAex, double* gKu1, double gB_ext[3]);
+/* With a region map: Aex, Ku1 host arrays of nregions values, B_ext host
+ * [nregions][3] (T); the gradients per region in host arrays of the same
+ * shapes (gMs device N floats, gm0 device 3N floats or NULL).  No
+ * counterpart in the reference. */
+int umag_adj_forward_regions(umag_adj* a, const float* m0, const float* Ms, const float* Aex, const float* Ku1,
+                             const float* B_ext, double* loss);
+int umag_adj_backward_regions(umag_adj* a, float* gMs, float* gm0, double* gAex, double* gKu1, double* gB_ext);
 
 /* ---- field files (oommf/*.go, dump/*.go) ----------------------------------
  * Host arrays of float32, structure of arrays [c][z][y][x] (x fastest), the

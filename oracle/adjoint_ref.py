@@ -130,7 +130,7 @@ class Problem:
 
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, probe, avg_from, w_probe=1.0, w_target=1.0,
                  target=(0.0, 0.0, 1.0), demag=True, gamma_ll=GAMMA_LL, solver=4, backend="numpy", device="cuda",
-                 Dind=0.0, pbc=(0, 0, 0), geom=None):
+                 Dind=0.0, pbc=(0, 0, 0), geom=None, regions=None):
         """backend: "numpy" (host) or "torch" (float64 on `device`), the same
         operations in the same order.  Dind: uniform interfacial DMI (J/m^2),
         a fixed (not differentiated) parameter.  pbc: periodic repetitions
@@ -140,7 +140,11 @@ class Problem:
         m is zero where geom is 0 (normalize2.cl), the demag source is
         Ms * geom * m (copypadmul2.cl), and a neighbour outside the geometry
         is a missing neighbour of the stencils (exchange.cl, dmi.cl: a zero
-        m)."""
+        m).  regions: a region map (Nz, Ny, Nx) of small integers or None;
+        with it the parameters A, K1 are per-region arrays and B a
+        (regions, 3) array, the exchange coefficient of a cell pair is the
+        harmonic mean of its regions' A (engine/exchange.go:153-167), and
+        the gradients come per region (no interfacial DMI with regions)."""
         if solver not in (2, 4):
             raise ValueError("solver must be 4 (RK4) or 2 (Heun)")
         self.xp = _Numpy() if backend == "numpy" else _Torch(device)
@@ -163,6 +167,13 @@ class Problem:
         self.D = float(Dind)
         self.pbc = tuple(int(p) for p in pbc)
         shape = (self.N[2], self.N[1], self.N[0])
+        if regions is None:
+            self.reg = None
+        else:
+            if float(Dind) != 0:
+                raise ValueError("region maps with interfacial DMI are not supported here")
+            self.reg = np.asarray(regions).astype(np.int64).reshape(shape)
+            self.nreg = int(self.reg.max()) + 1
         if geom is None:
             self.vol, self.inside = None, None
         else:
@@ -299,10 +310,72 @@ class Problem:
         g = g + (2.0 / (self.cell[2] ** 2)) * self._zstencil(m)
         return g if self.inside is None else self.inside[None] * g
 
+    # ------------------------------------------------------------ regions
+    def _pair(self, A, ax, n, sd):
+        """exchange coefficient of each cell with its neighbour along array
+        axis ax: the harmonic mean of the two regions' A, and its derivative
+        with respect to the cell's own region's A (A_i^2 / ... = a^2/(2 A_i^2))"""
+        A = np.asarray(A, np.float64)
+        ri = self.reg
+        rj = np.take(self.reg[None], self._nb(ax, n, sd), ax)[0]
+        Ai, Aj = A[ri], A[rj]
+        a = 2.0 / (1.0 / Ai + 1.0 / Aj)
+        return self.xp.asarray(a), self.xp.asarray(a * a / (2.0 * Ai * Ai))
+
+    def _stencil_r(self, v, A, dA=False):
+        """the exchange stencil with per-pair coefficients (sum_d w_d a_ij
+        (v_j - v_i)); dA: with the derivatives w.r.t. the cell's region's A
+        instead of the coefficients"""
+        xp = self.xp
+        out = xp.zeros_like(v)
+        Nz = v.shape[1]
+        axes = [(3, self.w[0]), (2, self.w[1])] + ([(1, self.w[2])] if Nz > 1 else [])
+        for ax, w in axes:
+            n = v.shape[ax]
+            for sd in (-1, 1):
+                nb = xp.take(v, xp.index(self._nb(ax, n, sd)), ax)
+                a, da = self._pair(A, ax, n, sd)
+                c = (da if dA else a)[None]
+                pr = self._present(ax, n, sd)
+                out += w * c * (nb - v) if pr is None else w * c * pr * (nb - v)
+        return out if self.inside is None else self.inside[None] * out
+
+    def _pair_grad(self, m, x, A):
+        """dL/dA per region: at each cell i, sum over its neighbours j of
+        (c_ij + c_ji) da_ij/dA_i, c_ij = w_d x_i.(m_j - m_i) (the field
+        cotangent over Ms); every pair is seen from both cells, so each side
+        takes the derivative with respect to its own region's A"""
+        xp = self.xp
+        g = xp.zeros_like(m[0])
+        Nz = m.shape[1]
+        axes = [(3, self.w[0]), (2, self.w[1])] + ([(1, self.w[2])] if Nz > 1 else [])
+        for ax, w in axes:
+            n = m.shape[ax]
+            for sd in (-1, 1):
+                idx = xp.index(self._nb(ax, n, sd))
+                mj, xj = xp.take(m, idx, ax), xp.take(x, idx, ax)
+                _, da = self._pair(A, ax, n, sd)
+                c = (x * (mj - m)).sum(0) + (xj * (m - mj)).sum(0)
+                pr = self._present(ax, n, sd)
+                g += w * da * c if pr is None else w * da * pr[0] * c
+        if self.inside is not None:
+            g = g * self.inside
+        return self._bin(g)
+
+    def _rmap(self, vals):
+        """a per-region value (or 3-vector) as a field"""
+        v = np.asarray(vals, np.float64)
+        return self.xp.asarray(v[self.reg] if v.ndim == 1 else np.moveaxis(v[self.reg], -1, 0))
+
     def field(self, m, th):
         Ms, A, K1, Bext = th["Ms"], th["A"], th["K1"], th["B"]
         src = Ms * m if self.vol is None else Ms * self.vol * m
         B = self.demag_field(src) if self.demag else self.xp.zeros_like(m)
+        if self.reg is not None:
+            B = B + self._stencil_r(m, A) / Ms
+            mu = (m * self.ucol).sum(0)
+            B = B + (2 * self._rmap(K1) / Ms * mu)[None] * self.ucol
+            return B + self._rmap(Bext)
         B = B + (self.dmi(m, A) if self.D != 0 else A * self.stencil(m)) / Ms
         if K1 != 0:
             mu = (m * self.ucol).sum(0)
@@ -366,6 +439,9 @@ class Problem:
     def _params(self, th):
         """th on this backend (Ms a field, B a 3-vector, A and K1 floats)."""
         xp = self.xp
+        if self.reg is not None:  # per-region arrays (host)
+            return {"Ms": xp.asarray(th["Ms"]), "A": np.asarray(th["A"], np.float64),
+                    "K1": np.asarray(th["K1"], np.float64), "B": np.asarray(th["B"], np.float64)}
         return {"Ms": xp.asarray(th["Ms"]), "A": float(th["A"]), "K1": float(th["K1"]), "B": xp.asarray(th["B"])}
 
     # ------------------------------------------------------------ adjoint
@@ -388,6 +464,10 @@ class Problem:
         g = (w - n * (n * w).sum(0)[None]) / ln
         return g if self.inside is None else self.inside[None] * g
 
+    def _bin(self, f):
+        """sum of a per-cell field over each region (host)"""
+        return np.bincount(self.reg.ravel(), weights=self.xp.host(f).ravel(), minlength=self.nreg)
+
     def _field_vjp(self, m, wB, th, grads):
         Ms, A, K1 = th["Ms"], th["A"], th["K1"]
         gm = self.xp.zeros_like(m)
@@ -397,6 +477,23 @@ class Problem:
                 dw = self.vol[None] * dw
             gm += Ms * dw
             grads["Ms"] += (m * dw).sum(0)
+        if self.reg is not None:
+            # exchange: the per-pair operator is symmetric; dL/dA_r collects,
+            # at each cell of region r, (c_ij + c_ji) da_ij/dA_i over its
+            # neighbours, c_ij = w_d (wB_i/Ms_i).(m_j - m_i)
+            x = wB / Ms
+            e = self._stencil_r(m, A)
+            gm += self._stencil_r(x, A)
+            grads["Ms"] -= (wB * e).sum(0) / Ms ** 2
+            grads["A"] += self._pair_grad(m, x, A)
+            mu = (m * self.ucol).sum(0)
+            wu = (wB * self.ucol).sum(0)
+            K1c = self._rmap(K1)
+            gm += (2 * K1c / Ms * wu)[None] * self.ucol
+            grads["Ms"] -= 2 * K1c * mu * wu / Ms ** 2
+            grads["K1"] += self._bin(2 * mu * wu / Ms)
+            grads["B"] += np.stack([self._bin(wB[c]) for c in range(3)], axis=1)
+            return gm
         if self.D != 0:
             h = self.dmi(m, A)
             gm += self.dmi(wB / Ms, A)  # the operator is symmetric
@@ -445,7 +542,11 @@ class Problem:
         th = self._params(th)
         loss, states = self.forward(m0, th, keep=True)
         xp = self.xp
-        grads = {"Ms": xp.zeros_like(th["Ms"]), "A": 0.0, "K1": 0.0, "B": xp.zeros((3,))}
+        if self.reg is not None:
+            grads = {"Ms": xp.zeros_like(th["Ms"]), "A": np.zeros(self.nreg), "K1": np.zeros(self.nreg),
+                     "B": np.zeros((self.nreg, 3))}
+        else:
+            grads = {"Ms": xp.zeros_like(th["Ms"]), "A": 0.0, "K1": 0.0, "B": xp.zeros((3,))}
         h = self.h
         lam = self._loss_grad(states[-1], self.nsteps >= self.avg_from, True)
         fin = (h / 6, h / 3, h / 3, h / 6)
@@ -475,18 +576,26 @@ class Problem:
             if n - 1 >= self.avg_from:
                 lam = lam + self._loss_grad(states[n - 1], True, False)
         grads["m0"] = self._norm_vjp(xp.asarray(m0), lam)
-        grads = {k: (float(v) if k in ("A", "K1") else xp.host(v)) for k, v in grads.items()}
+        if self.reg is not None:
+            grads = {k: (v if isinstance(v, np.ndarray) else xp.host(v)) for k, v in grads.items()}
+        else:
+            grads = {k: (float(v) if k in ("A", "K1") else xp.host(v)) for k, v in grads.items()}
         return loss, grads
 
 
 def params(Ms, A, K1, B):
-    return {"Ms": np.asarray(Ms, np.float64), "A": float(A), "K1": float(K1), "B": np.asarray(B, np.float64)}
+    """the parameter record: scalars A, K1 and a 3-vector B, or per-region
+    arrays (A[r], K1[r], B[r, c]) for a problem with a region map"""
+    def sc(v):
+        return float(v) if np.ndim(v) == 0 else np.asarray(v, np.float64)
+    return {"Ms": np.asarray(Ms, np.float64), "A": sc(A), "K1": sc(K1), "B": np.asarray(B, np.float64)}
 
 
 def fd_gradient(prob, m0, th, which, rel=1e-4):
     """Central finite differences of the FP64 loss with relative step rel.
 
-    which: ("Ms", (z, y, x)), ("A", None), ("K1", None) or ("B", c); for a
+    which: ("Ms", (z, y, x)), ("A", None), ("K1", None) or ("B", c), or
+    with a region map ("A", r), ("K1", r), ("B", (r, c)); for a
     zero-valued parameter the step is rel (absolute)."""
     name, idx = which
 

@@ -228,3 +228,61 @@ def test_geometry_reverse_pass_matches_central_fd(N, D, solver):
         fd = R.fd_gradient(prob, m0, th, which, rel=1e-4)
         ad = gr[which[0]] if which[1] is None else gr[which[0]][which[1]]
         assert abs(fd - ad) <= 1e-4 * abs(fd) + 1e-12 * max(1.0, abs(ad)), (which, fd, ad)
+
+
+def region_case(N=(10, 8, 1), steps=16, seed=8, solver=4, geom=None, pbc=(0, 0, 0)):
+    """Three regions (stripes along x and a block) with their own A, K1 and
+    applied field."""
+    rng = np.random.default_rng(seed)
+    shape = (N[2], N[1], N[0])
+    reg = np.zeros(shape, np.uint8)
+    reg[:, :, N[0] // 3:] = 1
+    reg[:, N[1] // 2:, 2 * N[0] // 3:] = 2
+    Ms = rng.uniform(9e5, 1.2e6, shape)
+    m0 = rng.normal(size=(3,) + shape)
+    t = rng.normal(size=3)
+    t /= np.linalg.norm(t)
+    prob = R.Problem(N, (2e-9, 2e-9, 1e-9), 0.3, (0.0, 0.6, 0.8), 5e-14, steps, (1, 1, N[0] // 2, N[1] // 2),
+                     steps - steps // 4 + 1, target=t, solver=solver, regions=reg, geom=geom, pbc=pbc)
+    th = R.params(Ms, [1.6e-11, 0.9e-11, 1.3e-11], [5e5, 2e5, 0.0],
+                  [(0.0, 0.0, 0.05), (0.02, 0.0, 0.03), (0.0, -0.01, 0.04)])
+    return prob, m0, th, rng, reg
+
+
+def test_one_region_equals_the_uniform_problem():
+    """A region map with a single region gives the uniform problem's loss
+    and gradients (per-region arrays of length one)."""
+    N = (9, 7, 2)
+    prob, m0, th, rng, reg = region_case(N=N)
+    one = np.zeros_like(reg)
+    pr = R.Problem(N, prob.cell, 0.3, (0.0, 0.6, 0.8), 5e-14, 16, prob.probe, prob.avg_from, target=prob.target,
+                   regions=one)
+    pu = R.Problem(N, prob.cell, 0.3, (0.0, 0.6, 0.8), 5e-14, 16, prob.probe, prob.avg_from, target=prob.target)
+    thr = R.params(th["Ms"], [1.4e-11], [3e5], [(0.01, 0.0, 0.05)])
+    thu = R.params(th["Ms"], 1.4e-11, 3e5, (0.01, 0.0, 0.05))
+    lr, gr = pr.backward(m0, thr)
+    lu, gu = pu.backward(m0, thu)
+    assert abs(lr - lu) <= 1e-14 * abs(lu)
+    assert abs(gr["A"][0] - gu["A"]) <= 1e-10 * abs(gu["A"])
+    assert abs(gr["K1"][0] - gu["K1"]) <= 1e-10 * abs(gu["K1"])
+    np.testing.assert_allclose(gr["B"][0], gu["B"], rtol=1e-10)
+    np.testing.assert_allclose(gr["Ms"], gu["Ms"], rtol=1e-9, atol=1e-12 * np.abs(gu["Ms"]).max())
+
+
+@pytest.mark.parametrize("N,geom,pbc", [((10, 8, 1), False, (0, 0, 0)), ((8, 8, 2), True, (0, 0, 0)),
+                                        ((10, 8, 1), False, (2, 0, 0))])
+def test_region_reverse_pass_matches_central_fd(N, geom, pbc):
+    """Per-region A (pair coefficients the harmonic means), K1 and B_ext
+    with a region map, on an open, masked or periodic mesh: the reverse
+    pass against central differences."""
+    g = _holes(N) if geom else None
+    prob, m0, th, rng, reg = region_case(N=N, geom=g, pbc=pbc)
+    _, gr = prob.backward(m0, th)
+    checks = [("A", 0), ("A", 1), ("A", 2), ("K1", 0), ("K1", 1), ("B", (1, 0)), ("B", (2, 1)), ("B", (0, 2))]
+    cells = np.argwhere(g > 0) if geom else np.argwhere(np.ones(reg.shape))
+    for z, y, x in cells[rng.choice(len(cells), size=8, replace=False)]:
+        checks.append(("Ms", (int(z), int(y), int(x))))
+    for which in checks:
+        fd = R.fd_gradient(prob, m0, th, which, rel=1e-4)
+        ad = gr[which[0]][which[1]]
+        assert abs(fd - ad) <= 1e-4 * abs(fd) + 1e-12 * max(1.0, abs(ad)), (which, fd, ad)

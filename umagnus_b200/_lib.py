@@ -65,7 +65,7 @@ class AdjParams(ctypes.Structure):
                 ("dt", c_double), ("gamma_ll", c_double), ("nsteps", c_int), ("K", c_int), ("probe", c_int * 4),
                 ("avg_from", c_int), ("w_probe", c_double), ("w_target", c_double), ("target", c_double * 3),
                 ("no_graph", c_int), ("solver", c_int), ("Dind", c_float), ("pbc", c_int * 3),
-                ("vol", c_void_p)]
+                ("vol", c_void_p), ("regions", c_void_p), ("nregions", c_int)]
 
 
 # name -> argtypes (restype int unless listed in _RESTYPE)
@@ -132,6 +132,10 @@ _SIGS = {
     "umag_adj_forward": [P, P, P, c_float, c_float, ctypes.POINTER(c_float), ctypes.POINTER(c_double)],
     "umag_adj_final_m": [P, P],
     "umag_adj_backward": [P, P, P, ctypes.POINTER(c_double), ctypes.POINTER(c_double), ctypes.POINTER(c_double)],
+    "umag_adj_forward_regions": [P, P, P, ctypes.POINTER(c_float), ctypes.POINTER(c_float), ctypes.POINTER(c_float),
+                                 ctypes.POINTER(c_double)],
+    "umag_adj_backward_regions": [P, P, P, ctypes.POINTER(c_double), ctypes.POINTER(c_double),
+                                  ctypes.POINTER(c_double)],
 }
 _RESTYPE = {"umag_last_error": ctypes.c_char_p, "umag_version": ctypes.c_char_p, "umag_solver_defaults": None}
 

@@ -34,7 +34,7 @@ GAMMA_LL = 1.7595e11  # engine/torque.go:27
 class AdjointRK4:
     def __init__(self, N, cell, alpha, anisU, dt, nsteps, K, probe, avg_from, w_probe=1.0, w_target=1.0,
                  target=(0.0, 0.0, 1.0), demag=True, demag_kernel="newell", demag_accuracy=6.0, gamma_ll=GAMMA_LL,
-                 use_graph=True, device=0, solver=4, Dind=0.0, pbc=(0, 0, 0), geom=None):
+                 use_graph=True, device=0, solver=4, Dind=0.0, pbc=(0, 0, 0), geom=None, regions=None):
         self.L = _lib.init(device)
         p = AdjParams()
         p.N[:] = [int(n) for n in N]
@@ -60,6 +60,16 @@ class AdjointRK4:
             self._vol = g.to(torch.device("cuda", device)).contiguous()
             torch.cuda.synchronize()
             p.vol = self._vol.data_ptr()
+        # a region map: Aex, Ku1 and B_ext become per-region arrays in
+        # forward() and backward() (regions 0 .. max of the map)
+        self._reg, self.nregions = None, 0
+        if regions is not None:
+            r = np.asarray(regions).astype(np.uint8).reshape(-1)
+            self.nregions = int(r.max()) + 1
+            self._reg = torch.as_tensor(r).to(torch.device("cuda", device)).contiguous()
+            torch.cuda.synchronize()
+            p.regions = self._reg.data_ptr()
+            p.nregions = self.nregions
         self.N = tuple(int(n) for n in N)
         self.ncell = self.N[0] * self.N[1] * self.N[2]
         h = ctypes.c_void_p()
@@ -75,12 +85,23 @@ class AdjointRK4:
 
     def forward(self, m0, Ms, Aex, Ku1, B_ext):
         """Run the forward pass; returns the loss (float).  m0 (3, Nz, Ny, Nx)
-        and Ms (Nz, Ny, Nx) as arrays or tensors."""
+        and Ms (Nz, Ny, Nx) as arrays or tensors; with a region map Aex and
+        Ku1 are per-region sequences and B_ext is (regions, 3)."""
         self._m0 = self._dev(m0, 3 * self.ncell)
         self._Ms = self._dev(Ms, self.ncell)
-        b = (ctypes.c_float * 3)(*[float(v) for v in B_ext])
         loss = ctypes.c_double()
         torch.cuda.synchronize(self.device)
+        if self._reg is not None:
+            nr = self.nregions
+            A = np.asarray(Aex, np.float32).reshape(nr)
+            K = np.asarray(Ku1, np.float32).reshape(nr)
+            B = np.ascontiguousarray(np.asarray(B_ext, np.float32).reshape(nr, 3))
+            fp = ctypes.POINTER(ctypes.c_float)
+            check(self.L.umag_adj_forward_regions(self._h, self._m0.data_ptr(), self._Ms.data_ptr(),
+                                                  A.ctypes.data_as(fp), K.ctypes.data_as(fp), B.ctypes.data_as(fp),
+                                                  ctypes.byref(loss)))
+            return loss.value
+        b = (ctypes.c_float * 3)(*[float(v) for v in B_ext])
         check(self.L.umag_adj_forward(self._h, self._m0.data_ptr(), self._Ms.data_ptr(), float(Aex), float(Ku1), b,
                                       ctypes.byref(loss)))
         return loss.value
@@ -95,6 +116,17 @@ class AdjointRK4:
         Aex, Ku1 (floats), B_ext (3 floats) and m0 (tensor, if asked)."""
         gMs = torch.empty(self.N[::-1], dtype=torch.float32, device=self.device)
         gm0 = torch.empty((3,) + self.N[::-1], dtype=torch.float32, device=self.device) if want_m0 else None
+        if self._reg is not None:  # per-region arrays
+            nr = self.nregions
+            gA, gK, gB = np.zeros(nr), np.zeros(nr), np.zeros((nr, 3))
+            dp = ctypes.POINTER(ctypes.c_double)
+            check(self.L.umag_adj_backward_regions(self._h, gMs.data_ptr(), gm0.data_ptr() if want_m0 else None,
+                                                   gA.ctypes.data_as(dp), gK.ctypes.data_as(dp),
+                                                   gB.ctypes.data_as(dp)))
+            out = {"Ms": gMs, "Aex": gA, "Ku1": gK, "B_ext": gB}
+            if want_m0:
+                out["m0"] = gm0
+            return out
         gA, gK = ctypes.c_double(), ctypes.c_double()
         gB = (ctypes.c_double * 3)()
         check(self.L.umag_adj_backward(self._h, gMs.data_ptr(), gm0.data_ptr() if want_m0 else None,
@@ -137,8 +169,12 @@ class _AdjFn(torch.autograd.Function):
         ctx.shapes = (m0.shape, Ms.shape)
         ctx.devs = (m0.device, Ms.device, torch.as_tensor(Aex).device, torch.as_tensor(Ku1).device,
                     torch.as_tensor(B_ext).device)
-        loss = sim.forward(m0.detach(), Ms.detach(), float(Aex), float(Ku1),
-                           [float(v) for v in torch.as_tensor(B_ext).detach().cpu()])
+        if sim.nregions:  # per-region parameters
+            host = lambda t: torch.as_tensor(t).detach().cpu().numpy()
+            loss = sim.forward(m0.detach(), Ms.detach(), host(Aex), host(Ku1), host(B_ext))
+        else:
+            loss = sim.forward(m0.detach(), Ms.detach(), float(Aex), float(Ku1),
+                               [float(v) for v in torch.as_tensor(B_ext).detach().cpu()])
         return torch.tensor(loss, dtype=torch.float64)
 
     @staticmethod
@@ -148,7 +184,7 @@ class _AdjFn(torch.autograd.Function):
         d = ctx.devs
         gm0 = (g["m0"] * s).reshape(ctx.shapes[0]).to(d[0]) if ctx.needs_input_grad[1] else None
         gMs = (g["Ms"] * s).reshape(ctx.shapes[1]).to(d[1])
-        gA = torch.tensor(g["Aex"] * s, dtype=torch.float64, device=d[2])
-        gK = torch.tensor(g["Ku1"] * s, dtype=torch.float64, device=d[3])
+        gA = torch.tensor(np.asarray(g["Aex"]) * s, dtype=torch.float64, device=d[2])
+        gK = torch.tensor(np.asarray(g["Ku1"]) * s, dtype=torch.float64, device=d[3])
         gB = torch.tensor(np.asarray(g["B_ext"]) * s, dtype=torch.float64, device=d[4])
         return None, gm0, gMs, gA, gK, gB

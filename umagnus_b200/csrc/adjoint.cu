@@ -47,6 +47,12 @@ struct AdjField {
     int N;
     const float* Ms;   // per-cell map
     const float* vol;  // geometry (cell volume fractions) or NULL: m is zero where it is 0
+    // region map (or NULL) with per-region parameters: the exchange LUT of
+    // the engine (harmonic means of the regions' A, symidx layout), each
+    // region's A, K1 and applied field (bext[c * 256 + r]); w_d = 2/c_d^2
+    const uint8_t* regions;
+    const float *aLUT, *Ar, *K1r, *bextr;
+    float wx, wy, wz;
     PairCoef pc;       // exchange pair coefficients w_d * A (region (0,0)); with DMI also 2A/c^2, D/c, c D/(2A)
     int dmi;           // exchange + interfacial DMI (dmi.cl) instead of exchange (exchange.cl)
     float dq[2];       // DMI: (D/c)(c D/(2A)) = D^2/(2A) per in-plane axis, the missing neighbour's net weight
@@ -83,9 +89,12 @@ __device__ __forceinline__ void adj_field_cell(const AdjField& a, const float* _
     const f3 m0 = ld3(mx, my, mz, I);
     b = f3{0.f, 0.f, 0.f};
     if (bd) b = f3{bd[I], bd[N + I], bd[2 * N + I]};
+    const int r0 = a.regions ? a.regions[I] : 0;
     if (!is0(m0)) {
-        const f3 e = a.dmi ? dmi_sum_u(mx, my, mz, a.pc, a.g, false, ix, iy, iz, m0)
-                           : exchange_sum_u(mx, my, mz, a.pc, a.g, ix, iy, iz, m0);
+        // with a region map, the engine's exchange stencil over its LUT
+        const f3 e = a.regions ? exchange_sum(mx, my, mz, a.aLUT, a.regions, a.wx, a.wy, a.wz, a.g, ix, iy, iz, m0, r0)
+                     : a.dmi   ? dmi_sum_u(mx, my, mz, a.pc, a.g, false, ix, iy, iz, m0)
+                               : exchange_sum_u(mx, my, mz, a.pc, a.g, ix, iy, iz, m0);
         const float inv = inv_msat(a.Ms, 1.0f, I);
         b.x = fa(b.x, fm(e.x, inv));
         b.y = fa(b.y, fm(e.y, inv));
@@ -93,12 +102,12 @@ __device__ __forceinline__ void adj_field_cell(const AdjField& a, const float* _
     }
     if (a.anis) {
         const UniaxParams up{a.Ms, nullptr, nullptr, nullptr, nullptr, nullptr,
-                             1.0f, a.K1, 0.0f, a.u[0], a.u[1], a.u[2]};
+                             1.0f, a.regions ? a.K1r[r0] : a.K1, 0.0f, a.u[0], a.u[1], a.u[2]};
         add_uniaxial(b, up, m0, I);
     }
-    b.x = fa(b.x, a.bext[0]);
-    b.y = fa(b.y, a.bext[1]);
-    b.z = fa(b.z, a.bext[2]);
+    b.x = fa(b.x, a.regions ? a.bextr[r0] : a.bext[0]);
+    b.y = fa(b.y, a.regions ? a.bextr[256 + r0] : a.bext[1]);
+    b.z = fa(b.z, a.regions ? a.bextr[512 + r0] : a.bext[2]);
     const f3 mxB = cross3(m0, b), mmxB = cross3(m0, mxB);
     t = f3{fm(a.gilb, fa(mxB.x, fm(a.alpha, mmxB.x))), fm(a.gilb, fa(mxB.y, fm(a.alpha, mmxB.y))),
            fm(a.gilb, fa(mxB.z, fm(a.alpha, mmxB.z)))};
@@ -371,27 +380,47 @@ __global__ void __launch_bounds__(256) k_adj_rev_stage(AdjField a, StepFac f, in
             const int nn = a.g.Nz != 1 ? 6 : 4;
             f3 sx{0.f, 0.f, 0.f}, e{0.f, 0.f, 0.f};
             const f3 x0 = sc3(inv, w);
+            const int ri = a.regions ? a.regions[I] : 0;
+            double gA = 0;  // with regions: dL/dA of this cell's region, from its pairs
             for (int k = 0; k < nn; k++) {
-                const float s = k < 2 ? a.pc.wax : (k < 4 ? a.pc.way : a.pc.waz);
                 const int j = nb[k];
                 if (hole(j)) continue;  // a zero neighbour: the term vanishes
+                const float wd = k < 2 ? a.wx : (k < 4 ? a.wy : a.wz);
+                float s;
+                if (a.regions) {
+                    const int rj = a.regions[j];
+                    s = wd * a.aLUT[symidx(ri, rj)];
+                } else {
+                    s = k < 2 ? a.pc.wax : (k < 4 ? a.pc.way : a.pc.waz);
+                }
                 const float msj = a.Ms[j];
                 const float ij = msj == 0.f ? 0.f : 1.0f / msj;
-                sx = ad3(sx, sc3(s, f3{wB[j] * ij - x0.x, wB[N + j] * ij - x0.y, wB[2 * N + j] * ij - x0.z}));
-                e = ad3(e, sc3(s, f3{mq[j] - m0.x, mq[N + j] - m0.y, mq[2 * N + j] - m0.z}));
+                const f3 xn{wB[j] * ij, wB[N + j] * ij, wB[2 * N + j] * ij};
+                const f3 dm{mq[j] - m0.x, mq[N + j] - m0.y, mq[2 * N + j] - m0.z};
+                sx = ad3(sx, sc3(s, f3{xn.x - x0.x, xn.y - x0.y, xn.z - x0.z}));
+                e = ad3(e, sc3(s, dm));
+                if (a.regions) {
+                    // the pair coefficient a = 2/(1/A_i + 1/A_j); seen from
+                    // this cell: (c_ij + c_ji) da/dA_i, c = w_d x.(m_other - m_own)
+                    const double cij = (double)x0.x * dm.x + (double)x0.y * dm.y + (double)x0.z * dm.z;
+                    const double cji = -((double)xn.x * dm.x + (double)xn.y * dm.y + (double)xn.z * dm.z);
+                    const double ap = 2.0 / (1.0 / (double)a.Ar[ri] + 1.0 / (double)a.Ar[a.regions[j]]);
+                    gA += (double)wd * (cij + cji) * ap * ap / (2.0 * (double)a.Ar[ri] * (double)a.Ar[ri]);
+                }
             }
             g = ad3(g, sx);
             const double we = (double)w.x * e.x + (double)w.y * e.y + (double)w.z * e.z;
             gms -= we * (double)inv * (double)inv;
-            acc[(size_t)N + I] += we * (double)inv / (double)A;
+            acc[(size_t)N + I] += a.regions ? gA : we * (double)inv / (double)A;
         }
         if (a.anis) {
             f3 u{a.u[0], a.u[1], a.u[2]};
             const float len = sqrtf(d3(u, u));
             u = sc3(len > 0.f ? 1.0f / len : 0.f, u);
             const float mu = d3(m0, u), wu = d3(w, u);
-            g = ad3(g, sc3(2.f * a.K1 * inv * wu, u));
-            gms -= 2.0 * (double)a.K1 * (double)mu * (double)wu * (double)inv * (double)inv;
+            const float K1 = a.regions ? a.K1r[a.regions[I]] : a.K1;
+            g = ad3(g, sc3(2.f * K1 * inv * wu, u));
+            gms -= 2.0 * (double)K1 * (double)mu * (double)wu * (double)inv * (double)inv;
             acc[2 * (size_t)N + I] += 2.0 * (double)mu * (double)wu * (double)inv;
         }
         acc[I] += gms;
@@ -467,6 +496,30 @@ __global__ void __launch_bounds__(1024) k_adj_reduce(int N, const double* __rest
     }
 }
 
+// per-region sums of the accumulators 1..5 (A, K1, B_x, B_y, B_z): block r
+// adds the cells of region r in a fixed order (deterministic)
+__global__ void __launch_bounds__(1024) k_adj_reduce_regions(int N, const double* __restrict__ acc,
+                                                              const uint8_t* __restrict__ regions, double* out) {
+    __shared__ double sh[5][32];
+    const int r = blockIdx.x;
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int I = threadIdx.x; I < N; I += blockDim.x)
+        if (regions[I] == r)
+            for (int t = 0; t < 5; t++) s[t] += acc[(size_t)(t + 1) * N + I];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int t = 0; t < 5; t++) {
+        double v = s[t];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[t][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double v = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sh[threadIdx.x][w];
+        out[(size_t)r * 5 + threadIdx.x] = v;
+    }
+}
+
 // ---------------------------------------------------------------- host
 // work buffers (3N floats each)
 enum : int {
@@ -503,6 +556,11 @@ struct AdjImpl {
     float* work = nullptr;     // W_COUNT x 3N
     double* acc = nullptr;     // per-cell FP64 gradient accumulators, 6 x N
     double* dsum = nullptr;    // 8 doubles: probe sum / scalar gradients
+    // region maps (p.regions): the exchange LUT and per-region A, K1 and
+    // field on the device, per-region gradient sums [nregions][5]
+    float* reg_par = nullptr;  // aLUT (32896) | A (256) | K1 (256) | bext (3 x 256)
+    double* reg_sum = nullptr;
+    std::vector<float> hA, hK1;
     bool have_forward = false;
     double avg[3] = {0, 0, 0};
     std::vector<AdjGraph> graphs;  // segment graphs by key (parameters are baked in)
@@ -512,6 +570,7 @@ struct AdjImpl {
 };
 
 static cudaStream_t AS() { return ctx().stream; }
+constexpr int kLutSize = 256 * 257 / 2;  // symidx LUT entries (kernels_src/clh/exchange.clh:5)
 
 static AdjField adj_field(const AdjImpl* s) {
     AdjField a{};
@@ -519,6 +578,16 @@ static AdjField adj_field(const AdjImpl* s) {
     a.N = s->N;
     a.Ms = s->Ms;
     a.vol = s->p.vol;
+    if (s->p.regions) {
+        a.regions = s->p.regions;
+        a.aLUT = s->reg_par;
+        a.Ar = s->reg_par + kLutSize;
+        a.K1r = a.Ar + 256;
+        a.bextr = a.K1r + 256;
+    }
+    a.wx = (float)(2 / (s->p.cell[0] * s->p.cell[0]));
+    a.wy = (float)(2 / (s->p.cell[1] * s->p.cell[1]));
+    a.wz = (float)(2 / (s->p.cell[2] * s->p.cell[2]));
     // engine/exchange.go: w_d = 2/c_d^2 (float32), coefficient w_d * A(0,0)
     const float wx = (float)(2 / (s->p.cell[0] * s->p.cell[0])), wy = (float)(2 / (s->p.cell[1] * s->p.cell[1])),
                 wz = (float)(2 / (s->p.cell[2] * s->p.cell[2]));
@@ -650,7 +719,10 @@ static void adj_drop_graphs(AdjImpl* s) {
 // the values baked into a graph besides pointers: exchange, anisotropy, field
 static std::string param_key(const AdjImpl* s) {
     char buf[128];
-    snprintf(buf, sizeof buf, "/%a/%a/%a/%a/%a/%a", s->A, s->A00, s->K1, s->B[0], s->B[1], s->B[2]);
+    if (s->p.regions)  // per-region values live in device arrays the graphs read
+        snprintf(buf, sizeof buf, "/R%d", s->K1 != 0.f ? 1 : 0);
+    else
+        snprintf(buf, sizeof buf, "/%a/%a/%a/%a/%a/%a", s->A, s->A00, s->K1, s->B[0], s->B[1], s->B[2]);
     return buf;
 }
 
@@ -666,6 +738,8 @@ int adj_free(umag_adj* h) {
     cudaFree(s->work);
     cudaFree(s->acc);
     cudaFree(s->dsum);
+    cudaFree(s->reg_par);
+    cudaFree(s->reg_sum);
     delete s;
     return UMAG_OK;
 }
@@ -682,6 +756,11 @@ int adj_new(const umag_adj_params* p, umag_adj** out) {
                  "probe window outside the mesh");
     UMAG_REQUIRE(p->solver == 0 || p->solver == 2 || p->solver == 4, "solver must be 4 (RK4) or 2 (Heun)");
     UMAG_REQUIRE(p->pbc[0] >= 0 && p->pbc[1] >= 0 && p->pbc[2] >= 0, "PBC repetitions must be non-negative");
+    if (p->regions) {
+        UMAG_REQUIRE(p->nregions >= 1 && p->nregions <= 256, "nregions must lie in 1..256");
+        if (p->Dind != 0.f)
+            return set_error(UMAG_E_UNSUPPORTED, "region maps with interfacial DMI are not supported by the adjoint");
+    }
     AdjImpl* s = new AdjImpl();
     s->p = *p;
     s->N = p->N[0] * p->N[1] * p->N[2];
@@ -701,6 +780,10 @@ int adj_new(const umag_adj_params* p, umag_adj** out) {
         cudaMalloc(&s->acc, sizeof(double) * 6 * (size_t)s->N) != cudaSuccess ||
         cudaMalloc(&s->dsum, sizeof(double) * 8) != cudaSuccess)
         return fail(set_error(UMAG_E_NOMEM, "adjoint buffers"));
+    if (p->regions &&
+        (cudaMalloc(&s->reg_par, sizeof(float) * (kLutSize + 5 * 256)) != cudaSuccess ||
+         cudaMalloc(&s->reg_sum, sizeof(double) * 5 * 256) != cudaSuccess))
+        return fail(set_error(UMAG_E_NOMEM, "adjoint region tables"));
     const int nck = (p->nsteps + p->K - 1) / p->K;  // segment starts: states 0, K, 2K, ...
     for (int i = 0; i < nck; i++) {
         float* c = nullptr;
@@ -720,20 +803,67 @@ int adj_new(const umag_adj_params* p, umag_adj** out) {
     return UMAG_OK;
 }
 
+static int adj_forward_impl(AdjImpl* s, const float* m0, const float* Ms, double* loss);
+
 int adj_forward(umag_adj* hd, const float* m0, const float* Ms, float A, float K1, const float Bext[3], double* loss) {
     AdjImpl* s = reinterpret_cast<AdjImpl*>(hd);
     UMAG_REQUIRE(s && m0 && Ms && Bext && loss, "NULL argument");
+    UMAG_REQUIRE(!s->p.regions, "this handle has a region map: use umag_adj_forward_regions");
     UMAG_REQUIRE(A > 0, "Aex must be positive");
-    const umag_adj_params& p = s->p;
-    const size_t n3 = s->n3();
-    s->have_forward = false;
-    UMAG_CUDA(cudaMemcpyAsync(s->Ms, Ms, sizeof(float) * s->N, cudaMemcpyDeviceToDevice, AS()));
     s->A = A;
     s->A00 = 2.0f / (1.0f / A + 1.0f / A);  // engine/exchange.go:153-167, region 0 with itself
     const float D = s->p.Dind;
     s->D00 = D == 0.f ? 0.f : 2.0f / (1.0f / D + 1.0f / D);  // the same average for the DMI LUT
     s->K1 = K1;
     for (int c = 0; c < 3; c++) s->B[c] = Bext[c];
+    return adj_forward_impl(s, m0, Ms, loss);
+}
+
+// per-region values (host arrays of nregions, B_ext as [r][3]): the engine's
+// exchange LUT (engine/exchange.go:153-167: 2/(1/A_i + 1/A_j) in float32 at
+// symidx(i, j); regions past nregions take A of region 0, as no cell uses
+// them), A, K1 and the field per region, to the device
+int adj_forward_regions(umag_adj* hd, const float* m0, const float* Ms, const float* A, const float* K1,
+                        const float* Bext, double* loss) {
+    AdjImpl* s = reinterpret_cast<AdjImpl*>(hd);
+    UMAG_REQUIRE(s && m0 && Ms && A && K1 && Bext && loss, "NULL argument");
+    UMAG_REQUIRE(s->p.regions, "this handle has no region map: use umag_adj_forward");
+    const int nr = s->p.nregions;
+    for (int r = 0; r < nr; r++) UMAG_REQUIRE(A[r] > 0, "Aex of region %d must be positive", r);
+    std::vector<float> hp((size_t)kLutSize + 5 * 256, 0.f);
+    float ex[256];
+    for (int r = 0; r < 256; r++) ex[r] = A[r < nr ? r : 0];
+    for (int i = 0; i < 256; i++)
+        for (int j = 0; j <= i; j++) {
+            const volatile float inv_i = 1.0f / ex[i], inv_j = 1.0f / ex[j];
+            const volatile float sum = inv_i + inv_j;
+            hp[(size_t)i * (i + 1) / 2 + j] = 2.0f / sum;
+        }
+    float* Ar = hp.data() + kLutSize;
+    bool anis = false;
+    for (int r = 0; r < nr; r++) {
+        Ar[r] = A[r];
+        Ar[256 + r] = K1[r];
+        anis |= K1[r] != 0.f;
+        for (int c = 0; c < 3; c++) Ar[512 + c * 256 + r] = Bext[3 * r + c];
+    }
+    UMAG_CUDA(cudaMemcpyAsync(s->reg_par, hp.data(), sizeof(float) * hp.size(), cudaMemcpyHostToDevice, AS()));
+    UMAG_CUDA(cudaStreamSynchronize(AS()));  // the host table is released on return
+    s->hA.assign(A, A + nr);
+    s->hK1.assign(K1, K1 + nr);
+    s->A = A[0];
+    s->A00 = 0.f;
+    s->D00 = 0.f;
+    s->K1 = anis ? 1.f : 0.f;  // (the flag of the anisotropy term; the values are per region)
+    for (int c = 0; c < 3; c++) s->B[c] = 0.f;
+    return adj_forward_impl(s, m0, Ms, loss);
+}
+
+static int adj_forward_impl(AdjImpl* s, const float* m0, const float* Ms, double* loss) {
+    const umag_adj_params& p = s->p;
+    const size_t n3 = s->n3();
+    s->have_forward = false;
+    UMAG_CUDA(cudaMemcpyAsync(s->Ms, Ms, sizeof(float) * s->N, cudaMemcpyDeviceToDevice, AS()));
     const AdjField af = adj_field(s);
     const StepFac f = step_fac(s->h, s->heun);
     UMAG_CUDA(cudaMemcpyAsync(s->w(W_M0), m0, sizeof(float) * n3, cudaMemcpyDeviceToDevice, AS()));
@@ -843,9 +973,41 @@ static int adj_rev_segment(AdjImpl* s, const AdjField& af, const StepFac& f, int
     return UMAG_OK;
 }
 
+static int adj_backward_impl(AdjImpl* s, float* gMs, float* gm0, double* hs);
+
 int adj_backward(umag_adj* hd, float* gMs, float* gm0, double* gA, double* gK1, double gB[3]) {
     AdjImpl* s = reinterpret_cast<AdjImpl*>(hd);
     UMAG_REQUIRE(s && gMs && gA && gK1 && gB, "NULL argument");
+    UMAG_REQUIRE(!s->p.regions, "this handle has a region map: use umag_adj_backward_regions");
+    double hs[5];
+    UMAG_TRY(adj_backward_impl(s, gMs, gm0, hs));
+    *gA = hs[0];
+    *gK1 = hs[1];
+    for (int c = 0; c < 3; c++) gB[c] = hs[2 + c];
+    return UMAG_OK;
+}
+
+// per-region gradients (host arrays of nregions; gB as [r][3])
+int adj_backward_regions(umag_adj* hd, float* gMs, float* gm0, double* gA, double* gK1, double* gB) {
+    AdjImpl* s = reinterpret_cast<AdjImpl*>(hd);
+    UMAG_REQUIRE(s && gMs && gA && gK1 && gB, "NULL argument");
+    UMAG_REQUIRE(s->p.regions, "this handle has no region map: use umag_adj_backward");
+    UMAG_TRY(adj_backward_impl(s, gMs, gm0, nullptr));
+    const int nr = s->p.nregions;
+    k_adj_reduce_regions<<<nr, 1024, 0, AS()>>>(s->N, s->acc, s->p.regions, s->reg_sum);
+    UMAG_LAUNCH_CHECK();
+    std::vector<double> hs((size_t)5 * nr);
+    UMAG_CUDA(cudaMemcpyAsync(hs.data(), s->reg_sum, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, AS()));
+    UMAG_CUDA(cudaStreamSynchronize(AS()));
+    for (int r = 0; r < nr; r++) {
+        gA[r] = hs[5 * r];
+        gK1[r] = hs[5 * r + 1];
+        for (int c = 0; c < 3; c++) gB[3 * r + c] = hs[5 * r + 2 + c];
+    }
+    return UMAG_OK;
+}
+
+static int adj_backward_impl(AdjImpl* s, float* gMs, float* gm0, double* hs_out) {
     UMAG_REQUIRE(s->have_forward, "backward needs a forward pass first");
     const umag_adj_params& p = s->p;
     const int N = s->N;
@@ -875,12 +1037,10 @@ int adj_backward(umag_adj* hd, float* gMs, float* gm0, double* gA, double* gK1, 
     }
     k_adj_reduce<<<1, 1024, 0, AS()>>>(N, s->acc, gMs, s->dsum);
     UMAG_LAUNCH_CHECK();
-    double hs[5];
-    UMAG_CUDA(cudaMemcpyAsync(hs, s->dsum, sizeof(hs), cudaMemcpyDeviceToHost, AS()));
+    if (hs_out) {
+        UMAG_CUDA(cudaMemcpyAsync(hs_out, s->dsum, sizeof(double) * 5, cudaMemcpyDeviceToHost, AS()));
+    }
     UMAG_CUDA(cudaStreamSynchronize(AS()));
-    *gA = hs[0];
-    *gK1 = hs[1];
-    for (int c = 0; c < 3; c++) gB[c] = hs[2 + c];
     return UMAG_OK;
 }
 

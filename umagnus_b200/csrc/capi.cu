@@ -258,5 +258,12 @@ int umag_adj_final_m(umag_adj* a, float* m) { return adj_final_m(a, m); }
 int umag_adj_backward(umag_adj* a, float* gMs, float* gm0, double* gAex, double* gKu1, double gB_ext[3]) {
     return adj_backward(a, gMs, gm0, gAex, gKu1, gB_ext);
 }
+int umag_adj_forward_regions(umag_adj* a, const float* m0, const float* Ms, const float* Aex, const float* Ku1,
+                             const float* B_ext, double* loss) {
+    return adj_forward_regions(a, m0, Ms, Aex, Ku1, B_ext, loss);
+}
+int umag_adj_backward_regions(umag_adj* a, float* gMs, float* gm0, double* gAex, double* gKu1, double* gB_ext) {
+    return adj_backward_regions(a, gMs, gm0, gAex, gKu1, gB_ext);
+}
 
 }  // extern "C"

@@ -43,4 +43,7 @@ int adj_free(umag_adj* a);
 int adj_forward(umag_adj* a, const float* m0, const float* Ms, float A, float K1, const float Bext[3], double* loss);
 int adj_final_m(umag_adj* a, float* m);
 int adj_backward(umag_adj* a, float* gMs, float* gm0, double* gA, double* gK1, double gB[3]);
+int adj_forward_regions(umag_adj* a, const float* m0, const float* Ms, const float* A, const float* K1,
+                        const float* Bext, double* loss);
+int adj_backward_regions(umag_adj* a, float* gMs, float* gm0, double* gA, double* gK1, double* gB);
 }  // namespace umag

@@ -401,7 +401,6 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     // carries Pz/WB such CTAs instead of Pz mostly idle ones.
     const bool nyq = bx * WB == hx - 1 && WB > 1 && Pz % WB == 0 && Pz >= WB;
     if (nyq && by * WB >= Pz) return;
-    rg_tw_fill<PY>(tw, a.fy.tw, tid, NT);
     const int kx0 = bx * WB;
     const int kx = nyq ? hx - 1 : kx0 + w, kz = nyq ? by * WB + w : by;
     auto kz_mirror = [&](int z) { return z > Pz / 2 ? Pz - z : z; };
@@ -461,6 +460,7 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
             const int y = t + T * m;
             v[c][m] = (m < 4 && col) ? in[c * cs + y * rs] : make_float2(0.f, 0.f);
         }
+    rg_tw_fill<PY>(tw, a.fy.tw, tid, NT);  // while the loads above are in flight
     __syncthreads();  // twiddles, barrier initialised
     float2* exl = ex + w * LP;
     const int exs = WB * LP;
@@ -551,9 +551,6 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
     float2* ex = Xs + NZ * XP; // exchange lines
     if (inst_inactive(a, ib)) return;
     const int tid = threadIdx.x;
-    for (int i = tid; i < M; i += NT) twr[i] = a.twr[i];
-    rg_tw_fill<M>(twx, a.fx.tw, tid, NT);
-    if constexpr (PZ != 16 && PZ != 32) rg_tw_fill<PZ>(twz, a.fz.tw, tid, NT);  // (the pair z phase has none)
     const int y = bx, c = by, Ny = a.Ny;
     const float* __restrict__ mp = inst_m(a, ib, c);
     const float msm = inst_msmul(a, ib);
@@ -585,6 +582,10 @@ __device__ __forceinline__ void k_reg_a_body(const PassArgs& a, const int bx, co
             }
         }
     }
+    // the twiddle tables while the loads of m are in flight
+    for (int i = tid; i < M; i += NT) twr[i] = a.twr[i];
+    rg_tw_fill<M>(twx, a.fx.tw, tid, NT);
+    if constexpr (PZ != 16 && PZ != 32) rg_tw_fill<PZ>(twz, a.fz.tw, tid, NT);  // (the pair z phase has none)
     __syncthreads();
     rg_fft_fwd<M, 1, true, 4, rg_radix(M, 0) == 8, 2>(v, t, ex + z * S::LX, 0, twx);  // n >= M/2 is zero padding
     // R2C unpack: partner element Z[M-k] lives in lane (TX - t) % TX, element 7-j
@@ -773,21 +774,24 @@ __device__ __forceinline__ void k_reg_c_body(const PassArgs& a, const int bx, co
     // (Xs is 16-byte aligned, so the 128-byte rounding below moves it by a
     // whole number of float2)
     const bool slab = kSlabShape && a.slab_map != nullptr && ib == 0 && (smem_u32(Xs) & 15u) == 0;
-    if (slab && tid == 0) mbar_init(&slab_bar, 1);
-    for (int i = tid; i < M; i += NT) twr[i] = a.twr[i];
-    rg_tw_fill<M>(twx, a.fx.tw, tid, NT);
-    if constexpr (PZ != 16 && PZ != 32) rg_tw_fill<PZ>(twz, a.fz.tw, tid, NT);  // (the pair z phase has none)
-    __syncthreads();
     const int y = bx, c = by, Ny = a.Ny;
     const int KB = a.Lx >> 2;  // four-column blocks per kz row of the slab
     // the copy's destination on a 128-byte boundary (the dynamic region
     // need not start on one; the plan leaves 128 bytes of slack)
     float2* const sl = Xs + ((128u - (smem_u32(Xs) & 127u)) & 127u) / sizeof(float2);
+    // the copy is issued first (its initialisation is fenced for the async
+    // proxy), so that it is in flight while the twiddle tables are filled;
+    // the barrier below makes the initialisation visible to the other threads
+    if (slab && tid == 0) {
+        mbar_init(&slab_bar, 1);
+        mbar_expect_tx(&slab_bar, (uint32_t)(sizeof(float2) * 4 * KB * PZ));
+        tma_load_5d(sl, a.slab_map, 0, y, 0, 0, c, &slab_bar);
+    }
+    for (int i = tid; i < M; i += NT) twr[i] = a.twr[i];
+    rg_tw_fill<M>(twx, a.fx.tw, tid, NT);
+    if constexpr (PZ != 16 && PZ != 32) rg_tw_fill<PZ>(twz, a.fz.tw, tid, NT);  // (the pair z phase has none)
+    __syncthreads();
     if (slab) {
-        if (tid == 0) {
-            mbar_expect_tx(&slab_bar, (uint32_t)(sizeof(float2) * 4 * KB * PZ));
-            tma_load_5d(sl, a.slab_map, 0, y, 0, 0, c, &slab_bar);
-        }
         for (int it = 0; !mbar_try_wait(&slab_bar, 0); it++) {
             if (it == kTileWaitLimit && tid == 0) pass_timeout(a, ib);
             if (it >= 2 * kTileWaitLimit) return;

@@ -401,6 +401,7 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
     // carries Pz/WB such CTAs instead of Pz mostly idle ones.
     const bool nyq = bx * WB == hx - 1 && WB > 1 && Pz % WB == 0 && Pz >= WB;
     if (nyq && by * WB >= Pz) return;
+    rg_tw_fill<PY>(tw, a.fy.tw, tid, NT);
     const int kx0 = bx * WB;
     const int kx = nyq ? hx - 1 : kx0 + w, kz = nyq ? by * WB + w : by;
     auto kz_mirror = [&](int z) { return z > Pz / 2 ? Pz - z : z; };
@@ -460,7 +461,6 @@ __device__ __forceinline__ void k_reg_b_body(const PassArgs& a, const int bx, co
             const int y = t + T * m;
             v[c][m] = (m < 4 && col) ? in[c * cs + y * rs] : make_float2(0.f, 0.f);
         }
-    rg_tw_fill<PY>(tw, a.fy.tw, tid, NT);  // while the loads above are in flight
     __syncthreads();  // twiddles, barrier initialised
     float2* exl = ex + w * LP;
     const int exs = WB * LP;
